@@ -1,0 +1,173 @@
+"""Packing of cosmologies into the flat C-ABI layout of include/abcmb_b200.h.
+
+One ``abcmb_cosmo`` record per cosmology plus three shared FP64 buffers
+(tables, k values, PT output) and an int32 (cosmology, k) work list.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from .specs import StateLayout
+
+NFIELDS = 21
+FIELD_NAMES = (
+    "delta_m", "theta_b_prime", "metric_eta", "metric_h_prime", "metric_eta_prime",
+    "metric_alpha", "metric_alpha_prime", "cdm_delta", "b_delta", "b_theta",
+    "g_delta", "g_theta", "g_sigma", "g_G0", "g_G2",
+    "nu_delta", "nu_theta", "nu_sigma", "ncdm_delta", "ncdm_theta", "ncdm_sigma",
+)
+F = {name: i for i, name in enumerate(FIELD_NAMES)}
+
+_DOUBLES = ["h", "omega_b", "omega_cdm", "omega_Lambda", "A_s", "n_s", "TCMB0", "YHe",
+            "N_nu_massless", "T_nu_massless", "N_nu_massive", "T_nu_massive", "m_nu_massive",
+            "R_nu", "R_b", "om", "tau0", "lna_transfer_start",
+            "lna_xe0", "lna_xe_max", "lna_xe_last", "xe_first", "xe_last",
+            "lna_tm0", "lna_tm_max", "lna_tm_last", "tm_last"]
+_INT64 = ["off_tau", "off_xe", "off_tm", "off_los", "off_k", "off_pt"]
+_INT32 = ["n_xe", "n_tm", "lmax_g", "lmax_pol_g", "lmax_nu", "lmax_ncdm", "has_ncdm", "ny", "nk", "pad_"]
+
+COSMO_DTYPE = np.dtype([(n, "<f8") for n in _DOUBLES] + [(n, "<i8") for n in _INT64]
+                       + [(n, "<i4") for n in _INT32], align=True)
+assert COSMO_DTYPE.itemsize == 304
+
+
+class CPertSettings(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in
+                ["R_tc", "R_large", "k_split", "rtol_small", "rtol_large", "atol_small", "atol_large",
+                 "pcoeff", "icoeff", "dcoeff", "dt0"]] + [("max_steps", ctypes.c_int32), ("n_save", ctypes.c_int32)]
+
+
+class CLosSettings(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ["k_pivot", "scale_sw", "scale_isw", "scale_dop", "scale_pol"]] + \
+               [(n, ctypes.c_int32) for n in ["l_min", "l_max", "idx_min", "idx_max", "nkt", "precision"]]
+
+
+class CKStat(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("n_accepted", ctypes.c_int32), ("n_rejected", ctypes.c_int32),
+                ("n_newton", ctypes.c_int32), ("lna_start", ctypes.c_double)]
+
+
+KSTAT_DTYPE = np.dtype([("status", "<i4"), ("n_accepted", "<i4"), ("n_rejected", "<i4"),
+                        ("n_newton", "<i4"), ("lna_start", "<f8")], align=True)
+
+
+def pert_settings(specs: dict, n_save: int = 500) -> CPertSettings:
+    return CPertSettings(R_tc=specs["R_tc"], R_large=specs["R_large"], k_split=specs["k_split_PE"],
+                         rtol_small=specs["rtol_small_k_PE"], rtol_large=specs["rtol_large_k_PE"],
+                         atol_small=specs["atol_small_k_PE"], atol_large=specs["atol_large_k_PE"],
+                         pcoeff=specs["pcoeff_PE"], icoeff=specs["icoeff_PE"], dcoeff=specs["dcoeff_PE"],
+                         dt0=1.0e-2, max_steps=int(specs["max_steps_PE"]), n_save=n_save)
+
+
+def los_settings(specs: dict, idx_min: int, idx_max: int, nkt: int, l_out_max: int,
+                 precision: int = 0) -> CLosSettings:
+    return CLosSettings(k_pivot=specs["k_pivot"], scale_sw=specs["scale_sw"], scale_isw=specs["scale_isw"],
+                        scale_dop=specs["scale_dop"], scale_pol=specs["scale_pol"],
+                        l_min=int(specs["l_min"]), l_max=int(l_out_max), idx_min=idx_min, idx_max=idx_max,
+                        nkt=nkt, precision=precision)
+
+
+@dataclass
+class Batch:
+    """Host-side packed batch of cosmologies."""
+    cosmo: np.ndarray           # COSMO_DTYPE records
+    tables: np.ndarray          # float64
+    kbuf: np.ndarray            # float64
+    items: np.ndarray           # int32 (n_items, 2)
+    pt_size: int                # doubles of PT output
+    n_save: int
+    bgs: list
+    layouts: list
+
+    @property
+    def n_cosmo(self):
+        return len(self.cosmo)
+
+    @property
+    def n_items(self):
+        return len(self.items)
+
+    def pt_view(self, pt: np.ndarray, ci: int) -> np.ndarray:
+        c = self.cosmo[ci]
+        n = NFIELDS * self.n_save * int(c["nk"])
+        return pt[int(c["off_pt"]):int(c["off_pt"]) + n].reshape(NFIELDS, self.n_save, int(c["nk"]))
+
+    def k_of(self, ci: int) -> np.ndarray:
+        c = self.cosmo[ci]
+        return self.kbuf[int(c["off_k"]):int(c["off_k"]) + int(c["nk"])]
+
+
+def pack(bgs, layouts, kgrids, n_save: int = 500, order: str = "cost") -> Batch:
+    """Pack cosmologies (BackgroundTables, StateLayout, k grid) into a Batch.
+
+    order="cost" hands the persistent queue the expensive items first:
+    large k (many steps) and large state vectors, which keeps the tail of
+    the launch short.
+    """
+    n = len(bgs)
+    rec = np.zeros(n, dtype=COSMO_DTYPE)
+    chunks = []
+    kchunks = []
+    off = 0
+    koff = 0
+    ptoff = 0
+    nl = n_save - 1
+    for i, (bg, lay, kg) in enumerate(zip(bgs, layouts, kgrids)):
+        p = bg.params
+        r = rec[i]
+        for name in ["h", "omega_b", "omega_cdm", "omega_Lambda", "A_s", "n_s", "TCMB0", "YHe",
+                     "N_nu_massless", "T_nu_massless", "N_nu_massive", "T_nu_massive", "m_nu_massive",
+                     "R_nu", "R_b", "om"]:
+            r[name] = float(p[name])
+        r["tau0"] = bg.tau0
+        r["lna_transfer_start"] = bg.lna_transfer_start
+        nxe = bg.xe_arr.shape[0]
+        ntm = bg.tm_arr.shape[0]
+        r["lna_xe0"] = bg.lna_xe0
+        r["lna_xe_max"] = bg.lna_xe0 + nxe * bg.lna_xe_dx
+        r["lna_xe_last"] = bg.lna_xe_last
+        r["xe_first"] = bg.xe_arr[0]
+        r["xe_last"] = bg.xe_last
+        r["lna_tm0"] = bg.lna_tm0
+        r["lna_tm_max"] = bg.lna_tm0 + ntm * bg.lna_tm_dx
+        r["lna_tm_last"] = bg.lna_tm_last
+        r["tm_last"] = bg.tm_last
+        los = bg.los_arrays(n_save)
+        r["off_tau"] = off
+        chunks.append(bg.tau_tab); off += bg.tau_tab.shape[0]
+        r["off_xe"] = off
+        chunks.append(bg.xe_arr); off += nxe
+        r["off_tm"] = off
+        chunks.append(bg.tm_arr); off += ntm
+        r["off_los"] = off
+        chunks.append(los.reshape(-1)); off += 6 * nl
+        pad = (-off) % 32          # keep every cosmology's block 256-byte aligned
+        if pad:
+            chunks.append(np.zeros(pad)); off += pad
+        kg = np.asarray(kg, dtype=np.float64)
+        r["off_k"] = koff
+        kchunks.append(kg); koff += kg.shape[0]
+        kp = (-koff) % 32
+        if kp:
+            kchunks.append(np.ones(kp)); koff += kp
+        r["off_pt"] = ptoff
+        ptoff += NFIELDS * n_save * kg.shape[0]
+        ptoff += (-ptoff) % 32
+        r["n_xe"] = nxe
+        r["n_tm"] = ntm
+        r["lmax_g"] = lay.lmax_g
+        r["lmax_pol_g"] = lay.lmax_pol_g
+        r["lmax_nu"] = lay.lmax_nu
+        r["lmax_ncdm"] = lay.lmax_ncdm
+        r["has_ncdm"] = int(lay.has_ncdm)
+        r["ny"] = lay.ny
+        r["nk"] = kg.shape[0]
+    items = [(i, j) for i in range(n) for j in range(int(rec[i]["nk"]))]
+    if order == "cost":
+        items.sort(key=lambda it: (-rec[it[0]]["ny"], -kgrids[it[0]][it[1]]))
+    return Batch(cosmo=rec, tables=np.concatenate(chunks), kbuf=np.concatenate(kchunks),
+                 items=np.asarray(items, dtype=np.int32).reshape(-1, 2), pt_size=ptoff, n_save=n_save,
+                 bgs=list(bgs), layouts=list(layouts))

@@ -1,0 +1,253 @@
+/*
+ * abcmb_b200.h -- C ABI of the B200 implementation of ABCMB's hot path:
+ * the per-k linear Einstein-Boltzmann hierarchy integration
+ * (abcmb/perturbations.py + abcmb/species.py) and the line-of-sight C_l
+ * projection (abcmb/spectrum.py).
+ *
+ * Every entry point takes plain pointers and sizes.  Device pointers are
+ * marked "dev"; the caller (XLA, torch, or any CUDA client) owns every
+ * buffer.  All calls are stream ordered and return 0 on success or a
+ * negative ABCMB_ERR_* code; per-k solver failures are reported through the
+ * per-item status array (ABCMB_STATUS_*), mirroring diffrax raising when
+ * max_steps is hit (abcmb/perturbations.py:304-312, docs/FAQ.rst:42-47).
+ *
+ * Data layout shared by every entry point
+ * ---------------------------------------
+ *  - abcmb_cosmo[n_cosmo]: one descriptor per cosmology (parameters after
+ *    Model.add_derived_parameters, abcmb/main.py:368-612; background scalars;
+ *    state layout from model_specs.populate_species, abcmb/model_specs.py:84-118;
+ *    offsets into the shared table / k / output buffers).
+ *  - tables (double): per cosmology the conformal-time table (10000 values on
+ *    lna in [-33, 0], abcmb/background.py:59,252-319), the x_e and T_m HyRex
+ *    tables with their inf padding already replaced by the last value
+ *    (abcmb/background.py:544-550), and the six 1-D line-of-sight arrays on
+ *    PT.lna[:-1] (tau, g, dg/dlna, aH, exp(-kappa), d(aH)/dtau;
+ *    abcmb/spectrum.py:640-651).
+ *  - PT output (double): per cosmology ABCMB_NFIELDS fields x n_save x nk,
+ *    field-major, each field laid out [save][k] like the (Nlna, Nk) arrays
+ *    of PerturbationTable (abcmb/perturbations.py:406-450).
+ */
+#ifndef ABCMB_B200_H
+#define ABCMB_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ABCMB_B200_VERSION 100   /* 1.0.0 */
+
+/* ---- error codes (return values) ---- */
+#define ABCMB_OK                 0
+#define ABCMB_ERR_ARG           -1   /* bad argument / unsupported layout   */
+#define ABCMB_ERR_CUDA          -2   /* a CUDA runtime call failed          */
+#define ABCMB_ERR_WORKSPACE     -3   /* workspace too small                 */
+#define ABCMB_ERR_TABLES        -4   /* Bessel tables not uploaded          */
+#define ABCMB_ERR_SOLVER        -5   /* at least one item has status != OK  */
+
+/* ---- per-k status codes ---- */
+#define ABCMB_STATUS_OK          0
+#define ABCMB_STATUS_MAX_STEPS   1   /* diffrax RESULTS.max_steps_reached     */
+#define ABCMB_STATUS_NONFINITE   2   /* NaN/Inf in the state or the error     */
+#define ABCMB_STATUS_DT_UNDERFLOW 3  /* step size collapsed below 1e-14       */
+
+/* ---- PerturbationTable field indices (abcmb/perturbations.py:393-404) ---- */
+enum {
+  ABCMB_F_DELTA_M = 0,        /* delta_m                                  */
+  ABCMB_F_THETA_B_PRIME,      /* theta_b_prime                            */
+  ABCMB_F_ETA,                /* metric_eta                               */
+  ABCMB_F_H_PRIME,            /* metric_h_prime                           */
+  ABCMB_F_ETA_PRIME,          /* metric_eta_prime                         */
+  ABCMB_F_ALPHA,              /* metric_alpha                             */
+  ABCMB_F_ALPHA_PRIME,        /* metric_alpha_prime                       */
+  ABCMB_F_CDM_DELTA,          /* species_perturbations["ColdDarkMatter"]  */
+  ABCMB_F_B_DELTA,            /* ["Baryon"]["delta"]                      */
+  ABCMB_F_B_THETA,            /* ["Baryon"]["theta"]                      */
+  ABCMB_F_G_DELTA,            /* ["Photon"]["delta"]                      */
+  ABCMB_F_G_THETA,            /* ["Photon"]["theta"]                      */
+  ABCMB_F_G_SIGMA,            /* ["Photon"]["sigma"]                      */
+  ABCMB_F_G_G0,               /* ["Photon"]["G0"]                         */
+  ABCMB_F_G_G2,               /* ["Photon"]["G2"]                         */
+  ABCMB_F_NU_DELTA,           /* ["MasslessNeutrino"]["delta"]            */
+  ABCMB_F_NU_THETA,           /* ["MasslessNeutrino"]["theta"]            */
+  ABCMB_F_NU_SIGMA,           /* ["MasslessNeutrino"]["sigma"]            */
+  ABCMB_F_NCDM_DELTA,         /* ["MassiveNeutrino"]["delta"] (0 if absent) */
+  ABCMB_F_NCDM_THETA,         /* ["MassiveNeutrino"]["theta"]             */
+  ABCMB_F_NCDM_SIGMA,         /* ["MassiveNeutrino"]["sigma"]             */
+  ABCMB_NFIELDS
+};
+
+/* Fixed background grids of the reference. */
+#define ABCMB_NTAU_TAB   10000    /* lna_tau_tab = linspace(-33, 0, 10000)  */
+#define ABCMB_LNA_TAU_MIN (-33.0)
+#define ABCMB_LNA_TAU_MAX (0.0)
+#define ABCMB_NLOS_ARR   6        /* tau, g, g', aH, exp(-kappa), aH_dot    */
+
+/*
+ * One cosmology.  Parameters are the derived dict of
+ * Model.add_derived_parameters (abcmb/main.py:368-612); background scalars
+ * are fields of abcmb.background.Background.
+ */
+typedef struct abcmb_cosmo {
+  /* parameters */
+  double h, omega_b, omega_cdm, omega_Lambda, A_s, n_s, TCMB0, YHe;
+  double N_nu_massless, T_nu_massless, N_nu_massive, T_nu_massive, m_nu_massive;
+  double R_nu, R_b, om;
+  /* background scalars */
+  double tau0;                /* BG.tau0 = BG.tau(0.)                        */
+  double lna_transfer_start;  /* BG.lna_transfer_start                        */
+  /* x_e table: fast_interp(lna, lna_xe0, lna_xe0 + n_xe*dx, xe) with n_xe the
+   * padded length (abcmb/background.py:593-603) */
+  double lna_xe0, lna_xe_max, lna_xe_last, xe_first, xe_last;
+  /* T_m table (abcmb/background.py:647-657) */
+  double lna_tm0, lna_tm_max, lna_tm_last, tm_last;
+  /* offsets (in doubles) into the shared table buffer */
+  int64_t off_tau;            /* ABCMB_NTAU_TAB values                        */
+  int64_t off_xe;             /* n_xe values                                  */
+  int64_t off_tm;             /* n_tm values                                  */
+  int64_t off_los;            /* ABCMB_NLOS_ARR x (n_save-1) values           */
+  /* offsets into the k buffer and the PT output buffer (doubles) */
+  int64_t off_k;              /* nk perturbation wavenumbers, increasing      */
+  int64_t off_pt;             /* ABCMB_NFIELDS x n_save x nk                  */
+  int32_t n_xe, n_tm;
+  /* state layout: y = [eta | d_cdm | d_b, th_b | F_0..F_lg | G_0..G_lp |
+   *                    N_0..N_lnu | (Psi_0..Psi_lm) x 3 bins]            */
+  int32_t lmax_g, lmax_pol_g, lmax_nu, lmax_ncdm, has_ncdm, ny;
+  int32_t nk;
+  int32_t pad_;
+} abcmb_cosmo;
+
+/* Perturbation solver settings (specs dict, abcmb/model_specs.py:55-69). */
+typedef struct abcmb_pert_settings {
+  double R_tc, R_large;             /* start-time thresholds              */
+  double k_split;                   /* k_split_PE                         */
+  double rtol_small, rtol_large;    /* rtol_{small,large}_k_PE            */
+  double atol_small, atol_large;    /* atol_{small,large}_k_PE            */
+  double pcoeff, icoeff, dcoeff;    /* PIDController coefficients         */
+  double dt0;                       /* first step (perturbations.py:306)  */
+  int32_t max_steps;                /* max_steps_PE                       */
+  int32_t n_save;                   /* 500 save points                    */
+} abcmb_pert_settings;
+
+/* Per-k solver statistics. */
+typedef struct abcmb_kstat {
+  int32_t status;        /* ABCMB_STATUS_*            */
+  int32_t n_accepted;
+  int32_t n_rejected;
+  int32_t n_newton;      /* chord iterations          */
+  double lna_start;      /* integration start         */
+} abcmb_kstat;
+
+/* Line-of-sight / C_l settings (SpectrumSolver, abcmb/spectrum.py:180-248). */
+typedef struct abcmb_los_settings {
+  double k_pivot;
+  double scale_sw, scale_isw, scale_dop, scale_pol;
+  int32_t l_min, l_max;          /* output ells = l_min..l_max (l_min == 2)   */
+  int32_t idx_min, idx_max;      /* bessel_l_tab indices covered             */
+  int32_t nkt;                   /* transfer k grid length                   */
+  int32_t precision;             /* 0 = FP64, 1 = FP32 + compensated sums    */
+} abcmb_los_settings;
+
+/* ------------------------------------------------------------------------ */
+/* Library information                                                      */
+/* ------------------------------------------------------------------------ */
+
+/* Version number (ABCMB_B200_VERSION). */
+int abcmb_version(void);
+
+/* Human readable message for the last error on the calling thread. */
+const char* abcmb_last_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* Bessel tables (abcmb/bessel_tab, loaded at import by spectrum.py:20-46). */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Upload the tabulated spherical-Bessel functions once per device.  host
+ * arrays: l_tab[n_l] (int32), for n = 0,1,2: x range xmin_n[n_l], xmax_n[n_l]
+ * (column min/max of xphi<n>.txt) and values phi_n[n_l * n_x] laid out
+ * column-major as [l][x] (i.e. the transpose of phi<n>.txt).  Replaces the
+ * module-level device_put of spectrum.py:29-46.
+ */
+int abcmb_upload_bessel(int n_l, int n_x, const int32_t* l_tab,
+                        const double* xmin0, const double* xmax0, const double* phi0,
+                        const double* xmin1, const double* xmax1, const double* phi1,
+                        const double* xmin2, const double* xmax2, const double* phi2);
+
+/* ------------------------------------------------------------------------ */
+/* Perturbations: PerturbationEvolver.full_evolution (perturbations.py:75)  */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Bytes of device workspace abcmb_pert_forward needs for n_cosmo cosmologies
+ * and n_items (cosmology, k) work items.
+ */
+int64_t abcmb_pert_workspace_size(int n_cosmo, int n_items);
+
+/*
+ * Integrate every (cosmology, k) item from its start time to lna = 0 and
+ * write the PerturbationTable fields at the n_save points
+ * linspace(lna_transfer_start, 0, n_save) of each cosmology.
+ *   cosmo_dev   [n_cosmo]            descriptors (device copy)
+ *   tables_dev                       shared table buffer
+ *   k_dev                            shared k buffer (abcmb_cosmo.off_k)
+ *   items_dev   [n_items] int32 x2   (cosmology index, k index) pairs, in the
+ *                                    order the persistent queue hands them out
+ *   pt_dev                           PT output buffer (abcmb_cosmo.off_pt)
+ *   kstat_dev   [n_items]            per-item statistics / status
+ *   workspace_dev, workspace_bytes   scratch (abcmb_pert_workspace_size)
+ *   stream                           cudaStream_t
+ * Replaces: PerturbationEvolver.full_evolution -> evolution_one_k ->
+ * diffrax.diffeqsolve (perturbations.py:75-117, 250-316) and
+ * make_output_table (perturbations.py:318-404).
+ */
+int abcmb_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev,
+                       const double* tables_dev, const double* k_dev,
+                       int n_items, const int32_t* items_dev,
+                       const abcmb_pert_settings* settings,
+                       double* pt_dev, abcmb_kstat* kstat_dev,
+                       void* workspace_dev, int64_t workspace_bytes,
+                       void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Spectrum: SpectrumSolver.get_Cl (spectrum.py:574-614)                   */
+/* ------------------------------------------------------------------------ */
+
+/* Bytes of device workspace abcmb_los_forward needs. */
+int64_t abcmb_los_workspace_size(int n_cosmo, int max_nk, int nkt, int n_ell_tab,
+                                 int n_save, int precision);
+
+/*
+ * For every cosmology: k-resample the PT source fields onto the transfer k
+ * grid (cubic spline in log10 k), form the T0/T1/T2/E sources, run the
+ * line-of-sight integral for every tabulated l in [idx_min, idx_max], do the
+ * k quadrature, and spline C_l onto the integer ells l_min..l_max.
+ *   kt_dev     [nkt]                            transfer k grid
+ *   cl_raw_dev [n_cosmo x n_ell_tab x 3]        C_l at tabulated l (TT,TE,EE)
+ *   cl_dev     [n_cosmo x 3 x (l_max-l_min+1)]  ClTT, ClTE, ClEE at integer l
+ * Replaces: get_Cl, Cl_one_ell (spectrum.py:574-797).
+ */
+int abcmb_los_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev,
+                      const double* tables_dev, const double* k_dev,
+                      const double* pt_dev, const double* kt_dev,
+                      const abcmb_los_settings* settings,
+                      double* cl_raw_dev, double* cl_dev,
+                      void* workspace_dev, int64_t workspace_bytes,
+                      void* stream);
+
+/*
+ * Linear matter power spectrum P(k, z) (SpectrumSolver.Pk_lin,
+ * spectrum.py:268-302): delta_m interpolated linearly in lna to z, then
+ * linearly in k (clamped), times the primordial spectrum.
+ *   kout_dev [n_kout], z_dev [n_z], pk_dev [n_cosmo x n_z x n_kout]
+ */
+int abcmb_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* k_dev,
+                 const double* pt_dev, int n_save, double k_pivot,
+                 int n_kout, const double* kout_dev, int n_z, const double* z_dev,
+                 double* pk_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ABCMB_B200_H */

@@ -1,0 +1,1158 @@
+/*
+ * abcmb_oracle.c -- CPU FP64 restatement of ABCMB's hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker the CUDA kernels are
+ * compared against (tests/, __graft_entry__.smoke) and the timed CPU
+ * baseline (bench.py cpu_baseline / --impl reference).  Nothing in the
+ * product path (abcmb_b200/) loads or calls it.
+ *
+ * It follows the reference line by line, in plain C with straightforward
+ * data structures (dense Jacobian, dense LU with partial pivoting -- the
+ * reference builds the Jacobian with JAX autodiff and solves it with a dense
+ * LU through lineax):
+ *   constants            abcmb/constants.py:8-39
+ *   fast_interp          abcmb/ABCMBTools.py:268-308
+ *   jnp.interp           numpy.interp semantics (perturbations.py:150,155)
+ *   species rho / P      abcmb/species.py:454-1346
+ *   background           abcmb/background.py:101-187 (rho_tot, H, aH,
+ *                        aH_prime), 321-387 (tau, nH, TCMB), 568-680 (xe, Tm,
+ *                        tau_c), hyrex/recomb_functions.py:127-153
+ *   start time           abcmb/perturbations.py:119-159, 279
+ *   initial conditions   abcmb/perturbations.py:161-199 + species y_ini
+ *   RHS                  abcmb/perturbations.py:201-248 + species y_prime
+ *   ODE solve            diffrax.diffeqsolve(Kvaerno5, PIDController,
+ *                        SaveAt(ts)) as called at perturbations.py:285-312:
+ *                        ESDIRK 5(4) tableau of Kvaerno (BIT 44, 2004), the
+ *                        "very chord" stage solve (Jacobian once per step),
+ *                        the PID step controller, cubic Hermite dense output.
+ *   output table         abcmb/perturbations.py:318-404 + output_perturbations
+ *   k resampling         interpax CubicSpline (not-a-knot, extrapolating),
+ *                        spectrum.py:664-678
+ *   sources              abcmb/spectrum.py:681-696
+ *   line of sight        abcmb/spectrum.py:638-786 (phi0/1/2 with the large-x
+ *                        asymptotic j_l of spectrum.py:48-51)
+ *   k quadrature         abcmb/spectrum.py:789-796 (trapezoid)
+ *   l spline             abcmb/spectrum.py:594-608
+ *   Pk_lin               abcmb/spectrum.py:250-302
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <stdio.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/abcmb_b200.h"
+#include "abcmb_oracle.h"
+
+/* ---------------------------------------------------------------------- */
+/* constants.py                                                            */
+/* ---------------------------------------------------------------------- */
+#define C_CM     29979245800.0
+#define C_MPC    9.71561e-15
+#define H0H      3.24078e-18
+#define HBAR     6.582119569509e-16
+#define GN       1.18980205e-40
+#define MP       938271999.0
+#define ME       510998.9461
+#define MH       (MP + ME + 13.5982860719383)
+#define MHE      3.72839e9
+#define SIGT     6.652458734e-25
+#define PI       3.14159265358979323846
+#define STEF_BOLT (PI * PI / (60. * HBAR * HBAR * HBAR * C_CM * C_CM))
+#define RHO_CRIT_UNIT (3. * H0H * H0H / 8. / PI / GN)
+
+/* MassiveNeutrino quadratures (species.py:791-794) */
+static const double Q3[3] = {0.913201, 3.37517, 7.79184};
+static const double W3[3] = {0.0687359, 3.31435, 2.29911};
+static const double Q5[5] = {0.583165, 2.0, 4.0, 7.26582, 13.0};
+static const double W5[5] = {0.0081201, 0.689407, 2.8063, 2.05156, 0.12681};
+
+/* ---------------------------------------------------------------------- */
+/* interpolation helpers                                                   */
+/* ---------------------------------------------------------------------- */
+
+/* ABCMBTools.fast_interp (ABCMBTools.py:268-308). */
+double oracle_fast_interp(double x, double xp_min, double xp_max, const double* fp, int n) {
+  const double eps = 1.e-6;
+  double i = (x - xp_min) / (xp_max - xp_min) * (double)(n - 1);
+  if (i < eps) i = eps;
+  if (i > (double)(n - 1) - eps) i = (double)(n - 1) - eps;
+  int il = (int)floor(i);
+  int iu = il + 1 < n - 1 ? il + 1 : n - 1;
+  double wu = i - (double)il;
+  double wl = 1.0 - wu;
+  return wl * fp[il] + wu * fp[iu];
+}
+
+/* jnp.interp(x, xp, fp) for increasing xp (numpy semantics, clamped). */
+double oracle_np_interp(double x, const double* xp, const double* fp, int n) {
+  /* searchsorted(xp, x, side='right') */
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (xp[mid] <= x) lo = mid + 1; else hi = mid;
+  }
+  int i = lo;
+  if (i < 1) i = 1;
+  if (i > n - 1) i = n - 1;
+  double df = fp[i] - fp[i - 1];
+  double dx = xp[i] - xp[i - 1];
+  double delta = x - xp[i - 1];
+  double f;
+  if (fabs(dx) <= 2.220446049250313e-16) f = fp[i - 1];
+  else f = fp[i - 1] + (delta / dx) * df;
+  if (x < xp[0]) f = fp[0];
+  if (x > xp[n - 1]) f = fp[n - 1];
+  return f;
+}
+
+/* jnp.linspace(a, b, n)[i] */
+static double linspace_at(double a, double b, int n, int i) {
+  if (i == n - 1) return b;
+  return a + (double)i * ((b - a) / (double)(n - 1));
+}
+
+/* ---------------------------------------------------------------------- */
+/* background                                                              */
+/* ---------------------------------------------------------------------- */
+
+typedef struct {
+  double lna, a, aH, tau, xe, tau_c, Tm, TCMB, cs2, R;
+  double rho_tot, P_tot;
+  double rho_cdm, rho_b, rho_g, rho_nu, rho_ncdm, P_ncdm;
+  double ncdm_T, ncdm_x, ncdm_fac;  /* N * 4/pi^2 T^4 / hbar^3 / c^3 */
+  double eps3[3];
+} bgs_t;
+
+static double rho_ncdm_fn(const abcmb_cosmo* c, double lna, double* P_out) {
+  double a = exp(lna);
+  double T = c->T_nu_massive * c->TCMB0 / a;
+  double x = c->m_nu_massive / T;
+  double ir = 0., ip = 0.;
+  for (int j = 0; j < 5; ++j) {
+    double q = Q5[j];
+    ir += (1. + exp(-q)) / (q * q) * sqrt(q * q + x * x) * W5[j];
+    ip += (1. + exp(-q)) / sqrt(q * q + x * x) * W5[j];
+  }
+  double T4 = T * T * T * T;
+  double rho = c->N_nu_massive * 4. * T4 / (PI * PI) * ir / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
+  double P = c->N_nu_massive * 4. / 3. * T4 / (PI * PI) * ip / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
+  if (P_out) *P_out = P;
+  return rho;
+}
+
+/* rho_tot / P_tot (background.py:101-145) in species order. */
+static void rho_P_tot(const abcmb_cosmo* c, double lna, double* rho_tot, double* P_tot,
+                      double* rcdm, double* rb, double* rg, double* rnu, double* rncdm, double* pncdm) {
+  double a = exp(lna);
+  double a3 = a * a * a, a4 = a * a * a * a;
+  double chb3 = (C_CM * HBAR) * (C_CM * HBAR) * (C_CM * HBAR);
+  double rde = c->omega_Lambda * RHO_CRIT_UNIT;
+  double rc = c->omega_cdm * RHO_CRIT_UNIT / a3;
+  double rbb = c->omega_b * RHO_CRIT_UNIT / a3;
+  double T04 = c->TCMB0 * c->TCMB0 * c->TCMB0 * c->TCMB0;
+  double r_g = PI * PI / 15. * T04 / a4 / chb3;
+  double tn = c->T_nu_massless;
+  double r_nu = c->N_nu_massless * 2. * 7. / 8. * PI * PI / 30. * (tn * tn * tn * tn) * T04 / a4;
+  r_nu = r_nu / chb3;
+  double r_ncdm = 0., p_ncdm = 0.;
+  if (c->has_ncdm) r_ncdm = rho_ncdm_fn(c, lna, &p_ncdm);
+  double rt = 0., pt = 0.;
+  rt += rde; pt += -rde;
+  rt += rc;
+  rt += rbb;
+  rt += r_g; pt += r_g / 3.;
+  rt += r_nu; pt += r_nu / 3.;
+  if (c->has_ncdm) { rt += r_ncdm; pt += p_ncdm; }
+  *rho_tot = rt; *P_tot = pt;
+  if (rcdm) *rcdm = rc;
+  if (rb) *rb = rbb;
+  if (rg) *rg = r_g;
+  if (rnu) *rnu = r_nu;
+  if (rncdm) *rncdm = r_ncdm;
+  if (pncdm) *pncdm = p_ncdm;
+}
+
+double oracle_aH(const abcmb_cosmo* c, double lna) {
+  double rt, pt;
+  rho_P_tot(c, lna, &rt, &pt, 0, 0, 0, 0, 0, 0);
+  double H = sqrt(8. * PI * GN * rt / 3.);
+  return exp(lna) * H / C_MPC;
+}
+
+static double bg_H(const abcmb_cosmo* c, double lna) {
+  double rt, pt;
+  rho_P_tot(c, lna, &rt, &pt, 0, 0, 0, 0, 0, 0);
+  return sqrt(8. * PI * GN * rt / 3.);
+}
+
+double oracle_tau(const abcmb_cosmo* c, const double* tables, double lna) {
+  return oracle_fast_interp(lna, ABCMB_LNA_TAU_MIN, ABCMB_LNA_TAU_MAX, tables + c->off_tau, ABCMB_NTAU_TAB);
+}
+
+double oracle_xe(const abcmb_cosmo* c, const double* tables, double lna) {
+  if (lna < c->lna_xe0) return c->xe_first;
+  if (lna >= c->lna_xe_last) return c->xe_last;
+  return oracle_fast_interp(lna, c->lna_xe0, c->lna_xe_max, tables + c->off_xe, c->n_xe);
+}
+
+static double nH_fn(const abcmb_cosmo* c, double lna) {
+  double a = exp(lna);
+  return (1. - c->YHe) * 3. * c->omega_b * H0H * H0H / 8. / PI / GN / MH / (a * a * a);
+}
+
+static double gamma_compton(double xe, double TCMB, double YHe) {
+  double FHe = YHe * MH / MHE / (1. - YHe);
+  return xe / (1. + FHe + xe) * 8. * SIGT * (4. * STEF_BOLT) * (TCMB * TCMB * TCMB * TCMB) / (3. * ME);
+}
+
+double oracle_Tm(const abcmb_cosmo* c, const double* tables, double lna) {
+  if (lna < c->lna_tm0) {
+    double TCMB = c->TCMB0 / exp(lna);
+    double xe = oracle_xe(c, tables, lna);
+    return TCMB * (1. - bg_H(c, lna) / gamma_compton(xe, TCMB, c->YHe));
+  }
+  if (lna >= c->lna_tm_last) return c->tm_last;
+  return oracle_fast_interp(lna, c->lna_tm0, c->lna_tm_max, tables + c->off_tm, c->n_tm);
+}
+
+double oracle_tau_c(const abcmb_cosmo* c, const double* tables, double lna) {
+  double a = exp(lna);
+  double ne = nH_fn(c, lna) * oracle_xe(c, tables, lna);
+  return 1. / a / ne / SIGT / C_CM * C_MPC;
+}
+
+/* All background scalars the RHS needs at one lna. */
+static void bg_eval(const abcmb_cosmo* c, const double* tables, double lna, bgs_t* b) {
+  b->lna = lna;
+  b->a = exp(lna);
+  rho_P_tot(c, lna, &b->rho_tot, &b->P_tot, &b->rho_cdm, &b->rho_b, &b->rho_g, &b->rho_nu,
+            &b->rho_ncdm, &b->P_ncdm);
+  double H = sqrt(8. * PI * GN * b->rho_tot / 3.);
+  b->aH = exp(lna) * H / C_MPC;
+  b->tau = oracle_tau(c, tables, lna);
+  b->xe = oracle_xe(c, tables, lna);
+  b->tau_c = oracle_tau_c(c, tables, lna);
+  b->Tm = oracle_Tm(c, tables, lna);
+  b->TCMB = c->TCMB0 / exp(lna);
+  /* Baryon.cs2 (species.py:1163-1196), mean_mass (1198-1220) */
+  double denom = (1. + b->xe) * (1. - c->YHe) + MH / MHE * c->YHe;
+  double mu = MH / denom;
+  b->R = 4. * b->rho_g / 3. / b->rho_b;
+  b->cs2 = b->Tm / mu * (5. / 3. - 2. / 3. * mu * b->R / ME / b->aH / b->tau_c * (b->TCMB / b->Tm - 1.));
+  if (c->has_ncdm) {
+    b->ncdm_T = c->T_nu_massive * c->TCMB0 / b->a;
+    b->ncdm_x = c->m_nu_massive / b->ncdm_T;
+    double T4 = b->ncdm_T * b->ncdm_T * b->ncdm_T * b->ncdm_T;
+    b->ncdm_fac = c->N_nu_massive * 4. / (PI * PI) * T4 / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
+    for (int i = 0; i < 3; ++i) b->eps3[i] = sqrt(Q3[i] * Q3[i] + b->ncdm_x * b->ncdm_x);
+  } else {
+    b->ncdm_T = b->ncdm_x = b->ncdm_fac = 0.;
+    b->eps3[0] = b->eps3[1] = b->eps3[2] = 1.;
+  }
+}
+
+double oracle_aH_prime(const abcmb_cosmo* c, double lna) {
+  double rt, pt;
+  rho_P_tot(c, lna, &rt, &pt, 0, 0, 0, 0, 0, 0);
+  double aH = oracle_aH(c, lna);
+  double a = exp(lna);
+  return -4. * PI * GN * a * a / 3. / aH * (rt + 3. * pt) / (C_MPC * C_MPC);
+}
+
+/* ---------------------------------------------------------------------- */
+/* state layout (model_specs.populate_species)                            */
+/* ---------------------------------------------------------------------- */
+typedef struct {
+  int i_eta, i_cdm, i_b, i_g, i_G, i_nu, i_ncdm;
+  int nF, nG, nN, nM, ny;
+} layout_t;
+
+static void make_layout(const abcmb_cosmo* c, layout_t* L) {
+  L->i_eta = 0;
+  L->i_cdm = 1;
+  L->i_b = 2;
+  L->nF = c->lmax_g + 1;
+  L->nG = c->lmax_pol_g + 1;
+  L->nN = c->lmax_nu + 1;
+  L->nM = c->has_ncdm ? c->lmax_ncdm + 1 : 0;
+  L->i_g = 4;
+  L->i_G = L->i_g + L->nF;
+  L->i_nu = L->i_G + L->nG;
+  L->i_ncdm = L->i_nu + L->nN;
+  L->ny = L->i_ncdm + 3 * L->nM;
+}
+
+/* Species sums entering the metric (perturbations.py:231-236). */
+static void species_sums(const abcmb_cosmo* c, const layout_t* L, const bgs_t* b, const double* y,
+                         double* srd, double* srt, double* srs) {
+  double rd = 0., rt = 0., rs = 0.;
+  /* DE: 0 */
+  rd += b->rho_cdm * y[L->i_cdm];
+  rd += b->rho_b * y[L->i_b];
+  rt += (b->rho_b + 0.) * y[L->i_b + 1];
+  rd += b->rho_g * y[L->i_g];
+  rt += (b->rho_g + b->rho_g / 3.) * y[L->i_g + 1];
+  rs += (b->rho_g + b->rho_g / 3.) * y[L->i_g + 2];
+  rd += b->rho_nu * y[L->i_nu];
+  rt += (b->rho_nu + b->rho_nu / 3.) * y[L->i_nu + 1];
+  rs += (b->rho_nu + b->rho_nu / 3.) * y[L->i_nu + 2];
+  if (c->has_ncdm) {
+    double r0 = 0., r1 = 0., r2 = 0.;
+    for (int i = 0; i < 3; ++i) {
+      double q = Q3[i], w = W3[i];
+      const double* Psi = y + L->i_ncdm + i * L->nM;
+      r0 += w * (1. + exp(-q)) * b->eps3[i] / (q * q) * Psi[0];
+      r1 += w * (1. + exp(-q)) / q * Psi[1];
+      r2 += w * (1. + exp(-q)) / b->eps3[i] * Psi[2];
+    }
+    double T4 = b->ncdm_T * b->ncdm_T * b->ncdm_T * b->ncdm_T;
+    rd += c->N_nu_massive * r0 * 4. / (PI * PI) * T4 / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
+    rt += c->N_nu_massive * r1 * 4. / (PI * PI) * T4 / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
+    rs += c->N_nu_massive * r2 * 8. / 3. / (PI * PI) * T4 / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
+  }
+  *srd = rd; *srt = rt; if (srs) *srs = rs;
+}
+
+/* get_derivatives (perturbations.py:201-248) with every species' y_prime. */
+static void rhs(const abcmb_cosmo* c, const layout_t* L, double k, const bgs_t* b,
+                const double* y, double* f) {
+  const double aH = b->aH, a = b->a, tau = b->tau, tau_c = b->tau_c;
+  double srd, srt;
+  species_sums(c, L, b, y, &srd, &srt, 0);
+  double hp = 2. / (aH * aH) * (k * k * y[0] + 4. * PI * GN * a * a / (C_MPC * C_MPC) * srd);
+  double etap = 4. * PI * GN * a * a / aH / (k * k) * srt / (C_MPC * C_MPC);
+  f[0] = etap;
+  /* ColdDarkMatter.y_prime (species.py:583-607) */
+  f[L->i_cdm] = -0.5 * hp;
+  /* Baryon.y_prime (species.py:1245-1285) */
+  {
+    double d = y[L->i_b], th = y[L->i_b + 1], thg = y[L->i_g + 1];
+    f[L->i_b] = -th / aH - hp / 2.;
+    f[L->i_b + 1] = -th + b->cs2 * k * k * d / aH + b->R / tau_c / aH * (thg - th);
+  }
+  /* Photon.y_prime (species.py:1390-1448) */
+  {
+    const double* F = y + L->i_g;
+    const double* G = y + L->i_G;
+    double* fF = f + L->i_g;
+    double* fG = f + L->i_G;
+    int Fl = L->nF - 1, Gl = L->nG - 1;
+    double thb = y[L->i_b + 1];
+    double delta = F[0], theta = F[1], sigma = F[2];
+    fF[0] = -4. / 3. / aH * theta - 2. / 3. * hp;
+    fF[1] = k * k / aH * (delta / 4. - sigma) + (thb - theta) / aH / tau_c;
+    fF[2] = 4. / 15. / aH * theta - 3. / 10. * k / aH * F[3] + 2. / 15. * hp + 4. / 5. * etap
+            - 9. / 10. / aH / tau_c * sigma + (G[0] + G[2]) / 20. / aH / tau_c;
+    fF[3] = k / 7. / aH * (6. * sigma - 4. * F[4]) - F[3] / aH / tau_c;
+    for (int l = 4; l < Fl; ++l)
+      fF[l] = 1. / (2. * l + 1.) * k / aH * (l * F[l - 1] - (l + 1) * F[l + 1]) - F[l] / aH / tau_c;
+    fF[Fl] = k / aH * F[Fl - 1] - (Fl + 1) / aH / tau * F[Fl] - F[Fl] / aH / tau_c;
+    double src = (2. * sigma + G[0] + G[2]) / 2. / aH / tau_c;
+    for (int l = 0; l < Gl; ++l) {
+      double s = (l == 0) ? 1. : (l == 2 ? 0.2 : 0.);
+      double gm1 = (l == 0) ? G[Gl] : G[l - 1];   /* G[-1] * 0 (quirk q4) */
+      fG[l] = 1. / (2. * l + 1.) * k / aH * (l * gm1 - (l + 1) * G[l + 1]) - G[l] / aH / tau_c + src * s;
+    }
+    fG[Gl] = k / aH * G[Gl - 1] - (Gl + 1) / aH / tau * G[Gl] - G[Gl] / aH / tau_c;
+  }
+  /* MasslessNeutrino.y_prime (species.py:707-753) */
+  {
+    const double* F = y + L->i_nu;
+    double* fF = f + L->i_nu;
+    int lmax = L->nN - 1;
+    double delta = F[0], theta = F[1], sigma = F[2];
+    fF[0] = -4. / 3. / aH * theta - 2. / 3. * hp;
+    fF[1] = k * k / aH * (delta / 4. - sigma);
+    fF[2] = 4. / 15. / aH * theta - 3. / 10. * k / aH * F[3] + 2. / 15. * hp + 4. / 5. * etap;
+    fF[3] = 1. / 7. * k / aH * (6. * sigma - 4. * F[4]);
+    for (int l = 4; l < lmax; ++l)
+      fF[l] = 1. / (2. * l + 1.) * k / aH * (l * F[l - 1] - (l + 1) * F[l + 1]);
+    fF[lmax] = k / aH * F[lmax - 1] - (lmax + 1) / aH / tau * F[lmax];
+  }
+  /* MassiveNeutrino.y_prime (species.py:919-977) */
+  if (c->has_ncdm) {
+    int lmax = L->nM - 1;
+    for (int i = 0; i < 3; ++i) {
+      double q = Q3[i];
+      double eps = b->eps3[i];
+      double dlnf0 = -q / (1 + exp(-q));
+      const double* P = y + L->i_ncdm + i * L->nM;
+      double* fP = f + L->i_ncdm + i * L->nM;
+      fP[0] = -q / eps / aH * P[1] + hp / 6. * dlnf0;
+      fP[1] = q * k * k / 3. / eps / aH * (P[0] - 2. * P[2]);
+      fP[2] = q * k / 5. / eps / aH * (2. * P[1] / k - 3. * P[3]) - (hp / 15. + 2. * etap / 5.) * dlnf0;
+      for (int l = 3; l < lmax; ++l)
+        fP[l] = q * k / eps / aH / (2 * l + 1) * (l * P[l - 1] - (l + 1) * P[l + 1]);
+      fP[lmax] = q * k / aH / eps * P[lmax - 1] - (lmax + 1) / aH / tau * P[lmax];
+    }
+  }
+}
+
+/* ---------------------------------------------------------------------- */
+/* start time and initial conditions                                       */
+/* ---------------------------------------------------------------------- */
+
+/* Per-cosmology part of get_starting_time: the 10000-point grids. */
+typedef struct {
+  double* lna;   /* linspace(-20, -10, 10000) */
+  double* f1;    /* tau_c * aH                */
+  double* aH;
+  double lna1;   /* interp(R_tc, f1, lna)     */
+} start_grid_t;
+
+#define NSTART 10000
+
+static void start_grid_init(const abcmb_cosmo* c, const double* tables, double R_tc, start_grid_t* g) {
+  g->lna = (double*)malloc(sizeof(double) * NSTART);
+  g->f1 = (double*)malloc(sizeof(double) * NSTART);
+  g->aH = (double*)malloc(sizeof(double) * NSTART);
+  for (int i = 0; i < NSTART; ++i) {
+    double l = linspace_at(-20.0, -10.0, NSTART, i);
+    g->lna[i] = l;
+    g->aH[i] = oracle_aH(c, l);
+    g->f1[i] = oracle_tau_c(c, tables, l) * g->aH[i];
+  }
+  g->lna1 = oracle_np_interp(R_tc, g->f1, g->lna, NSTART);
+}
+
+static void start_grid_free(start_grid_t* g) { free(g->lna); free(g->f1); free(g->aH); }
+
+double oracle_start_time(const abcmb_cosmo* c, const double* tables, double k, double R_tc, double R_large) {
+  start_grid_t g;
+  start_grid_init(c, tables, R_tc, &g);
+  double* f2 = (double*)malloc(sizeof(double) * NSTART);
+  for (int i = 0; i < NSTART; ++i) f2[i] = k / g.aH[i];
+  double lna2 = oracle_np_interp(R_large, f2, g.lna, NSTART);
+  double s = g.lna1 < lna2 ? g.lna1 : lna2;
+  free(f2);
+  start_grid_free(&g);
+  return s < -10. ? s : -10.;
+}
+
+static double start_time_from_grid(const start_grid_t* g, double k, double R_large, double* f2) {
+  for (int i = 0; i < NSTART; ++i) f2[i] = k / g->aH[i];
+  double lna2 = oracle_np_interp(R_large, f2, g->lna, NSTART);
+  double s = g->lna1 < lna2 ? g->lna1 : lna2;
+  return s < -10. ? s : -10.;
+}
+
+/* initial_conditions_one_k (perturbations.py:161-199). */
+static void initial_conditions(const abcmb_cosmo* c, const layout_t* L, const double* tables,
+                               double k, double lna_ini, double* y) {
+  double tau_ini = oracle_tau(c, tables, lna_ini);
+  double om = c->om, Rn = c->R_nu, Rb = c->R_b;
+  memset(y, 0, sizeof(double) * L->ny);
+  y[0] = (1. - k * k * tau_ini * tau_ini / 12. / (15. + 4. * Rn) *
+                   (5. + 4. * Rn - (16. * Rn * Rn + 280. * Rn + 325) / 10. / (2. * Rn + 15.) * tau_ini * om));
+  double kt = k * tau_ini;
+  /* CDM */
+  y[L->i_cdm] = -(kt * kt) / 4. * (1. - om * tau_ini / 5.);
+  /* Baryon */
+  y[L->i_b] = -(kt * kt) / 4. * (1. - om * tau_ini / 5.);
+  y[L->i_b + 1] = -k * k * k * k * tau_ini * tau_ini * tau_ini / 36. *
+                  (1. - 3. * (1. + 5. * Rb - Rn) / 20. / (1. - Rn) * om * tau_ini);
+  /* Photon */
+  y[L->i_g] = -(kt * kt) / 3. * (1. - om * tau_ini / 5.);
+  y[L->i_g + 1] = -k * k * k * k * tau_ini * tau_ini * tau_ini / 36. *
+                  (1. - 3. * (1. + 5. * Rb - Rn) / 20. / (1. - Rn) * om * tau_ini);
+  /* Massless neutrinos */
+  double nd = -(kt * kt) / 3. * (1. - om * tau_ini / 5.);
+  double nth = -k * (kt * kt * kt) / 36. / (4. * Rn + 15.) *
+               (4. * Rn + 11. + 12. - 3. * (8. * Rn * Rn + 50. * Rn + 275.) / 20. / (2. * Rn + 15.) * tau_ini * om);
+  double ns = (kt * kt) / (45. + 12. * Rn) * 2. * (1. + (4. * Rn - 5.) / 4. / (2. * Rn + 15.) * tau_ini * om);
+  y[L->i_nu] = nd;
+  y[L->i_nu + 1] = nth;
+  y[L->i_nu + 2] = ns;
+  /* Massive neutrinos (species.py:882-917) */
+  if (c->has_ncdm) {
+    for (int i = 0; i < 3; ++i) {
+      double q = Q3[i];
+      double fac = q / (1. + exp(-q));
+      double* P = y + L->i_ncdm + i * L->nM;
+      P[0] = nd / 4. * fac;
+      P[1] = nth / 3. * fac;
+      P[2] = ns / 2. * fac;
+    }
+  }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Kvaerno5 tableau (Kvaerno, BIT 44 (2004) 489-502; ESDIRK 5(4), 7 stages) */
+/* ---------------------------------------------------------------------- */
+#define KV_GAMMA 0.26
+static const double KV_C[7] = {0.0, 0.52, 1.230333209967908, 0.8957659843500759,
+                               0.43639360985864756, 1.0, 1.0};
+static const double KV_A[7][7] = {
+  {0, 0, 0, 0, 0, 0, 0},
+  {0.26, 0, 0, 0, 0, 0, 0},
+  {0.13, 0.84033320996790809, 0, 0, 0, 0, 0},
+  {0.22371961478320505, 0.47675532319799699, -0.06470895363112615, 0, 0, 0, 0},
+  {0.16648564323248321, 0.10450018841591720, 0.03631482272098715, -0.13090704451073998, 0, 0, 0},
+  {0.13855640231268224, 0.0, -0.04245337201752043, 0.02446657898003141, 0.61943039072480676, 0, 0},
+  {0.13659751177640291, 0.0, -0.05496908796538376, -0.04118626728321046, 0.62993304899016403,
+   0.06962479448202728, 0}};
+
+void oracle_kvaerno5_tableau(double* A49, double* c7, double* gamma) {
+  for (int i = 0; i < 7; ++i) {
+    for (int j = 0; j < 7; ++j) A49[i * 7 + j] = KV_A[i][j];
+    if (i > 0) A49[i * 7 + i] = KV_GAMMA;
+    c7[i] = KV_C[i];
+  }
+  *gamma = KV_GAMMA;
+}
+
+/* ---------------------------------------------------------------------- */
+/* dense linear algebra                                                    */
+/* ---------------------------------------------------------------------- */
+
+/* LU with partial pivoting, in place; returns 0 on success. */
+static int lu_factor(double* M, int n, int* piv) {
+  for (int p = 0; p < n; ++p) {
+    int im = p;
+    double vm = fabs(M[p * n + p]);
+    for (int i = p + 1; i < n; ++i) {
+      double v = fabs(M[i * n + p]);
+      if (v > vm) { vm = v; im = i; }
+    }
+    piv[p] = im;
+    if (vm == 0.0) return -1;
+    if (im != p)
+      for (int j = 0; j < n; ++j) { double t = M[p * n + j]; M[p * n + j] = M[im * n + j]; M[im * n + j] = t; }
+    double inv = 1.0 / M[p * n + p];
+    for (int i = p + 1; i < n; ++i) {
+      double m = M[i * n + p] * inv;
+      M[i * n + p] = m;
+      if (m != 0.0)
+        for (int j = p + 1; j < n; ++j) M[i * n + j] -= m * M[p * n + j];
+    }
+  }
+  return 0;
+}
+
+static void lu_solve(const double* M, int n, const int* piv, double* b) {
+  for (int p = 0; p < n; ++p) {
+    if (piv[p] != p) { double t = b[p]; b[p] = b[piv[p]]; b[piv[p]] = t; }
+  }
+  for (int i = 1; i < n; ++i) {
+    double s = b[i];
+    for (int j = 0; j < i; ++j) s -= M[i * n + j] * b[j];
+    b[i] = s;
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    double s = b[i];
+    for (int j = i + 1; j < n; ++j) s -= M[i * n + j] * b[j];
+    b[i] = s / M[i * n + i];
+  }
+}
+
+static double rms_norm(const double* v, int n) {
+  double s = 0.;
+  for (int i = 0; i < n; ++i) s += v[i] * v[i];
+  return sqrt(s / n);
+}
+
+/* ---------------------------------------------------------------------- */
+/* output table at one save point (perturbations.py:318-404)               */
+/* ---------------------------------------------------------------------- */
+static void output_fields(const abcmb_cosmo* c, const layout_t* L, const double* tables,
+                          double k, double lna, const double* y, double* out) {
+  bgs_t b;
+  bg_eval(c, tables, lna, &b);
+  double srd, srt, srs;
+  species_sums(c, L, &b, y, &srd, &srt, &srs);
+  double a = b.a, aH = b.aH;
+  double eta = y[0];
+  double delta_b = y[L->i_b], theta_b = y[L->i_b + 1], theta_g = y[L->i_g + 1];
+  out[ABCMB_F_THETA_B_PRIME] = -theta_b + b.cs2 / aH * (k * k * delta_b) + b.R / aH / b.tau_c * (theta_g - theta_b);
+  /* delta_m: matter species CDM, Baryon, MassiveNeutrino (is_matter) */
+  double rdm = b.rho_cdm * y[L->i_cdm] + b.rho_b * y[L->i_b];
+  double rm = b.rho_cdm + b.rho_b;
+  double ncdm_d = 0., ncdm_t = 0., ncdm_s = 0.;
+  if (c->has_ncdm) {
+    double r0 = 0., r1 = 0., r2 = 0.;
+    for (int i = 0; i < 3; ++i) {
+      double q = Q3[i], w = W3[i];
+      const double* Psi = y + L->i_ncdm + i * L->nM;
+      r0 += w * (1. + exp(-q)) * b.eps3[i] / (q * q) * Psi[0];
+      r1 += w * (1. + exp(-q)) / q * Psi[1];
+      r2 += w * (1. + exp(-q)) / b.eps3[i] * Psi[2];
+    }
+    double T4 = b.ncdm_T * b.ncdm_T * b.ncdm_T * b.ncdm_T;
+    double rd_n = c->N_nu_massive * r0 * 4. / (PI * PI) * T4 / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
+    double rt_n = c->N_nu_massive * r1 * 4. / (PI * PI) * T4 / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
+    double rs_n = c->N_nu_massive * r2 * 8. / 3. / (PI * PI) * T4 / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
+    rdm += rd_n;
+    rm += b.rho_ncdm;
+    double rhoP = b.rho_ncdm + b.P_ncdm;
+    ncdm_d = rd_n / b.rho_ncdm;
+    ncdm_t = rt_n / rhoP;
+    ncdm_s = rs_n / rhoP;
+  }
+  out[ABCMB_F_DELTA_M] = rdm / rm;
+  double hp = 2. / (aH * aH) * (k * k * eta + 4. * PI * GN * a * a / (C_MPC * C_MPC) * srd);
+  double etap = 4. * PI * GN * a * a / aH * srt / (C_MPC * C_MPC) / (k * k);
+  double alpha = aH * (hp + 6. * etap) / 2. / (k * k);
+  double alphap = eta / aH - 2. * alpha - 12. * PI * GN * a * a / aH * srs / (C_MPC * C_MPC) / (k * k);
+  out[ABCMB_F_ETA] = eta;
+  out[ABCMB_F_H_PRIME] = hp;
+  out[ABCMB_F_ETA_PRIME] = etap;
+  out[ABCMB_F_ALPHA] = alpha;
+  out[ABCMB_F_ALPHA_PRIME] = alphap;
+  out[ABCMB_F_CDM_DELTA] = y[L->i_cdm];
+  out[ABCMB_F_B_DELTA] = delta_b;
+  out[ABCMB_F_B_THETA] = theta_b;
+  out[ABCMB_F_G_DELTA] = y[L->i_g];
+  out[ABCMB_F_G_THETA] = theta_g;
+  out[ABCMB_F_G_SIGMA] = y[L->i_g + 2];
+  out[ABCMB_F_G_G0] = y[L->i_G];
+  out[ABCMB_F_G_G2] = y[L->i_G + 2];
+  out[ABCMB_F_NU_DELTA] = y[L->i_nu];
+  out[ABCMB_F_NU_THETA] = y[L->i_nu + 1];
+  out[ABCMB_F_NU_SIGMA] = y[L->i_nu + 2];
+  out[ABCMB_F_NCDM_DELTA] = ncdm_d;
+  out[ABCMB_F_NCDM_THETA] = ncdm_t;
+  out[ABCMB_F_NCDM_SIGMA] = ncdm_s;
+}
+
+/* ---------------------------------------------------------------------- */
+/* one k mode: diffeqsolve(Kvaerno5, PIDController, SaveAt(ts))            */
+/* ---------------------------------------------------------------------- */
+
+/* scaled rms error as in PIDController.adapt_step_size */
+static double scaled_err(const double* y0, const double* y1, const double* e, int n, double rtol, double atol) {
+  double s = 0.;
+  for (int i = 0; i < n; ++i) {
+    double ym = fabs(y0[i]) > fabs(y1[i]) ? fabs(y0[i]) : fabs(y1[i]);
+    double v = e[i] / (atol + ym * rtol);
+    s += v * v;
+  }
+  return sqrt(s / n);
+}
+
+typedef struct {
+  double* y0; double* y1; double* F;  /* F: 7 x ny stage derivatives */
+  double* base; double* v; double* r; double* yerr; double* Jm; int* piv;
+  double* col; double* tmp; double* f2;
+} work_t;
+
+static void work_alloc(work_t* w, int ny) {
+  w->y0 = (double*)calloc(ny, sizeof(double));
+  w->y1 = (double*)calloc(ny, sizeof(double));
+  w->F = (double*)calloc(7 * ny, sizeof(double));
+  w->base = (double*)calloc(ny, sizeof(double));
+  w->v = (double*)calloc(ny, sizeof(double));
+  w->r = (double*)calloc(ny, sizeof(double));
+  w->yerr = (double*)calloc(ny, sizeof(double));
+  w->Jm = (double*)calloc((size_t)ny * ny, sizeof(double));
+  w->piv = (int*)calloc(ny, sizeof(int));
+  w->col = (double*)calloc(ny, sizeof(double));
+  w->tmp = (double*)calloc(ny, sizeof(double));
+  w->f2 = (double*)calloc(NSTART, sizeof(double));
+}
+
+static void work_free(work_t* w) {
+  free(w->y0); free(w->y1); free(w->F); free(w->base); free(w->v); free(w->r); free(w->yerr);
+  free(w->Jm); free(w->piv); free(w->col); free(w->tmp); free(w->f2);
+}
+
+/* Jacobian of the stage root function at lna_lin: M = I - h*gamma*A(lna_lin).
+ * A is obtained column by column (the RHS is linear in y), the way JAX
+ * materialises the Jacobian from JVPs of basis vectors. */
+static void build_newton_matrix(const abcmb_cosmo* c, const layout_t* L, double k, const bgs_t* b,
+                                double hg, work_t* w) {
+  int n = L->ny;
+  for (int j = 0; j < n; ++j) {
+    memset(w->col, 0, sizeof(double) * n);
+    w->col[j] = 1.0;
+    rhs(c, L, k, b, w->col, w->tmp);
+    for (int i = 0; i < n; ++i) w->Jm[i * n + j] = (i == j ? 1.0 : 0.0) - hg * w->tmp[i];
+  }
+}
+
+/* One k mode from its start time to lna = 0 (perturbations.py:250-316). */
+static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kbuf,
+                    const abcmb_pert_settings* s, const start_grid_t* sg, int ik,
+                    double* pt, abcmb_kstat* st, work_t* w) {
+  layout_t L;
+  make_layout(c, &L);
+  const int n = L.ny;
+  const double k = kbuf[c->off_k + ik];
+  const int nsave = s->n_save;
+  const double rtol = k > s->k_split ? s->rtol_large : s->rtol_small;
+  const double atol = k > s->k_split ? s->atol_large : s->atol_small;
+  const double err_order = 5.0;       /* Kvaerno5.order */
+  const double safety = 0.9, factormin = 0.2, factormax = 10.0;
+  const double coeff1 = (s->icoeff + s->pcoeff + s->dcoeff) / err_order;
+  const double coeff2 = -(s->pcoeff + 2. * s->dcoeff) / err_order;
+  const double coeff3 = s->dcoeff / err_order;
+  const double kappa = 1e-2;          /* VeryChord kappa          */
+  const int root_max = 10;            /* Kvaerno5.root_find_max_steps */
+  const double small_res = 1e-13;     /* 10**(2 - precision(float64)) */
+
+  double lna_start = start_time_from_grid(sg, k, s->R_large, w->f2);
+  st->lna_start = lna_start;
+  st->status = ABCMB_STATUS_OK;
+  st->n_accepted = st->n_rejected = st->n_newton = 0;
+
+  initial_conditions(c, &L, tables, k, lna_start, w->y0);
+
+  const double t_end = 0.0;
+  double t0 = lna_start;
+  double t1 = t0 + s->dt0;
+  if (t1 > t_end) t1 = t_end;
+  double prev_inv = 1.0, prev_prev_inv = 1.0;
+  int isave = 0;
+  const double lts = c->lna_transfer_start;
+  double* ptc = pt + c->off_pt;
+  const int nk = c->nk;
+  double outv[ABCMB_NFIELDS];
+  double* ysave = w->tmp;  /* reuse */
+
+  /* FSAL: stage 1 derivative at (t0, y0) */
+  bgs_t b;
+  bg_eval(c, tables, t0, &b);
+  rhs(c, &L, k, &b, w->y0, w->F);
+
+  int nsteps = 0;
+  while (t0 < t_end) {
+    if (nsteps >= s->max_steps) { st->status = ABCMB_STATUS_MAX_STEPS; break; }
+    nsteps++;
+    const double h = t1 - t0;
+    const double hg = h * KV_GAMMA;
+    /* VeryChord: one Jacobian per step, linearised at the first implicit stage */
+    bgs_t blin;
+    bg_eval(c, tables, t0 + KV_C[1] * h, &blin);
+    build_newton_matrix(c, &L, k, &blin, hg, w);
+    int ok = lu_factor(w->Jm, n, w->piv) == 0;
+    for (int i = 1; i < 7 && ok; ++i) {
+      double ti = t0 + KV_C[i] * h;
+      bgs_t bi;
+      bg_eval(c, tables, ti, &bi);
+      for (int e = 0; e < n; ++e) {
+        double acc = 0.;
+        for (int j = 0; j < i; ++j) acc += KV_A[i][j] * w->F[j * n + e];
+        w->base[e] = w->y0[e] + h * acc;
+      }
+      double* fi = w->F + i * n;
+      memcpy(fi, w->F + (i - 1) * n, sizeof(double) * n);   /* predictor: previous stage */
+      double diffsize = INFINITY, diffsize_prev = INFINITY;
+      int conv = 0;
+      for (int it = 1; it <= root_max; ++it) {
+        for (int e = 0; e < n; ++e) w->v[e] = w->base[e] + hg * fi[e];
+        rhs(c, &L, k, &bi, w->v, w->r);
+        /* R = A v - f ; diff = J^{-1} R with J = h*gamma*A_lin - I = -M  => diff = -M^{-1} R */
+        for (int e = 0; e < n; ++e) w->r[e] = -(w->r[e] - fi[e]);
+        lu_solve(w->Jm, n, w->piv, w->r);
+        double ss = 0.;
+        for (int e = 0; e < n; ++e) {
+          double fnew = fi[e] - w->r[e];
+          fi[e] = fnew;
+          double sc = atol + rtol * fabs(fnew);
+          double q = w->r[e] / sc;
+          ss += q * q;
+        }
+        diffsize_prev = diffsize;
+        diffsize = sqrt(ss / n);
+        st->n_newton++;
+        if (it >= 2) {
+          double rate = diffsize / diffsize_prev;
+          double factor = diffsize * rate / (1. - rate);
+          int small = diffsize < small_res;
+          int diverged = !isfinite(rate) || rate > 2.;
+          int converged = factor > 0. && factor < kappa;
+          if (small || converged) { conv = 1; break; }
+          if (diverged) break;
+        }
+      }
+      if (!conv) ok = 0;
+    }
+    double scaled;
+    if (ok) {
+      /* y1 = z7 = y0 + h sum_j a7j F_j + h gamma F_7 ;  y_err = z7 - z6 */
+      for (int e = 0; e < n; ++e) {
+        double acc = 0., acce = 0.;
+        for (int j = 0; j < 6; ++j) {
+          acc += KV_A[6][j] * w->F[j * n + e];
+          acce += (KV_A[6][j] - KV_A[5][j]) * w->F[j * n + e];
+        }
+        acc += KV_GAMMA * w->F[6 * n + e];
+        /* b_error = b_sol - b_embedded: the embedded row 6 carries gamma on
+         * stage 6, the solution row 7 carries gamma on stage 7 */
+        acce += -KV_GAMMA * w->F[5 * n + e] + KV_GAMMA * w->F[6 * n + e];
+        w->y1[e] = w->y0[e] + h * acc;
+        w->yerr[e] = h * acce;
+      }
+      scaled = scaled_err(w->y0, w->y1, w->yerr, n, rtol, atol);
+      if (!isfinite(scaled)) scaled = INFINITY;
+    } else {
+      scaled = INFINITY;
+    }
+    int keep = scaled < 1.0;
+    double inv = 1.0 / scaled;
+    double f1v = (coeff1 == 0.) ? 1. : pow(inv, coeff1);
+    double f2v = (coeff2 == 0.) ? 1. : pow(prev_inv, coeff2);
+    double f3v = (coeff3 == 0.) ? 1. : pow(prev_prev_inv, coeff3);
+    double fmin = keep ? 1.0 : factormin;
+    double factor = safety * f1v * f2v * f3v;
+    if (factor < fmin) factor = fmin;
+    if (factor > factormax) factor = factormax;
+    double dt_new = h * factor;
+    if (inv == 0. || isinf(inv)) inv = 1.;
+    if (keep) {
+      st->n_accepted++;
+      /* dense output: cubic Hermite on [t0, t1] (ThirdOrderHermitePolynomialInterpolation) */
+      const double* fa = w->F;            /* f(t0, y0) */
+      const double* fb = w->F + 6 * n;    /* f(t1, y1) */
+      while (isave < nsave) {
+        double ts = linspace_at(lts, 0.0, nsave, isave);
+        if (!(ts <= t1)) break;
+        if (ts < t0) { isave++; continue; }   /* cannot happen: start < lts */
+        double th = (ts - t0) / h;
+        for (int e = 0; e < n; ++e) {
+          double y0e = w->y0[e], y1e = w->y1[e];
+          double k0 = h * fa[e], k1 = h * fb[e];
+          ysave[e] = y0e + th * (k0 + th * ((3. * (y1e - y0e) - 2. * k0 - k1) +
+                                            th * (2. * (y0e - y1e) + k0 + k1)));
+        }
+        output_fields(c, &L, tables, k, ts, ysave, outv);
+        for (int f = 0; f < ABCMB_NFIELDS; ++f)
+          ptc[((size_t)f * nsave + isave) * nk + ik] = outv[f];
+        isave++;
+      }
+      prev_prev_inv = prev_inv;
+      prev_inv = inv;
+      memcpy(w->y0, w->y1, sizeof(double) * n);
+      memcpy(w->F, w->F + 6 * n, sizeof(double) * n);   /* FSAL */
+      t0 = t1;
+    } else {
+      st->n_rejected++;
+    }
+    if (t0 >= t_end) break;
+    double tn = t0 + dt_new;
+    const double tol = 1e-10;
+    if (tn > t_end - tol) tn = keep ? t_end : t0 + 0.5 * (t_end - t0);
+    t1 = tn;
+    if (!(h > 1e-14) || !isfinite(t1)) { st->status = ABCMB_STATUS_DT_UNDERFLOW; break; }
+  }
+  if (st->status == ABCMB_STATUS_OK && isave < nsave) st->status = ABCMB_STATUS_NONFINITE;
+}
+
+int oracle_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
+                        int n_items, const int32_t* items, const abcmb_pert_settings* s,
+                        double* pt, abcmb_kstat* kstat, int n_threads) {
+  start_grid_t* sg = (start_grid_t*)calloc(n_cosmo, sizeof(start_grid_t));
+  int maxny = 0;
+  for (int c = 0; c < n_cosmo; ++c) {
+    start_grid_init(&cosmo[c], tables, s->R_tc, &sg[c]);
+    if (cosmo[c].ny > maxny) maxny = cosmo[c].ny;
+  }
+#ifdef _OPENMP
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+#endif
+#pragma omp parallel
+  {
+    work_t w;
+    work_alloc(&w, maxny);
+#pragma omp for schedule(dynamic, 1)
+    for (int it = 0; it < n_items; ++it) {
+      int ci = items[2 * it], ik = items[2 * it + 1];
+      solve_k(&cosmo[ci], tables, kbuf, s, &sg[ci], ik, pt, &kstat[it], &w);
+    }
+    work_free(&w);
+  }
+  for (int c = 0; c < n_cosmo; ++c) start_grid_free(&sg[c]);
+  free(sg);
+  int bad = 0;
+  for (int it = 0; it < n_items; ++it) if (kstat[it].status != ABCMB_STATUS_OK) bad = 1;
+  return bad ? ABCMB_ERR_SOLVER : ABCMB_OK;
+}
+
+/* Single-k helpers for unit tests. */
+void oracle_rhs(const abcmb_cosmo* c, const double* tables, double k, double lna, const double* y, double* f) {
+  layout_t L;
+  make_layout(c, &L);
+  bgs_t b;
+  bg_eval(c, tables, lna, &b);
+  rhs(c, &L, k, &b, y, f);
+}
+
+void oracle_initial_conditions(const abcmb_cosmo* c, const double* tables, double k, double lna, double* y) {
+  layout_t L;
+  make_layout(c, &L);
+  initial_conditions(c, &L, tables, k, lna, y);
+}
+
+void oracle_output_fields(const abcmb_cosmo* c, const double* tables, double k, double lna,
+                          const double* y, double* out) {
+  layout_t L;
+  make_layout(c, &L);
+  output_fields(c, &L, tables, k, lna, y, out);
+}
+
+/* ---------------------------------------------------------------------- */
+/* cubic spline, not-a-knot, extrapolating (interpax / scipy CubicSpline)   */
+/* ---------------------------------------------------------------------- */
+
+/* Derivatives s[n] of the not-a-knot spline through (x, y); n >= 4. */
+void oracle_spline_slopes(const double* x, const double* y, int n, double* s) {
+  double* lo = (double*)malloc(sizeof(double) * n);
+  double* di = (double*)malloc(sizeof(double) * n);
+  double* up = (double*)malloc(sizeof(double) * n);
+  double* b = (double*)malloc(sizeof(double) * n);
+  double* dx = (double*)malloc(sizeof(double) * n);
+  double* sl = (double*)malloc(sizeof(double) * n);
+  for (int i = 0; i < n - 1; ++i) { dx[i] = x[i + 1] - x[i]; sl[i] = (y[i + 1] - y[i]) / dx[i]; }
+  /* first row */
+  {
+    double d = x[2] - x[0];
+    di[0] = dx[1]; up[0] = d; lo[0] = 0.;
+    b[0] = ((dx[0] + 2. * d) * dx[1] * sl[0] + dx[0] * dx[0] * sl[1]) / d;
+  }
+  for (int i = 1; i < n - 1; ++i) {
+    lo[i] = dx[i];
+    di[i] = 2. * (dx[i - 1] + dx[i]);
+    up[i] = dx[i - 1];
+    b[i] = 3. * (dx[i] * sl[i - 1] + dx[i - 1] * sl[i]);
+  }
+  {
+    double d = x[n - 1] - x[n - 3];
+    lo[n - 1] = d; di[n - 1] = dx[n - 3]; up[n - 1] = 0.;
+    b[n - 1] = (dx[n - 2] * dx[n - 2] * sl[n - 3] + (2. * d + dx[n - 2]) * dx[n - 3] * sl[n - 2]) / d;
+  }
+  /* Thomas algorithm */
+  for (int i = 1; i < n; ++i) {
+    double m = lo[i] / di[i - 1];
+    di[i] -= m * up[i - 1];
+    b[i] -= m * b[i - 1];
+  }
+  s[n - 1] = b[n - 1] / di[n - 1];
+  for (int i = n - 2; i >= 0; --i) s[i] = (b[i] - up[i] * s[i + 1]) / di[i];
+  free(lo); free(di); free(up); free(b); free(dx); free(sl);
+}
+
+/* Evaluate the spline with slopes s at xq (extrapolating with end pieces). */
+double oracle_spline_eval(const double* x, const double* y, const double* s, int n, double xq) {
+  /* i = clip(searchsorted(x, xq, 'right'), 1, n-1) - 1 */
+  int lo = 0, hi = n;
+  while (lo < hi) { int mid = (lo + hi) >> 1; if (x[mid] <= xq) lo = mid + 1; else hi = mid; }
+  int i = lo;
+  if (i < 1) i = 1;
+  if (i > n - 1) i = n - 1;
+  i -= 1;
+  double dx = x[i + 1] - x[i];
+  double sl = (y[i + 1] - y[i]) / dx;
+  double t = (s[i] + s[i + 1] - 2. * sl) / dx;
+  double c3 = t / dx;
+  double c2 = (sl - s[i]) / dx - t;
+  double c1 = s[i];
+  double c0 = y[i];
+  double u = xq - x[i];
+  return ((c3 * u + c2) * u + c1) * u + c0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Bessel lookups (spectrum.py:48-109, 719-753)                            */
+/* ---------------------------------------------------------------------- */
+static double jasym(double l, double x) {
+  double nu = l + 0.5;
+  double r = sqrt(x * x - nu * nu);
+  double Q = r - nu * PI / 2 + nu * asin(nu / x);
+  double J = sqrt(2 / PI / r) * cos(Q - PI / 4);
+  return sqrt(PI / 2 / x) * J;
+}
+
+double oracle_phi(int which, const oracle_bessel* B, int idx, double x) {
+  double l = (double)B->l_tab[idx];
+  double xmin = B->xmin[which][idx], xmax = B->xmax[which][idx];
+  const double* col = B->phi[which] + (size_t)idx * B->n_x;
+  if (x < xmin) return 0.;
+  if (x >= xmax) {
+    if (which == 0) return jasym(l, x);
+    if (which == 1) return l / x * jasym(l, x) - jasym(l + 1, x);
+    return ((3 * l * (l - 1) - 2 * x * x) * jasym(l, x) + 6 * x * jasym(l + 1, x)) / 2 / (x * x);
+  }
+  return oracle_fast_interp(x, xmin, xmax, col, B->n_x);
+}
+
+/* ---------------------------------------------------------------------- */
+/* SpectrumSolver.get_Cl                                                   */
+/* ---------------------------------------------------------------------- */
+
+/* Transfer sources S[4][n_lna][nkt] for one cosmology (spectrum.py:640-696). */
+void oracle_sources(const abcmb_cosmo* c, const double* tables, const double* kbuf, const double* pt,
+                    const double* kt, int nkt, int n_save, const abcmb_los_settings* ls, double* S) {
+  const int nk = c->nk;
+  const int nl = n_save - 1;
+  const double* kp = kbuf + c->off_k;
+  const double* los = tables + c->off_los;
+  const double* ptc = pt + c->off_pt;
+  double* lk = (double*)malloc(sizeof(double) * nk);
+  double* lkt = (double*)malloc(sizeof(double) * nkt);
+  for (int i = 0; i < nk; ++i) lk[i] = log10(kp[i]);
+  for (int i = 0; i < nkt; ++i) lkt[i] = log10(kt[i]);
+  static const int fields[10] = {ABCMB_F_G_DELTA, ABCMB_F_B_THETA, ABCMB_F_THETA_B_PRIME, ABCMB_F_G_SIGMA,
+                                 ABCMB_F_G_G0, ABCMB_F_G_G2, ABCMB_F_ETA, ABCMB_F_ETA_PRIME,
+                                 ABCMB_F_ALPHA, ABCMB_F_ALPHA_PRIME};
+#pragma omp parallel
+  {
+    double* sl = (double*)malloc(sizeof(double) * nk);
+    double* val = (double*)malloc(sizeof(double) * 10 * nkt);
+#pragma omp for schedule(static)
+    for (int il = 0; il < nl; ++il) {
+      for (int f = 0; f < 10; ++f) {
+        const double* col = ptc + ((size_t)fields[f] * n_save + il) * nk;
+        oracle_spline_slopes(lk, col, nk, sl);
+        for (int j = 0; j < nkt; ++j) val[f * nkt + j] = oracle_spline_eval(lk, col, sl, nk, lkt[j]);
+      }
+      double g = los[1 * nl + il], gp = los[2 * nl + il], aH = los[3 * nl + il];
+      double em = los[4 * nl + il], aHd = los[5 * nl + il];
+      for (int j = 0; j < nkt; ++j) {
+        double k = kt[j];
+        double dg = val[0 * nkt + j], thb = val[1 * nkt + j], thbp = val[2 * nkt + j], sg = val[3 * nkt + j];
+        double G0 = val[4 * nkt + j], G2 = val[5 * nkt + j], eta = val[6 * nkt + j], etap = val[7 * nkt + j];
+        double al = val[8 * nkt + j], alp = val[9 * nkt + j];
+        double sT0 = ls->scale_sw * g * (dg / 4. + aH * alp)
+                     + ls->scale_isw * (g * (eta - aH * alp - 2. * aH * al)
+                                        + 2. * em * (aH * etap - aHd * al - aH * aH * alp))
+                     + ls->scale_dop * (aH * (g * ((thbp / (k * k)) + alp) + gp * ((thb / (k * k)) + al)));
+        double sT1 = ls->scale_isw * em * ((aH * alp + 2. * aH * al - eta) * k);
+        double sT2 = ls->scale_pol * g * (2 * sg + G0 + G2) / 8.;
+        double sE = sqrt(6.) * g * (2 * sg + G0 + G2) / 8.;
+        S[((size_t)0 * nl + il) * nkt + j] = sT0;
+        S[((size_t)1 * nl + il) * nkt + j] = sT1;
+        S[((size_t)2 * nl + il) * nkt + j] = sT2;
+        S[((size_t)3 * nl + il) * nkt + j] = sE;
+      }
+    }
+    free(sl); free(val);
+  }
+  free(lk); free(lkt);
+}
+
+/* Transfer functions Delta_T(l,k), Delta_E(l,k) for tabulated l index idx. */
+static void los_one_ell(const abcmb_cosmo* c, const double* tables, const double* S, const double* kt, int nkt,
+                        int n_save, double lna_first, double lna_last_delta, const oracle_bessel* B, int idx,
+                        double* T, double* E) {
+  const int nl = n_save - 1;
+  const double* los = tables + c->off_los;
+  const double tau0 = c->tau0;
+  double l = (double)B->l_tab[idx];
+  double ef = sqrt(3. / 8. * (l + 2) * (l + 1) * l * (l - 1));
+  (void)lna_first;
+  for (int j = 0; j < nkt; ++j) {
+    double k = kt[j];
+    double a0 = 0., a1 = 0., a2 = 0., aE = 0.;
+    for (int il = 0; il < nl; ++il) {
+      double w = il == 0 ? 0.5 * lna_last_delta : lna_last_delta;
+      double tau = los[0 * nl + il], aH = los[3 * nl + il];
+      double chi = (tau0 - tau) * k;
+      double p0 = oracle_phi(0, B, idx, chi);
+      double p1 = oracle_phi(1, B, idx, chi);
+      double p2 = oracle_phi(2, B, idx, chi);
+      double eps = p0 / (chi * chi) * ef;
+      double inv_aH = 1.0 / aH;
+      a0 = a0 + w * S[((size_t)0 * nl + il) * nkt + j] * inv_aH * p0;
+      a1 = a1 + w * S[((size_t)1 * nl + il) * nkt + j] * inv_aH * p1;
+      a2 = a2 + w * S[((size_t)2 * nl + il) * nkt + j] * inv_aH * p2;
+      aE = aE + w * S[((size_t)3 * nl + il) * nkt + j] * inv_aH * eps;
+    }
+    T[j] = a0 + a1 + a2;
+    E[j] = aE;
+  }
+}
+
+static double trapz(const double* y, const double* x, int n) {
+  double s = 0.;
+  for (int i = 0; i < n - 1; ++i) s += (x[i + 1] - x[i]) * (y[i] + y[i + 1]) / 2.;
+  return s;
+}
+
+int oracle_los_forward(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
+                       const double* pt, const double* kt, const abcmb_los_settings* ls, int n_save,
+                       const oracle_bessel* B, double* cl_raw, double* cl, int n_threads) {
+#ifdef _OPENMP
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+#endif
+  const int nkt = ls->nkt;
+  const int nl = n_save - 1;
+  const int n_ell_tab = ls->idx_max - ls->idx_min + 1;
+  const int n_out = ls->l_max - ls->l_min + 1;
+  double* S = (double*)malloc(sizeof(double) * 4 * (size_t)nl * nkt);
+  for (int ci = 0; ci < n_cosmo; ++ci) {
+    const abcmb_cosmo* c = &cosmo[ci];
+    oracle_sources(c, tables, kbuf, pt, kt, nkt, n_save, ls, S);
+    double lts = c->lna_transfer_start;
+    double dl = linspace_at(lts, 0., n_save, n_save - 1) - linspace_at(lts, 0., n_save, n_save - 2);
+    double* raw = cl_raw + (size_t)ci * n_ell_tab * 3;
+#pragma omp parallel
+    {
+      double* T = (double*)malloc(sizeof(double) * nkt);
+      double* E = (double*)malloc(sizeof(double) * nkt);
+      double* itg = (double*)malloc(sizeof(double) * nkt * 3);
+#pragma omp for schedule(dynamic, 1)
+      for (int ie = 0; ie < n_ell_tab; ++ie) {
+        int idx = ls->idx_min + ie;
+        los_one_ell(c, tables, S, kt, nkt, n_save, lts, dl, B, idx, T, E);
+        for (int j = 0; j < nkt; ++j) {
+          double k = kt[j];
+          double pr = 4. * PI * c->A_s * pow(k / ls->k_pivot, c->n_s - 1.);
+          itg[j] = pr * T[j] * T[j] / k;
+          itg[nkt + j] = pr * T[j] * E[j] / k;
+          itg[2 * nkt + j] = pr * E[j] * E[j] / k;
+        }
+        raw[ie * 3 + 0] = trapz(itg, kt, nkt);
+        raw[ie * 3 + 1] = trapz(itg + nkt, kt, nkt);
+        raw[ie * 3 + 2] = trapz(itg + 2 * nkt, kt, nkt);
+      }
+      free(T); free(E); free(itg);
+    }
+    /* spline over tabulated l onto integer l (spectrum.py:597-608) */
+    double* lx = (double*)malloc(sizeof(double) * n_ell_tab);
+    double* yy = (double*)malloc(sizeof(double) * n_ell_tab);
+    double* sl = (double*)malloc(sizeof(double) * n_ell_tab);
+    for (int ie = 0; ie < n_ell_tab; ++ie) lx[ie] = (double)B->l_tab[ls->idx_min + ie];
+    for (int X = 0; X < 3; ++X) {
+      for (int ie = 0; ie < n_ell_tab; ++ie) yy[ie] = raw[ie * 3 + X];
+      oracle_spline_slopes(lx, yy, n_ell_tab, sl);
+      for (int o = 0; o < n_out; ++o)
+        cl[((size_t)ci * 3 + X) * n_out + o] = oracle_spline_eval(lx, yy, sl, n_ell_tab, (double)(ls->l_min + o));
+    }
+    free(lx); free(yy); free(sl);
+  }
+  free(S);
+  return ABCMB_OK;
+}
+
+/* SpectrumSolver.Pk_lin (spectrum.py:268-302) */
+int oracle_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* kbuf, const double* pt, int n_save,
+                  double k_pivot, int n_kout, const double* kout, int n_z, const double* z, double* pk) {
+  for (int ci = 0; ci < n_cosmo; ++ci) {
+    const abcmb_cosmo* c = &cosmo[ci];
+    const int nk = c->nk;
+    const double* kp = kbuf + c->off_k;
+    const double* dm = pt + c->off_pt + (size_t)ABCMB_F_DELTA_M * n_save * nk;
+    double* lna = (double*)malloc(sizeof(double) * n_save);
+    double* colv = (double*)malloc(sizeof(double) * n_save);
+    double* dml = (double*)malloc(sizeof(double) * nk);
+    for (int i = 0; i < n_save; ++i) lna[i] = linspace_at(c->lna_transfer_start, 0., n_save, i);
+    for (int iz = 0; iz < n_z; ++iz) {
+      double l = -log(1. + z[iz]);
+      for (int ik = 0; ik < nk; ++ik) {
+        for (int i = 0; i < n_save; ++i) colv[i] = dm[(size_t)i * nk + ik];
+        dml[ik] = oracle_np_interp(l, lna, colv, n_save);
+      }
+      for (int j = 0; j < n_kout; ++j) {
+        double k = kout[j];
+        double d = oracle_np_interp(k, kp, dml, nk);
+        double prim = c->A_s * pow(k / k_pivot, c->n_s - 1.) * (2 * PI * PI / (k * k * k));
+        pk[((size_t)ci * n_z + iz) * n_kout + j] = d * d * prim;
+      }
+    }
+    free(lna); free(colv); free(dml);
+  }
+  return ABCMB_OK;
+}

@@ -1,0 +1,55 @@
+/*
+ * abcmb_oracle.h -- CPU FP64 restatement of ABCMB's hot path.
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA kernels and the timed
+ * CPU baseline.  The product library never includes or links this.
+ */
+#ifndef ABCMB_ORACLE_H
+#define ABCMB_ORACLE_H
+#include <stdint.h>
+#include "../include/abcmb_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Tabulated spherical-Bessel functions (abcmb/bessel_tab). */
+typedef struct oracle_bessel {
+  int n_l, n_x;
+  const int32_t* l_tab;
+  const double* xmin[3];
+  const double* xmax[3];
+  const double* phi[3];   /* [l][x] */
+} oracle_bessel;
+
+double oracle_fast_interp(double x, double xp_min, double xp_max, const double* fp, int n);
+double oracle_np_interp(double x, const double* xp, const double* fp, int n);
+double oracle_aH(const abcmb_cosmo* c, double lna);
+double oracle_aH_prime(const abcmb_cosmo* c, double lna);
+double oracle_tau(const abcmb_cosmo* c, const double* tables, double lna);
+double oracle_xe(const abcmb_cosmo* c, const double* tables, double lna);
+double oracle_Tm(const abcmb_cosmo* c, const double* tables, double lna);
+double oracle_tau_c(const abcmb_cosmo* c, const double* tables, double lna);
+double oracle_start_time(const abcmb_cosmo* c, const double* tables, double k, double R_tc, double R_large);
+void oracle_kvaerno5_tableau(double* A49, double* c7, double* gamma);
+void oracle_rhs(const abcmb_cosmo* c, const double* tables, double k, double lna, const double* y, double* f);
+void oracle_initial_conditions(const abcmb_cosmo* c, const double* tables, double k, double lna, double* y);
+void oracle_output_fields(const abcmb_cosmo* c, const double* tables, double k, double lna,
+                          const double* y, double* out);
+int oracle_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
+                        int n_items, const int32_t* items, const abcmb_pert_settings* s,
+                        double* pt, abcmb_kstat* kstat, int n_threads);
+void oracle_spline_slopes(const double* x, const double* y, int n, double* s);
+double oracle_spline_eval(const double* x, const double* y, const double* s, int n, double xq);
+double oracle_phi(int which, const oracle_bessel* B, int idx, double x);
+void oracle_sources(const abcmb_cosmo* c, const double* tables, const double* kbuf, const double* pt,
+                    const double* kt, int nkt, int n_save, const abcmb_los_settings* ls, double* S);
+int oracle_los_forward(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
+                       const double* pt, const double* kt, const abcmb_los_settings* ls, int n_save,
+                       const oracle_bessel* B, double* cl_raw, double* cl, int n_threads);
+int oracle_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* kbuf, const double* pt, int n_save,
+                  double k_pivot, int n_kout, const double* kout, int n_z, const double* z, double* pk);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,134 @@
+"""ctypes front-end of the CPU oracle (oracle/abcmb_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline / reference arm, never by the abcmb_b200 package.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+
+
+class COracleBessel(ctypes.Structure):
+    _fields_ = [("n_l", ctypes.c_int), ("n_x", ctypes.c_int), ("l_tab", _ip),
+                ("xmin", _dp * 3), ("xmax", _dp * 3), ("phi", _dp * 3)]
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.isfile(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        L.oracle_fast_interp.restype = ctypes.c_double
+        L.oracle_fast_interp.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_int]
+        L.oracle_np_interp.restype = ctypes.c_double
+        L.oracle_np_interp.argtypes = [ctypes.c_double, _dp, _dp, ctypes.c_int]
+        for name in ["oracle_aH", "oracle_aH_prime"]:
+            getattr(L, name).restype = ctypes.c_double
+            getattr(L, name).argtypes = [vp, ctypes.c_double]
+        for name in ["oracle_tau", "oracle_xe", "oracle_Tm", "oracle_tau_c"]:
+            getattr(L, name).restype = ctypes.c_double
+            getattr(L, name).argtypes = [vp, _dp, ctypes.c_double]
+        L.oracle_start_time.restype = ctypes.c_double
+        L.oracle_start_time.argtypes = [vp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.oracle_kvaerno5_tableau.argtypes = [_dp, _dp, _dp]
+        L.oracle_rhs.argtypes = [vp, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp]
+        L.oracle_initial_conditions.argtypes = [vp, _dp, ctypes.c_double, ctypes.c_double, _dp]
+        L.oracle_output_fields.argtypes = [vp, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp]
+        L.oracle_pert_forward.restype = ctypes.c_int
+        L.oracle_pert_forward.argtypes = [ctypes.c_int, vp, _dp, _dp, ctypes.c_int, _ip, vp, _dp, vp, ctypes.c_int]
+        L.oracle_spline_slopes.argtypes = [_dp, _dp, ctypes.c_int, _dp]
+        L.oracle_spline_eval.restype = ctypes.c_double
+        L.oracle_spline_eval.argtypes = [_dp, _dp, _dp, ctypes.c_int, ctypes.c_double]
+        L.oracle_phi.restype = ctypes.c_double
+        L.oracle_phi.argtypes = [ctypes.c_int, ctypes.POINTER(COracleBessel), ctypes.c_int, ctypes.c_double]
+        L.oracle_sources.argtypes = [vp, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, vp, _dp]
+        L.oracle_los_forward.restype = ctypes.c_int
+        L.oracle_los_forward.argtypes = [ctypes.c_int, vp, _dp, _dp, _dp, _dp, vp, ctypes.c_int,
+                                         ctypes.POINTER(COracleBessel), _dp, _dp, ctypes.c_int]
+        L.oracle_pk_lin.restype = ctypes.c_int
+        L.oracle_pk_lin.argtypes = [ctypes.c_int, vp, _dp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                    _dp, ctypes.c_int, _dp, _dp]
+        _lib = L
+    return _lib
+
+
+def dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def iptr(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_ip)
+
+
+def vptr(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def bessel_struct(bt):
+    """Keep-alive tuple (struct, arrays) for oracle_bessel."""
+    arrays = [np.ascontiguousarray(bt.l_tab, dtype=np.int32)]
+    s = COracleBessel()
+    s.n_l = bt.n_l
+    s.n_x = bt.n_x
+    s.l_tab = iptr(arrays[0])
+    for n in range(3):
+        a = np.ascontiguousarray(bt.xmin[n]); b = np.ascontiguousarray(bt.xmax[n])
+        c = np.ascontiguousarray(bt.phi[n])
+        arrays += [a, b, c]
+        s.xmin[n] = dptr(a); s.xmax[n] = dptr(b); s.phi[n] = dptr(c)
+    return s, arrays
+
+
+def pert_forward(batch, settings, n_threads: int = 0):
+    """Oracle PerturbationEvolver.full_evolution for a packed Batch."""
+    from abcmb_b200.packing import KSTAT_DTYPE
+    pt = np.zeros(batch.pt_size)
+    kstat = np.zeros(batch.n_items, dtype=KSTAT_DTYPE)
+    items = np.ascontiguousarray(batch.items, dtype=np.int32)
+    rc = lib().oracle_pert_forward(batch.n_cosmo, vptr(batch.cosmo), dptr(batch.tables), dptr(batch.kbuf),
+                                   batch.n_items, iptr(items), ctypes.byref(settings), dptr(pt), vptr(kstat),
+                                   n_threads)
+    return rc, pt, kstat
+
+
+def los_forward(batch, pt, kt, ls, bt, n_threads: int = 0):
+    n_ell_tab = ls.idx_max - ls.idx_min + 1
+    n_out = ls.l_max - ls.l_min + 1
+    cl_raw = np.zeros(batch.n_cosmo * n_ell_tab * 3)
+    cl = np.zeros(batch.n_cosmo * 3 * n_out)
+    s, keep = bessel_struct(bt)
+    kt = np.ascontiguousarray(kt, dtype=np.float64)
+    rc = lib().oracle_los_forward(batch.n_cosmo, vptr(batch.cosmo), dptr(batch.tables), dptr(batch.kbuf),
+                                  dptr(pt), dptr(kt), ctypes.byref(ls), batch.n_save, ctypes.byref(s),
+                                  dptr(cl_raw), dptr(cl), n_threads)
+    del keep
+    return rc, cl_raw.reshape(batch.n_cosmo, n_ell_tab, 3), cl.reshape(batch.n_cosmo, 3, n_out)
+
+
+def pk_lin(batch, pt, k_pivot, kout, z):
+    kout = np.ascontiguousarray(kout, dtype=np.float64)
+    z = np.ascontiguousarray(z, dtype=np.float64)
+    pk = np.zeros(batch.n_cosmo * len(z) * len(kout))
+    lib().oracle_pk_lin(batch.n_cosmo, vptr(batch.cosmo), dptr(batch.kbuf), dptr(pt), batch.n_save,
+                        float(k_pivot), len(kout), dptr(kout), len(z), dptr(z), dptr(pk))
+    return pk.reshape(batch.n_cosmo, len(z), len(kout))
