@@ -1,0 +1,102 @@
+"""Seeded synthetic workloads.
+
+The reference publishes no benchmark inputs for this path; these are the
+configurations it is measured on, built from its own defaults:
+
+  C1  flat LCDM h=0.674, omega_b=0.0224, omega_cdm=0.120, A_s=2.1e-9,
+      n_s=0.965, tau_reio=0.054, N_eff=3.044 (massless nu), no lensing;
+      200 k log-spaced 1e-4..0.5 / Mpc; hierarchies l_max=12; C_l to 1500.
+  C2  C1 + one massive nu (m=0.06 eV, N_nu_massive=1); all hierarchies at
+      l_max=30; 600 k log-spaced 1e-5..1 / Mpc; C_l to 2500.
+  C4  batch of cosmologies, parameters uniform within +-5% of C1, massive-nu
+      count drawn from {0, 1, 3} (0 = species absent), per-cosmology k grids
+      geomspace(1e-5, 1, Nk) with Nk uniform in 400..800; the reference's
+      default hierarchy cut-offs (l_max_g=12, l_max_pol_g=10,
+      l_max_massless_nu=17, l_max_massive_nu=17); C_l to 2500.
+
+Background tables come from background_tables.make_background (synthetic
+recombination standing in for HyRex).  Seed: numpy default_rng(20261203).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import background_tables as bt
+from . import bessel as bessel_mod
+from . import cosmology, packing
+from . import specs as sp
+
+SEED = 20261203
+FIDUCIAL = dict(h=0.674, omega_b=0.0224, omega_cdm=0.120, A_s=2.1e-9, n_s=0.965, tau_reion=0.054, Neff=3.044)
+GRAD_PARAMS = ("h", "omega_b", "omega_cdm", "A_s", "n_s", "tau_reion")
+
+
+@dataclass
+class Workload:
+    name: str
+    specs: dict
+    params_in: list            # input params per cosmology (before derivation)
+    has_ncdm: list
+    kgrids: list
+    l_max: int
+    bgs: list = field(default_factory=list)
+    layouts: list = field(default_factory=list)
+    batch: packing.Batch = None
+    kt: np.ndarray = None
+    idx_min: int = 0
+    idx_max: int = 0
+
+    def build(self, n_save: int = 500):
+        self.bgs = []
+        self.layouts = []
+        for p_in, ncdm in zip(self.params_in, self.has_ncdm):
+            p = cosmology.add_derived_parameters(p_in, ncdm, self.specs)
+            self.bgs.append(bt.make_background(p, ncdm))
+            self.layouts.append(sp.state_layout(self.specs, ncdm))
+        self.batch = packing.pack(self.bgs, self.layouts, self.kgrids, n_save=n_save)
+        ks = dict(self.specs)
+        sp.get_k_axis_perturbations(ks)
+        self.kt = sp.get_k_axis_transfer(ks)
+        B = bessel_mod.load()
+        self.idx_min, self.idx_max, _ = sp.ell_index_range(B.l_tab, int(self.specs["l_min"]), self.l_max, False)
+        return self
+
+    def pert_settings(self):
+        return packing.pert_settings(self.specs, self.batch.n_save, self.batch)
+
+    def los_settings(self, precision: int = 0):
+        return packing.los_settings(self.specs, self.idx_min, self.idx_max, len(self.kt), self.l_max,
+                                    precision=precision, n_save=self.batch.n_save)
+
+
+def c1(nk: int = 200, l_max: int = 1500) -> Workload:
+    specs = sp.load_specs(dict(l_max=l_max, lensing=False, l_max_g=12, l_max_pol_g=12, l_max_massless_nu=12))
+    return Workload("C1", specs, [dict(FIDUCIAL)], [False], [np.geomspace(1e-4, 0.5, nk)], l_max)
+
+
+def c2(nk: int = 600, l_max: int = 2500, lmax_h: int = 30) -> Workload:
+    specs = sp.load_specs(dict(l_max=l_max, lensing=False, l_max_g=lmax_h, l_max_pol_g=lmax_h,
+                               l_max_massless_nu=lmax_h, l_max_massive_nu=lmax_h))
+    p = dict(FIDUCIAL)
+    p.update(N_nu_massive=1, m_nu_massive=0.06)
+    return Workload("C2", specs, [p], [True], [np.geomspace(1e-5, 1.0, nk)], l_max)
+
+
+def c4(n_cosmo: int = 64, l_max: int = 2500, nk_range=(400, 800), seed: int = SEED) -> Workload:
+    rng = np.random.default_rng(seed)
+    specs = sp.load_specs(dict(l_max=l_max, lensing=False))
+    params, ncdm, kgrids = [], [], []
+    for _ in range(n_cosmo):
+        p = dict(FIDUCIAL)
+        for name in GRAD_PARAMS:
+            p[name] = FIDUCIAL[name] * rng.uniform(0.95, 1.05)
+        nnu = int(rng.choice([0, 1, 3]))
+        if nnu:
+            p.update(N_nu_massive=nnu, m_nu_massive=0.06)
+        nk = int(rng.integers(nk_range[0], nk_range[1] + 1))
+        params.append(p)
+        ncdm.append(nnu > 0)
+        kgrids.append(np.geomspace(1e-5, 1.0, nk))
+    return Workload("C4", specs, params, ncdm, kgrids, l_max)

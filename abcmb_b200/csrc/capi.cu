@@ -1,0 +1,189 @@
+// capi.cu -- the extern "C" entry points of include/abcmb_b200.h.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace abcmb {
+int64_t pert_workspace_bytes(int n_cosmo);
+cudaError_t launch_pert(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
+                        int n_items, const int32_t* items, const abcmb_pert_settings& s, double* pt,
+                        abcmb_kstat* kstat, void* ws, cudaStream_t stream, int warps_per_block, int* grid_out);
+int64_t los_workspace_bytes(int max_nk, int nkt, int n_ell_tab, int n_save, int precision);
+cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_cosmo* cosmo_host,
+                       const double* tables, const double* kbuf, const double* pt, const double* kt,
+                       const abcmb_los_settings& ls, int n_save, const BesselDev& B, double* cl_raw,
+                       double* cl, void* ws, cudaStream_t stream);
+cudaError_t launch_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* kbuf, const double* pt,
+                          int n_save, double k_pivot, int n_kout, const double* kout, int n_z, const double* z,
+                          double* pk, cudaStream_t stream);
+}  // namespace abcmb
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+  return fail(ABCMB_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+// Bessel tables, resident once per device (spectrum.py loads them once at import).
+struct BesselCache {
+  bool ready = false;
+  abcmb::BesselDev dev{};
+  void* mem = nullptr;
+};
+std::mutex g_mu;
+std::vector<BesselCache> g_bessel;
+
+BesselCache* bessel_for_current_device() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lk(g_mu);
+  if ((int)g_bessel.size() <= d) g_bessel.resize(d + 1);
+  return &g_bessel[d];
+}
+
+int g_warps_per_block = 4;
+int g_last_grid = 0;
+
+}  // namespace
+
+extern "C" {
+
+int abcmb_version(void) { return ABCMB_B200_VERSION; }
+
+const char* abcmb_last_error(void) { return g_last_error.c_str(); }
+
+int abcmb_upload_bessel(int n_l, int n_x, const int32_t* l_tab, const double* xmin0, const double* xmax0,
+                        const double* phi0, const double* xmin1, const double* xmax1, const double* phi1,
+                        const double* xmin2, const double* xmax2, const double* phi2) {
+  if (n_l <= 0 || n_x <= 1 || !l_tab || !phi0 || !phi1 || !phi2) return fail(ABCMB_ERR_ARG, "bad Bessel table");
+  BesselCache* bc = bessel_for_current_device();
+  if (!bc) return fail(ABCMB_ERR_CUDA, "cudaGetDevice failed");
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (bc->mem) {
+    cudaFree(bc->mem);
+    bc->mem = nullptr;
+    bc->ready = false;
+  }
+  const size_t nl = (size_t)n_l, nx = (size_t)n_x;
+  const size_t bytes = 256 + nl * 4 + 6 * nl * 8 + 3 * nl * nx * 8 + 256;
+  void* mem = nullptr;
+  cudaError_t e = cudaMalloc(&mem, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "abcmb_upload_bessel cudaMalloc");
+  char* p = static_cast<char*>(mem);
+  int32_t* dl = reinterpret_cast<int32_t*>(p);
+  p += (nl * 4 + 255) / 256 * 256;
+  double* dxmin = reinterpret_cast<double*>(p);
+  p += 3 * nl * 8;
+  double* dxmax = reinterpret_cast<double*>(p);
+  p += 3 * nl * 8;
+  double* dphi = reinterpret_cast<double*>(p);
+  const double* xmins[3] = {xmin0, xmin1, xmin2};
+  const double* xmaxs[3] = {xmax0, xmax1, xmax2};
+  const double* phis[3] = {phi0, phi1, phi2};
+  e = cudaMemcpy(dl, l_tab, nl * 4, cudaMemcpyHostToDevice);
+  for (int n = 0; n < 3 && e == cudaSuccess; ++n) {
+    e = cudaMemcpy(dxmin + n * nl, xmins[n], nl * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dxmax + n * nl, xmaxs[n], nl * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dphi + n * nl * nx, phis[n], nl * nx * 8, cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    cudaFree(mem);
+    return cuda_fail(e, "abcmb_upload_bessel cudaMemcpy");
+  }
+  bc->mem = mem;
+  bc->dev = abcmb::BesselDev{n_l, n_x, dl, dxmin, dxmax, dphi};
+  bc->ready = true;
+  return ABCMB_OK;
+}
+
+int64_t abcmb_pert_workspace_size(int n_cosmo, int n_items) {
+  (void)n_items;
+  return abcmb::pert_workspace_bytes(n_cosmo);
+}
+
+int abcmb_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* tables_dev, const double* k_dev,
+                       int n_items, const int32_t* items_dev, const abcmb_pert_settings* settings, double* pt_dev,
+                       abcmb_kstat* kstat_dev, void* workspace_dev, int64_t workspace_bytes, void* stream) {
+  if (n_cosmo <= 0 || n_items < 0 || !cosmo_dev || !tables_dev || !k_dev || !settings || !pt_dev || !kstat_dev)
+    return fail(ABCMB_ERR_ARG, "abcmb_pert_forward: null argument");
+  if (settings->max_ny <= 0 || settings->n_save < 2 || settings->max_steps <= 0)
+    return fail(ABCMB_ERR_ARG, "abcmb_pert_forward: settings.max_ny / n_save / max_steps");
+  if (workspace_bytes < abcmb::pert_workspace_bytes(n_cosmo) || !workspace_dev)
+    return fail(ABCMB_ERR_WORKSPACE, "abcmb_pert_forward: workspace too small");
+  if (n_items == 0) return ABCMB_OK;
+  cudaError_t e = abcmb::launch_pert(n_cosmo, cosmo_dev, tables_dev, k_dev, n_items, items_dev, *settings, pt_dev,
+                                     kstat_dev, workspace_dev, static_cast<cudaStream_t>(stream), g_warps_per_block,
+                                     &g_last_grid);
+  if (e != cudaSuccess) return cuda_fail(e, "abcmb_pert_forward");
+  return ABCMB_OK;
+}
+
+int64_t abcmb_los_workspace_size(int n_cosmo, int max_nk, int nkt, int n_ell_tab, int n_save, int precision) {
+  (void)n_cosmo;
+  return abcmb::los_workspace_bytes(max_nk, nkt, n_ell_tab, n_save, precision);
+}
+
+int abcmb_los_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* tables_dev, const double* k_dev,
+                      const double* pt_dev, const double* kt_dev, const abcmb_los_settings* settings,
+                      double* cl_raw_dev, double* cl_dev, void* workspace_dev, int64_t workspace_bytes,
+                      void* stream) {
+  if (n_cosmo <= 0 || !cosmo_dev || !tables_dev || !k_dev || !pt_dev || !kt_dev || !settings || !cl_raw_dev ||
+      !cl_dev)
+    return fail(ABCMB_ERR_ARG, "abcmb_los_forward: null argument");
+  const abcmb_los_settings& ls = *settings;
+  if (ls.l_min != 2) return fail(ABCMB_ERR_ARG, "abcmb_los_forward: get_Cl indexes [ells-2], l_min must be 2");
+  if (ls.idx_max - ls.idx_min + 1 < 4 || ls.nkt < 2) return fail(ABCMB_ERR_ARG, "abcmb_los_forward: sizes");
+  BesselCache* bc = bessel_for_current_device();
+  if (!bc || !bc->ready) return fail(ABCMB_ERR_TABLES, "abcmb_los_forward: Bessel tables not uploaded");
+  if (ls.idx_min < 0 || ls.idx_max >= bc->dev.n_l) return fail(ABCMB_ERR_ARG, "abcmb_los_forward: l index range");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // the launcher needs the per-cosmology sizes on the host
+  std::vector<abcmb_cosmo> host(n_cosmo);
+  cudaError_t e = cudaMemcpyAsync(host.data(), cosmo_dev, sizeof(abcmb_cosmo) * n_cosmo, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "abcmb_los_forward descriptor read");
+  int max_nk = 0;
+  for (const auto& c : host) max_nk = c.nk > max_nk ? c.nk : max_nk;
+  const int n_save = ls.n_save;
+  if (n_save < 3) return fail(ABCMB_ERR_ARG, "abcmb_los_forward: n_save");
+  int64_t need = abcmb::los_workspace_bytes(max_nk, ls.nkt, ls.idx_max - ls.idx_min + 1, n_save, ls.precision);
+  if (!workspace_dev || workspace_bytes < need) return fail(ABCMB_ERR_WORKSPACE, "abcmb_los_forward: workspace");
+  e = abcmb::launch_los(n_cosmo, cosmo_dev, host.data(), tables_dev, k_dev, pt_dev, kt_dev, ls, n_save, bc->dev,
+                        cl_raw_dev, cl_dev, workspace_dev, st);
+  if (e != cudaSuccess) return cuda_fail(e, "abcmb_los_forward");
+  return ABCMB_OK;
+}
+
+int abcmb_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* k_dev, const double* pt_dev, int n_save,
+                 double k_pivot, int n_kout, const double* kout_dev, int n_z, const double* z_dev, double* pk_dev,
+                 void* stream) {
+  if (n_cosmo <= 0 || n_kout <= 0 || n_z <= 0 || !cosmo_dev || !k_dev || !pt_dev || !kout_dev || !z_dev || !pk_dev)
+    return fail(ABCMB_ERR_ARG, "abcmb_pk_lin: bad argument");
+  cudaError_t e = abcmb::launch_pk_lin(n_cosmo, cosmo_dev, k_dev, pt_dev, n_save, k_pivot, n_kout, kout_dev, n_z,
+                                       z_dev, pk_dev, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "abcmb_pk_lin");
+  return ABCMB_OK;
+}
+
+/* Tuning knob: warps per block of the perturbation kernel (1..8). */
+int abcmb_set_pert_warps_per_block(int w) {
+  if (w < 1 || w > 8) return fail(ABCMB_ERR_ARG, "warps per block must be 1..8");
+  g_warps_per_block = w;
+  return ABCMB_OK;
+}
+
+/* Grid size of the last perturbation launch (diagnostics). */
+int abcmb_last_pert_grid(void) { return g_last_grid; }
+
+}  // extern "C"

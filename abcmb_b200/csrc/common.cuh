@@ -1,0 +1,193 @@
+// common.cuh -- device-side background cosmology shared by the kernels.
+//
+// Every function here restates one evaluator of the reference in FP64:
+//   fast_interp                 abcmb/ABCMBTools.py:268-308
+//   species rho / P             abcmb/species.py:454-1346
+//   aH, aH_prime                abcmb/background.py:147-208
+//   tau, nH, TCMB               abcmb/background.py:321-387
+//   xe, Tm, tau_c               abcmb/background.py:568-680
+//   Gamma_compton               abcmb/hyrex/recomb_functions.py:127-153
+//   Baryon.cs2, mean_mass       abcmb/species.py:1163-1220
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "../../include/abcmb_b200.h"
+
+namespace abcmb {
+
+// constants.py
+constexpr double C_CM = 29979245800.0;
+constexpr double C_MPC = 9.71561e-15;
+constexpr double H0H = 3.24078e-18;
+constexpr double HBAR = 6.582119569509e-16;
+constexpr double GN = 1.18980205e-40;
+constexpr double MP = 938271999.0;
+constexpr double ME = 510998.9461;
+constexpr double MH = MP + ME + 13.5982860719383;
+constexpr double MHE = 3.72839e9;
+constexpr double SIGT = 6.652458734e-25;
+constexpr double PI = 3.14159265358979323846;
+constexpr double STEF_BOLT = PI * PI / (60. * HBAR * HBAR * HBAR * C_CM * C_CM);
+constexpr double RHO_CRIT_UNIT = 3. * H0H * H0H / 8. / PI / GN;
+constexpr double CHB3 = (C_CM * HBAR) * (C_CM * HBAR) * (C_CM * HBAR);
+constexpr double HB3C3 = (HBAR * HBAR * HBAR) * (C_CM * C_CM * C_CM);
+
+// MassiveNeutrino quadratures (species.py:791-794)
+static __constant__ double Q3[3] = {0.913201, 3.37517, 7.79184};
+static __constant__ double W3[3] = {0.0687359, 3.31435, 2.29911};
+static __constant__ double Q5[5] = {0.583165, 2.0, 4.0, 7.26582, 13.0};
+static __constant__ double W5[5] = {0.0081201, 0.689407, 2.8063, 2.05156, 0.12681};
+
+__device__ __forceinline__ double fast_interp(double x, double xp_min, double xp_max,
+                                              const double* __restrict__ fp, int n) {
+  const double eps = 1.e-6;
+  double i = (x - xp_min) / (xp_max - xp_min) * (double)(n - 1);
+  i = fmin(fmax(i, eps), (double)(n - 1) - eps);
+  int il = (int)floor(i);
+  int iu = min(il + 1, n - 1);
+  double wu = i - (double)il;
+  double wl = 1.0 - wu;
+  return wl * __ldg(fp + il) + wu * __ldg(fp + iu);
+}
+
+// fast_interp on a table held in shared memory (no read-only-cache loads).
+__device__ __forceinline__ double fast_interp_smem(double x, double xp_min, double xp_max, const double* fp, int n) {
+  const double eps = 1.e-6;
+  double i = (x - xp_min) / (xp_max - xp_min) * (double)(n - 1);
+  i = fmin(fmax(i, eps), (double)(n - 1) - eps);
+  int il = (int)floor(i);
+  int iu = min(il + 1, n - 1);
+  double wu = i - (double)il;
+  double wl = 1.0 - wu;
+  return wl * fp[il] + wu * fp[iu];
+}
+
+// jnp.linspace(a, b, n)[i]
+__device__ __forceinline__ double linspace_at(double a, double b, int n, int i) {
+  return (i == n - 1) ? b : a + (double)i * ((b - a) / (double)(n - 1));
+}
+
+struct Rho {
+  double tot, P, cdm, b, g, nu, ncdm, Pncdm;
+};
+
+__device__ __forceinline__ void rho_ncdm(const abcmb_cosmo& c, double a, double& rho, double& P) {
+  double T = c.T_nu_massive * c.TCMB0 / a;
+  double x = c.m_nu_massive / T;
+  double ir = 0., ip = 0.;
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    double q = Q5[j];
+    double e = sqrt(q * q + x * x);
+    ir += (1. + exp(-q)) / (q * q) * e * W5[j];
+    ip += (1. + exp(-q)) / e * W5[j];
+  }
+  double T4 = T * T * T * T;
+  rho = c.N_nu_massive * 4. * T4 / (PI * PI) * ir / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
+  P = c.N_nu_massive * 4. / 3. * T4 / (PI * PI) * ip / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
+}
+
+__device__ __forceinline__ Rho rho_all(const abcmb_cosmo& c, double a) {
+  Rho r;
+  double a3 = a * a * a, a4 = a3 * a;
+  double rde = c.omega_Lambda * RHO_CRIT_UNIT;
+  r.cdm = c.omega_cdm * RHO_CRIT_UNIT / a3;
+  r.b = c.omega_b * RHO_CRIT_UNIT / a3;
+  double T04 = c.TCMB0 * c.TCMB0 * c.TCMB0 * c.TCMB0;
+  r.g = PI * PI / 15. * T04 / a4 / CHB3;
+  double tn = c.T_nu_massless;
+  r.nu = c.N_nu_massless * 2. * 7. / 8. * PI * PI / 30. * (tn * tn * tn * tn) * T04 / a4 / CHB3;
+  r.ncdm = 0.;
+  r.Pncdm = 0.;
+  if (c.has_ncdm) rho_ncdm(c, a, r.ncdm, r.Pncdm);
+  r.tot = rde + r.cdm + r.b + r.g + r.nu + r.ncdm;
+  r.P = -rde + r.g / 3. + r.nu / 3. + r.Pncdm;
+  return r;
+}
+
+__device__ __forceinline__ double aH_of(const abcmb_cosmo& c, double lna) {
+  double a = exp(lna);
+  Rho r = rho_all(c, a);
+  return a * sqrt(8. * PI * GN * r.tot / 3.) / C_MPC;
+}
+
+__device__ __forceinline__ double tau_of(const abcmb_cosmo& c, const double* __restrict__ tables, double lna) {
+  return fast_interp(lna, ABCMB_LNA_TAU_MIN, ABCMB_LNA_TAU_MAX, tables + c.off_tau, ABCMB_NTAU_TAB);
+}
+
+__device__ __forceinline__ double xe_of(const abcmb_cosmo& c, const double* __restrict__ tables, double lna) {
+  if (lna < c.lna_xe0) return c.xe_first;
+  if (lna >= c.lna_xe_last) return c.xe_last;
+  return fast_interp(lna, c.lna_xe0, c.lna_xe_max, tables + c.off_xe, c.n_xe);
+}
+
+__device__ __forceinline__ double nH_of(const abcmb_cosmo& c, double a) {
+  return (1. - c.YHe) * 3. * c.omega_b * H0H * H0H / 8. / PI / GN / MH / (a * a * a);
+}
+
+__device__ __forceinline__ double gamma_compton(double xe, double TCMB, double YHe) {
+  double FHe = YHe * MH / MHE / (1. - YHe);
+  return xe / (1. + FHe + xe) * 8. * SIGT * (4. * STEF_BOLT) * (TCMB * TCMB * TCMB * TCMB) / (3. * ME);
+}
+
+// Device copy of the Bessel tables (abcmb/bessel_tab).
+struct BesselDev {
+  int n_l, n_x;
+  const int32_t* l_tab;
+  const double* xmin;   // [3][n_l]
+  const double* xmax;   // [3][n_l]
+  const double* phi;    // [3][n_l][n_x]
+};
+
+// Every background scalar the perturbation equations use at one lna.
+struct BG {
+  double a, aH, tau, tau_c, cs2, R;
+  double rho_cdm, rho_b, rho_g, rho_nu, rho_ncdm, P_ncdm;
+  double ncdm_fac;   // N * 4/pi^2 * T^4 / hbar^3 / c^3
+  double eps[3];     // sqrt(q^2 + (m/T)^2) for the 3 perturbation q-bins
+};
+
+__device__ __forceinline__ void bg_eval(const abcmb_cosmo& c, const double* __restrict__ tables, double lna,
+                                        BG& b) {
+  double a = exp(lna);
+  b.a = a;
+  Rho r = rho_all(c, a);
+  b.rho_cdm = r.cdm;
+  b.rho_b = r.b;
+  b.rho_g = r.g;
+  b.rho_nu = r.nu;
+  b.rho_ncdm = r.ncdm;
+  b.P_ncdm = r.Pncdm;
+  double H = sqrt(8. * PI * GN * r.tot / 3.);
+  b.aH = a * H / C_MPC;
+  b.tau = tau_of(c, tables, lna);
+  double xe = xe_of(c, tables, lna);
+  double ne = nH_of(c, a) * xe;
+  b.tau_c = 1. / a / ne / SIGT / C_CM * C_MPC;
+  double TCMB = c.TCMB0 / a;
+  double Tm;
+  if (lna < c.lna_tm0) {
+    Tm = TCMB * (1. - H / gamma_compton(xe, TCMB, c.YHe));
+  } else if (lna >= c.lna_tm_last) {
+    Tm = c.tm_last;
+  } else {
+    Tm = fast_interp(lna, c.lna_tm0, c.lna_tm_max, tables + c.off_tm, c.n_tm);
+  }
+  double denom = (1. + xe) * (1. - c.YHe) + MH / MHE * c.YHe;
+  double mu = MH / denom;
+  b.R = 4. * r.g / 3. / r.b;
+  b.cs2 = Tm / mu * (5. / 3. - 2. / 3. * mu * b.R / ME / b.aH / b.tau_c * (TCMB / Tm - 1.));
+  if (c.has_ncdm) {
+    double T = c.T_nu_massive * c.TCMB0 / a;
+    double x = c.m_nu_massive / T;
+    double T4 = T * T * T * T;
+    b.ncdm_fac = c.N_nu_massive * 4. / (PI * PI) * T4 / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) b.eps[i] = sqrt(Q3[i] * Q3[i] + x * x);
+  } else {
+    b.ncdm_fac = 0.;
+    b.eps[0] = b.eps[1] = b.eps[2] = 1.;
+  }
+}
+
+}  // namespace abcmb

@@ -1,0 +1,485 @@
+// los.cu -- line-of-sight C_l projection (SpectrumSolver.get_Cl).
+//
+// Per cosmology, five launches:
+//   spline_prep   not-a-knot cubic-spline factorisation in log10 k of the
+//                 perturbation k grid (interpax CubicSpline, spectrum.py:664)
+//                 and the interval of every transfer k;
+//   spline_slopes the spline slopes of the 10 source fields on every lna row;
+//   sources       the splined fields at the transfer k and the T0/T1/T2/E
+//                 sources (spectrum.py:681-696);
+//   los           one CTA per (tabulated l, k tile): the l column of the
+//                 phi0/phi1/phi2 Bessel tables is staged in shared memory and
+//                 every thread accumulates the four lna integrals of one
+//                 transfer k (spectrum.py:755-786), then the block reduces its
+//                 share of the k trapezoid (spectrum.py:789-796);
+//   cl_final      fixed-order sum of the tile partials and the cubic spline
+//                 over tabulated l onto the integer ells (spectrum.py:597-608).
+#include "common.cuh"
+
+namespace abcmb {
+
+constexpr int NSRC_FIELDS = 10;
+__constant__ int SRC_FIELDS[NSRC_FIELDS] = {ABCMB_F_G_DELTA, ABCMB_F_B_THETA, ABCMB_F_THETA_B_PRIME,
+                                            ABCMB_F_G_SIGMA, ABCMB_F_G_G0, ABCMB_F_G_G2, ABCMB_F_ETA,
+                                            ABCMB_F_ETA_PRIME, ABCMB_F_ALPHA, ABCMB_F_ALPHA_PRIME};
+
+
+// Thomas factors of the not-a-knot system for x[0..n): di (modified
+// diagonal inverse), up, lo multipliers; plus x itself.
+struct SplineFac {
+  double* x;      // n
+  double* dinv;   // n  1 / modified diagonal
+  double* mlo;    // n  elimination multipliers
+  double* up;     // n  super-diagonal
+};
+
+// Not-a-knot right-hand side row i (scipy CubicSpline / interpax).
+__device__ __forceinline__ double nak_rhs(const double* x, const double* y, int n, int i) {
+  if (i == 0) {
+    double dx0 = x[1] - x[0], dx1 = x[2] - x[1];
+    double s0 = (y[1] - y[0]) / dx0, s1 = (y[2] - y[1]) / dx1;
+    double d = x[2] - x[0];
+    return ((dx0 + 2. * d) * dx1 * s0 + dx0 * dx0 * s1) / d;
+  }
+  if (i == n - 1) {
+    double dxa = x[n - 2] - x[n - 3], dxb = x[n - 1] - x[n - 2];
+    double sa = (y[n - 2] - y[n - 3]) / dxa, sb = (y[n - 1] - y[n - 2]) / dxb;
+    double d = x[n - 1] - x[n - 3];
+    return (dxb * dxb * sa + (2. * d + dxb) * dxa * sb) / d;
+  }
+  double dxm = x[i] - x[i - 1], dxp = x[i + 1] - x[i];
+  double sm = (y[i] - y[i - 1]) / dxm, sp = (y[i + 1] - y[i]) / dxp;
+  return 3. * (dxp * sm + dxm * sp);
+}
+
+// Factorise the not-a-knot tridiagonal matrix (one thread; n sequential steps).
+__device__ void nak_factor(const double* x, int n, double* dinv, double* mlo, double* up) {
+  double di_prev = 0., up_prev = 0.;
+  for (int i = 0; i < n; ++i) {
+    double lo, di, u;
+    if (i == 0) { di = x[2] - x[1]; u = x[2] - x[0]; lo = 0.; }
+    else if (i == n - 1) { lo = x[n - 1] - x[n - 3]; di = x[n - 2] - x[n - 3]; u = 0.; }
+    else { lo = x[i + 1] - x[i]; di = 2. * ((x[i] - x[i - 1]) + (x[i + 1] - x[i])); u = x[i] - x[i - 1]; }
+    double m = 0.;
+    if (i > 0) { m = lo * di_prev; di -= m * up_prev; }
+    mlo[i] = m;
+    up[i] = u;
+    dinv[i] = 1. / di;
+    di_prev = dinv[i];
+    up_prev = u;
+  }
+}
+
+// Slopes s of the not-a-knot spline through (x, y) using the factorisation.
+__device__ void nak_solve(const double* x, const double* y, int n, const double* dinv, const double* mlo,
+                          const double* up, double* s) {
+  double bprev = 0.;
+  for (int i = 0; i < n; ++i) {
+    double bi = nak_rhs(x, y, n, i) - mlo[i] * bprev;
+    s[i] = bi;
+    bprev = bi;
+  }
+  double snext = s[n - 1] * dinv[n - 1];
+  s[n - 1] = snext;
+  for (int i = n - 2; i >= 0; --i) {
+    snext = (s[i] - up[i] * snext) * dinv[i];
+    s[i] = snext;
+  }
+}
+
+__device__ __forceinline__ double spline_piece(double y0, double y1, double s0, double s1, double dx, double u) {
+  double sl = (y1 - y0) / dx;
+  double t = (s0 + s1 - 2. * sl) / dx;
+  double c3 = t / dx;
+  double c2 = (sl - s0) / dx - t;
+  return ((c3 * u + c2) * u + s0) * u + y0;
+}
+
+// i = clip(searchsorted(x, xq, 'right'), 1, n-1) - 1
+__device__ __forceinline__ int spline_interval(const double* x, int n, double xq) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (x[mid] <= xq) lo = mid + 1; else hi = mid;
+  }
+  return min(max(lo, 1), n - 1) - 1;
+}
+
+__global__ void spline_prep_kernel(const double* __restrict__ kp, int nk, const double* __restrict__ kt, int nkt,
+                                   double* xk, double* dinv, double* mlo, double* up, int* kidx) {
+  // xk = log10(PT.k); one block: threads fill x, thread 0 factorises, all map kt
+  for (int i = threadIdx.x; i < nk; i += blockDim.x) xk[i] = log10(kp[i]);
+  __syncthreads();
+  if (threadIdx.x == 0) nak_factor(xk, nk, dinv, mlo, up);
+  for (int j = threadIdx.x; j < nkt; j += blockDim.x) kidx[j] = spline_interval(xk, nk, log10(kt[j]));
+}
+
+__global__ void spline_slopes_kernel(const double* __restrict__ ptc, int n_save, int nk, int nl,
+                                     const double* __restrict__ xk, const double* __restrict__ dinv,
+                                     const double* __restrict__ mlo, const double* __restrict__ up,
+                                     double* __restrict__ slopes) {
+  int col = blockIdx.x * blockDim.x + threadIdx.x;    // f * nl + il
+  if (col >= NSRC_FIELDS * nl) return;
+  int f = col / nl, il = col % nl;
+  const double* y = ptc + ((int64_t)SRC_FIELDS[f] * n_save + il) * nk;
+  nak_solve(xk, y, nk, dinv, mlo, up, slopes + (int64_t)col * nk);
+}
+
+template <typename SrcT>
+__global__ void sources_kernel(const abcmb_cosmo* __restrict__ cosmo, int ci, const double* __restrict__ tables,
+                               const double* __restrict__ ptc, int n_save, int nk, int nl,
+                               const double* __restrict__ xk, const double* __restrict__ slopes,
+                               const int* __restrict__ kidx, const double* __restrict__ kt, int nkt,
+                               abcmb_los_settings ls, SrcT* __restrict__ S) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int il = blockIdx.y;
+  if (j >= nkt) return;
+  const abcmb_cosmo& c = cosmo[ci];
+  const double* los = tables + c.off_los;
+  const double k = kt[j];
+  const int i = kidx[j];
+  const double dx = xk[i + 1] - xk[i];
+  const double u = log10(k) - xk[i];
+  double v[NSRC_FIELDS];
+#pragma unroll
+  for (int f = 0; f < NSRC_FIELDS; ++f) {
+    const double* y = ptc + ((int64_t)SRC_FIELDS[f] * n_save + il) * nk;
+    const double* s = slopes + ((int64_t)f * nl + il) * nk;
+    v[f] = spline_piece(y[i], y[i + 1], s[i], s[i + 1], dx, u);
+  }
+  const double dg = v[0], thb = v[1], thbp = v[2], sg = v[3], G0 = v[4], G2 = v[5];
+  const double eta = v[6], etap = v[7], al = v[8], alp = v[9];
+  const double g = los[1 * nl + il], gp = los[2 * nl + il], aH = los[3 * nl + il];
+  const double em = los[4 * nl + il], aHd = los[5 * nl + il];
+  double sT0 = ls.scale_sw * g * (dg / 4. + aH * alp) +
+               ls.scale_isw * (g * (eta - aH * alp - 2. * aH * al) + 2. * em * (aH * etap - aHd * al - aH * aH * alp)) +
+               ls.scale_dop * (aH * (g * ((thbp / (k * k)) + alp) + gp * ((thb / (k * k)) + al)));
+  double sT1 = ls.scale_isw * em * ((aH * alp + 2. * aH * al - eta) * k);
+  double sT2 = ls.scale_pol * g * (2 * sg + G0 + G2) / 8.;
+  double sE = sqrt(6.) * g * (2 * sg + G0 + G2) / 8.;
+  const int64_t plane = (int64_t)nl * nkt;
+  const int64_t o = (int64_t)il * nkt + j;
+  S[o] = (SrcT)sT0;
+  S[plane + o] = (SrcT)sT1;
+  S[2 * plane + o] = (SrcT)sT2;
+  S[3 * plane + o] = (SrcT)sE;
+}
+
+// large-x asymptotic spherical Bessel j_l (spectrum.py:48-51)
+__device__ __forceinline__ double jasym(double l, double x) {
+  double nu = l + 0.5;
+  double r = sqrt(x * x - nu * nu);
+  double Q = r - nu * PI / 2 + nu * asin(nu / x);
+  double J = sqrt(2 / PI / r) * cos(Q - PI / 4);
+  return sqrt(PI / 2 / x) * J;
+}
+
+constexpr int LOS_THREADS = 256;
+
+// Kahan-compensated accumulator for the FP32 path.
+struct KahanF {
+  float s, c;
+  __device__ void add(float v) {
+    float y = v - c;
+    float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+};
+
+template <int PREC>
+__global__ void __launch_bounds__(LOS_THREADS) los_kernel(const abcmb_cosmo* __restrict__ cosmo, int ci,
+                                                          const double* __restrict__ tables, int nl,
+                                                          double delta_lna, const void* __restrict__ Sv,
+                                                          const double* __restrict__ kt, int nkt,
+                                                          BesselDev B, int idx_min, double A_s, double n_s,
+                                                          double k_pivot, double* __restrict__ partial) {
+  extern __shared__ double sm[];
+  const int ie = blockIdx.x;
+  const int idx = idx_min + ie;
+  const int tile = blockIdx.y;
+  const int ntile = gridDim.y;
+  const int nx = B.n_x;
+  double* ph0 = sm;
+  double* ph1 = sm + nx;
+  double* ph2 = sm + 2 * nx;
+  double* stau = sm + 3 * nx;
+  double* sinv = stau + nl;
+  const abcmb_cosmo& c = cosmo[ci];
+  const double* los = tables + c.off_los;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+    ph0[i] = B.phi[((int64_t)0 * B.n_l + idx) * nx + i];
+    ph1[i] = B.phi[((int64_t)1 * B.n_l + idx) * nx + i];
+    ph2[i] = B.phi[((int64_t)2 * B.n_l + idx) * nx + i];
+  }
+  for (int i = threadIdx.x; i < nl; i += blockDim.x) {
+    stau[i] = los[i];
+    sinv[i] = 1.0 / los[3 * nl + i];
+  }
+  __syncthreads();
+  const double l = (double)B.l_tab[idx];
+  const double x0min = B.xmin[idx], x0max = B.xmax[idx];
+  const double x1min = B.xmin[B.n_l + idx], x1max = B.xmax[B.n_l + idx];
+  const double x2min = B.xmin[2 * B.n_l + idx], x2max = B.xmax[2 * B.n_l + idx];
+  const double ef = sqrt(3. / 8. * (l + 2) * (l + 1) * l * (l - 1));
+  const double tau0 = c.tau0;
+  const int j = tile * blockDim.x + threadIdx.x;
+  double contrib[3] = {0., 0., 0.};
+  if (j < nkt) {
+    const double k = kt[j];
+    const int64_t plane = (int64_t)nl * nkt;
+    double a0 = 0., a1 = 0., a2 = 0., aE = 0.;
+    KahanF f0{0.f, 0.f}, f1{0.f, 0.f}, f2{0.f, 0.f}, fE{0.f, 0.f};
+    for (int il = 0; il < nl; ++il) {
+      const double w = (il == 0) ? 0.5 * delta_lna : delta_lna;
+      const double chi = (tau0 - stau[il]) * k;
+      // phi0/phi1/phi2 (spectrum.py:719-753): 0 below the table, table
+      // lerp inside, asymptotic j_l above; only the taken branch is evaluated
+      double p0;
+      if (chi < x0min) p0 = 0.;
+      else if (chi >= x0max) p0 = jasym(l, chi);
+      else p0 = fast_interp_smem(chi, x0min, x0max, ph0, nx);
+      const bool as1 = chi >= x1max, as2 = chi >= x2max;
+      double jl = 0., jl1 = 0.;
+      if (as1 || as2) {
+        jl = (chi >= x0max) ? p0 : jasym(l, chi);
+        jl1 = jasym(l + 1, chi);
+      }
+      double p1, p2;
+      if (chi < x1min) p1 = 0.;
+      else if (as1) p1 = l / chi * jl - jl1;
+      else p1 = fast_interp_smem(chi, x1min, x1max, ph1, nx);
+      if (chi < x2min) p2 = 0.;
+      else if (as2) p2 = ((3 * l * (l - 1) - 2 * chi * chi) * jl + 6 * chi * jl1) / 2 / (chi * chi);
+      else p2 = fast_interp_smem(chi, x2min, x2max, ph2, nx);
+      const double eps = p0 / (chi * chi) * ef;
+      const double wi = w * sinv[il];
+      const int64_t o = (int64_t)il * nkt + j;
+      if (PREC == 0) {
+        const double* S = static_cast<const double*>(Sv);
+        a0 = a0 + w * S[o] * sinv[il] * p0;
+        a1 = a1 + w * S[plane + o] * sinv[il] * p1;
+        a2 = a2 + w * S[2 * plane + o] * sinv[il] * p2;
+        aE = aE + w * S[3 * plane + o] * sinv[il] * eps;
+      } else {
+        const float* S = static_cast<const float*>(Sv);
+        f0.add((float)wi * S[o] * (float)p0);
+        f1.add((float)wi * S[plane + o] * (float)p1);
+        f2.add((float)wi * S[2 * plane + o] * (float)p2);
+        fE.add((float)wi * S[3 * plane + o] * (float)eps);
+      }
+    }
+    if (PREC != 0) {
+      a0 = (double)f0.s - (double)f0.c;
+      a1 = (double)f1.s - (double)f1.c;
+      a2 = (double)f2.s - (double)f2.c;
+      aE = (double)fE.s - (double)fE.c;
+    }
+    const double T = a0 + a1 + a2;
+    const double E = aE;
+    const double pr = 4. * PI * A_s * pow(k / k_pivot, n_s - 1.) / k;
+    // trapezoid weight of node j
+    double wj;
+    if (nkt == 1) wj = 0.;
+    else if (j == 0) wj = 0.5 * (kt[1] - kt[0]);
+    else if (j == nkt - 1) wj = 0.5 * (kt[nkt - 1] - kt[nkt - 2]);
+    else wj = 0.5 * (kt[j + 1] - kt[j - 1]);
+    contrib[0] = wj * pr * T * T;
+    contrib[1] = wj * pr * T * E;
+    contrib[2] = wj * pr * E * E;
+  }
+  // block reduction (fixed order: deterministic)
+  __shared__ double red[3][LOS_THREADS / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int X = 0; X < 3; ++X) {
+    double v = contrib[X];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) red[X][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double s = 0.;
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) s += red[threadIdx.x][w];
+    partial[((int64_t)ie * ntile + tile) * 3 + threadIdx.x] = s;
+  }
+}
+
+__global__ void cl_final_kernel(const double* __restrict__ partial, int n_ell_tab, int ntile, BesselDev B,
+                                int idx_min, int l_min, int n_out, double* __restrict__ cl_raw,
+                                double* __restrict__ cl, double* __restrict__ scratch) {
+  // scratch: x[n], y[3][n], s[3][n], dinv, mlo, up  (n = n_ell_tab)
+  const int n = n_ell_tab;
+  double* x = scratch;
+  double* y = x + n;
+  double* s = y + 3 * n;
+  double* dinv = s + 3 * n;
+  double* mlo = dinv + n;
+  double* up = mlo + n;
+  for (int i = threadIdx.x; i < n * 3; i += blockDim.x) {
+    int ie = i / 3, X = i % 3;
+    double acc = 0.;
+    for (int t = 0; t < ntile; ++t) acc += partial[((int64_t)ie * ntile + t) * 3 + X];
+    cl_raw[i] = acc;
+    y[X * n + ie] = acc;
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = (double)B.l_tab[idx_min + i];
+  __syncthreads();
+  if (threadIdx.x == 0) nak_factor(x, n, dinv, mlo, up);
+  __syncthreads();
+  if (threadIdx.x < 3) nak_solve(x, y + threadIdx.x * n, n, dinv, mlo, up, s + threadIdx.x * n);
+  __syncthreads();
+  for (int i = threadIdx.x; i < 3 * n_out; i += blockDim.x) {
+    int X = i / n_out, o = i % n_out;
+    double xq = (double)(l_min + o);
+    int iv = spline_interval(x, n, xq);
+    double v = spline_piece(y[X * n + iv], y[X * n + iv + 1], s[X * n + iv], s[X * n + iv + 1],
+                            x[iv + 1] - x[iv], xq - x[iv]);
+    cl[(int64_t)X * n_out + o] = v;
+  }
+}
+
+// jnp.interp(x, xp, fp) for increasing xp
+__device__ double np_interp(double x, const double* xp, const double* fp, int n, int stride) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (xp[mid] <= x) lo = mid + 1; else hi = mid;
+  }
+  int i = min(max(lo, 1), n - 1);
+  double df = fp[(int64_t)i * stride] - fp[(int64_t)(i - 1) * stride];
+  double dx = xp[i] - xp[i - 1];
+  double delta = x - xp[i - 1];
+  double f = (fabs(dx) <= 2.220446049250313e-16) ? fp[(int64_t)(i - 1) * stride]
+                                                  : fp[(int64_t)(i - 1) * stride] + (delta / dx) * df;
+  if (x < xp[0]) f = fp[0];
+  if (x > xp[n - 1]) f = fp[(int64_t)(n - 1) * stride];
+  return f;
+}
+
+__global__ void pk_lin_kernel(const abcmb_cosmo* __restrict__ cosmo, const double* __restrict__ kbuf,
+                              const double* __restrict__ pt, int n_save, double k_pivot, int n_kout,
+                              const double* __restrict__ kout, int n_z, const double* __restrict__ z,
+                              double* __restrict__ pk, double* __restrict__ lna_scratch) {
+  // one block per (cosmology, z); lna grid in shared memory
+  extern __shared__ double slna[];
+  const int ci = blockIdx.x, iz = blockIdx.y;
+  const abcmb_cosmo& c = cosmo[ci];
+  for (int i = threadIdx.x; i < n_save; i += blockDim.x)
+    slna[i] = linspace_at(c.lna_transfer_start, 0., n_save, i);
+  __syncthreads();
+  const double lna = -log(1. + z[iz]);
+  const double* dm = pt + c.off_pt + (int64_t)ABCMB_F_DELTA_M * n_save * c.nk;
+  const double* kp = kbuf + c.off_k;
+  const int nk = c.nk;
+  for (int j = threadIdx.x; j < n_kout; j += blockDim.x) {
+    double k = kout[j];
+    // jnp.interp(k, PT.k, delta_m_lna) needs delta_m_lna at the two bracketing k
+    int lo = 0, hi = nk;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (kp[mid] <= k) lo = mid + 1; else hi = mid;
+    }
+    int i = min(max(lo, 1), nk - 1);
+    double d0 = np_interp(lna, slna, dm + (i - 1), n_save, nk);
+    double d1 = np_interp(lna, slna, dm + i, n_save, nk);
+    double dx = kp[i] - kp[i - 1];
+    double d = (fabs(dx) <= 2.220446049250313e-16) ? d0 : d0 + ((k - kp[i - 1]) / dx) * (d1 - d0);
+    if (k < kp[0]) d = np_interp(lna, slna, dm, n_save, nk);
+    if (k > kp[nk - 1]) d = np_interp(lna, slna, dm + (nk - 1), n_save, nk);
+    double prim = c.A_s * pow(k / k_pivot, c.n_s - 1.) * (2 * PI * PI / (k * k * k));
+    pk[((int64_t)ci * n_z + iz) * n_kout + j] = d * d * prim;
+  }
+  (void)lna_scratch;
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+static int64_t al256(int64_t b) { return (b + 255) / 256 * 256; }
+
+int64_t los_workspace_bytes(int max_nk, int nkt, int n_ell_tab, int n_save, int precision) {
+  const int nl = n_save - 1;
+  const int ntile = (nkt + LOS_THREADS - 1) / LOS_THREADS;
+  int64_t b = 0;
+  b += 4 * al256((int64_t)max_nk * 8);                         // xk, dinv, mlo, up
+  b += al256((int64_t)nkt * 4);                                // kidx
+  b += al256((int64_t)NSRC_FIELDS * nl * max_nk * 8);          // slopes
+  b += al256((int64_t)4 * nl * nkt * (precision ? 4 : 8));     // sources
+  b += al256((int64_t)n_ell_tab * ntile * 3 * 8);              // partials
+  b += al256((int64_t)10 * n_ell_tab * 8);                     // l-spline scratch
+  return b;
+}
+
+cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_cosmo* cosmo_host,
+                       const double* tables, const double* kbuf, const double* pt, const double* kt,
+                       const abcmb_los_settings& ls, int n_save, const BesselDev& B, double* cl_raw,
+                       double* cl, void* ws, cudaStream_t stream) {
+  const int nl = n_save - 1;
+  const int nkt = ls.nkt;
+  const int n_ell_tab = ls.idx_max - ls.idx_min + 1;
+  const int n_out = ls.l_max - ls.l_min + 1;
+  const int ntile = (nkt + LOS_THREADS - 1) / LOS_THREADS;
+  int max_nk = 0;
+  for (int c = 0; c < n_cosmo; ++c) max_nk = cosmo_host[c].nk > max_nk ? cosmo_host[c].nk : max_nk;
+  char* w = static_cast<char*>(ws);
+  double* xk = reinterpret_cast<double*>(w); w += al256((int64_t)max_nk * 8);
+  double* dinv = reinterpret_cast<double*>(w); w += al256((int64_t)max_nk * 8);
+  double* mlo = reinterpret_cast<double*>(w); w += al256((int64_t)max_nk * 8);
+  double* up = reinterpret_cast<double*>(w); w += al256((int64_t)max_nk * 8);
+  int* kidx = reinterpret_cast<int*>(w); w += al256((int64_t)nkt * 4);
+  double* slopes = reinterpret_cast<double*>(w); w += al256((int64_t)NSRC_FIELDS * nl * max_nk * 8);
+  void* S = w; w += al256((int64_t)4 * nl * nkt * (ls.precision ? 4 : 8));
+  double* partial = reinterpret_cast<double*>(w); w += al256((int64_t)n_ell_tab * ntile * 3 * 8);
+  double* lscr = reinterpret_cast<double*>(w);
+  const size_t smem = (size_t)(3 * B.n_x + 2 * nl) * sizeof(double);
+  cudaError_t e;
+  if (ls.precision == 0) {
+    e = cudaFuncSetAttribute(los_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  } else {
+    e = cudaFuncSetAttribute(los_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  }
+  if (e != cudaSuccess) return e;
+  for (int ci = 0; ci < n_cosmo; ++ci) {
+    const abcmb_cosmo& ch = cosmo_host[ci];
+    const int nk = ch.nk;
+    const double* kp = kbuf + ch.off_k;
+    const double* ptc = pt + ch.off_pt;
+    spline_prep_kernel<<<1, 256, 0, stream>>>(kp, nk, kt, nkt, xk, dinv, mlo, up, kidx);
+    const int ncol = NSRC_FIELDS * nl;
+    spline_slopes_kernel<<<(ncol + 127) / 128, 128, 0, stream>>>(ptc, n_save, nk, nl, xk, dinv, mlo, up, slopes);
+    dim3 gs((nkt + 127) / 128, nl);
+    if (ls.precision == 0)
+      sources_kernel<double><<<gs, 128, 0, stream>>>(cosmo_dev, ci, tables, ptc, n_save, nk, nl, xk, slopes, kidx,
+                                                     kt, nkt, ls, static_cast<double*>(S));
+    else
+      sources_kernel<float><<<gs, 128, 0, stream>>>(cosmo_dev, ci, tables, ptc, n_save, nk, nl, xk, slopes, kidx,
+                                                    kt, nkt, ls, static_cast<float*>(S));
+    const double lts = ch.lna_transfer_start;
+    const double dl = 0.0 - (lts + (double)(n_save - 2) * ((0.0 - lts) / (double)(n_save - 1)));
+    dim3 gl(n_ell_tab, ntile);
+    if (ls.precision == 0)
+      los_kernel<0><<<gl, LOS_THREADS, smem, stream>>>(cosmo_dev, ci, tables, nl, dl, S, kt, nkt, B, ls.idx_min,
+                                                       ch.A_s, ch.n_s, ls.k_pivot, partial);
+    else
+      los_kernel<1><<<gl, LOS_THREADS, smem, stream>>>(cosmo_dev, ci, tables, nl, dl, S, kt, nkt, B, ls.idx_min,
+                                                       ch.A_s, ch.n_s, ls.k_pivot, partial);
+    cl_final_kernel<<<1, 256, 0, stream>>>(partial, n_ell_tab, ntile, B, ls.idx_min, ls.l_min, n_out,
+                                           cl_raw + (int64_t)ci * n_ell_tab * 3, cl + (int64_t)ci * 3 * n_out, lscr);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* kbuf, const double* pt,
+                          int n_save, double k_pivot, int n_kout, const double* kout, int n_z, const double* z,
+                          double* pk, cudaStream_t stream) {
+  dim3 g(n_cosmo, n_z);
+  pk_lin_kernel<<<g, 256, n_save * sizeof(double), stream>>>(cosmo, kbuf, pt, n_save, k_pivot, n_kout, kout, n_z,
+                                                              z, pk, nullptr);
+  return cudaGetLastError();
+}
+
+}  // namespace abcmb

@@ -1,0 +1,156 @@
+"""Device runtime: uploads a packed batch and drives the C-ABI calls.
+
+torch supplies device memory and the stream (plumbing only); every kernel is
+in libabcmb_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from . import bessel as bessel_mod
+from .packing import Batch, NFIELDS, CPertSettings, CLosSettings
+
+_uploaded_devices: set = set()
+
+
+def _ptr(t: torch.Tensor) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def require_cuda(device=None) -> torch.device:
+    if not torch.cuda.is_available():
+        raise _lib.ABCMBError("no CUDA device: the abcmb_b200 kernels have no CPU fallback")
+    return torch.device(device if device is not None else "cuda")
+
+
+def ensure_bessel(device: torch.device):
+    """Upload the Bessel tables once per device (spectrum.py:29-46)."""
+    lib = _lib.load()
+    idx = device.index if device.index is not None else torch.cuda.current_device()
+    if idx in _uploaded_devices:
+        return
+    bt = bessel_mod.load()
+    with torch.cuda.device(idx):
+        keep = [np.ascontiguousarray(bt.l_tab, dtype=np.int32)]
+        args = [bt.n_l, bt.n_x, ctypes.c_void_p(keep[0].ctypes.data)]
+        for n in range(3):
+            for a in (bt.xmin[n], bt.xmax[n], bt.phi[n]):
+                a = np.ascontiguousarray(a, dtype=np.float64)
+                keep.append(a)
+                args.append(ctypes.c_void_p(a.ctypes.data))
+        _lib.check(lib.abcmb_upload_bessel(*args), "abcmb_upload_bessel")
+    _uploaded_devices.add(idx)
+
+
+@dataclass
+class DeviceBatch:
+    """A Batch resident in HBM plus the output and workspace buffers."""
+    batch: Batch
+    device: torch.device
+    cosmo: torch.Tensor
+    tables: torch.Tensor
+    kbuf: torch.Tensor
+    items: torch.Tensor
+    pt: torch.Tensor
+    kstat: torch.Tensor
+    ws_pert: torch.Tensor
+
+    @classmethod
+    def upload(cls, batch: Batch, device=None, non_blocking: bool = False) -> "DeviceBatch":
+        dev = require_cuda(device)
+
+        def to_dev(a: np.ndarray, dtype):
+            t = torch.from_numpy(np.ascontiguousarray(a)).view(dtype)
+            if non_blocking:
+                t = t.pin_memory()
+            return t.to(dev, non_blocking=non_blocking)
+
+        cos = to_dev(batch.cosmo.view(np.uint8), torch.uint8)
+        tables = to_dev(batch.tables, torch.float64)
+        kbuf = to_dev(batch.kbuf, torch.float64)
+        items = to_dev(batch.items.reshape(-1), torch.int32)
+        pt = torch.empty(max(batch.pt_size, 1), dtype=torch.float64, device=dev)
+        kstat = torch.zeros(batch.n_items * 24, dtype=torch.uint8, device=dev)
+        lib = _lib.load()
+        nws = int(lib.abcmb_pert_workspace_size(batch.n_cosmo, batch.n_items))
+        ws = torch.empty(nws, dtype=torch.uint8, device=dev)
+        return cls(batch, dev, cos, tables, kbuf, items, pt, kstat, ws)
+
+    def pert_forward(self, settings: CPertSettings, stream=None):
+        lib = _lib.load()
+        st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        rc = lib.abcmb_pert_forward(self.batch.n_cosmo, _ptr(self.cosmo), _ptr(self.tables), _ptr(self.kbuf),
+                                    self.batch.n_items, _ptr(self.items), ctypes.byref(settings), _ptr(self.pt),
+                                    _ptr(self.kstat), _ptr(self.ws_pert), self.ws_pert.numel(),
+                                    ctypes.c_void_p(st.cuda_stream))
+        _lib.check(rc, "abcmb_pert_forward")
+
+    def kstat_host(self) -> np.ndarray:
+        from .packing import KSTAT_DTYPE
+        return self.kstat.cpu().numpy().view(KSTAT_DTYPE).copy()
+
+    def check_status(self):
+        ks = self.kstat_host()
+        bad = np.nonzero(ks["status"] != 0)[0]
+        if bad.size:
+            it = self.batch.items[bad[0]]
+            raise _lib.ABCMBError(
+                f"{bad.size} perturbation items failed; first: cosmology {it[0]} k index {it[1]} "
+                f"status {int(ks['status'][bad[0]])} (1 = max_steps_PE reached: raise max_steps_PE or loosen "
+                f"rtol/atol, as for diffrax)")
+        return ks
+
+
+class LosRunner:
+    """Workspace + outputs of abcmb_los_forward for a fixed transfer k grid."""
+
+    def __init__(self, dbatch: DeviceBatch, kt: np.ndarray, ls: CLosSettings):
+        self.db = dbatch
+        self.ls = ls
+        dev = dbatch.device
+        ensure_bessel(dev)
+        lib = _lib.load()
+        self.kt = torch.from_numpy(np.ascontiguousarray(kt, dtype=np.float64)).to(dev)
+        self.n_ell_tab = ls.idx_max - ls.idx_min + 1
+        self.n_out = ls.l_max - ls.l_min + 1
+        max_nk = int(dbatch.batch.cosmo["nk"].max())
+        nws = int(lib.abcmb_los_workspace_size(dbatch.batch.n_cosmo, max_nk, ls.nkt, self.n_ell_tab, ls.n_save,
+                                               ls.precision))
+        self.ws = torch.empty(nws, dtype=torch.uint8, device=dev)
+        n = dbatch.batch.n_cosmo
+        self.cl_raw = torch.empty(n * self.n_ell_tab * 3, dtype=torch.float64, device=dev)
+        self.cl = torch.empty(n * 3 * self.n_out, dtype=torch.float64, device=dev)
+
+    def run(self, stream=None):
+        lib = _lib.load()
+        st = stream if stream is not None else torch.cuda.current_stream(self.db.device)
+        db = self.db
+        rc = lib.abcmb_los_forward(db.batch.n_cosmo, _ptr(db.cosmo), _ptr(db.tables), _ptr(db.kbuf), _ptr(db.pt),
+                                   _ptr(self.kt), ctypes.byref(self.ls), _ptr(self.cl_raw), _ptr(self.cl),
+                                   _ptr(self.ws), self.ws.numel(), ctypes.c_void_p(st.cuda_stream))
+        _lib.check(rc, "abcmb_los_forward")
+
+    def cl_host(self) -> np.ndarray:
+        return self.cl.cpu().numpy().reshape(self.db.batch.n_cosmo, 3, self.n_out)
+
+    def cl_raw_host(self) -> np.ndarray:
+        return self.cl_raw.cpu().numpy().reshape(self.db.batch.n_cosmo, self.n_ell_tab, 3)
+
+
+def pk_lin(db: DeviceBatch, k_pivot: float, kout: np.ndarray, z: np.ndarray, stream=None) -> np.ndarray:
+    lib = _lib.load()
+    dev = db.device
+    kt = torch.from_numpy(np.ascontiguousarray(kout, dtype=np.float64)).to(dev)
+    zt = torch.from_numpy(np.ascontiguousarray(z, dtype=np.float64)).to(dev)
+    out = torch.empty(db.batch.n_cosmo * len(z) * len(kout), dtype=torch.float64, device=dev)
+    st = stream if stream is not None else torch.cuda.current_stream(dev)
+    rc = lib.abcmb_pk_lin(db.batch.n_cosmo, _ptr(db.cosmo), _ptr(db.kbuf), _ptr(db.pt), db.batch.n_save,
+                          float(k_pivot), len(kout), _ptr(kt), len(z), _ptr(zt), _ptr(out),
+                          ctypes.c_void_p(st.cuda_stream))
+    _lib.check(rc, "abcmb_pk_lin")
+    return out.cpu().numpy().reshape(db.batch.n_cosmo, len(z), len(kout))

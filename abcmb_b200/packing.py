@@ -37,12 +37,14 @@ assert COSMO_DTYPE.itemsize == 304
 class CPertSettings(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in
                 ["R_tc", "R_large", "k_split", "rtol_small", "rtol_large", "atol_small", "atol_large",
-                 "pcoeff", "icoeff", "dcoeff", "dt0"]] + [("max_steps", ctypes.c_int32), ("n_save", ctypes.c_int32)]
+                 "pcoeff", "icoeff", "dcoeff", "dt0"]] + [("max_steps", ctypes.c_int32), ("n_save", ctypes.c_int32),
+                                                           ("max_ny", ctypes.c_int32), ("any_ncdm", ctypes.c_int32)]
 
 
 class CLosSettings(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in ["k_pivot", "scale_sw", "scale_isw", "scale_dop", "scale_pol"]] + \
-               [(n, ctypes.c_int32) for n in ["l_min", "l_max", "idx_min", "idx_max", "nkt", "precision"]]
+               [(n, ctypes.c_int32) for n in ["l_min", "l_max", "idx_min", "idx_max", "nkt", "precision",
+                                              "n_save", "pad_"]]
 
 
 class CKStat(ctypes.Structure):
@@ -54,8 +56,11 @@ KSTAT_DTYPE = np.dtype([("status", "<i4"), ("n_accepted", "<i4"), ("n_rejected",
                         ("n_newton", "<i4"), ("lna_start", "<f8")], align=True)
 
 
-def pert_settings(specs: dict, n_save: int = 500) -> CPertSettings:
-    return CPertSettings(R_tc=specs["R_tc"], R_large=specs["R_large"], k_split=specs["k_split_PE"],
+def pert_settings(specs: dict, n_save: int = 500, batch=None) -> CPertSettings:
+    max_ny = int(batch.cosmo["ny"].max()) if batch is not None else 0
+    any_ncdm = int(batch.cosmo["has_ncdm"].max()) if batch is not None else 0
+    return CPertSettings(max_ny=max_ny, any_ncdm=any_ncdm,
+                         R_tc=specs["R_tc"], R_large=specs["R_large"], k_split=specs["k_split_PE"],
                          rtol_small=specs["rtol_small_k_PE"], rtol_large=specs["rtol_large_k_PE"],
                          atol_small=specs["atol_small_k_PE"], atol_large=specs["atol_large_k_PE"],
                          pcoeff=specs["pcoeff_PE"], icoeff=specs["icoeff_PE"], dcoeff=specs["dcoeff_PE"],
@@ -63,11 +68,11 @@ def pert_settings(specs: dict, n_save: int = 500) -> CPertSettings:
 
 
 def los_settings(specs: dict, idx_min: int, idx_max: int, nkt: int, l_out_max: int,
-                 precision: int = 0) -> CLosSettings:
+                 precision: int = 0, n_save: int = 500) -> CLosSettings:
     return CLosSettings(k_pivot=specs["k_pivot"], scale_sw=specs["scale_sw"], scale_isw=specs["scale_isw"],
                         scale_dop=specs["scale_dop"], scale_pol=specs["scale_pol"],
                         l_min=int(specs["l_min"]), l_max=int(l_out_max), idx_min=idx_min, idx_max=idx_max,
-                        nkt=nkt, precision=precision)
+                        nkt=nkt, precision=precision, n_save=n_save, pad_=0)
 
 
 @dataclass

@@ -128,6 +128,8 @@ typedef struct abcmb_pert_settings {
   double dt0;                       /* first step (perturbations.py:306)  */
   int32_t max_steps;                /* max_steps_PE                       */
   int32_t n_save;                   /* 500 save points                    */
+  int32_t max_ny;                   /* largest state size in the batch    */
+  int32_t any_ncdm;                 /* 1 if any cosmology has massive nu  */
 } abcmb_pert_settings;
 
 /* Per-k solver statistics. */
@@ -147,6 +149,8 @@ typedef struct abcmb_los_settings {
   int32_t idx_min, idx_max;      /* bessel_l_tab indices covered             */
   int32_t nkt;                   /* transfer k grid length                   */
   int32_t precision;             /* 0 = FP64, 1 = FP32 + compensated sums    */
+  int32_t n_save;                /* PT save points (500)                     */
+  int32_t pad_;
 } abcmb_los_settings;
 
 /* ------------------------------------------------------------------------ */
@@ -246,6 +250,16 @@ int abcmb_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* k_dev,
                  const double* pt_dev, int n_save, double k_pivot,
                  int n_kout, const double* kout_dev, int n_z, const double* z_dev,
                  double* pk_dev, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Tuning and diagnostics                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Warps per block of the perturbation kernel (1..8; default 4). */
+int abcmb_set_pert_warps_per_block(int warps);
+
+/* Grid size (blocks) of the last perturbation launch on this process. */
+int abcmb_last_pert_grid(void);
 
 #ifdef __cplusplus
 }

@@ -1156,3 +1156,14 @@ int oracle_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* kbuf, con
   }
   return ABCMB_OK;
 }
+
+/* sizeof of the C-ABI records, so tests can check the Python layouts. */
+int oracle_sizeof(int which) {
+  switch (which) {
+    case 0: return (int)sizeof(abcmb_cosmo);
+    case 1: return (int)sizeof(abcmb_pert_settings);
+    case 2: return (int)sizeof(abcmb_kstat);
+    case 3: return (int)sizeof(abcmb_los_settings);
+  }
+  return -1;
+}

@@ -46,6 +46,7 @@ void oracle_sources(const abcmb_cosmo* c, const double* tables, const double* kb
 int oracle_los_forward(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
                        const double* pt, const double* kt, const abcmb_los_settings* ls, int n_save,
                        const oracle_bessel* B, double* cl_raw, double* cl, int n_threads);
+int oracle_sizeof(int which);
 int oracle_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* kbuf, const double* pt, int n_save,
                   double k_pivot, int n_kout, const double* kout, int n_z, const double* z, double* pk);
 

@@ -1,0 +1,159 @@
+"""GPU parity: the CUDA path against the CPU oracle on the same seeded inputs.
+
+Tolerances (stated per test): the GPU kernels run the same algorithm as the
+oracle (Kvaerno5 + very-chord + PID, same tableau, same dense output) in
+FP64, so step sequences coincide and results agree far below the 1e-4
+relative C_l budget of the north star; the FP32 + compensated line of sight
+is checked against the FP64 path at its own stated bound.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from abcmb_b200 import engine
+    return engine
+
+
+def _field_err(a, b):
+    scale = np.abs(b).max(axis=(-2, -1), keepdims=True) + 1e-300
+    return (np.abs(a - b) / scale).max(axis=(-2, -1))
+
+
+def test_pert_parity_c1(gpu, c1_small, c1_oracle):
+    w = c1_small
+    pt_o, ks_o = c1_oracle
+    db = gpu.DeviceBatch.upload(w.batch)
+    db.pert_forward(w.pert_settings())
+    ks = db.check_status()
+    assert (ks["n_accepted"] == ks_o["n_accepted"]).mean() >= 0.95
+    err = _field_err(w.batch.pt_view(db.pt.cpu().numpy(), 0), w.batch.pt_view(pt_o, 0))
+    assert err[:18].max() < 1e-5, err                       # relative to each field's max |value|
+    assert np.all(err[18:] == 0)                            # no massive species: zero fields
+
+
+def test_los_parity_on_oracle_pt(gpu, c1_small, c1_oracle):
+    """LOS alone: GPU vs oracle on the same PT, FP64: agreement to rounding."""
+    from abcmb_b200 import bessel
+    from oracle import oracle
+    import torch
+    w = c1_small
+    pt_o, _ = c1_oracle
+    db = gpu.DeviceBatch.upload(w.batch)
+    db.pt.copy_(torch.from_numpy(pt_o))
+    ls = w.los_settings()
+    lr = gpu.LosRunner(db, w.kt, ls)
+    lr.run()
+    _, raw_o, cl_o = oracle.los_forward(w.batch, pt_o, w.kt, ls, bessel.load())
+    np.testing.assert_allclose(lr.cl_raw_host(), raw_o, rtol=1e-10, atol=0)
+    scale = np.abs(cl_o[:, 0:1, :]) + np.abs(cl_o)          # TE crosses zero: relative to |TT| + |XY|
+    assert np.max(np.abs(lr.cl_host() - cl_o) / scale) < 1e-10
+
+
+def test_end_to_end_c1(gpu, c1_small, c1_oracle):
+    """PT + C_l on the GPU vs the oracle: |dC_l/C_l| <= 1e-6 (budget 1e-4)."""
+    from abcmb_b200 import bessel
+    from oracle import oracle
+    w = c1_small
+    pt_o, _ = c1_oracle
+    db = gpu.DeviceBatch.upload(w.batch)
+    db.pert_forward(w.pert_settings())
+    db.check_status()
+    lr = gpu.LosRunner(db, w.kt, w.los_settings())
+    lr.run()
+    _, _, cl_o = oracle.los_forward(w.batch, pt_o, w.kt, w.los_settings(), bessel.load())
+    cl = lr.cl_host()
+    rel = np.abs(cl - cl_o) / np.abs(cl_o)
+    assert rel[0, 0].max() < 1e-6 and rel[0, 2].max() < 1e-6
+    assert np.max(np.abs(cl[0, 1] - cl_o[0, 1]) / (np.abs(cl_o[0, 0]) + np.abs(cl_o[0, 1]))) < 1e-6
+
+
+def test_uneven_batch_with_massive_neutrinos(gpu):
+    """Three cosmologies with 0/1/3 massive nu and different k grids in one launch."""
+    from abcmb_b200 import configs, bessel
+    from oracle import oracle
+    w = configs.c4(n_cosmo=3, nk_range=(10, 16), seed=7)
+    w.has_ncdm = [False, True, True]
+    w.params_in[1].update(N_nu_massive=1, m_nu_massive=0.06)
+    w.params_in[2].update(N_nu_massive=3, m_nu_massive=0.06)
+    w.params_in[0].pop("N_nu_massive", None)
+    w.build()
+    st = w.pert_settings()
+    assert st.any_ncdm == 1
+    rc, pt_o, ks_o = oracle.pert_forward(w.batch, st)
+    assert rc == 0
+    db = gpu.DeviceBatch.upload(w.batch)
+    db.pert_forward(st)
+    db.check_status()
+    pt = db.pt.cpu().numpy()
+    for ci in range(3):
+        err = _field_err(w.batch.pt_view(pt, ci), w.batch.pt_view(pt_o, ci))
+        assert err.max() < 1e-5, (ci, err)
+    lr = gpu.LosRunner(db, w.kt, w.los_settings())
+    lr.run()
+    _, _, cl_o = oracle.los_forward(w.batch, pt_o, w.kt, w.los_settings(), bessel.load())
+    cl = lr.cl_host()
+    assert np.max(np.abs(cl[:, 0] - cl_o[:, 0]) / np.abs(cl_o[:, 0])) < 1e-5
+
+
+def test_pk_lin_parity(gpu, c1_small, c1_oracle):
+    from oracle import oracle
+    import torch
+    w = c1_small
+    pt_o, _ = c1_oracle
+    db = gpu.DeviceBatch.upload(w.batch)
+    db.pt.copy_(torch.from_numpy(pt_o))
+    kout = np.geomspace(5e-5, 0.8, 77)          # includes clamped ends below/above PT.k
+    z = np.array([0.0, 1.0, 2.0, 3.0])
+    got = gpu.pk_lin(db, 0.05, kout, z)
+    want = oracle.pk_lin(w.batch, pt_o, 0.05, kout, z)
+    np.testing.assert_allclose(got, want, rtol=1e-12)
+
+
+def test_max_steps_reported_and_raised(gpu, c1_small):
+    """A too-small max_steps_PE flags the items and raises, as diffrax does."""
+    from abcmb_b200 import _lib
+    w = c1_small
+    st = w.pert_settings()
+    st.max_steps = 40
+    db = gpu.DeviceBatch.upload(w.batch)
+    db.pert_forward(st)
+    ks = db.kstat_host()
+    assert (ks["status"] == 1).any()
+    with pytest.raises(_lib.ABCMBError, match="max_steps"):
+        db.check_status()
+
+
+def test_los_fp32_compensated_error(gpu, c1_small, c1_oracle):
+    """FP32 sources + Kahan sums vs the FP64 path: |dC_l/C_l| < 1e-4 for l <= 1500."""
+    import torch
+    w = c1_small
+    pt_o, _ = c1_oracle
+    db = gpu.DeviceBatch.upload(w.batch)
+    db.pt.copy_(torch.from_numpy(pt_o))
+    l64 = gpu.LosRunner(db, w.kt, w.los_settings(0))
+    l64.run()
+    l32 = gpu.LosRunner(db, w.kt, w.los_settings(1))
+    l32.run()
+    a, b = l32.cl_host(), l64.cl_host()
+    rel = np.abs(a - b) / (np.abs(b[:, 0:1]) + np.abs(b))
+    assert rel.max() < 1e-4, rel.max()
+
+
+def test_los_deterministic(gpu, c1_small, c1_oracle):
+    import torch
+    w = c1_small
+    pt_o, _ = c1_oracle
+    db = gpu.DeviceBatch.upload(w.batch)
+    db.pt.copy_(torch.from_numpy(pt_o))
+    lr = gpu.LosRunner(db, w.kt, w.los_settings())
+    lr.run()
+    a = lr.cl_host().copy()
+    lr.run()
+    np.testing.assert_array_equal(a, lr.cl_host())

@@ -1,0 +1,88 @@
+"""Host-side logic: specs, grids, layouts, packing and the C ABI surface (no GPU)."""
+import ctypes
+import re
+
+import numpy as np
+import pytest
+
+from abcmb_b200 import cosmology, specs as sp
+
+
+def test_default_k_axes_match_reference_sizes():
+    s = sp.load_specs({"l_max": 2500})
+    k, kout = sp.get_k_axis_perturbations(s)
+    assert len(k) == 548                        # ABCMB_basics.ipynb: PT.k f64[548]
+    kt = sp.get_k_axis_transfer(s)
+    assert len(kt) == 1704
+    s = sp.load_specs({"l_max": 1500})
+    sp.get_k_axis_perturbations(s)
+    assert len(sp.get_k_axis_transfer(s)) == 1078
+    assert kt[0] == pytest.approx(0.1 / 1.418668e04)
+
+
+def test_ell_index_ranges():
+    from abcmb_b200 import bessel
+    lt = bessel.load().l_tab
+    i0, i1, _ = sp.ell_index_range(lt, 2, 1500, False)
+    assert (i0, i1 - i0 + 1) == (0, 74)
+    i0, i1, _ = sp.ell_index_range(lt, 2, 2500, False)
+    assert i1 - i0 + 1 == 99
+    i0, i1, lmax = sp.ell_index_range(lt, 2, 3000, True)
+    assert lmax == 3500 and lt[i1] >= 3500
+
+
+def test_state_layout_sizes():
+    s1 = sp.load_specs(dict(l_max_g=12, l_max_pol_g=12, l_max_massless_nu=12))
+    assert sp.state_layout(s1, False).ny == 43
+    s2 = sp.load_specs(dict(l_max_g=30, l_max_pol_g=30, l_max_massless_nu=30, l_max_massive_nu=30))
+    assert sp.state_layout(s2, True).ny == 190
+    with pytest.raises(ValueError):
+        sp.state_layout(sp.load_specs(dict(l_max_pol_g=3)), False)
+
+
+def test_derived_parameters():
+    p = cosmology.add_derived_parameters(dict(h=0.674, omega_b=0.0224, omega_cdm=0.12, Neff=3.044), False)
+    assert p["omega_Lambda"] == pytest.approx(0.674 ** 2 - p["omega_r"] - p["omega_m"])
+    assert p["N_nu_massless"] == pytest.approx(3.0, rel=1e-3)
+    assert 0.40 < p["R_nu"] < 0.42
+    pm = cosmology.add_derived_parameters(dict(Neff=3.044, N_nu_massive=1, m_nu_massive=0.06), True)
+    assert pm["N_nu_massless"] == pytest.approx(2.0, abs=0.05)
+    with pytest.raises(ValueError):
+        cosmology.add_derived_parameters(dict(Neff=3.0, N_nu_massless=3), False)
+
+
+def test_pack_offsets_and_order():
+    from abcmb_b200 import configs
+    w = configs.c4(n_cosmo=3, nk_range=(10, 14)).build()
+    b = w.batch
+    assert b.cosmo.dtype.itemsize == 304
+    assert (b.cosmo["off_tau"] % 32 == 0).all() and (b.cosmo["off_pt"] % 32 == 0).all()
+    assert b.n_items == int(b.cosmo["nk"].sum())
+    ny = b.cosmo["ny"][b.items[:, 0]]
+    assert (np.diff(ny) <= 0).all()             # largest state first
+    for ci in range(b.n_cosmo):
+        np.testing.assert_array_equal(b.k_of(ci), w.kgrids[ci])
+
+
+def test_c_abi_library_exports_every_declared_symbol():
+    from abcmb_b200 import _lib
+    import os
+    hdr = open(os.path.join(os.path.dirname(_lib.__file__), "..", "include", "abcmb_b200.h")).read()
+    declared = set(re.findall(r"^\s*(?:int|int64_t|const char\*)\s+(abcmb_\w+)\(", hdr, re.M))
+    assert {"abcmb_pert_forward", "abcmb_los_forward", "abcmb_version"} <= declared
+    lib = _lib.load()
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert {n for n, _, _ in _lib.SIGNATURES} == declared
+    assert lib.abcmb_version() == 100
+    assert lib.abcmb_pert_workspace_size(2, 10) > 2 * 10000 * 8
+
+
+def test_los_argument_errors_without_gpu():
+    from abcmb_b200 import _lib, packing
+    lib = _lib.load()
+    ls = packing.CLosSettings(l_min=3, l_max=10, idx_min=0, idx_max=5, nkt=10, n_save=500)
+    rc = lib.abcmb_los_forward(1, ctypes.c_void_p(8), ctypes.c_void_p(8), ctypes.c_void_p(8), ctypes.c_void_p(8),
+                               ctypes.c_void_p(8), ctypes.byref(ls), ctypes.c_void_p(8), ctypes.c_void_p(8),
+                               ctypes.c_void_p(8), 0, None)
+    assert rc == -1 and b"l_min" in lib.abcmb_last_error()
