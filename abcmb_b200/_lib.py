@@ -9,7 +9,8 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libabcmb_b200.so")
+# ABCMB_B200_LIB points at an alternative build of the same library (tuning builds)
+LIB_PATH = os.environ.get("ABCMB_B200_LIB") or os.path.join(_HERE, "libabcmb_b200.so")
 
 _vp = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -27,11 +28,13 @@ SIGNATURES = [
                                           _vp]),
     ("abcmb_los_workspace_size", _i64, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int]),
-    ("abcmb_los_forward", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp]),
+    ("abcmb_los_forward", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64,
+                                         _vp]),
     ("abcmb_pk_lin", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _d, ctypes.c_int, _vp, ctypes.c_int,
                                     _vp, _vp, _vp]),
     ("abcmb_set_pert_warps_per_block", ctypes.c_int, [ctypes.c_int]),
     ("abcmb_last_pert_grid", ctypes.c_int, []),
+    ("abcmb_probe_fp64_tflops", ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.c_int, _vp]),
 ]
 
 _lib = None

@@ -16,7 +16,7 @@ int64_t los_workspace_bytes(int max_nk, int nkt, int n_ell_tab, int n_save, int 
 cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_cosmo* cosmo_host,
                        const double* tables, const double* kbuf, const double* pt, const double* kt,
                        const abcmb_los_settings& ls, int n_save, const BesselDev& B, double* cl_raw,
-                       double* cl, void* ws, cudaStream_t stream);
+                       double* cl, double* dcl_dns, void* ws, cudaStream_t stream);
 cudaError_t launch_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* kbuf, const double* pt,
                           int n_save, double k_pivot, int n_kout, const double* kout, int n_z, const double* z,
                           double* pk, cudaStream_t stream);
@@ -134,10 +134,10 @@ int64_t abcmb_los_workspace_size(int n_cosmo, int max_nk, int nkt, int n_ell_tab
   return abcmb::los_workspace_bytes(max_nk, nkt, n_ell_tab, n_save, precision);
 }
 
-int abcmb_los_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* tables_dev, const double* k_dev,
-                      const double* pt_dev, const double* kt_dev, const abcmb_los_settings* settings,
-                      double* cl_raw_dev, double* cl_dev, void* workspace_dev, int64_t workspace_bytes,
-                      void* stream) {
+int abcmb_los_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_cosmo* cosmo_host,
+                      const double* tables_dev, const double* k_dev, const double* pt_dev, const double* kt_dev,
+                      const abcmb_los_settings* settings, double* cl_raw_dev, double* cl_dev, double* dcl_dns_dev,
+                      void* workspace_dev, int64_t workspace_bytes, void* stream) {
   if (n_cosmo <= 0 || !cosmo_dev || !tables_dev || !k_dev || !pt_dev || !kt_dev || !settings || !cl_raw_dev ||
       !cl_dev)
     return fail(ABCMB_ERR_ARG, "abcmb_los_forward: null argument");
@@ -148,11 +148,17 @@ int abcmb_los_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* t
   if (!bc || !bc->ready) return fail(ABCMB_ERR_TABLES, "abcmb_los_forward: Bessel tables not uploaded");
   if (ls.idx_min < 0 || ls.idx_max >= bc->dev.n_l) return fail(ABCMB_ERR_ARG, "abcmb_los_forward: l index range");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  // the launcher needs the per-cosmology sizes on the host
+  // the launcher needs the per-cosmology sizes on the host: use the caller's
+  // host copy (no synchronisation, graph-capturable) or read them back
   std::vector<abcmb_cosmo> host(n_cosmo);
-  cudaError_t e = cudaMemcpyAsync(host.data(), cosmo_dev, sizeof(abcmb_cosmo) * n_cosmo, cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return cuda_fail(e, "abcmb_los_forward descriptor read");
+  cudaError_t e = cudaSuccess;
+  if (cosmo_host) {
+    std::memcpy(host.data(), cosmo_host, sizeof(abcmb_cosmo) * n_cosmo);
+  } else {
+    e = cudaMemcpyAsync(host.data(), cosmo_dev, sizeof(abcmb_cosmo) * n_cosmo, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "abcmb_los_forward descriptor read");
+  }
   int max_nk = 0;
   for (const auto& c : host) max_nk = c.nk > max_nk ? c.nk : max_nk;
   const int n_save = ls.n_save;
@@ -160,7 +166,7 @@ int abcmb_los_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* t
   int64_t need = abcmb::los_workspace_bytes(max_nk, ls.nkt, ls.idx_max - ls.idx_min + 1, n_save, ls.precision);
   if (!workspace_dev || workspace_bytes < need) return fail(ABCMB_ERR_WORKSPACE, "abcmb_los_forward: workspace");
   e = abcmb::launch_los(n_cosmo, cosmo_dev, host.data(), tables_dev, k_dev, pt_dev, kt_dev, ls, n_save, bc->dev,
-                        cl_raw_dev, cl_dev, workspace_dev, st);
+                        cl_raw_dev, cl_dev, dcl_dns_dev, workspace_dev, st);
   if (e != cudaSuccess) return cuda_fail(e, "abcmb_los_forward");
   return ABCMB_OK;
 }

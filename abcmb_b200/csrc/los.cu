@@ -287,56 +287,64 @@ __global__ void __launch_bounds__(LOS_THREADS) los_kernel(const abcmb_cosmo* __r
     contrib[0] = wj * pr * T * T;
     contrib[1] = wj * pr * T * E;
     contrib[2] = wj * pr * E * E;
+    // n_s enters only the primordial factor (k/k_pivot)^(n_s-1): d/dn_s = ln(k/k_pivot)
+    const double lk = log(k / k_pivot);
+    contrib[3] = contrib[0] * lk;
+    contrib[4] = contrib[1] * lk;
+    contrib[5] = contrib[2] * lk;
   }
   // block reduction (fixed order: deterministic)
-  __shared__ double red[3][LOS_THREADS / 32];
+  __shared__ double red[6][LOS_THREADS / 32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-  for (int X = 0; X < 3; ++X) {
+  for (int X = 0; X < 6; ++X) {
     double v = contrib[X];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     if (lane == 0) red[X][wid] = v;
   }
   __syncthreads();
-  if (threadIdx.x < 3) {
+  if (threadIdx.x < 6) {
     double s = 0.;
     for (int w = 0; w < (int)(blockDim.x / 32); ++w) s += red[threadIdx.x][w];
-    partial[((int64_t)ie * ntile + tile) * 3 + threadIdx.x] = s;
+    partial[((int64_t)ie * ntile + tile) * 6 + threadIdx.x] = s;
   }
 }
 
 __global__ void cl_final_kernel(const double* __restrict__ partial, int n_ell_tab, int ntile, BesselDev B,
                                 int idx_min, int l_min, int n_out, double* __restrict__ cl_raw,
-                                double* __restrict__ cl, double* __restrict__ scratch) {
-  // scratch: x[n], y[3][n], s[3][n], dinv, mlo, up  (n = n_ell_tab)
+                                double* __restrict__ cl, double* __restrict__ dcl_dns,
+                                double* __restrict__ scratch) {
+  // scratch: x[n], y[6][n], s[6][n], dinv, mlo, up  (n = n_ell_tab); series 3..5 are dC/dn_s
   const int n = n_ell_tab;
+  const int nser = dcl_dns ? 6 : 3;
   double* x = scratch;
   double* y = x + n;
-  double* s = y + 3 * n;
-  double* dinv = s + 3 * n;
+  double* s = y + 6 * n;
+  double* dinv = s + 6 * n;
   double* mlo = dinv + n;
   double* up = mlo + n;
-  for (int i = threadIdx.x; i < n * 3; i += blockDim.x) {
-    int ie = i / 3, X = i % 3;
+  for (int i = threadIdx.x; i < n * nser; i += blockDim.x) {
+    int ie = i / nser, X = i % nser;
     double acc = 0.;
-    for (int t = 0; t < ntile; ++t) acc += partial[((int64_t)ie * ntile + t) * 3 + X];
-    cl_raw[i] = acc;
+    for (int t = 0; t < ntile; ++t) acc += partial[((int64_t)ie * ntile + t) * 6 + X];
+    if (X < 3) cl_raw[ie * 3 + X] = acc;
     y[X * n + ie] = acc;
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = (double)B.l_tab[idx_min + i];
   __syncthreads();
   if (threadIdx.x == 0) nak_factor(x, n, dinv, mlo, up);
   __syncthreads();
-  if (threadIdx.x < 3) nak_solve(x, y + threadIdx.x * n, n, dinv, mlo, up, s + threadIdx.x * n);
+  if (threadIdx.x < nser) nak_solve(x, y + threadIdx.x * n, n, dinv, mlo, up, s + threadIdx.x * n);
   __syncthreads();
-  for (int i = threadIdx.x; i < 3 * n_out; i += blockDim.x) {
+  for (int i = threadIdx.x; i < nser * n_out; i += blockDim.x) {
     int X = i / n_out, o = i % n_out;
     double xq = (double)(l_min + o);
     int iv = spline_interval(x, n, xq);
     double v = spline_piece(y[X * n + iv], y[X * n + iv + 1], s[X * n + iv], s[X * n + iv + 1],
                             x[iv + 1] - x[iv], xq - x[iv]);
-    cl[(int64_t)X * n_out + o] = v;
+    if (X < 3) cl[(int64_t)X * n_out + o] = v;
+    else dcl_dns[(int64_t)(X - 3) * n_out + o] = v;
   }
 }
 
@@ -407,15 +415,15 @@ int64_t los_workspace_bytes(int max_nk, int nkt, int n_ell_tab, int n_save, int 
   b += al256((int64_t)nkt * 4);                                // kidx
   b += al256((int64_t)NSRC_FIELDS * nl * max_nk * 8);          // slopes
   b += al256((int64_t)4 * nl * nkt * (precision ? 4 : 8));     // sources
-  b += al256((int64_t)n_ell_tab * ntile * 3 * 8);              // partials
-  b += al256((int64_t)10 * n_ell_tab * 8);                     // l-spline scratch
+  b += al256((int64_t)n_ell_tab * ntile * 6 * 8);              // partials
+  b += al256((int64_t)16 * n_ell_tab * 8);                     // l-spline scratch
   return b;
 }
 
 cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_cosmo* cosmo_host,
                        const double* tables, const double* kbuf, const double* pt, const double* kt,
                        const abcmb_los_settings& ls, int n_save, const BesselDev& B, double* cl_raw,
-                       double* cl, void* ws, cudaStream_t stream) {
+                       double* cl, double* dcl_dns, void* ws, cudaStream_t stream) {
   const int nl = n_save - 1;
   const int nkt = ls.nkt;
   const int n_ell_tab = ls.idx_max - ls.idx_min + 1;
@@ -431,7 +439,7 @@ cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_co
   int* kidx = reinterpret_cast<int*>(w); w += al256((int64_t)nkt * 4);
   double* slopes = reinterpret_cast<double*>(w); w += al256((int64_t)NSRC_FIELDS * nl * max_nk * 8);
   void* S = w; w += al256((int64_t)4 * nl * nkt * (ls.precision ? 4 : 8));
-  double* partial = reinterpret_cast<double*>(w); w += al256((int64_t)n_ell_tab * ntile * 3 * 8);
+  double* partial = reinterpret_cast<double*>(w); w += al256((int64_t)n_ell_tab * ntile * 6 * 8);
   double* lscr = reinterpret_cast<double*>(w);
   const size_t smem = (size_t)(3 * B.n_x + 2 * nl) * sizeof(double);
   cudaError_t e;
@@ -466,7 +474,8 @@ cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_co
       los_kernel<1><<<gl, LOS_THREADS, smem, stream>>>(cosmo_dev, ci, tables, nl, dl, S, kt, nkt, B, ls.idx_min,
                                                        ch.A_s, ch.n_s, ls.k_pivot, partial);
     cl_final_kernel<<<1, 256, 0, stream>>>(partial, n_ell_tab, ntile, B, ls.idx_min, ls.l_min, n_out,
-                                           cl_raw + (int64_t)ci * n_ell_tab * 3, cl + (int64_t)ci * 3 * n_out, lscr);
+                                           cl_raw + (int64_t)ci * n_ell_tab * 3, cl + (int64_t)ci * 3 * n_out,
+                                           dcl_dns ? dcl_dns + (int64_t)ci * 3 * n_out : nullptr, lscr);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

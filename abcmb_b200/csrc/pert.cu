@@ -12,12 +12,12 @@
 // Linear algebra: the RHS is linear in y, f = A(lna) y.  The stage root find
 // ("very chord": one Jacobian per step, linearised at the first implicit
 // stage) needs solves with M = I - h*gamma*A(t_lin).  M is not factored
-// densely: every hierarchy's l >= 4 tail is a tridiagonal chain that couples
-// to the rest of the system only through its l = 3 element, so the tails are
+// densely: every hierarchy's l >= 3 tail is a tridiagonal chain that couples
+// to the rest of the system only through its l = 2 element, so the tails are
 // eliminated bottom-up (pivots >= 1: the free-streaming couplings have
 // opposite signs and the damping is non-negative) and fold into one diagonal
 // entry each of a dense "core" block holding eta, delta_c, delta_b, theta_b
-// and l <= 3 of every hierarchy (16 unknowns, 28 with massive neutrinos).
+// and l <= 2 of every hierarchy (13 unknowns, 22 with massive neutrinos).
 // The core is inverted once per step by a warp-parallel Gauss-Jordan with
 // partial pivoting; every chord iteration then costs two chain sweeps and a
 // core mat-vec instead of a dense LU solve.
@@ -26,7 +26,6 @@
 namespace abcmb {
 
 constexpr int WARP = 32;
-constexpr int MAX_CORE = 28;
 constexpr int NCHAIN = 6;            // F, G, N, Psi(q0), Psi(q1), Psi(q2)
 constexpr int NSTART = 10000;        // get_starting_time grid
 
@@ -44,15 +43,19 @@ __constant__ double KV_A[7][6] = {
     {0.13659751177640291, 0.0, -0.05496908796538376, -0.04118626728321046, 0.62993304899016403,
      0.06962479448202728}};
 
+// Scalar layout of one item's state vector (kept in registers; the per-chain
+// arrays live in shared memory, see WarpMem::chs / chL).
 struct Layout {
   int ny, nc, nchain, ntail;
   int i_g, i_G, i_nu, i_ncdm, nM;
-  int ch_start[NCHAIN];   // state index of the l = 4 element
-  int ch_L[NCHAIN];       // l_max of the chain
-  int ch_off[NCHAIN + 1]; // prefix offsets of the tails
+  int lg, lp, lnu, lm;
 };
 
 __device__ __forceinline__ void make_layout(const abcmb_cosmo& c, Layout& L) {
+  L.lg = c.lmax_g;
+  L.lp = c.lmax_pol_g;
+  L.lnu = c.lmax_nu;
+  L.lm = c.lmax_ncdm;
   L.i_g = 4;
   L.i_G = L.i_g + c.lmax_g + 1;
   L.i_nu = L.i_G + c.lmax_pol_g + 1;
@@ -60,85 +63,114 @@ __device__ __forceinline__ void make_layout(const abcmb_cosmo& c, Layout& L) {
   L.nM = c.has_ncdm ? c.lmax_ncdm + 1 : 0;
   L.ny = L.i_ncdm + 3 * L.nM;
   L.nchain = c.has_ncdm ? 6 : 3;
-  L.nc = 4 * (1 + L.nchain);
-  L.ch_start[0] = L.i_g + 4;   L.ch_L[0] = c.lmax_g;
-  L.ch_start[1] = L.i_G + 4;   L.ch_L[1] = c.lmax_pol_g;
-  L.ch_start[2] = L.i_nu + 4;  L.ch_L[2] = c.lmax_nu;
-  for (int b = 0; b < 3; ++b) {
-    L.ch_start[3 + b] = L.i_ncdm + b * L.nM + 4;
-    L.ch_L[3 + b] = c.lmax_ncdm;
+  L.nc = 4 + 3 * L.nchain;
+  L.ntail = (L.lg - 2) + (L.lp - 2) + (L.lnu - 2) + (c.has_ncdm ? 3 * (L.lm - 2) : 0);
+}
+
+// chain ch: state index of its l = 3 element (first tail element), its
+// l_max, its offset in the tail enumeration
+__device__ __forceinline__ void chain_info(const Layout& L, int ch, int& start, int& lmax, int& off) {
+  if (ch == 0) { start = L.i_g + 3; lmax = L.lg; off = 0; }
+  else if (ch == 1) { start = L.i_G + 3; lmax = L.lp; off = L.lg - 2; }
+  else if (ch == 2) { start = L.i_nu + 3; lmax = L.lnu; off = (L.lg - 2) + (L.lp - 2); }
+  else {
+    const int b = ch - 3;
+    start = L.i_ncdm + b * L.nM + 3;
+    lmax = L.lm;
+    off = (L.lg - 2) + (L.lp - 2) + (L.lnu - 2) + b * (L.lm - 2);
   }
-  L.ch_off[0] = 0;
-  for (int ch = 0; ch < NCHAIN; ++ch)
-    L.ch_off[ch + 1] = L.ch_off[ch] + (ch < L.nchain ? L.ch_L[ch] - 3 : 0);
-  L.ntail = L.ch_off[L.nchain];
 }
 
-// state index of core unknown ci (groups of four: [eta,dc,db,thb], F0-3, G0-3, N0-3, Psi_b 0-3)
+// state index of core unknown ci: [eta, dc, db, thb], then l = 0..2 of the
+// chains F, G, N, Psi(q0), Psi(q1), Psi(q2) in groups of three
 __device__ __forceinline__ int core_state(const Layout& L, int ci) {
-  int g = ci >> 2, o = ci & 3;
-  if (g == 0) return o;
-  if (g == 1) return L.i_g + o;
-  if (g == 2) return L.i_G + o;
-  if (g == 3) return L.i_nu + o;
-  return L.i_ncdm + (g - 4) * L.nM + o;
+  if (ci < 4) return ci;
+  const int g = (ci - 4) / 3, o = (ci - 4) % 3;
+  if (g == 0) return L.i_g + o;
+  if (g == 1) return L.i_G + o;
+  if (g == 2) return L.i_nu + o;
+  return L.i_ncdm + (g - 3) * L.nM + o;
 }
 
-// tail element t -> chain, l
-__device__ __forceinline__ void tail_elem(const Layout& L, int t, int& ch, int& l) {
+// core index of chain ch's l = 2 row (the row its tail hangs off)
+__device__ __forceinline__ int chain_core_l2(int ch) { return 4 + 3 * ch + 2; }
+
+// tail slot t -> chain, l, state index, l_max
+__device__ __forceinline__ void tail_elem(const Layout& L, int t, int& ch, int& l, int& e, int& lmax) {
   ch = 0;
-#pragma unroll
-  for (int j = 1; j < NCHAIN; ++j)
-    if (t >= L.ch_off[j]) ch = j;
-  l = 4 + (t - L.ch_off[ch]);
+  int start = 0, off = 0;
+  for (int j = 0; j < L.nchain; ++j) {
+    int s, lm, o;
+    chain_info(L, j, s, lm, o);
+    if (t >= o) { ch = j; start = s; lmax = lm; off = o; }
+  }
+  l = 3 + (t - off);
+  e = start + (l - 3);
 }
 
-// Per-warp shared-memory arrays.
+// Per-warp shared-memory arrays, addressed from one base pointer so that the
+// kernel keeps two registers instead of one pointer per array.
 struct WarpMem {
-  double* y0;     // ny
-  double* y1;     // ny
-  double* F;      // 7 * ny stage derivatives
-  double* base;   // ny
-  double* v;      // ny
-  double* r;      // ny
-  double* tA;     // ny  tail coefficient of v[e-1] (per unit chain speed)
-  double* tG;     // ny  tail coefficient of v[e+1]
-  double* invd;   // ny  tail pivots
-  double* mult;   // ny  upward-sweep multipliers
-  double* sub;    // ny  tail sub-diagonal of M
-  double* Ac;     // ncm * cs   A_core(t) of the current stage
-  double* Mc;     // ncm * cs   (I - h g A_core(t_lin))^-1 after inversion
-  double* wv;     // 2 * ncm    metric functionals w_h, w_eta
-  double* vc;     // ncm        gathered core vector
-  double* ch;     // 4 * NCHAIN chain speed, damping, trunc, M_{3,4} inv_d_4
-  int* perm;      // ncm
-  int ncm, cs;    // core capacity (16 or 28) and row stride
+  double* p;      // base of this warp's region
+  int my, ncm, cs;
+  __device__ __forceinline__ double* y0() const { return p; }                 // ny
+  __device__ __forceinline__ double* y1() const { return p + my; }            // ny
+  __device__ __forceinline__ double* F() const { return p + 2 * my; }         // 7 ny stage derivatives
+  __device__ __forceinline__ double* base() const { return p + 9 * my; }      // ny
+  __device__ __forceinline__ double* v() const { return p + 10 * my; }        // ny
+  __device__ __forceinline__ double* r() const { return p + 11 * my; }        // ny
+  __device__ __forceinline__ double* tA() const { return p + 12 * my; }       // tail coefficient of v[e-1]
+  __device__ __forceinline__ double* tG() const { return p + 13 * my; }       // tail coefficient of v[e+1]
+  __device__ __forceinline__ double* invd() const { return p + 14 * my; }     // tail pivots
+  __device__ __forceinline__ double* mult() const { return p + 15 * my; }     // upward-sweep multipliers
+  __device__ __forceinline__ double* sub() const { return p + 16 * my; }      // tail sub-diagonal of M
+  __device__ __forceinline__ double* Mc() const { return p + 17 * my; }       // ncm x cs core inverse
+  __device__ __forceinline__ double* vc() const { return Mc() + ncm * cs; }   // gathered core vector
+  __device__ __forceinline__ double* SB() const { return vc() + ncm; }        // NSLOT x NB basis
+  __device__ __forceinline__ double* m3() const { return SB() + 6 * 32; }     // M_{3,4} / d_4 per chain
+  __device__ __forceinline__ int* cmap() const { return reinterpret_cast<int*>(m3() + NCHAIN); }
+  __device__ __forceinline__ int* perm() const { return cmap() + ncm; }
+  __device__ __forceinline__ int* rstate() const { return perm() + ncm; }    // 5 ncm
+  __device__ __forceinline__ int* chs() const { return rstate() + 5 * ncm; }  // 8
+  __device__ __forceinline__ int* chL() const { return chs() + 8; }           // 8
+  __device__ __forceinline__ int* tinfo() const { return chL() + 8; }         // max_ny
 };
 
+// Static sparsity of the core rows, shared by the block (filled once).
+constexpr int MAXC = 22;
+struct RowTab {
+  int n[MAXC];
+  int bid[MAXC * 5];
+  int col[MAXC * 5];
+  int tch[MAXC];
+  double cst[MAXC * 5];
+  double uh[MAXC], ue[MAXC], tco[MAXC];
+};
+
+// Background "basis" of one time: every coefficient of A(lna) is a constant
+// times one of these.  Slots: 0 = t0, 1..5 = t0 + c_i h for c = 0.52,
+// 1.2303, 0.8958, 0.4364, 1 (stages 6 and 7 share slot 5).
+constexpr int NB = 32;
+constexpr int NSLOT = 6;
+enum {
+  B_ONE = 0, B_IAH, B_KIAH, B_K2IAH, B_KAP, B_RKAP, B_CS2K2IAH,
+  B_NCDM = 7,        // 3 per bin: q/(eps aH), q k/(eps aH), q k^2/(eps aH)
+  B_TRUNC = 16,      // 1/(aH tau)
+  B_WH = 17,         // 8 weights of h': eta, dc, db, F0, N0, Psi0 x 3
+  B_WE = 25,         // 6 weights of eta': thb, F1, N1, kPsi1 x 3
+};
+__device__ __forceinline__ int chain_speed_bid(int chn) { return chn < 3 ? B_KIAH : B_NCDM + 3 * (chn - 3) + 1; }
+
 __host__ __device__ inline size_t warp_mem_doubles(int max_ny, int ncm) {
-  return (size_t)17 * max_ny + 2 * (size_t)ncm * (ncm + 1) + 3 * ncm + 4 * NCHAIN + ncm / 2 + 2;
+  const size_t ints = (size_t)ncm * 7 + (size_t)max_ny + 16;
+  return (size_t)17 * max_ny + (size_t)ncm * (ncm + 1) + (size_t)ncm + NSLOT * NB + NCHAIN + (ints + 1) / 2;
 }
 
 __device__ __forceinline__ void carve(double* p, int max_ny, int ncm, WarpMem& m) {
+  m.p = p;
+  m.my = max_ny;
   m.ncm = ncm;
   m.cs = ncm + 1;
-  m.y0 = p; p += max_ny;
-  m.y1 = p; p += max_ny;
-  m.F = p; p += 7 * max_ny;
-  m.base = p; p += max_ny;
-  m.v = p; p += max_ny;
-  m.r = p; p += max_ny;
-  m.tA = p; p += max_ny;
-  m.tG = p; p += max_ny;
-  m.invd = p; p += max_ny;
-  m.mult = p; p += max_ny;
-  m.sub = p; p += max_ny;
-  m.Ac = p; p += ncm * m.cs;
-  m.Mc = p; p += ncm * m.cs;
-  m.wv = p; p += 2 * ncm;
-  m.vc = p; p += ncm;
-  m.ch = p; p += 4 * NCHAIN;
-  m.perm = reinterpret_cast<int*>(p);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -148,154 +180,201 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // ---------------------------------------------------------------------------
-// A_core(t) and the chain scalars at one time.  Lane r builds row r.
+// Background basis at one time (one lane per time; abcmb/background.py and
+// species.py evaluators through bg_eval).
 // ---------------------------------------------------------------------------
-__device__ void build_core(const abcmb_cosmo& c, const Layout& L, double k, const BG& b,
-                           WarpMem& m, int lane) {
-  const int nc = L.nc;
-  const double aH = b.aH, tc = b.tau_c;
+__device__ __noinline__ void stage_basis(const abcmb_cosmo& c, const double* __restrict__ tables, double k,
+                                         double lna, double* B) {
+  BG b;
+  bg_eval(c, tables, lna, b);
+  const double aH = b.aH;
   const double iaH = 1. / aH;
-  const double kap = 1. / aH / tc;                         // 1/(aH tau_c)
-  const double Ca2 = 4. * PI * GN * b.a * b.a / (C_MPC * C_MPC);
-  const double whf = 2. / (aH * aH) * Ca2;                  // h' per rho*delta
-  const double wef = Ca2 / aH / (k * k);                    // eta' per (rho+P) theta
+  const double kap = iaH / b.tau_c;                          // 1/(aH tau_c)
+  B[B_ONE] = 1.;
+  B[B_IAH] = iaH;
+  B[B_KIAH] = k * iaH;
+  B[B_K2IAH] = k * k * iaH;
+  B[B_KAP] = kap;
+  B[B_RKAP] = b.R * kap;
+  B[B_CS2K2IAH] = b.cs2 * k * k * iaH;
+  for (int bb = 0; bb < 3; ++bb) {
+    double s = Q3[bb] / b.eps[bb] * iaH;                     // q/(eps aH)
+    B[B_NCDM + 3 * bb] = s;
+    B[B_NCDM + 3 * bb + 1] = s * k;
+    B[B_NCDM + 3 * bb + 2] = s * k * k;
+  }
+  B[B_TRUNC] = iaH / b.tau;
   // metric functionals (perturbations.py:238-239)
-  if (lane < nc) {
-    double wh = 0., we = 0.;
-    int g = lane >> 2, o = lane & 3;
-    if (g == 0) {
-      if (o == 0) wh = 2. / (aH * aH) * k * k;
-      if (o == 1) wh = whf * b.rho_cdm;
-      if (o == 2) wh = whf * b.rho_b;
-      if (o == 3) we = wef * b.rho_b;
-    } else if (g == 1) {
-      if (o == 0) wh = whf * b.rho_g;
-      if (o == 1) we = wef * (b.rho_g + b.rho_g / 3.);
-    } else if (g == 3) {
-      if (o == 0) wh = whf * b.rho_nu;
-      if (o == 1) we = wef * (b.rho_nu + b.rho_nu / 3.);
-    } else if (g >= 4) {
-      int bb = g - 4;
-      double q = Q3[bb], w = W3[bb];
-      if (o == 0) wh = whf * b.ncdm_fac * (w * (1. + exp(-q)) * b.eps[bb] / (q * q));
-      if (o == 1) we = wef * b.ncdm_fac * (w * (1. + exp(-q)) / q);
-    }
-    m.wv[lane] = wh;
-    m.wv[m.ncm + lane] = we;
+  const double Ca2 = 4. * PI * GN * b.a * b.a / (C_MPC * C_MPC);
+  const double whf = 2. * iaH * iaH * Ca2;
+  const double wef = Ca2 * iaH / (k * k);
+  B[B_WH + 0] = 2. * iaH * iaH * k * k;
+  B[B_WH + 1] = whf * b.rho_cdm;
+  B[B_WH + 2] = whf * b.rho_b;
+  B[B_WH + 3] = whf * b.rho_g;
+  B[B_WH + 4] = whf * b.rho_nu;
+  B[B_WE + 0] = wef * b.rho_b;
+  B[B_WE + 1] = wef * (b.rho_g + b.rho_g / 3.);
+  B[B_WE + 2] = wef * (b.rho_nu + b.rho_nu / 3.);
+  for (int bb = 0; bb < 3; ++bb) {
+    double q = Q3[bb], w = W3[bb];
+    double g = w * (1. + exp(-q));
+    B[B_WH + 5 + bb] = whf * b.ncdm_fac * (g * b.eps[bb] / (q * q));
+    B[B_WE + 3 + bb] = wef * b.ncdm_fac * (g / q);
   }
-  // chain scalars: speed s, damping, truncation 1/(aH tau)
-  if (lane < L.nchain) {
-    double s, d;
-    if (lane == 0 || lane == 1) { s = k * iaH; d = kap; }
-    else if (lane == 2) { s = k * iaH; d = 0.; }
-    else { s = Q3[lane - 3] * k / b.eps[lane - 3] * iaH; d = 0.; }
-    m.ch[lane] = s;
-    m.ch[NCHAIN + lane] = d;
-  }
-  if (lane == 0) m.ch[2 * NCHAIN] = 1. / aH / b.tau;
-  __syncwarp();
-  if (lane < nc) {
-    double* row = m.Ac + lane * m.cs;
-    double uh = 0., ue = 0.;
-    int g = lane >> 2, o = lane & 3;
-    for (int j = 0; j < nc; ++j) row[j] = 0.;
-    const double k2 = k * k;
-    if (g == 0) {
-      if (o == 0) ue = 1.;
-      if (o == 1) uh = -0.5;
-      if (o == 2) { uh = -0.5; row[3] = -iaH; }
-      if (o == 3) { row[3] = -1. - b.R * kap; row[2] = b.cs2 * k2 * iaH; row[5] = b.R * kap; }
-    } else if (g == 1) {            // photon temperature F0..F3
-      if (o == 0) { uh = -2. / 3.; row[5] = -4. / 3. * iaH; }
-      if (o == 1) { row[4] = k2 / 4. * iaH; row[6] = -k2 * iaH; row[3] = kap; row[5] = -kap; }
-      if (o == 2) {
-        uh = 2. / 15.; ue = 4. / 5.;
-        row[5] = 4. / 15. * iaH; row[7] = -3. / 10. * k * iaH; row[6] = -9. / 10. * kap;
-        row[8] = kap / 20.; row[10] = kap / 20.;
-      }
-      if (o == 3) { row[6] = 6. / 7. * k * iaH; row[7] = -kap; }
-    } else if (g == 2) {            // photon polarisation G0..G3
-      if (o == 0) { row[9] = -k * iaH; row[8] = -kap + kap / 2.; row[6] = kap; row[10] = kap / 2.; }
-      if (o == 1) { row[8] = k / 3. * iaH; row[10] = -2. * k / 3. * iaH; row[9] = -kap; }
-      if (o == 2) {
-        row[9] = 2. * k / 5. * iaH; row[11] = -3. * k / 5. * iaH; row[10] = -kap + 0.2 * kap / 2.;
-        row[6] = 0.2 * kap; row[8] = 0.2 * kap / 2.;
-      }
-      if (o == 3) { row[10] = 3. * k / 7. * iaH; row[11] = -kap; }
-    } else if (g == 3) {            // massless neutrinos N0..N3
-      if (o == 0) { uh = -2. / 3.; row[13] = -4. / 3. * iaH; }
-      if (o == 1) { row[12] = k2 / 4. * iaH; row[14] = -k2 * iaH; }
-      if (o == 2) { uh = 2. / 15.; ue = 4. / 5.; row[13] = 4. / 15. * iaH; row[15] = -3. / 10. * k * iaH; }
-      if (o == 3) { row[14] = 6. / 7. * k * iaH; }
-    } else {                        // massive neutrino q-bin Psi0..Psi3
-      int bb = g - 4, i0 = 4 * g;
-      double q = Q3[bb], eps = b.eps[bb];
-      double dl = -q / (1. + exp(-q));
-      if (o == 0) { uh = dl / 6.; row[i0 + 1] = -q / eps * iaH; }
-      if (o == 1) { row[i0 + 0] = q * k2 / 3. / eps * iaH; row[i0 + 2] = -2. * q * k2 / 3. / eps * iaH; }
-      if (o == 2) {
-        uh = -dl / 15.; ue = -2. / 5. * dl;
-        row[i0 + 1] = 2. * q / 5. / eps * iaH; row[i0 + 3] = -3. * q * k / 5. / eps * iaH;
-      }
-      if (o == 3) { row[i0 + 2] = 3. * q * k / 7. / eps * iaH; }
-    }
-    if (uh != 0. || ue != 0.)
-      for (int j = 0; j < nc; ++j) row[j] += uh * m.wv[j] + ue * m.wv[m.ncm + j];
-  }
-  __syncwarp();
+  B[31] = 0.;
 }
 
-// f = A(t) v, written to out (core rows by lanes < nc, tails round robin).
-// Requires build_core for t.  v, out in shared memory; out may alias nothing.
-__device__ void apply_A(const Layout& L, const WarpMem& m, const double* v, double* out, int lane) {
-  const int nc = L.nc;
-  if (lane < nc) m.vc[lane] = v[core_state(L, lane)];
-  __syncwarp();
-  if (lane < nc) {
-    const double* row = m.Ac + lane * m.cs;
-    double acc = 0.;
-    for (int j = 0; j < nc; ++j) acc = fma(row[j], m.vc[j], acc);
-    int g = lane >> 2;
-    if ((lane & 3) == 3 && g >= 1) {      // l = 3 row couples to the chain's l = 4
-      int chn = g - 1;
-      acc += -4. / 7. * m.ch[chn] * v[L.ch_start[chn]];
+// Sparse description of one core row of A: up to five terms
+// cst * basis[bid] * y[col] plus the metric terms uh * h' + ue * eta' and,
+// for the l = 2 row of a hierarchy, the coupling tcoef * speed * y[l = 3].
+struct RowDesc {
+  int n;
+  int col[5];      // core index
+  int bid[5];
+  double cst[5];
+  double uh, ue;
+  int tchain;      // chain whose tail hangs off this (l = 2) row, or -1
+  double tcoef;    // coefficient of that tail's l = 3 element, per unit chain speed
+};
+
+// Core rows (core indices: 0 eta, 1 dc, 2 db, 3 thb, 4-6 F0-2, 7-9 G0-2,
+// 10-12 N0-2, 13+3b..15+3b Psi0-2 of q-bin b).
+__device__ __noinline__ void make_row(int r, RowDesc& d) {
+  d.n = 0;
+  d.uh = 0.;
+  d.ue = 0.;
+  d.tchain = -1;
+  d.tcoef = 0.;
+  auto add = [&](int col, int bid, double cst) {
+    d.col[d.n] = col;
+    d.bid[d.n] = bid;
+    d.cst[d.n] = cst;
+    ++d.n;
+  };
+  if (r < 4) {
+    if (r == 0) d.ue = 1.;                                        // eta' (perturbations.py:239)
+    if (r == 1) d.uh = -0.5;                                      // CDM (species.py:607)
+    if (r == 2) { d.uh = -0.5; add(3, B_IAH, -1.); }              // Baryon (species.py:1282)
+    if (r == 3) {                                                 // species.py:1283
+      add(3, B_ONE, -1.); add(3, B_RKAP, -1.); add(2, B_CS2K2IAH, 1.); add(5, B_RKAP, 1.);
     }
-    out[core_state(L, lane)] = acc;
+    return;
   }
-  const double trunc = m.ch[2 * NCHAIN];
+  const int g = (r - 4) / 3, o = (r - 4) % 3;
+  if (g == 0) {                                                   // Photon F (species.py:1432-1434)
+    if (o == 0) { d.uh = -2. / 3.; add(5, B_IAH, -4. / 3.); }
+    if (o == 1) { add(4, B_K2IAH, 0.25); add(6, B_K2IAH, -1.); add(3, B_KAP, 1.); add(5, B_KAP, -1.); }
+    if (o == 2) {
+      d.uh = 2. / 15.; d.ue = 4. / 5.;
+      add(5, B_IAH, 4. / 15.); add(6, B_KAP, -9. / 10.); add(7, B_KAP, 1. / 20.); add(9, B_KAP, 1. / 20.);
+      d.tchain = 0; d.tcoef = -3. / 10.;
+    }
+  } else if (g == 1) {                                            // Photon G (species.py:1443-1445)
+    if (o == 0) { add(8, B_KIAH, -1.); add(7, B_KAP, -0.5); add(6, B_KAP, 1.); add(9, B_KAP, 0.5); }
+    if (o == 1) { add(7, B_KIAH, 1. / 3.); add(9, B_KIAH, -2. / 3.); add(8, B_KAP, -1.); }
+    if (o == 2) {
+      add(8, B_KIAH, 2. / 5.); add(9, B_KAP, -0.9); add(6, B_KAP, 0.2); add(7, B_KAP, 0.1);
+      d.tchain = 1; d.tcoef = -3. / 5.;
+    }
+  } else if (g == 2) {                                            // MasslessNeutrino (species.py:742-744)
+    if (o == 0) { d.uh = -2. / 3.; add(11, B_IAH, -4. / 3.); }
+    if (o == 1) { add(10, B_K2IAH, 0.25); add(12, B_K2IAH, -1.); }
+    if (o == 2) { d.uh = 2. / 15.; d.ue = 4. / 5.; add(11, B_IAH, 4. / 15.); d.tchain = 2; d.tcoef = -3. / 10.; }
+  } else {                                                        // MassiveNeutrino (species.py:962-964)
+    const int bb = g - 3, i0 = 13 + 3 * bb, bs = B_NCDM + 3 * bb;
+    const double q = Q3[bb];
+    const double dl = -q / (1. + exp(-q));
+    if (o == 0) { d.uh = dl / 6.; add(i0 + 1, bs, -1.); }
+    if (o == 1) { add(i0 + 0, bs + 2, 1. / 3.); add(i0 + 2, bs + 2, -2. / 3.); }
+    if (o == 2) {
+      d.uh = -dl / 15.; d.ue = -2. / 5. * dl; add(i0 + 1, bs, 2. / 5.);
+      d.tchain = 3 + bb; d.tcoef = -3. / 5.;
+    }
+  }
+}
+
+// h' and eta' of the state v (perturbations.py:238-239) with basis B.
+__device__ __forceinline__ void metric(const Layout& L, const double* B, const double* v, bool ncdm, double& hp,
+                                       double& etap) {
+  hp = B[B_WH] * v[0] + B[B_WH + 1] * v[1] + B[B_WH + 2] * v[2] + B[B_WH + 3] * v[L.i_g] + B[B_WH + 4] * v[L.i_nu];
+  etap = B[B_WE] * v[3] + B[B_WE + 1] * v[L.i_g + 1] + B[B_WE + 2] * v[L.i_nu + 1];
+  if (ncdm) {
+    for (int bb = 0; bb < 3; ++bb) {
+      hp += B[B_WH + 5 + bb] * v[L.i_ncdm + bb * L.nM];
+      etap += B[B_WE + 3 + bb] * v[L.i_ncdm + bb * L.nM + 1];
+    }
+  }
+}
+
+// out = A(t) v for the time whose basis is B (get_derivatives, perturbations.py:201-248).
+__device__ void apply_A(const Layout& L, const WarpMem& m, const RowTab& R, const double* B, const double* v,
+                        double* out, bool ncdm, int lane) {
+  double hp, etap;
+  metric(L, B, v, ncdm, hp, etap);
+  if (lane < L.nc) {
+    double acc = R.uh[lane] * hp + R.ue[lane] * etap;
+    const int nt = R.n[lane];
+#pragma unroll
+    for (int t = 0; t < 5; ++t)
+      if (t < nt) acc = fma(R.cst[lane * 5 + t] * B[R.bid[lane * 5 + t]], v[m.rstate()[lane * 5 + t]], acc);
+    const int tc = R.tch[lane];
+    if (tc >= 0) acc = fma(R.tco[lane] * B[chain_speed_bid(tc)], v[m.chs()[tc]], acc);
+    out[m.cmap()[lane]] = acc;
+  }
+  const double trunc = B[B_TRUNC];
   for (int t = lane; t < L.ntail; t += WARP) {
-    int chn, l;
-    tail_elem(L, t, chn, l);
-    int e = L.ch_start[chn] + (l - 4);
-    double s = m.ch[chn], d = m.ch[NCHAIN + chn];
-    int Lc = L.ch_L[chn];
+    const int info = m.tinfo()[t];
+    const int e = info & 0xFFF, chn = (info >> 12) & 7;
+    const double s = B[chain_speed_bid(chn)];
+    const double d = chn < 2 ? B[B_KAP] : 0.;
     double fv;
-    if (l == Lc) fv = s * v[e - 1] - (d + (double)(Lc + 1) * trunc) * v[e];
-    else fv = s * (m.tA[e] * v[e - 1] - m.tG[e] * v[e + 1]) - d * v[e];
+    if (info >> 15) fv = s * v[e - 1] - (d + (double)(m.chL()[chn] + 1) * trunc) * v[e];
+    else fv = s * (m.tA()[e] * v[e - 1] - m.tG()[e] * v[e + 1]) - d * v[e];
     out[e] = fv;
   }
   __syncwarp();
 }
 
-// Factor M = I - hg A(t_lin): tails (lanes < nchain) then the core inverse.
-__device__ void factor_newton(const Layout& L, WarpMem& m, double hg, int lane) {
+// Factor M = I - hg A(t_lin) (basis B): tails bottom-up, then the core inverse.
+__device__ void factor_newton(const Layout& L, WarpMem& m, const RowTab& R, const double* B, double hg,
+                              bool ncdm, int lane) {
   const int nc = L.nc;
-  // M_core = I - hg A_core
+  const int CS = m.cs;
   if (lane < nc) {
-    double* row = m.Mc + lane * m.cs;
-    const double* arow = m.Ac + lane * m.cs;
-    for (int j = 0; j < nc; ++j) row[j] = (j == lane ? 1. : 0.) - hg * arow[j];
+    double* row = m.Mc() + lane * CS;
+    for (int j = 0; j < nc; ++j) row[j] = 0.;
+    const int nt = R.n[lane];
+#pragma unroll
+    for (int t = 0; t < 5; ++t)
+      if (t < nt) row[R.col[lane * 5 + t]] -= hg * R.cst[lane * 5 + t] * B[R.bid[lane * 5 + t]];
+    const double ruh = R.uh[lane], rue = R.ue[lane];
+    // metric columns (core indices): h' <- eta, dc, db, F0, N0, Psi0_b ; eta' <- thb, F1, N1, kPsi1_b
+    if (ruh != 0.) {
+      const double u = hg * ruh;
+      row[0] -= u * B[B_WH]; row[1] -= u * B[B_WH + 1]; row[2] -= u * B[B_WH + 2];
+      row[4] -= u * B[B_WH + 3]; row[10] -= u * B[B_WH + 4];
+      if (ncdm) for (int bb = 0; bb < 3; ++bb) row[13 + 3 * bb] -= u * B[B_WH + 5 + bb];
+    }
+    if (rue != 0.) {
+      const double u = hg * rue;
+      row[3] -= u * B[B_WE]; row[5] -= u * B[B_WE + 1]; row[11] -= u * B[B_WE + 2];
+      if (ncdm) for (int bb = 0; bb < 3; ++bb) row[14 + 3 * bb] -= u * B[B_WE + 3 + bb];
+    }
+    row[lane] += 1.;
   }
   __syncwarp();
-  const double trunc = m.ch[2 * NCHAIN];
+  const double trunc = B[B_TRUNC];
   if (lane < L.nchain) {
+    // tail l = 3..L_c eliminated bottom-up; pivots stay >= 1
     const int chn = lane;
-    const double s = m.ch[chn], d = m.ch[NCHAIN + chn];
-    const int Lc = L.ch_L[chn];
-    const int e4 = L.ch_start[chn];
+    const double s = B[chain_speed_bid(chn)];
+    const double d = chn < 2 ? B[B_KAP] : 0.;
+    const int Lc = m.chL()[chn];
+    const int e3 = m.chs()[chn];
     double inv_next = 0., sub_next = 0.;
-    for (int l = Lc; l >= 4; --l) {
-      int e = e4 + (l - 4);
+    for (int l = Lc; l >= 3; --l) {
+      int e = e3 + (l - 3);
       double diag, sup, sb;
       if (l == Lc) {
         diag = 1. + hg * (d + (double)(Lc + 1) * trunc);
@@ -303,50 +382,46 @@ __device__ void factor_newton(const Layout& L, WarpMem& m, double hg, int lane) 
         sb = -hg * s;
       } else {
         diag = 1. + hg * d;
-        sup = hg * s * m.tG[e];
-        sb = -hg * s * m.tA[e];
+        sup = hg * s * m.tG()[e];
+        sb = -hg * s * m.tA()[e];
       }
-      double dd = diag - sup * sub_next * inv_next;
-      double inv = 1. / dd;
-      m.invd[e] = inv;
-      m.mult[e] = sup * inv_next;
-      m.sub[e] = sb;
+      double inv = 1. / (diag - sup * sub_next * inv_next);
+      m.invd()[e] = inv;
+      m.mult()[e] = sup * inv_next;
+      m.sub()[e] = sb;
       inv_next = inv;
       sub_next = sb;
     }
-    // fold the tail into the l = 3 diagonal entry of the core
-    const double M34 = hg * (4. / 7.) * s;
-    const int cc = 4 * (chn + 1) + 3;
-    m.Mc[cc * m.cs + cc] -= M34 * sub_next * inv_next;
-    m.ch[3 * NCHAIN + chn] = M34 * inv_next;
+    // fold the tail into the l = 2 diagonal entry of the core
+    const int cc = chain_core_l2(chn);
+    const double M23 = -hg * R.tco[cc] * s;
+    m.Mc()[cc * CS + cc] -= M23 * sub_next * inv_next;
+    m.m3()[chn] = M23 * inv_next;
   }
   __syncwarp();
   // in-place Gauss-Jordan inverse of the core with partial (row) pivoting
-  const int CS = m.cs;
   for (int p = 0; p < nc; ++p) {
-    double val = (lane >= p && lane < nc) ? fabs(m.Mc[lane * CS + p]) : -1.;
-    int idx = lane;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      double ov = __shfl_xor_sync(0xffffffffu, val, o);
-      int oi = __shfl_xor_sync(0xffffffffu, idx, o);
-      if (ov > val || (ov == val && oi < idx)) { val = ov; idx = oi; }
-    }
-    const int q = idx;
-    if (lane == 0) m.perm[p] = q;
+    // pivot = row p..nc-1 of largest |M[.][p]|, compared on the high 32 bits
+    // of the IEEE representation (monotonic in magnitude; ties -> lowest row)
+    const bool elig = lane >= p && lane < nc;
+    const unsigned key = elig ? (unsigned)(__double_as_longlong(fabs(m.Mc()[lane * CS + p])) >> 32) : 0u;
+    const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
+    const unsigned hit = __ballot_sync(0xffffffffu, elig && key == kmax);
+    const int q = hit ? __ffs(hit) - 1 : p;
+    if (lane == 0) m.perm()[p] = q;
     if (q != p && lane < nc) {
-      double a = m.Mc[p * CS + lane], bq = m.Mc[q * CS + lane];
-      m.Mc[p * CS + lane] = bq;
-      m.Mc[q * CS + lane] = a;
+      double a = m.Mc()[p * CS + lane], bq = m.Mc()[q * CS + lane];
+      m.Mc()[p * CS + lane] = bq;
+      m.Mc()[q * CS + lane] = a;
     }
     __syncwarp();
-    const double pinv = 1. / m.Mc[p * CS + p];
+    const double pinv = 1. / m.Mc()[p * CS + p];
     __syncwarp();
-    if (lane < nc) m.Mc[p * CS + lane] = (lane == p ? 1. : m.Mc[p * CS + lane]) * pinv;
+    if (lane < nc) m.Mc()[p * CS + lane] = (lane == p ? 1. : m.Mc()[p * CS + lane]) * pinv;
     __syncwarp();
     if (lane < nc && lane != p) {
-      double* row = m.Mc + lane * CS;
-      const double* prow = m.Mc + p * CS;
+      double* row = m.Mc() + lane * CS;
+      const double* prow = m.Mc() + p * CS;
       double f = row[p];
       row[p] = 0.;
       for (int j = 0; j < nc; ++j) row[j] = fma(-f, prow[j], row[j]);
@@ -354,9 +429,9 @@ __device__ void factor_newton(const Layout& L, WarpMem& m, double hg, int lane) 
     __syncwarp();
   }
   for (int p = nc - 1; p >= 0; --p) {
-    int q = m.perm[p];
+    int q = m.perm()[p];
     if (q != p && lane < nc) {
-      double* row = m.Mc + lane * CS;
+      double* row = m.Mc() + lane * CS;
       double a = row[p];
       row[p] = row[q];
       row[q] = a;
@@ -368,48 +443,64 @@ __device__ void factor_newton(const Layout& L, WarpMem& m, double hg, int lane) 
 // Solve M x = r in place (r holds the right-hand side on entry).
 __device__ void solve_newton(const Layout& L, WarpMem& m, double* r, int lane) {
   const int nc = L.nc;
-  // upward sweeps of the tails; the l = 3 right-hand side picks up the tail
+  // upward sweeps of the tails (l = L-1 .. 3); the l = 2 right-hand side
+  // picks up the tail.  Two elements per trip so the loads run ahead.
+  const double* mult = m.mult();
   if (lane < L.nchain) {
     const int chn = lane;
-    const int e4 = L.ch_start[chn];
-    const int Lc = L.ch_L[chn];
-    double nxt = r[e4 + (Lc - 4)];
-    for (int l = Lc - 1; l >= 4; --l) {
-      int e = e4 + (l - 4);
-      double val = r[e] - m.mult[e] * nxt;
-      r[e] = val;
-      nxt = val;
+    const int e3 = m.chs()[chn];
+    int e = e3 + (m.chL()[chn] - 3);
+    double nxt = r[e];
+    --e;
+    for (; e - 1 >= e3; e -= 2) {
+      const double ra = r[e], ma = mult[e], rb = r[e - 1], mb = mult[e - 1];
+      const double va = ra - ma * nxt;
+      const double vb = rb - mb * va;
+      r[e] = va;
+      r[e - 1] = vb;
+      nxt = vb;
     }
-    const int cc = 4 * (chn + 1) + 3;
-    m.vc[cc] = r[core_state(L, cc)] - m.ch[3 * NCHAIN + chn] * nxt;
+    if (e >= e3) {
+      nxt = r[e] - mult[e] * nxt;
+      r[e] = nxt;
+    }
+    const int cc = chain_core_l2(chn);
+    m.vc()[cc] = r[m.cmap()[cc]] - m.m3()[chn] * nxt;
   }
-  if (lane < nc && !((lane & 3) == 3 && (lane >> 2) >= 1)) m.vc[lane] = r[core_state(L, lane)];
+  // every other core row gathers its right-hand side directly
+  if (lane < nc && !(lane >= 4 && (lane - 4) % 3 == 2)) m.vc()[lane] = r[m.cmap()[lane]];
   __syncwarp();
   double xc = 0.;
   if (lane < nc) {
-    const double* row = m.Mc + lane * m.cs;
-    for (int j = 0; j < nc; ++j) xc = fma(row[j], m.vc[j], xc);
+    const double* row = m.Mc() + lane * m.cs;
+    for (int j = 0; j < nc; ++j) xc = fma(row[j], m.vc()[j], xc);
   }
   __syncwarp();
-  if (lane < nc) r[core_state(L, lane)] = xc;
+  if (lane < nc) r[m.cmap()[lane]] = xc;
   __syncwarp();
   if (lane < L.nchain) {
+    const double* sub = m.sub();
+    const double* invd = m.invd();
     const int chn = lane;
-    const int e4 = L.ch_start[chn];
-    const int Lc = L.ch_L[chn];
-    double prev = r[e4 - 1];
-    for (int l = 4; l <= Lc; ++l) {
-      int e = e4 + (l - 4);
-      double x = (r[e] - m.sub[e] * prev) * m.invd[e];
-      r[e] = x;
-      prev = x;
+    const int e3 = m.chs()[chn];
+    const int eL = e3 + (m.chL()[chn] - 3);
+    double prev = r[e3 - 1];
+    int e = e3;
+    for (; e + 1 <= eL; e += 2) {
+      const double ra = r[e], sa = sub[e], ia = invd[e], rb = r[e + 1], sb = sub[e + 1], ib = invd[e + 1];
+      const double xa = (ra - sa * prev) * ia;
+      const double xb = (rb - sb * xa) * ib;
+      r[e] = xa;
+      r[e + 1] = xb;
+      prev = xb;
     }
+    if (e <= eL) r[e] = (r[e] - sub[e] * prev) * invd[e];
   }
   __syncwarp();
 }
 
 // Fields of make_output_table at one save point from the interpolated state ys.
-__device__ void write_fields(const abcmb_cosmo& c, const Layout& L, const double* tables, double k, double lna,
+__device__ __noinline__ void write_fields(const abcmb_cosmo& c, const Layout& L, const double* tables, double k, double lna,
                              const double* ys, double* pt, int n_save, int isave, int ik, int lane) {
   BG b;
   bg_eval(c, tables, lna, b);
@@ -533,10 +624,30 @@ struct PertArgs {
   abcmb_pert_settings s;
 };
 
-__global__ void __launch_bounds__(128) pert_kernel(PertArgs P) {
+#ifndef PERT_MIN_BLOCKS
+#define PERT_MIN_BLOCKS 3   // 168 registers: faster than 128 + spills (measured on C1, C2, C4)
+#endif
+__global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) {
   extern __shared__ double smem[];
+  __shared__ RowTab R;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
+  if (threadIdx.x < MAXC) {
+    RowDesc d;
+    make_row(threadIdx.x, d);
+    const int r = threadIdx.x;
+    R.n[r] = d.n;
+    R.tch[r] = d.tchain;
+    R.tco[r] = d.tcoef;
+    R.uh[r] = d.uh;
+    R.ue[r] = d.ue;
+    for (int t = 0; t < 5; ++t) {
+      R.bid[r * 5 + t] = t < d.n ? d.bid[t] : 0;
+      R.col[r * 5 + t] = t < d.n ? d.col[t] : 0;
+      R.cst[r * 5 + t] = t < d.n ? d.cst[t] : 0.;
+    }
+  }
+  __syncthreads();
   WarpMem m;
   carve(smem + (size_t)wib * warp_mem_doubles(P.max_ny, P.ncm), P.max_ny, P.ncm, m);
   const abcmb_pert_settings& S = P.s;
@@ -557,6 +668,7 @@ __global__ void __launch_bounds__(128) pert_kernel(PertArgs P) {
     Layout L;
     make_layout(c, L);
     const int n = L.ny;
+    const bool ncdm = c.has_ncdm != 0;
     const double k = P.kbuf[c.off_k + ik];
     const double rtol = k > S.k_split ? S.rtol_large : S.rtol_small;
     const double atol = k > S.k_split ? S.atol_large : S.atol_small;
@@ -564,50 +676,64 @@ __global__ void __launch_bounds__(128) pert_kernel(PertArgs P) {
     const double lts = c.lna_transfer_start;
 
     // start time (perturbations.py:274-279)
-    double lna2 = np_interp_lna(S.R_large, nullptr, P.aHg + (int64_t)ci * NSTART, k);
-    double lna_start = fmin(fmin(P.lna1[ci], lna2), -10.);
+    const double lna2 = np_interp_lna(S.R_large, nullptr, P.aHg + (int64_t)ci * NSTART, k);
+    const double lna_start = fmin(fmin(P.lna1[ci], lna2), -10.);
 
-    // tail coefficients
+    // per-item structure: tail coefficients, core map, this lane's core row
     for (int t = lane; t < L.ntail; t += WARP) {
-      int chn, l;
-      tail_elem(L, t, chn, l);
-      int e = L.ch_start[chn] + (l - 4);
-      m.tA[e] = (double)l / (2. * l + 1.);
-      m.tG[e] = (double)(l + 1) / (2. * l + 1.);
+      int chn, l, e, lmax = 0;
+      tail_elem(L, t, chn, l, e, lmax);
+      // F3' and N3' carry 6/7 on their l = 2 slot (which holds sigma = F_2 / 2;
+      // species.py:745 and 1435); every other l uses l / (2l + 1)
+      m.tA()[e] = (l == 3 && (chn == 0 || chn == 2)) ? 6. / 7. : (double)l / (2. * l + 1.);
+      m.tG()[e] = (double)(l + 1) / (2. * l + 1.);
+      m.tinfo()[t] = e | (chn << 12) | ((l == lmax) ? (1 << 15) : 0);
+    }
+    if (lane < NCHAIN) {
+      int s, lm, o;
+      chain_info(L, lane, s, lm, o);
+      m.chs()[lane] = s;
+      m.chL()[lane] = lm;
+    }
+    if (lane < L.nc) {
+      m.cmap()[lane] = core_state(L, lane);
+#pragma unroll
+      for (int t = 0; t < 5; ++t) m.rstate()[lane * 5 + t] = core_state(L, t < R.n[lane] ? R.col[lane * 5 + t] : 0);
     }
     // initial conditions (perturbations.py:161-199 + species y_ini)
-    for (int e = lane; e < n; e += WARP) m.y0[e] = 0.;
+    for (int e = lane; e < n; e += WARP) m.y0()[e] = 0.;
     __syncwarp();
     if (lane == 0) {
       const double tau_ini = tau_of(c, P.tables, lna_start);
       const double om = c.om, Rn = c.R_nu, Rb = c.R_b;
       const double kt = k * tau_ini;
-      m.y0[0] = (1. - k * k * tau_ini * tau_ini / 12. / (15. + 4. * Rn) *
+      m.y0()[0] = (1. - k * k * tau_ini * tau_ini / 12. / (15. + 4. * Rn) *
                           (5. + 4. * Rn - (16. * Rn * Rn + 280. * Rn + 325) / 10. / (2. * Rn + 15.) * tau_ini * om));
-      m.y0[1] = -(kt * kt) / 4. * (1. - om * tau_ini / 5.);
-      m.y0[2] = -(kt * kt) / 4. * (1. - om * tau_ini / 5.);
+      m.y0()[1] = -(kt * kt) / 4. * (1. - om * tau_ini / 5.);
+      m.y0()[2] = -(kt * kt) / 4. * (1. - om * tau_ini / 5.);
       const double thb = -k * k * k * k * tau_ini * tau_ini * tau_ini / 36. *
                          (1. - 3. * (1. + 5. * Rb - Rn) / 20. / (1. - Rn) * om * tau_ini);
-      m.y0[3] = thb;
-      m.y0[L.i_g] = -(kt * kt) / 3. * (1. - om * tau_ini / 5.);
-      m.y0[L.i_g + 1] = thb;
+      m.y0()[3] = thb;
+      m.y0()[L.i_g] = -(kt * kt) / 3. * (1. - om * tau_ini / 5.);
+      m.y0()[L.i_g + 1] = thb;
       const double nd = -(kt * kt) / 3. * (1. - om * tau_ini / 5.);
       const double nth = -k * (kt * kt * kt) / 36. / (4. * Rn + 15.) *
                          (4. * Rn + 11. + 12. - 3. * (8. * Rn * Rn + 50. * Rn + 275.) / 20. / (2. * Rn + 15.) * tau_ini * om);
       const double ns = (kt * kt) / (45. + 12. * Rn) * 2. * (1. + (4. * Rn - 5.) / 4. / (2. * Rn + 15.) * tau_ini * om);
-      m.y0[L.i_nu] = nd;
-      m.y0[L.i_nu + 1] = nth;
-      m.y0[L.i_nu + 2] = ns;
-      if (c.has_ncdm) {
+      m.y0()[L.i_nu] = nd;
+      m.y0()[L.i_nu + 1] = nth;
+      m.y0()[L.i_nu + 2] = ns;
+      if (ncdm) {
         for (int i = 0; i < 3; ++i) {
           double q = Q3[i];
           double fac = q / (1. + exp(-q));
-          double* Pb = m.y0 + L.i_ncdm + i * L.nM;
+          double* Pb = m.y0() + L.i_ncdm + i * L.nM;
           Pb[0] = nd / 4. * fac;
           Pb[1] = nth / 3. * fac;
           Pb[2] = ns / 2. * fac;
         }
       }
+      stage_basis(c, P.tables, k, lna_start, m.SB());
     }
     __syncwarp();
 
@@ -615,44 +741,40 @@ __global__ void __launch_bounds__(128) pert_kernel(PertArgs P) {
     double t1 = fmin(t0 + S.dt0, 0.0);
     double prev_inv = 1.0, prev_prev_inv = 1.0;
     int isave = 0, nsteps = 0, nacc = 0, nrej = 0, nnewton = 0, status = ABCMB_STATUS_OK;
-    BG b;
-    bg_eval(c, P.tables, t0, b);
-    build_core(c, L, k, b, m, lane);
-    apply_A(L, m, m.y0, m.F, lane);         // FSAL stage 1
+    apply_A(L, m, R, m.SB(), m.y0(), m.F(), ncdm, lane);         // FSAL stage 1
 
     while (t0 < 0.0) {
       if (nsteps >= S.max_steps) { status = ABCMB_STATUS_MAX_STEPS; break; }
       ++nsteps;
       const double h = t1 - t0;
       const double hg = h * KV_G;
+      // background of the five distinct stage times, one lane each
+      if (lane < NSLOT - 1) stage_basis(c, P.tables, k, t0 + KV_C[lane + 1] * h, m.SB() + (lane + 1) * NB);
+      __syncwarp();
+      factor_newton(L, m, R, m.SB() + NB, hg, ncdm, lane);
       bool ok = true;
       for (int i = 1; i < 7 && ok; ++i) {
-        const double ti = t0 + KV_C[i] * h;
-        if (i != 6) {                  // stages 6 and 7 share t0 + h
-          bg_eval(c, P.tables, ti, b);
-          build_core(c, L, k, b, m, lane);
-        }
-        if (i == 1) factor_newton(L, m, hg, lane);
-        double* fi = m.F + i * n;
+        const double* B = m.SB() + (i == 6 ? 5 : i) * NB;
+        double* fi = m.F() + i * n;
         for (int e = lane; e < n; e += WARP) {
           double acc = 0.;
-          for (int j = 0; j < i; ++j) acc = fma(KV_A[i][j], m.F[j * n + e], acc);
-          m.base[e] = m.y0[e] + h * acc;
-          fi[e] = m.F[(i - 1) * n + e];
+          for (int j = 0; j < i; ++j) acc = fma(KV_A[i][j], m.F()[j * n + e], acc);
+          m.base()[e] = m.y0()[e] + h * acc;
+          fi[e] = m.F()[(i - 1) * n + e];
         }
         __syncwarp();
         double diffsize = INFINITY, diffsize_prev;
         bool conv = false;
         for (int it = 1; it <= root_max; ++it) {
-          for (int e = lane; e < n; e += WARP) m.v[e] = m.base[e] + hg * fi[e];
+          for (int e = lane; e < n; e += WARP) m.v()[e] = m.base()[e] + hg * fi[e];
           __syncwarp();
-          apply_A(L, m, m.v, m.r, lane);
-          for (int e = lane; e < n; e += WARP) m.r[e] = m.r[e] - fi[e];
+          apply_A(L, m, R, B, m.v(), m.r(), ncdm, lane);
+          for (int e = lane; e < n; e += WARP) m.r()[e] = m.r()[e] - fi[e];
           __syncwarp();
-          solve_newton(L, m, m.r, lane);
+          solve_newton(L, m, m.r(), lane);
           double ss = 0.;
           for (int e = lane; e < n; e += WARP) {
-            double x = m.r[e];
+            double x = m.r()[e];
             double fnew = fi[e] + x;
             fi[e] = fnew;
             double q = x / (atol + rtol * fabs(fnew));
@@ -682,15 +804,15 @@ __global__ void __launch_bounds__(128) pert_kernel(PertArgs P) {
           double acc = 0., acce = 0.;
 #pragma unroll
           for (int j = 0; j < 6; ++j) {
-            double fj = m.F[j * n + e];
+            double fj = m.F()[j * n + e];
             acc = fma(KV_A[6][j], fj, acc);
             acce = fma(KV_A[6][j] - KV_A[5][j], fj, acce);
           }
-          acc = fma(KV_G, m.F[6 * n + e], acc);
-          acce += -KV_G * m.F[5 * n + e] + KV_G * m.F[6 * n + e];
-          double y0e = m.y0[e];
+          acc = fma(KV_G, m.F()[6 * n + e], acc);
+          acce += -KV_G * m.F()[5 * n + e] + KV_G * m.F()[6 * n + e];
+          double y0e = m.y0()[e];
           double y1e = y0e + h * acc;
-          m.y1[e] = y1e;
+          m.y1()[e] = y1e;
           double err = h * acce;
           double q = err / (atol + fmax(fabs(y0e), fabs(y1e)) * rtol);
           ss += q * q;
@@ -716,21 +838,22 @@ __global__ void __launch_bounds__(128) pert_kernel(PertArgs P) {
           if (!(ts <= t1)) break;
           double th = (ts - t0) / h;
           for (int e = lane; e < n; e += WARP) {
-            double y0e = m.y0[e], y1e = m.y1[e];
-            double k0 = h * m.F[e], k1 = h * m.F[6 * n + e];
-            m.v[e] = y0e + th * (k0 + th * ((3. * (y1e - y0e) - 2. * k0 - k1) + th * (2. * (y0e - y1e) + k0 + k1)));
+            double y0e = m.y0()[e], y1e = m.y1()[e];
+            double k0 = h * m.F()[e], k1 = h * m.F()[6 * n + e];
+            m.v()[e] = y0e + th * (k0 + th * ((3. * (y1e - y0e) - 2. * k0 - k1) + th * (2. * (y0e - y1e) + k0 + k1)));
           }
           __syncwarp();
-          write_fields(c, L, P.tables, k, ts, m.v, P.pt, nsave, isave, ik, lane);
+          write_fields(c, L, P.tables, k, ts, m.v(), P.pt, nsave, isave, ik, lane);
           __syncwarp();
           ++isave;
         }
         prev_prev_inv = prev_inv;
         prev_inv = inv;
         for (int e = lane; e < n; e += WARP) {
-          m.y0[e] = m.y1[e];
-          m.F[e] = m.F[6 * n + e];
+          m.y0()[e] = m.y1()[e];
+          m.F()[e] = m.F()[6 * n + e];
         }
+        m.SB()[lane] = m.SB()[5 * NB + lane];                  // basis at the new t0
         __syncwarp();
         t0 = t1;
       } else {
@@ -793,7 +916,7 @@ cudaError_t launch_pert(int n_cosmo, const abcmb_cosmo* cosmo, const double* tab
   A.n_cosmo = n_cosmo;
   A.n_items = n_items;
   A.max_ny = s.max_ny;
-  A.ncm = s.any_ncdm ? 28 : 16;
+  A.ncm = s.any_ncdm ? 22 : 13;
   A.cosmo = cosmo;
   A.tables = tables;
   A.kbuf = kbuf;

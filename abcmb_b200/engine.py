@@ -109,7 +109,7 @@ class DeviceBatch:
 class LosRunner:
     """Workspace + outputs of abcmb_los_forward for a fixed transfer k grid."""
 
-    def __init__(self, dbatch: DeviceBatch, kt: np.ndarray, ls: CLosSettings):
+    def __init__(self, dbatch: DeviceBatch, kt: np.ndarray, ls: CLosSettings, want_dns: bool = False):
         self.db = dbatch
         self.ls = ls
         dev = dbatch.device
@@ -125,13 +125,17 @@ class LosRunner:
         n = dbatch.batch.n_cosmo
         self.cl_raw = torch.empty(n * self.n_ell_tab * 3, dtype=torch.float64, device=dev)
         self.cl = torch.empty(n * 3 * self.n_out, dtype=torch.float64, device=dev)
+        self.dcl_dns = torch.empty(n * 3 * self.n_out, dtype=torch.float64, device=dev) if want_dns else None
+        self.cosmo_host = np.ascontiguousarray(dbatch.batch.cosmo)
 
     def run(self, stream=None):
         lib = _lib.load()
         st = stream if stream is not None else torch.cuda.current_stream(self.db.device)
         db = self.db
-        rc = lib.abcmb_los_forward(db.batch.n_cosmo, _ptr(db.cosmo), _ptr(db.tables), _ptr(db.kbuf), _ptr(db.pt),
-                                   _ptr(self.kt), ctypes.byref(self.ls), _ptr(self.cl_raw), _ptr(self.cl),
+        rc = lib.abcmb_los_forward(db.batch.n_cosmo, _ptr(db.cosmo), ctypes.c_void_p(self.cosmo_host.ctypes.data),
+                                   _ptr(db.tables), _ptr(db.kbuf), _ptr(db.pt), _ptr(self.kt), ctypes.byref(self.ls),
+                                   _ptr(self.cl_raw), _ptr(self.cl),
+                                   _ptr(self.dcl_dns) if self.dcl_dns is not None else None,
                                    _ptr(self.ws), self.ws.numel(), ctypes.c_void_p(st.cuda_stream))
         _lib.check(rc, "abcmb_los_forward")
 

@@ -1,0 +1,96 @@
+"""C_l gradients for theta = (h, omega_b, omega_cdm, A_s, n_s, tau_reion).
+
+A_s and n_s enter only the primordial factor of the k quadrature
+(spectrum.py:789-791), so dC_l/dA_s = C_l / A_s and dC_l/dn_s comes from the
+same line-of-sight launch as C_l (a ln(k/k_pivot)-weighted quadrature).
+h, omega_b, omega_cdm and tau_reion change the background and the
+perturbations; their derivatives are central differences with relative step
+1e-4 (the finite-difference check of the gradient configuration), all
+variants of all cosmologies integrated in one batched launch.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import background_tables as bt
+from . import cosmology, packing
+from . import specs as sp
+from .configs import GRAD_PARAMS, Workload
+
+FD_PARAMS = ("h", "omega_b", "omega_cdm", "tau_reion")
+REL_STEP = 1e-4
+
+
+def fd_variants(p_in: dict, rel_step: float = REL_STEP):
+    """[(param, sign, step, params)]: the base point and the +- variants."""
+    out = [(None, 0, 0.0, dict(p_in))]
+    for name in FD_PARAMS:
+        hstep = rel_step * p_in[name]
+        for sgn in (+1, -1):
+            p = dict(p_in)
+            p[name] = p_in[name] + sgn * hstep
+            out.append((name, sgn, hstep, p))
+    return out
+
+
+def _bg_job(args):
+    p_in, ncdm, specs = args
+    p = cosmology.add_derived_parameters(p_in, ncdm, specs)
+    return bt.make_background(p, ncdm)
+
+
+@dataclass
+class GradWorkload:
+    """A workload expanded into its finite-difference variants."""
+    base: Workload
+    variants: list          # per base cosmology: list of (param, sign, step) in batch order
+    batch: packing.Batch
+    n_var: int
+
+    def assemble(self, cl: np.ndarray, dcl_dns: np.ndarray):
+        """cl, dcl_dns: (n_base * n_var, 3, n_l) -> C_l (n_base, 3, n_l), grad (n_base, 6, 3, n_l)."""
+        nb = len(self.base.params_in)
+        cl = cl.reshape(nb, self.n_var, *cl.shape[1:])
+        dns = dcl_dns.reshape(nb, self.n_var, *dcl_dns.shape[1:])
+        grad = np.zeros((nb, len(GRAD_PARAMS)) + cl.shape[2:])
+        for i in range(nb):
+            var = self.variants[i]
+            for gi, name in enumerate(GRAD_PARAMS):
+                if name == "A_s":
+                    grad[i, gi] = cl[i, 0] / self.base.params_in[i]["A_s"]
+                elif name == "n_s":
+                    grad[i, gi] = dns[i, 0]
+                else:
+                    jp = next(j for j, v in enumerate(var) if v[0] == name and v[1] > 0)
+                    jm = next(j for j, v in enumerate(var) if v[0] == name and v[1] < 0)
+                    grad[i, gi] = (cl[i, jp] - cl[i, jm]) / (2.0 * var[jp][2])
+        return cl[:, 0], grad
+
+
+def expand(w: Workload, n_save: int = 500, processes: int = 0, rel_step: float = REL_STEP) -> GradWorkload:
+    """Background tables for every variant (host, optionally in a spawn pool)."""
+    jobs, variants, layouts, kgrids = [], [], [], []
+    for p_in, ncdm, kg in zip(w.params_in, w.has_ncdm, w.kgrids):
+        var = fd_variants(p_in, rel_step)
+        variants.append([(v[0], v[1], v[2]) for v in var])
+        for v in var:
+            jobs.append((v[3], ncdm, w.specs))
+            layouts.append(sp.state_layout(w.specs, ncdm))
+            kgrids.append(kg)
+    if processes and processes > 1:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(processes) as pool:
+            bgs = pool.map(_bg_job, jobs, chunksize=max(1, len(jobs) // (4 * processes)))
+    else:
+        bgs = [_bg_job(j) for j in jobs]
+    batch = packing.pack(bgs, layouts, kgrids, n_save=n_save)
+    if w.kt is None:
+        ks = dict(w.specs)
+        sp.get_k_axis_perturbations(ks)
+        w.kt = sp.get_k_axis_transfer(ks)
+        from . import bessel as bessel_mod
+        w.idx_min, w.idx_max, _ = sp.ell_index_range(bessel_mod.load().l_tab, int(w.specs["l_min"]), w.l_max, False)
+    w.batch = batch
+    return GradWorkload(base=w, variants=variants, batch=batch, n_var=len(variants[0]))

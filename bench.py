@@ -1,0 +1,345 @@
+#!/usr/bin/env python
+"""Benchmark: C_l + gradient cosmologies per second on B200.
+
+Workload (per GPU, weak scaling): the batched uneven configuration -- 64
+cosmologies with parameters uniform within +-5% of the LCDM fiducial,
+massive-neutrino count drawn from {0, 1, 3}, per-cosmology k grids of
+400..800 modes on [1e-5, 1] / Mpc, unlensed TT/TE/EE to l = 2500 -- with the
+C_l gradient with respect to (h, omega_b, omega_cdm, A_s, n_s, tau_reio):
+central differences (relative step 1e-4) for the four background
+parameters, exact A_s / n_s derivatives from the same line-of-sight launch.
+One step = perturbations of all 9 variants of all 64 cosmologies (one
+persistent launch) + line of sight + gradient assembly.  Inputs are seeded
+synthetic (numpy default_rng(20261203 + rank)); background tables are
+produced on the host before timing (they are inputs of this path).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Cl+grad cosmologies/s on 1 B200 (l≤2500, ΔCl/Cl≤1e-4) vs plain GPU fwd+FD"
+UNIT = "cosmologies/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n-cosmo", type=int, default=64)
+    ap.add_argument("--l-max", type=int, default=2500)
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--cpu-sample-stride", type=int, default=24)
+    return ap.parse_args()
+
+
+def workload_config(args, world):
+    return {"workload": f"batched uneven LCDM(+0/1/3 massive nu): {args.n_cosmo} cosmologies x 9 "
+                        f"gradient variants per GPU, Nk 400-800 on [1e-5,1]/Mpc, unlensed TT/TE/EE to "
+                        f"l={args.l_max}, grad wrt (h,omega_b,omega_cdm,A_s,n_s,tau_reio)",
+            "n_cosmo_per_gpu": args.n_cosmo, "grad": "central FD rel 1e-4 (h,ob,oc,tau) + exact A_s,n_s",
+            "hierarchies": "l_max_g=12 l_max_pol_g=10 l_max_nu=17 l_max_ncdm=17 (reference defaults)",
+            "precision": "FP64 ODE, FP64 LOS", "l2": "inputs > L2 (126 MB) per step",
+            "parallelism": f"dp{world} (independent cosmologies per GPU, no collective)"}
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,power.draw")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 6:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+def cpu_sample(gw, stride: int, n_threads: int):
+    """Oracle time for one cosmology's C_l + gradient (9 ODE variants + LOS),
+    measured on every `stride`-th k mode of its 9 variants plus one full
+    line-of-sight run, scaled to the whole unit."""
+    from oracle import oracle
+    from abcmb_b200 import bessel, packing
+    b = gw.batch
+    nvar = gw.n_var
+    sel = [i for i in range(b.n_items) if b.items[i, 0] < nvar and b.items[i, 1] % stride == 0]
+    n_full = sum(1 for i in range(b.n_items) if b.items[i, 0] < nvar)
+    sub = packing.Batch(cosmo=b.cosmo, tables=b.tables, kbuf=b.kbuf, items=b.items[sel].copy(), pt_size=b.pt_size,
+                        n_save=b.n_save, bgs=b.bgs, layouts=b.layouts)
+    st = gw.base.pert_settings()
+    t0 = time.perf_counter()
+    rc, pt, ks = oracle.pert_forward(sub, st, n_threads)
+    t_ode = (time.perf_counter() - t0) * n_full / len(sel)
+    one = packing.Batch(cosmo=b.cosmo[:1].copy(), tables=b.tables, kbuf=b.kbuf, items=b.items[:0], pt_size=b.pt_size,
+                        n_save=b.n_save, bgs=b.bgs[:1], layouts=b.layouts[:1])
+    ls = gw.base.los_settings()
+    t0 = time.perf_counter()
+    oracle.los_forward(one, pt, gw.base.kt, ls, bessel.load(), n_threads)
+    t_los = (time.perf_counter() - t0) * nvar
+    total = t_ode + t_los
+    return {"value": 1.0 / total, "unit": UNIT, "cores": n_threads, "kind": "port",
+            "sample": f"oracle (C, FP64, OpenMP) on 1 cosmology's 9 gradient variants: every {stride}th k mode of "
+                      f"the ODE ({len(sel)}/{n_full} items, scaled) + 1 full line-of-sight run (x{nvar}); "
+                      f"s per cosmology+grad: ode {t_ode:.2f} los {t_los:.2f}"}
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the CPU restatement of the path on the host cores."""
+    if rank != 0:
+        return
+    from abcmb_b200 import configs, gradients
+    w = configs.c4(n_cosmo=1, l_max=args.l_max)
+    gw = gradients.expand(w, processes=min(9, os.cpu_count() or 1))
+    nthr = os.cpu_count() or 1
+    vals = []
+    for _ in range(max(args.warmup, 0)):
+        cpu_sample(gw, args.cpu_sample_stride * 2, nthr)
+    for _ in range(max(args.steps, 1)):
+        vals.append(cpu_sample(gw, args.cpu_sample_stride, nthr))
+    v = statistics.median([x["value"] for x in vals])
+    cb = dict(vals[-1])
+    cb["value"] = v
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "impl": "reference", "config": workload_config(args, world),
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    # host-side inputs first (spawn pool before any CUDA call)
+    from abcmb_b200 import configs, gradients
+    t_build = time.perf_counter()
+    w = configs.c4(n_cosmo=args.n_cosmo, l_max=args.l_max, seed=configs.SEED + rank)
+    gw = gradients.expand(w, processes=os.cpu_count() or 1)
+    t_build = time.perf_counter() - t_build
+
+    import torch
+    import torch.distributed as dist
+    from abcmb_b200 import engine, _lib
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    lib = _lib.load()
+    b = gw.batch
+    st = w.pert_settings()
+    ls = w.los_settings()
+    db = engine.DeviceBatch.upload(b, dev)
+    lr = engine.LosRunner(db, w.kt, ls, want_dns=True)
+    stream = torch.cuda.current_stream(dev)
+    nb, nvar, n_out = len(w.params_in), gw.n_var, lr.n_out
+    # gradient assembly indices (device side)
+    plus = torch.tensor([[next(j for j, v in enumerate(var) if v[0] == p and v[1] > 0) for p in gradients.FD_PARAMS]
+                         for var in gw.variants], device=dev)
+    minus = torch.tensor([[next(j for j, v in enumerate(var) if v[0] == p and v[1] < 0) for p in gradients.FD_PARAMS]
+                          for var in gw.variants], device=dev)
+    hstep = torch.tensor([[var[plus[i, q].item()][2] for q in range(len(gradients.FD_PARAMS))]
+                          for i, var in enumerate(gw.variants)], dtype=torch.float64, device=dev)
+    A_s = torch.tensor([p["A_s"] for p in w.params_in], dtype=torch.float64, device=dev)
+    out_cl = torch.empty(nb, 3, n_out, dtype=torch.float64, device=dev)
+    out_grad = torch.empty(nb, 6, 3, n_out, dtype=torch.float64, device=dev)
+    ev_p0 = torch.cuda.Event(enable_timing=True)
+    ev_p1 = torch.cuda.Event(enable_timing=True)
+
+    def assemble():
+        cl = lr.cl.view(nb, nvar, 3, n_out)
+        dns = lr.dcl_dns.view(nb, nvar, 3, n_out)
+        out_cl.copy_(cl[:, 0])
+        ar = torch.arange(nb, device=dev)[:, None]
+        fd = (cl[ar, plus] - cl[ar, minus]) / (2.0 * hstep)[:, :, None, None]
+        # order (h, omega_b, omega_cdm, A_s, n_s, tau_reion)
+        out_grad[:, 0:3] = fd[:, 0:3]
+        out_grad[:, 3] = cl[:, 0] / A_s[:, None, None]
+        out_grad[:, 4] = dns[:, 0]
+        out_grad[:, 5] = fd[:, 3]
+
+    pert_ms = []
+
+    def step(record=False):
+        if record:
+            ev_p0.record(stream)
+        db.pert_forward(st, stream)
+        if record:
+            ev_p1.record(stream)
+        lr.run(stream)
+        assemble()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    ks = db.check_status()
+    # timed region: inputs resident in HBM (> L2 per step: PT output alone is ~GBs)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step(record=True)
+            ev_p1.synchronize()
+            pert_ms.append(ev_p0.elapsed_time(ev_p1))
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * nb / (ms / 1000.0)
+
+    # end to end through the C ABI with host buffers: H2D of this step's
+    # inputs (pinned), the kernels, D2H of C_l and the gradient
+    host_cos = torch.from_numpy(b.cosmo.view(np.uint8).copy()).pin_memory()
+    host_tab = torch.from_numpy(b.tables).pin_memory()
+    host_k = torch.from_numpy(b.kbuf).pin_memory()
+    host_items = torch.from_numpy(b.items.reshape(-1).copy()).pin_memory()
+    res_cl = torch.empty(out_cl.shape, dtype=torch.float64).pin_memory()
+    res_grad = torch.empty(out_grad.shape, dtype=torch.float64).pin_memory()
+    h2d = sum(t.numel() * t.element_size() for t in (host_cos, host_tab, host_k, host_items))
+    d2h = res_cl.numel() * 8 + res_grad.numel() * 8
+    barrier()
+    torch.cuda.synchronize(dev)
+    x0 = torch.cuda.Event(enable_timing=True)
+    x1 = torch.cuda.Event(enable_timing=True)
+    x0.record(stream)
+    for _ in range(args.e2e_steps):
+        db.cosmo.copy_(host_cos, non_blocking=True)
+        db.tables.copy_(host_tab, non_blocking=True)
+        db.kbuf.copy_(host_k, non_blocking=True)
+        db.items.copy_(host_items, non_blocking=True)
+        step()
+        res_cl.copy_(out_cl, non_blocking=True)
+        res_grad.copy_(out_grad, non_blocking=True)
+    x1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    ms_e2e = x0.elapsed_time(x1) / args.e2e_steps
+    if world > 1:
+        t = torch.tensor([ms_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = {"value": world * nb / (ms_e2e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e}
+
+    # roofline of the dominant kernel (the perturbation launch): FP64 work
+    steps_k = (ks["n_accepted"] + ks["n_rejected"]).astype(np.float64)
+    ny_k = b.cosmo["ny"][b.items[:, 0]].astype(np.float64)
+    flops = float(np.sum(steps_k * 7.0 * ((8.0 * ny_k + 200.0) + 20.0 * ny_k)))
+    pert_avg = float(np.mean(pert_ms))
+    peak = __import__("ctypes").c_double(0.0)
+    rc = lib.abcmb_probe_fp64_tflops(__import__("ctypes").byref(peak), 20000,
+                                     __import__("ctypes").c_void_p(stream.cuda_stream))
+    achieved = flops / (pert_avg / 1000.0) / 1e12
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "pert_kernel_traffic.json")
+    if os.path.isfile(tfile):
+        try:
+            tj = json.load(open(tfile))
+            traffic = tj["bytes_per_item"] * b.n_items
+        except (ValueError, KeyError):
+            traffic = None
+    roofline = {"bound": "fp64", "kernel": "pert_kernel", "achieved": achieved,
+                "peak": peak.value if rc == 0 else None, "unit": "TFLOP/s",
+                "frac": (achieved / peak.value) if rc == 0 and peak.value > 0 else None,
+                "traffic": traffic,
+                "peak_source": "measured in this run: FP64 FMA probe (abcmb_probe_fp64_tflops); "
+                               "MEASURED_PEAKS.json has no FP64 figure",
+                "flops_def": "sum_k steps_k * 7 * (8 Ny + 200 + 20 Ny)", "launch_ms": pert_avg,
+                "hbm_gbs_peak_measured": _peak_hbm()}
+    # our kernel launches per step: pert (memset + 2 start kernels + persistent) + 5 per LOS cosmology
+    launches = 3 + 5 * b.n_cosmo
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; background tables from a host model)",
+            "config": workload_config(args, world), "e2e": e2e, "roofline": roofline, "gpu_launches": launches,
+            "clocks": clk.summary(), "items_per_step": int(b.n_items),
+            "ode_steps_mean": float(steps_k.mean()), "host_build_s": t_build}
+    if rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_sample(gw, args.cpu_sample_stride, os.cpu_count() or 1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def _peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return json.load(open(p)).get("hbm_gbs")
+    except (OSError, ValueError):
+        return None
+
+
+if __name__ == "__main__":
+    main()

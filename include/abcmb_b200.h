@@ -227,16 +227,23 @@ int64_t abcmb_los_workspace_size(int n_cosmo, int max_nk, int nkt, int n_ell_tab
  * grid (cubic spline in log10 k), form the T0/T1/T2/E sources, run the
  * line-of-sight integral for every tabulated l in [idx_min, idx_max], do the
  * k quadrature, and spline C_l onto the integer ells l_min..l_max.
+ *   cosmo_host [n_cosmo]   optional host copy of the descriptors (NULL: the
+ *                          call reads them back and synchronises the stream;
+ *                          pass it to keep the call asynchronous/capturable)
  *   kt_dev     [nkt]                            transfer k grid
  *   cl_raw_dev [n_cosmo x n_ell_tab x 3]        C_l at tabulated l (TT,TE,EE)
  *   cl_dev     [n_cosmo x 3 x (l_max-l_min+1)]  ClTT, ClTE, ClEE at integer l
+ *   dcl_dns_dev (optional, NULL to skip) same layout as cl_dev: dC_l/dn_s,
+ *              exact because n_s enters only the primordial factor of the k
+ *              quadrature (spectrum.py:789-791); dC_l/dA_s = C_l / A_s.
  * Replaces: get_Cl, Cl_one_ell (spectrum.py:574-797).
  */
 int abcmb_los_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev,
+                      const abcmb_cosmo* cosmo_host,
                       const double* tables_dev, const double* k_dev,
                       const double* pt_dev, const double* kt_dev,
                       const abcmb_los_settings* settings,
-                      double* cl_raw_dev, double* cl_dev,
+                      double* cl_raw_dev, double* cl_dev, double* dcl_dns_dev,
                       void* workspace_dev, int64_t workspace_bytes,
                       void* stream);
 
@@ -260,6 +267,11 @@ int abcmb_set_pert_warps_per_block(int warps);
 
 /* Grid size (blocks) of the last perturbation launch on this process. */
 int abcmb_last_pert_grid(void);
+
+/* Measured FP64 FMA rate of the current device in TFLOP/s (best of 5 runs
+ * of `iters` x 128 independent FMAs per thread): the peak the perturbation
+ * kernel's roofline is quoted against. */
+int abcmb_probe_fp64_tflops(double* tflops, int iters, void* stream);
 
 #ifdef __cplusplus
 }

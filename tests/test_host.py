@@ -82,7 +82,7 @@ def test_los_argument_errors_without_gpu():
     from abcmb_b200 import _lib, packing
     lib = _lib.load()
     ls = packing.CLosSettings(l_min=3, l_max=10, idx_min=0, idx_max=5, nkt=10, n_save=500)
-    rc = lib.abcmb_los_forward(1, ctypes.c_void_p(8), ctypes.c_void_p(8), ctypes.c_void_p(8), ctypes.c_void_p(8),
-                               ctypes.c_void_p(8), ctypes.byref(ls), ctypes.c_void_p(8), ctypes.c_void_p(8),
-                               ctypes.c_void_p(8), 0, None)
+    rc = lib.abcmb_los_forward(1, ctypes.c_void_p(8), None, ctypes.c_void_p(8), ctypes.c_void_p(8),
+                               ctypes.c_void_p(8), ctypes.c_void_p(8), ctypes.byref(ls), ctypes.c_void_p(8),
+                               ctypes.c_void_p(8), None, ctypes.c_void_p(8), 0, None)
     assert rc == -1 and b"l_min" in lib.abcmb_last_error()
