@@ -114,17 +114,15 @@ struct WarpMem {
   double* p;      // base of this warp's region
   int my, ncm, cs;
   __device__ __forceinline__ double* y0() const { return p; }                 // ny
-  __device__ __forceinline__ double* y1() const { return p + my; }            // ny
-  __device__ __forceinline__ double* F() const { return p + 2 * my; }         // 7 ny stage derivatives
-  __device__ __forceinline__ double* base() const { return p + 9 * my; }      // ny
-  __device__ __forceinline__ double* v() const { return p + 10 * my; }        // ny
-  __device__ __forceinline__ double* r() const { return p + 11 * my; }        // ny
-  __device__ __forceinline__ double* tA() const { return p + 12 * my; }       // tail coefficient of v[e-1]
-  __device__ __forceinline__ double* tG() const { return p + 13 * my; }       // tail coefficient of v[e+1]
-  __device__ __forceinline__ double* invd() const { return p + 14 * my; }     // tail pivots
-  __device__ __forceinline__ double* mult() const { return p + 15 * my; }     // upward-sweep multipliers
-  __device__ __forceinline__ double* sub() const { return p + 16 * my; }      // tail sub-diagonal of M
-  __device__ __forceinline__ double* Mc() const { return p + 17 * my; }       // ncm x cs core inverse
+  __device__ __forceinline__ double* F() const { return p + my; }             // 7 ny stage derivatives
+  __device__ __forceinline__ double* base() const { return p + 8 * my; }      // ny stage base
+  __device__ __forceinline__ double* y1() const { return base(); }            // the step's result reuses base
+  __device__ __forceinline__ double* v() const { return p + 9 * my; }         // ny
+  __device__ __forceinline__ double* r() const { return p + 10 * my; }        // ny
+  __device__ __forceinline__ double* invd() const { return p + 11 * my; }     // tail pivots
+  __device__ __forceinline__ double* mult() const { return p + 12 * my; }     // upward-sweep multipliers
+  __device__ __forceinline__ double* sub() const { return p + 13 * my; }      // tail sub-diagonal of M
+  __device__ __forceinline__ double* Mc() const { return p + 14 * my; }       // ncm x cs core inverse
   __device__ __forceinline__ double* vc() const { return Mc() + ncm * cs; }   // gathered core vector
   __device__ __forceinline__ double* SB() const { return vc() + ncm; }        // NSLOT x NB basis
   __device__ __forceinline__ double* m3() const { return SB() + 6 * 32; }     // M_{3,4} / d_4 per chain
@@ -138,6 +136,7 @@ struct WarpMem {
 
 // Static sparsity of the core rows, shared by the block (filled once).
 constexpr int MAXC = 22;
+constexpr int LMAXT = 63;           // largest hierarchy l_max the kernel supports
 struct RowTab {
   int n[MAXC];
   int bid[MAXC * 5];
@@ -145,6 +144,10 @@ struct RowTab {
   int tch[MAXC];
   double cst[MAXC * 5];
   double uh[MAXC], ue[MAXC], tco[MAXC];
+  // tail coefficients of v[l-1] and v[l+1] per unit chain speed, by l:
+  // l / (2l+1) and (l+1) / (2l+1); slot 1 holds the l = 3 pair of the F and
+  // N hierarchies (6/7, 4/7: their l = 2 slot stores sigma = F_2 / 2)
+  double ta[LMAXT + 1], tg[LMAXT + 1];
 };
 
 // Background "basis" of one time: every coefficient of A(lna) is a constant
@@ -163,7 +166,7 @@ __device__ __forceinline__ int chain_speed_bid(int chn) { return chn < 3 ? B_KIA
 
 __host__ __device__ inline size_t warp_mem_doubles(int max_ny, int ncm) {
   const size_t ints = (size_t)ncm * 7 + (size_t)max_ny + 16;
-  return (size_t)17 * max_ny + (size_t)ncm * (ncm + 1) + (size_t)ncm + NSLOT * NB + NCHAIN + (ints + 1) / 2;
+  return (size_t)14 * max_ny + (size_t)ncm * (ncm + 1) + (size_t)ncm + NSLOT * NB + NCHAIN + (ints + 1) / 2;
 }
 
 __device__ __forceinline__ void carve(double* p, int max_ny, int ncm, WarpMem& m) {
@@ -308,19 +311,48 @@ __device__ __forceinline__ void metric(const Layout& L, const double* B, const d
 }
 
 // out = A(t) v for the time whose basis is B (get_derivatives, perturbations.py:201-248).
-__device__ void apply_A(const Layout& L, const WarpMem& m, const RowTab& R, const double* B, const double* v,
-                        double* out, bool ncdm, int lane) {
+// One core row of A at one stage time, kept in registers for all chord
+// iterations of that stage (unused terms have coefficient 0 and index 0).
+struct CoreRow {
+  double c[5];      // cst * basis[bid]
+  int s[5];         // state index of each term
+  double tc;        // coefficient of the hanging tail's l = 3 element
+  int ts;           // its state index
+  double uh, ue;
+  int out;          // state index of the row
+};
+
+__device__ __forceinline__ void core_row_at(const Layout& L, const RowTab& R, const WarpMem& m, const double* B,
+                                            int lane, CoreRow& cr) {
+  const int r = lane < L.nc ? lane : 0;
+  const int nt = R.n[r];
+#pragma unroll
+  for (int t = 0; t < 5; ++t) {
+    cr.c[t] = t < nt ? R.cst[r * 5 + t] * B[R.bid[r * 5 + t]] : 0.;
+    cr.s[t] = t < nt ? m.rstate()[r * 5 + t] : 0;
+  }
+  const int tc = R.tch[r];
+  cr.tc = tc >= 0 ? R.tco[r] * B[chain_speed_bid(tc)] : 0.;
+  cr.ts = tc >= 0 ? m.chs()[tc] : 0;
+  cr.uh = R.uh[r];
+  cr.ue = R.ue[r];
+  cr.out = m.cmap()[r];
+}
+
+#ifndef PERT_APPLY_ATTR
+#define PERT_APPLY_ATTR
+#endif
+__device__ PERT_APPLY_ATTR void apply_A(const Layout& L, const WarpMem& m, const RowTab& R, const CoreRow& cr,
+                                       const double* B,
+                        const double* v, double* out, bool ncdm, int lane) {
   double hp, etap;
   metric(L, B, v, ncdm, hp, etap);
   if (lane < L.nc) {
-    double acc = R.uh[lane] * hp + R.ue[lane] * etap;
-    const int nt = R.n[lane];
+    double acc = cr.uh * hp + cr.ue * etap;
 #pragma unroll
-    for (int t = 0; t < 5; ++t)
-      if (t < nt) acc = fma(R.cst[lane * 5 + t] * B[R.bid[lane * 5 + t]], v[m.rstate()[lane * 5 + t]], acc);
-    const int tc = R.tch[lane];
-    if (tc >= 0) acc = fma(R.tco[lane] * B[chain_speed_bid(tc)], v[m.chs()[tc]], acc);
-    out[m.cmap()[lane]] = acc;
+    for (int t = 0; t < 5; ++t) acc = fma(cr.c[t], v[cr.s[t]], acc);
+    acc = fma(cr.tc, v[cr.ts], acc);
+    out[cr.out] = acc;
   }
   const double trunc = B[B_TRUNC];
   for (int t = lane; t < L.ntail; t += WARP) {
@@ -329,8 +361,11 @@ __device__ void apply_A(const Layout& L, const WarpMem& m, const RowTab& R, cons
     const double s = B[chain_speed_bid(chn)];
     const double d = chn < 2 ? B[B_KAP] : 0.;
     double fv;
-    if (info >> 15) fv = s * v[e - 1] - (d + (double)(m.chL()[chn] + 1) * trunc) * v[e];
-    else fv = s * (m.tA()[e] * v[e - 1] - m.tG()[e] * v[e + 1]) - d * v[e];
+    if ((info >> 15) & 1) fv = s * v[e - 1] - (d + (double)(m.chL()[chn] + 1) * trunc) * v[e];
+    else {
+      const int li = info >> 16;
+      fv = s * (R.ta[li] * v[e - 1] - R.tg[li] * v[e + 1]) - d * v[e];
+    }
     out[e] = fv;
   }
   __syncwarp();
@@ -382,8 +417,9 @@ __device__ void factor_newton(const Layout& L, WarpMem& m, const RowTab& R, cons
         sb = -hg * s;
       } else {
         diag = 1. + hg * d;
-        sup = hg * s * m.tG()[e];
-        sb = -hg * s * m.tA()[e];
+        const int li = (l == 3 && (chn == 0 || chn == 2)) ? 1 : l;
+        sup = hg * s * R.tg[li];
+        sb = -hg * s * R.ta[li];
       }
       double inv = 1. / (diag - sup * sub_next * inv_next);
       m.invd()[e] = inv;
@@ -625,7 +661,7 @@ struct PertArgs {
 };
 
 #ifndef PERT_MIN_BLOCKS
-#define PERT_MIN_BLOCKS 3   // 168 registers: faster than 128 + spills (measured on C1, C2, C4)
+#define PERT_MIN_BLOCKS 2   // 250 registers, no spills: faster than 3 or 4 blocks/SM (measured on C2, C4)
 #endif
 __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) {
   extern __shared__ double smem[];
@@ -646,6 +682,10 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
       R.col[r * 5 + t] = t < d.n ? d.col[t] : 0;
       R.cst[r * 5 + t] = t < d.n ? d.cst[t] : 0.;
     }
+  }
+  for (int l = threadIdx.x; l <= LMAXT; l += blockDim.x) {
+    R.ta[l] = (l == 1) ? 6. / 7. : (double)l / (2. * l + 1.);
+    R.tg[l] = (l == 1) ? 4. / 7. : (double)(l + 1) / (2. * l + 1.);
   }
   __syncthreads();
   WarpMem m;
@@ -669,6 +709,18 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
     make_layout(c, L);
     const int n = L.ny;
     const bool ncdm = c.has_ncdm != 0;
+    // a descriptor this launch cannot hold is reported, never indexed
+    {
+      const int lmx = max(max(L.lg, L.lp), max(L.lnu, ncdm ? L.lm : 4));
+      const int lmn = min(min(L.lg, L.lp), min(L.lnu, ncdm ? L.lm : 4));
+      if (n > P.max_ny || L.nc > P.ncm || lmx > LMAXT || lmn < 4 || n != c.ny) {
+        if (lane == 0) {
+          abcmb_kstat st{ABCMB_STATUS_BAD_LAYOUT, 0, 0, 0, 0.};
+          P.kstat[item] = st;
+        }
+        continue;
+      }
+    }
     const double k = P.kbuf[c.off_k + ik];
     const double rtol = k > S.k_split ? S.rtol_large : S.rtol_small;
     const double atol = k > S.k_split ? S.atol_large : S.atol_small;
@@ -684,10 +736,9 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
       int chn, l, e, lmax = 0;
       tail_elem(L, t, chn, l, e, lmax);
       // F3' and N3' carry 6/7 on their l = 2 slot (which holds sigma = F_2 / 2;
-      // species.py:745 and 1435); every other l uses l / (2l + 1)
-      m.tA()[e] = (l == 3 && (chn == 0 || chn == 2)) ? 6. / 7. : (double)l / (2. * l + 1.);
-      m.tG()[e] = (double)(l + 1) / (2. * l + 1.);
-      m.tinfo()[t] = e | (chn << 12) | ((l == lmax) ? (1 << 15) : 0);
+      // species.py:745 and 1435): table slot 1; every other l uses slot l
+      const int li = (l == 3 && (chn == 0 || chn == 2)) ? 1 : l;
+      m.tinfo()[t] = e | (chn << 12) | ((l == lmax) ? (1 << 15) : 0) | (li << 16);
     }
     if (lane < NCHAIN) {
       int s, lm, o;
@@ -741,7 +792,9 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
     double t1 = fmin(t0 + S.dt0, 0.0);
     double prev_inv = 1.0, prev_prev_inv = 1.0;
     int isave = 0, nsteps = 0, nacc = 0, nrej = 0, nnewton = 0, status = ABCMB_STATUS_OK;
-    apply_A(L, m, R, m.SB(), m.y0(), m.F(), ncdm, lane);         // FSAL stage 1
+    CoreRow cr;
+    core_row_at(L, R, m, m.SB(), lane, cr);
+    apply_A(L, m, R, cr, m.SB(), m.y0(), m.F(), ncdm, lane);     // FSAL stage 1
 
     while (t0 < 0.0) {
       if (nsteps >= S.max_steps) { status = ABCMB_STATUS_MAX_STEPS; break; }
@@ -762,13 +815,14 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
           m.base()[e] = m.y0()[e] + h * acc;
           fi[e] = m.F()[(i - 1) * n + e];
         }
+        if (i != 6) core_row_at(L, R, m, B, lane, cr);       // stage 7 shares stage 6's time
         __syncwarp();
         double diffsize = INFINITY, diffsize_prev;
         bool conv = false;
         for (int it = 1; it <= root_max; ++it) {
           for (int e = lane; e < n; e += WARP) m.v()[e] = m.base()[e] + hg * fi[e];
           __syncwarp();
-          apply_A(L, m, R, B, m.v(), m.r(), ncdm, lane);
+          apply_A(L, m, R, cr, B, m.v(), m.r(), ncdm, lane);
           for (int e = lane; e < n; e += WARP) m.r()[e] = m.r()[e] - fi[e];
           __syncwarp();
           solve_newton(L, m, m.r(), lane);

@@ -122,10 +122,10 @@ def state_layout(specs: dict, has_ncdm: bool) -> StateLayout:
                       bool(has_ncdm))
     for name, l in (("l_max_g", lay.lmax_g), ("l_max_pol_g", lay.lmax_pol_g),
                     ("l_max_massless_nu", lay.lmax_nu)):
-        if l < 4:
-            raise ValueError(f"{name}={l}: the CUDA path needs every hierarchy to reach l >= 4")
-    if has_ncdm and lay.lmax_ncdm < 4:
-        raise ValueError("l_max_massive_nu must be >= 4")
+        if l < 4 or l > 63:
+            raise ValueError(f"{name}={l}: the CUDA path supports hierarchy cut-offs 4 <= l_max <= 63")
+    if has_ncdm and not 4 <= lay.lmax_ncdm <= 63:
+        raise ValueError("l_max_massive_nu must be within 4..63")
     return lay
 
 

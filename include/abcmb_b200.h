@@ -51,6 +51,8 @@ extern "C" {
 #define ABCMB_STATUS_MAX_STEPS   1   /* diffrax RESULTS.max_steps_reached     */
 #define ABCMB_STATUS_NONFINITE   2   /* NaN/Inf in the state or the error     */
 #define ABCMB_STATUS_DT_UNDERFLOW 3  /* step size collapsed below 1e-14       */
+#define ABCMB_STATUS_BAD_LAYOUT  4   /* descriptor outside the launch's limits
+                                        (ny > max_ny, l_max outside 4..63)   */
 
 /* ---- PerturbationTable field indices (abcmb/perturbations.py:393-404) ---- */
 enum {

@@ -157,3 +157,14 @@ def test_los_deterministic(gpu, c1_small, c1_oracle):
     a = lr.cl_host().copy()
     lr.run()
     np.testing.assert_array_equal(a, lr.cl_host())
+
+
+def test_bad_layout_is_reported_not_indexed(gpu, c1_small):
+    """A descriptor larger than the launch's shared-memory layout gets status 4."""
+    w = c1_small
+    st = w.pert_settings()
+    st.max_ny = 30                      # smaller than the 43-element state
+    db = gpu.DeviceBatch.upload(w.batch)
+    db.pert_forward(st)
+    ks = db.kstat_host()
+    assert (ks["status"] == 4).all()
