@@ -1,0 +1,102 @@
+"""Drop-in replacement of abcmb.perturbations (PerturbationEvolver / PerturbationTable).
+
+`B200PerturbationEvolver.full_evolution((BG, params))` has the signature and
+the result of `PerturbationEvolver.full_evolution` (abcmb/perturbations.py:75):
+a `PerturbationTable` with fields (Nlna, Nk) -- k, lna, delta_m,
+theta_b_prime, metric_eta, metric_h_prime, metric_eta_prime, metric_alpha,
+metric_alpha_prime and species_perturbations -- computed by the CUDA kernels
+(abcmb_pert_forward).  The background comes in as a
+`background_tables.BackgroundTables` (the tables the reference's
+BackgroundPreRecomb / HyRex / Background produce).  Only the six shipped
+species are supported; any other species tuple raises, as the CUDA path
+cannot compile arbitrary Python right-hand sides.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib, engine, packing
+from . import specs as sp
+
+SPECIES_FIELDS = {
+    "ColdDarkMatter": {"delta": "cdm_delta"},
+    "Baryon": {"delta": "b_delta", "theta": "b_theta"},
+    "Photon": {"delta": "g_delta", "theta": "g_theta", "sigma": "g_sigma", "G0": "g_G0", "G2": "g_G2"},
+    "MasslessNeutrino": {"delta": "nu_delta", "theta": "nu_theta", "sigma": "nu_sigma"},
+    "MassiveNeutrino": {"delta": "ncdm_delta", "theta": "ncdm_theta", "sigma": "ncdm_sigma"},
+    "DarkEnergy": {},
+}
+
+
+@dataclass
+class PerturbationTable:
+    """PerturbationTable (abcmb/perturbations.py:406-450).
+
+    Arrays are host numpy views of the device result, (Nlna, Nk) each; the
+    device buffers stay attached (`device_batch`) so the spectrum kernels
+    read them without a copy.
+    """
+    k: np.ndarray
+    lna: np.ndarray
+    delta_m: np.ndarray
+    theta_b_prime: np.ndarray
+    metric_eta: np.ndarray
+    metric_h_prime: np.ndarray
+    metric_eta_prime: np.ndarray
+    metric_alpha: np.ndarray
+    metric_alpha_prime: np.ndarray
+    species_perturbations: dict
+    device_batch: object = field(default=None, repr=False)
+    kstat: np.ndarray = field(default=None, repr=False)
+
+
+def table_from_fields(fields: np.ndarray, k: np.ndarray, lna: np.ndarray, species: tuple, dbatch=None,
+                      kstat=None) -> PerturbationTable:
+    F = packing.F
+    sp_dict = {}
+    for name in species:
+        sp_dict[name] = {q: fields[F[f]] for q, f in SPECIES_FIELDS[name].items()}
+    return PerturbationTable(k=k, lna=lna, delta_m=fields[F["delta_m"]], theta_b_prime=fields[F["theta_b_prime"]],
+                             metric_eta=fields[F["metric_eta"]], metric_h_prime=fields[F["metric_h_prime"]],
+                             metric_eta_prime=fields[F["metric_eta_prime"]], metric_alpha=fields[F["metric_alpha"]],
+                             metric_alpha_prime=fields[F["metric_alpha_prime"]], species_perturbations=sp_dict,
+                             device_batch=dbatch, kstat=kstat)
+
+
+class B200PerturbationEvolver:
+    """PerturbationEvolver (abcmb/perturbations.py:23-117) on the B200 kernels."""
+
+    def __init__(self, species=("DarkEnergy", "ColdDarkMatter", "Baryon", "Photon", "MasslessNeutrino"),
+                 k_axis_perturbations=None, specs: dict | None = None, device=None):
+        names = tuple(s if isinstance(s, str) else getattr(s, "name", type(s).__name__) for s in species)
+        unknown = [n for n in names if n not in SPECIES_FIELDS]
+        if unknown:
+            raise NotImplementedError(f"species {unknown} have no CUDA right-hand side; "
+                                      f"supported: {sorted(SPECIES_FIELDS)}")
+        if names[:5] != ("DarkEnergy", "ColdDarkMatter", "Baryon", "Photon", "MasslessNeutrino"):
+            raise NotImplementedError("the state layout follows populate_species: the five LCDM species first")
+        self.species = names
+        self.has_ncdm = "MassiveNeutrino" in names
+        self.specs = sp.load_specs(specs or {})
+        if k_axis_perturbations is None:
+            k_axis_perturbations, _ = sp.get_k_axis_perturbations(dict(self.specs))
+        self.k_axis_perturbations = np.asarray(k_axis_perturbations, dtype=np.float64)
+        self.layout = sp.state_layout(self.specs, self.has_ncdm)
+        self.device = device
+
+    def full_evolution(self, args, n_save: int = 500) -> PerturbationTable:
+        """args = (BG, params): BG a BackgroundTables; params unused beyond BG.params."""
+        BG, _params = args
+        batch = packing.pack([BG], [self.layout], [self.k_axis_perturbations], n_save=n_save)
+        st = packing.pert_settings(self.specs, n_save, batch)
+        db = engine.DeviceBatch.upload(batch, self.device)
+        db.pert_forward(st)
+        ks = db.check_status()
+        fields = batch.pt_view(db.pt.cpu().numpy(), 0)
+        lna = np.linspace(BG.lna_transfer_start, 0.0, n_save)
+        return table_from_fields(fields, self.k_axis_perturbations, lna, self.species, dbatch=db, kstat=ks)
+
+
+__all__ = ["B200PerturbationEvolver", "PerturbationTable", "table_from_fields", "_lib"]

@@ -1,0 +1,96 @@
+"""PyTorch registration of the C ABI.
+
+* ``torch.ops.abcmb_b200.pert_forward`` / ``torch.ops.abcmb_b200.los_forward``:
+  ``torch.library`` custom ops over ``abcmb_pert_forward`` /
+  ``abcmb_los_forward``; they write into caller-provided CUDA tensors on the
+  current stream (device memory and stream are torch's; every kernel is the
+  library's).
+* ``ClWithGrad``: a ``torch.autograd.Function`` mapping parameters
+  theta = (h, omega_b, omega_cdm, A_s, n_s, tau_reion) of a batch of
+  cosmologies to C_l^{TT,TE,EE}; its backward contracts the incoming
+  cotangent with dC_l/dtheta computed in the same batched launch
+  (central differences for h, omega_b, omega_cdm, tau_reion; exact A_s, n_s).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib, packing
+
+Tensor = torch.Tensor
+
+
+def _p(t: Tensor) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream() -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+@torch.library.custom_op("abcmb_b200::pert_forward", mutates_args=("pt", "kstat", "workspace"))
+def pert_forward(cosmo: Tensor, tables: Tensor, kbuf: Tensor, items: Tensor, settings: Tensor, pt: Tensor,
+                 kstat: Tensor, workspace: Tensor) -> None:
+    """abcmb_pert_forward; `settings` is the raw bytes of abcmb_pert_settings (CPU uint8)."""
+    st = packing.CPertSettings.from_buffer_copy(settings.numpy().tobytes())
+    n_cosmo = cosmo.numel() // packing.COSMO_DTYPE.itemsize
+    rc = _lib.load().abcmb_pert_forward(n_cosmo, _p(cosmo), _p(tables), _p(kbuf), items.numel() // 2, _p(items),
+                                        ctypes.byref(st), _p(pt), _p(kstat), _p(workspace), workspace.numel(),
+                                        _stream())
+    _lib.check(rc, "abcmb_pert_forward")
+
+
+@torch.library.custom_op("abcmb_b200::los_forward", mutates_args=("cl_raw", "cl", "dcl_dns", "workspace"))
+def los_forward(cosmo: Tensor, cosmo_host: Tensor, tables: Tensor, kbuf: Tensor, pt: Tensor, kt: Tensor,
+                settings: Tensor, cl_raw: Tensor, cl: Tensor, dcl_dns: Tensor, workspace: Tensor) -> None:
+    """abcmb_los_forward; `settings` = bytes of abcmb_los_settings; dcl_dns may be empty (skipped)."""
+    ls = packing.CLosSettings.from_buffer_copy(settings.numpy().tobytes())
+    n_cosmo = cosmo.numel() // packing.COSMO_DTYPE.itemsize
+    hc = cosmo_host.contiguous()
+    rc = _lib.load().abcmb_los_forward(n_cosmo, _p(cosmo), ctypes.c_void_p(hc.data_ptr()), _p(tables), _p(kbuf),
+                                       _p(pt), _p(kt), ctypes.byref(ls), _p(cl_raw), _p(cl),
+                                       _p(dcl_dns) if dcl_dns.numel() else None, _p(workspace), workspace.numel(),
+                                       _stream())
+    _lib.check(rc, "abcmb_los_forward")
+
+
+def settings_bytes(s) -> Tensor:
+    return torch.frombuffer(bytearray(bytes(s)), dtype=torch.uint8)
+
+
+class ClWithGrad(torch.autograd.Function):
+    """theta (n, 6) -> C_l (n, 3, n_l) with dC_l/dtheta from the batched launch.
+
+    `base` is a configs.Workload giving specs, massive-nu flags and k grids
+    of the n cosmologies; theta replaces their (h, omega_b, omega_cdm, A_s,
+    n_s, tau_reion).  Background tables for every finite-difference variant
+    are built on the host (the reference's JAX background would supply them).
+    """
+
+    @staticmethod
+    def forward(ctx, theta: Tensor, base) -> Tensor:
+        from . import configs, engine, gradients
+        th = theta.detach().cpu().numpy()
+        for i, p in enumerate(base.params_in):
+            for j, name in enumerate(configs.GRAD_PARAMS):
+                p[name] = float(th[i, j])
+        gw = gradients.expand(base)
+        db = engine.DeviceBatch.upload(gw.batch, theta.device if theta.is_cuda else None)
+        db.pert_forward(base.pert_settings())
+        db.check_status()
+        lr = engine.LosRunner(db, base.kt, base.los_settings(), want_dns=True)
+        lr.run()
+        n_out = lr.n_out
+        cl_all = lr.cl.cpu().numpy().reshape(-1, 3, n_out)
+        dns_all = lr.dcl_dns.cpu().numpy().reshape(-1, 3, n_out)
+        cl, grad = gw.assemble(cl_all, dns_all)
+        ctx.save_for_backward(torch.from_numpy(grad).to(theta.device))
+        return torch.from_numpy(cl).to(theta.device)
+
+    @staticmethod
+    def backward(ctx, g: Tensor):
+        (grad,) = ctx.saved_tensors                 # (n, 6, 3, n_l)
+        return torch.einsum("npxl,nxl->np", grad, g.to(grad.dtype)), None

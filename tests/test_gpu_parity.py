@@ -168,3 +168,41 @@ def test_bad_layout_is_reported_not_indexed(gpu, c1_small):
     db.pert_forward(st)
     ks = db.kstat_host()
     assert (ks["status"] == 4).all()
+
+
+def test_dropin_objects_match_engine(gpu, c1_small, c1_oracle):
+    """B200PerturbationEvolver / B200SpectrumSolver give the oracle's PT and C_l."""
+    from abcmb_b200.perturbations import B200PerturbationEvolver
+    from abcmb_b200.spectrum import B200SpectrumSolver
+    from abcmb_b200 import bessel
+    from oracle import oracle
+    w = c1_small
+    pt_o, _ = c1_oracle
+    PE = B200PerturbationEvolver(k_axis_perturbations=w.kgrids[0], specs=w.specs)
+    PT = PE.full_evolution((w.bgs[0], w.bgs[0].params))
+    o = w.batch.pt_view(pt_o, 0)
+    assert PT.delta_m.shape == (500, 40)
+    np.testing.assert_allclose(PT.species_perturbations["Photon"]["G0"], o[13], rtol=0, atol=1e-5 * np.abs(o[13]).max())
+    SS = B200SpectrumSolver(2, w.l_max, False, k_axis_transfer=w.kt)
+    tt, te, ee = SS.get_Cl(PT)
+    _, _, cl_o = oracle.los_forward(w.batch, pt_o, w.kt, w.los_settings(), bessel.load())
+    assert np.max(np.abs(tt - cl_o[0, 0]) / cl_o[0, 0]) < 1e-6
+    assert tt.shape == (w.l_max - 1,)
+    pk = SS.Pk_lin(np.geomspace(1e-3, 0.3, 20), 0.0, PT)
+    assert pk.shape == (20,) and np.all(pk > 0)
+
+
+def test_torch_ops_match_engine(gpu, c1_small):
+    import torch
+    from abcmb_b200 import torch_ops, engine
+    w = c1_small
+    st = w.pert_settings()
+    db = engine.DeviceBatch.upload(w.batch)
+    db.pert_forward(st)
+    ref = db.pt.clone()
+    pt2 = torch.empty_like(db.pt)
+    ks2 = torch.zeros_like(db.kstat)
+    torch.ops.abcmb_b200.pert_forward(db.cosmo, db.tables, db.kbuf, db.items, torch_ops.settings_bytes(st), pt2, ks2,
+                                      db.ws_pert)
+    torch.cuda.synchronize()
+    assert torch.equal(ref, pt2)

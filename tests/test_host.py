@@ -86,3 +86,42 @@ def test_los_argument_errors_without_gpu():
                                ctypes.c_void_p(8), ctypes.c_void_p(8), ctypes.byref(ls), ctypes.c_void_p(8),
                                ctypes.c_void_p(8), None, ctypes.c_void_p(8), 0, None)
     assert rc == -1 and b"l_min" in lib.abcmb_last_error()
+
+
+def test_torch_ops_registered_and_settings_roundtrip():
+    import torch
+    from abcmb_b200 import torch_ops, packing
+    assert hasattr(torch.ops.abcmb_b200, "pert_forward") and hasattr(torch.ops.abcmb_b200, "los_forward")
+    st = packing.CPertSettings(max_ny=77, rtol_large=1e-4, n_save=500)
+    back = packing.CPertSettings.from_buffer_copy(torch_ops.settings_bytes(st).numpy().tobytes())
+    assert (back.max_ny, back.rtol_large, back.n_save) == (77, 1e-4, 500)
+
+
+def test_dropin_rejects_species_without_cuda_rhs():
+    from abcmb_b200.perturbations import B200PerturbationEvolver
+    with pytest.raises(NotImplementedError):
+        B200PerturbationEvolver(species=("DarkEnergy", "ColdDarkMatter", "Baryon", "Photon", "MasslessNeutrino",
+                                         "SIDR"))
+    pe = B200PerturbationEvolver(specs={"l_max": 1500})
+    assert len(pe.k_axis_perturbations) > 100 and pe.layout.ny == 1 + 1 + 2 + 13 + 11 + 18
+
+
+def test_gradient_variants_and_assembly():
+    from abcmb_b200 import configs, gradients
+    var = gradients.fd_variants(dict(configs.FIDUCIAL))
+    assert len(var) == 9 and var[0][0] is None
+    assert {v[0] for v in var[1:]} == set(gradients.FD_PARAMS)
+    # assembly on synthetic C_l linear in the parameters recovers the slopes exactly
+    w = configs.c4(n_cosmo=1)
+    gw = gradients.GradWorkload(base=w, variants=[[(v[0], v[1], v[2]) for v in var]], batch=None, n_var=9)
+    slope = {"h": 2.0, "omega_b": -3.0, "omega_cdm": 0.5, "tau_reion": 7.0}
+    cl = np.zeros((9, 3, 4))
+    for j, v in enumerate(var):
+        p = v[3]
+        cl[j] = sum(slope[n] * (p[n] - configs.FIDUCIAL[n]) for n in slope) + 1.0
+    cl_base, grad = gw.assemble(cl, np.full((9, 3, 4), 5.0))
+    names = configs.GRAD_PARAMS
+    for n, s in slope.items():
+        np.testing.assert_allclose(grad[0, names.index(n)], s, rtol=1e-6)
+    np.testing.assert_allclose(grad[0, names.index("n_s")], 5.0)
+    np.testing.assert_allclose(grad[0, names.index("A_s")], cl_base[0] / w.params_in[0]["A_s"])
