@@ -57,6 +57,11 @@ int g_last_grid = 0;
 
 }  // namespace
 
+namespace abcmb {
+// error message for abcmb_last_error from entry points in other files
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace abcmb
+
 extern "C" {
 
 int abcmb_version(void) { return ABCMB_B200_VERSION; }

@@ -216,6 +216,28 @@ int abcmb_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev,
                        void* workspace_dev, int64_t workspace_bytes,
                        void* stream);
 
+/*
+ * abcmb_pert_forward for callers that cannot allocate device memory (no
+ * cudaMalloc, no workspace of their own: e.g. code inside a framework that
+ * owns every device byte).  No counterpart in the reference.  Same inputs,
+ * outputs and results as abcmb_pert_forward, but the scratch lives in a
+ * library-owned static device array (about 1.2 MiB per device, held until
+ * the process exits), so:
+ *   - n_cosmo must not exceed ABCMB_PERT_NOALLOC_MAX_COSMO
+ *     (ABCMB_ERR_WORKSPACE otherwise);
+ *   - calls whose kernels may overlap on the GPU (unordered streams) race on
+ *     the shared array: order them on one stream;
+ *   - the first call on a device looks up the array's address with that
+ *     device current: make it before any stream capture.
+ */
+#define ABCMB_PERT_NOALLOC_MAX_COSMO 8
+int abcmb_pert_forward_noalloc(int n_cosmo, const abcmb_cosmo* cosmo_dev,
+                               const double* tables_dev, const double* k_dev,
+                               int n_items, const int32_t* items_dev,
+                               const abcmb_pert_settings* settings,
+                               double* pt_dev, abcmb_kstat* kstat_dev,
+                               void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Spectrum: SpectrumSolver.get_Cl (spectrum.py:574-614)                   */
 /* ------------------------------------------------------------------------ */
