@@ -147,45 +147,90 @@ struct BG {
   double eps[3];     // sqrt(q^2 + (m/T)^2) for the 3 perturbation q-bins
 };
 
+// fast_interp index of one table (ABCMBTools.py:300-307): lower node and weight
+__device__ __forceinline__ void lerp_index(double x, double xp_min, double xp_max, int n, int& il, int& iu,
+                                           double& wu) {
+  double i = (x - xp_min) / (xp_max - xp_min) * (double)(n - 1);
+  i = fmin(fmax(i, 1.e-6), (double)(n - 1) - 1.e-6);
+  il = (int)floor(i);
+  iu = min(il + 1, n - 1);
+  wu = i - (double)il;
+}
+
+// Quadrature constants of MassiveNeutrino.rho / P (species.py:835-877),
+// w_j (1 + e^{-q_j}) / q_j^2 and w_j (1 + e^{-q_j}), evaluated in FP64.
+static __constant__ double R5[5] = {0.03720333831716864, 0.19567702290257588, 0.17860619858834093,
+                                    0.038888252814630056, 0.0007503567256353378};
+static __constant__ double P5[5] = {0.012652164020403861, 0.7827080916103035, 2.857699177413455,
+                                    2.052994097538504, 0.1268102866323721};
+
+// Every background scalar at one lna.  Same formulas as the reference; the
+// three table reads are issued before the density sums so their latencies
+// overlap, and powers of 1/a replace repeated divisions.
 __device__ __forceinline__ void bg_eval(const abcmb_cosmo& c, const double* __restrict__ tables, double lna,
                                         BG& b) {
-  double a = exp(lna);
+  int t0, t1, x0, x1, m0, m1;
+  double tw, xw, mw;
+  lerp_index(lna, ABCMB_LNA_TAU_MIN, ABCMB_LNA_TAU_MAX, ABCMB_NTAU_TAB, t0, t1, tw);
+  lerp_index(lna, c.lna_xe0, c.lna_xe_max, c.n_xe, x0, x1, xw);
+  lerp_index(lna, c.lna_tm0, c.lna_tm_max, c.n_tm, m0, m1, mw);
+  const double* tt = tables + c.off_tau;
+  const double* tx = tables + c.off_xe;
+  const double* tm = tables + c.off_tm;
+  const double ta = __ldg(tt + t0), tb = __ldg(tt + t1);
+  const double xa = __ldg(tx + x0), xb = __ldg(tx + x1);
+  const double ma = __ldg(tm + m0), mb = __ldg(tm + m1);
+  const double a = exp(lna);
+  const double ia = 1. / a;
+  const double ia2 = ia * ia, ia3 = ia2 * ia, ia4 = ia2 * ia2;
   b.a = a;
-  Rho r = rho_all(c, a);
-  b.rho_cdm = r.cdm;
-  b.rho_b = r.b;
-  b.rho_g = r.g;
-  b.rho_nu = r.nu;
-  b.rho_ncdm = r.ncdm;
-  b.P_ncdm = r.Pncdm;
-  double H = sqrt(8. * PI * GN * r.tot / 3.);
-  b.aH = a * H / C_MPC;
-  b.tau = tau_of(c, tables, lna);
-  double xe = xe_of(c, tables, lna);
-  double ne = nH_of(c, a) * xe;
-  b.tau_c = 1. / a / ne / SIGT / C_CM * C_MPC;
-  double TCMB = c.TCMB0 / a;
-  double Tm;
-  if (lna < c.lna_tm0) {
-    Tm = TCMB * (1. - H / gamma_compton(xe, TCMB, c.YHe));
-  } else if (lna >= c.lna_tm_last) {
-    Tm = c.tm_last;
-  } else {
-    Tm = fast_interp(lna, c.lna_tm0, c.lna_tm_max, tables + c.off_tm, c.n_tm);
+  const double T04 = c.TCMB0 * c.TCMB0 * c.TCMB0 * c.TCMB0;
+  const double tn = c.T_nu_massless;
+  const double rde = c.omega_Lambda * RHO_CRIT_UNIT;
+  b.rho_cdm = c.omega_cdm * RHO_CRIT_UNIT * ia3;
+  b.rho_b = c.omega_b * RHO_CRIT_UNIT * ia3;
+  b.rho_g = PI * PI / 15. * T04 * ia4 / CHB3;
+  b.rho_nu = c.N_nu_massless * (2. * 7. / 8. * PI * PI / 30.) * (tn * tn * tn * tn) * T04 * ia4 / CHB3;
+  b.rho_ncdm = 0.;
+  b.P_ncdm = 0.;
+  double x = 0.;
+  b.ncdm_fac = 0.;
+  if (c.has_ncdm) {
+    const double T = c.T_nu_massive * c.TCMB0 * ia;
+    x = c.m_nu_massive / T;
+    double ir = 0., ip = 0.;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const double e = sqrt(Q5[j] * Q5[j] + x * x);
+      ir = fma(R5[j], e, ir);
+      ip += P5[j] / e;
+    }
+    const double T4 = T * T * T * T;
+    const double f = c.N_nu_massive * T4 / (PI * PI) / HB3C3;
+    b.rho_ncdm = 4. * f * ir;
+    b.P_ncdm = 4. / 3. * f * ip;
+    b.ncdm_fac = 4. * f;
   }
-  double denom = (1. + xe) * (1. - c.YHe) + MH / MHE * c.YHe;
-  double mu = MH / denom;
-  b.R = 4. * r.g / 3. / r.b;
+  const double tot = rde + b.rho_cdm + b.rho_b + b.rho_g + b.rho_nu + b.rho_ncdm;
+  const double H = sqrt(8. * PI * GN / 3. * tot);
+  b.aH = a * H / C_MPC;
+  b.tau = (1. - tw) * ta + tw * tb;
+  const double xe = (lna < c.lna_xe0) ? c.xe_first : (lna >= c.lna_xe_last) ? c.xe_last : (1. - xw) * xa + xw * xb;
+  const double ne = nH_of(c, a) * xe;
+  b.tau_c = ia / ne * (C_MPC / (SIGT * C_CM));
+  const double TCMB = c.TCMB0 * ia;
+  double Tm;
+  if (lna < c.lna_tm0) Tm = TCMB * (1. - H / gamma_compton(xe, TCMB, c.YHe));
+  else if (lna >= c.lna_tm_last) Tm = c.tm_last;
+  else Tm = (1. - mw) * ma + mw * mb;
+  const double denom = (1. + xe) * (1. - c.YHe) + MH / MHE * c.YHe;
+  const double mu = MH / denom;
+  b.R = 4. / 3. * b.rho_g / b.rho_b;
   b.cs2 = Tm / mu * (5. / 3. - 2. / 3. * mu * b.R / ME / b.aH / b.tau_c * (TCMB / Tm - 1.));
   if (c.has_ncdm) {
-    double T = c.T_nu_massive * c.TCMB0 / a;
-    double x = c.m_nu_massive / T;
-    double T4 = T * T * T * T;
-    b.ncdm_fac = c.N_nu_massive * 4. / (PI * PI) * T4 / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
 #pragma unroll
     for (int i = 0; i < 3; ++i) b.eps[i] = sqrt(Q3[i] * Q3[i] + x * x);
   } else {
-    b.ncdm_fac = 0.;
     b.eps[0] = b.eps[1] = b.eps[2] = 1.;
   }
 }

@@ -27,6 +27,7 @@ namespace abcmb {
 
 constexpr int WARP = 32;
 constexpr int NCHAIN = 6;            // F, G, N, Psi(q0), Psi(q1), Psi(q2)
+constexpr int NSV = 18;              // saved background: 16 BG values + save-index tag
 constexpr int NSTART = 10000;        // get_starting_time grid
 
 // Kvaerno5 tableau (Kvaerno, BIT 44 (2004) 489-502), ESDIRK 5(4), 7 stages.
@@ -125,8 +126,9 @@ struct WarpMem {
   __device__ __forceinline__ double* Mc() const { return p + 14 * my; }       // ncm x cs core inverse
   __device__ __forceinline__ double* vc() const { return Mc() + ncm * cs; }   // gathered core vector
   __device__ __forceinline__ double* SB() const { return vc() + ncm; }        // NSLOT x NB basis
-  __device__ __forceinline__ double* m3() const { return SB() + 6 * 32; }     // M_{3,4} / d_4 per chain
-  __device__ __forceinline__ int* cmap() const { return reinterpret_cast<int*>(m3() + NCHAIN); }
+  __device__ __forceinline__ double* m3() const { return SB() + 6 * 32; }     // M_{2,3} / d_3 per chain
+  __device__ __forceinline__ double* SV() const { return m3() + NCHAIN; }     // background at the next save time
+  __device__ __forceinline__ int* cmap() const { return reinterpret_cast<int*>(SV() + NSV); }
   __device__ __forceinline__ int* perm() const { return cmap() + ncm; }
   __device__ __forceinline__ int* rstate() const { return perm() + ncm; }    // 5 ncm
   __device__ __forceinline__ int* chs() const { return rstate() + 5 * ncm; }  // 8
@@ -166,7 +168,7 @@ __device__ __forceinline__ int chain_speed_bid(int chn) { return chn < 3 ? B_KIA
 
 __host__ __device__ inline size_t warp_mem_doubles(int max_ny, int ncm) {
   const size_t ints = (size_t)ncm * 7 + (size_t)max_ny + 16;
-  return (size_t)14 * max_ny + (size_t)ncm * (ncm + 1) + (size_t)ncm + NSLOT * NB + NCHAIN + (ints + 1) / 2;
+  return (size_t)14 * max_ny + (size_t)ncm * (ncm + 1) + (size_t)ncm + NSLOT * NB + NCHAIN + NSV + (ints + 1) / 2;
 }
 
 __device__ __forceinline__ void carve(double* p, int max_ny, int ncm, WarpMem& m) {
@@ -174,6 +176,17 @@ __device__ __forceinline__ void carve(double* p, int max_ny, int ncm, WarpMem& m
   m.my = max_ny;
   m.ncm = ncm;
   m.cs = ncm + 1;
+}
+
+// 1/s for s > 0: an FP32 seed refined by two Newton steps (relative error
+// ~1e-15); used for the tolerance scales of the norms, far cheaper than an
+// FP64 division.  Values outside the FP32 range take the division.
+__device__ __forceinline__ double pos_rcp(double s) {
+  if (!(s > 1e-30 && s < 1e30)) return 1. / s;
+  double r = (double)__frcp_rn((float)s);
+  r = r * fma(-s, r, 2.);
+  r = r * fma(-s, r, 2.);
+  return r;
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -186,10 +199,29 @@ __device__ __forceinline__ double warp_sum(double v) {
 // Background basis at one time (one lane per time; abcmb/background.py and
 // species.py evaluators through bg_eval).
 // ---------------------------------------------------------------------------
+// BG <-> shared memory (the background of a save point computed ahead)
+__device__ __forceinline__ void bg_store(const BG& b, double* s) {
+  s[0] = b.a; s[1] = b.aH; s[2] = b.tau; s[3] = b.tau_c; s[4] = b.cs2; s[5] = b.R;
+  s[6] = b.rho_cdm; s[7] = b.rho_b; s[8] = b.rho_g; s[9] = b.rho_nu; s[10] = b.rho_ncdm; s[11] = b.P_ncdm;
+  s[12] = b.ncdm_fac; s[13] = b.eps[0]; s[14] = b.eps[1]; s[15] = b.eps[2];
+}
+__device__ __forceinline__ void bg_load(const double* s, BG& b) {
+  b.a = s[0]; b.aH = s[1]; b.tau = s[2]; b.tau_c = s[3]; b.cs2 = s[4]; b.R = s[5];
+  b.rho_cdm = s[6]; b.rho_b = s[7]; b.rho_g = s[8]; b.rho_nu = s[9]; b.rho_ncdm = s[10]; b.P_ncdm = s[11];
+  b.ncdm_fac = s[12]; b.eps[0] = s[13]; b.eps[1] = s[14]; b.eps[2] = s[15];
+}
+
+// Background basis of one stage time; with sv != null the same lane instead
+// stores the full background of a save time (lanes 0-4 stage times, lane 5
+// the next save point: one instruction stream, no divergence).
 __device__ __noinline__ void stage_basis(const abcmb_cosmo& c, const double* __restrict__ tables, double k,
-                                         double lna, double* B) {
+                                         double lna, double* B, double* sv) {
   BG b;
   bg_eval(c, tables, lna, b);
+  if (sv) {
+    bg_store(b, sv);
+    return;
+  }
   const double aH = b.aH;
   const double iaH = 1. / aH;
   const double kap = iaH / b.tau_c;                          // 1/(aH tau_c)
@@ -342,9 +374,10 @@ __device__ __forceinline__ void core_row_at(const Layout& L, const RowTab& R, co
 #ifndef PERT_APPLY_ATTR
 #define PERT_APPLY_ATTR
 #endif
+// out = A v - fsub (fsub may be null): the RHS, or the chord residual directly.
 __device__ PERT_APPLY_ATTR void apply_A(const Layout& L, const WarpMem& m, const RowTab& R, const CoreRow& cr,
-                                       const double* B,
-                        const double* v, double* out, bool ncdm, int lane) {
+                                       const double* B, const double* v, double* out, const double* fsub,
+                                       bool ncdm, int lane) {
   double hp, etap;
   metric(L, B, v, ncdm, hp, etap);
   if (lane < L.nc) {
@@ -352,7 +385,7 @@ __device__ PERT_APPLY_ATTR void apply_A(const Layout& L, const WarpMem& m, const
 #pragma unroll
     for (int t = 0; t < 5; ++t) acc = fma(cr.c[t], v[cr.s[t]], acc);
     acc = fma(cr.tc, v[cr.ts], acc);
-    out[cr.out] = acc;
+    out[cr.out] = fsub ? acc - fsub[cr.out] : acc;
   }
   const double trunc = B[B_TRUNC];
   for (int t = lane; t < L.ntail; t += WARP) {
@@ -366,7 +399,7 @@ __device__ PERT_APPLY_ATTR void apply_A(const Layout& L, const WarpMem& m, const
       const int li = info >> 16;
       fv = s * (R.ta[li] * v[e - 1] - R.tg[li] * v[e + 1]) - d * v[e];
     }
-    out[e] = fv;
+    out[e] = fsub ? fv - fsub[e] : fv;
   }
   __syncwarp();
 }
@@ -537,9 +570,11 @@ __device__ void solve_newton(const Layout& L, WarpMem& m, double* r, int lane) {
 
 // Fields of make_output_table at one save point from the interpolated state ys.
 __device__ __noinline__ void write_fields(const abcmb_cosmo& c, const Layout& L, const double* tables, double k, double lna,
-                             const double* ys, double* pt, int n_save, int isave, int ik, int lane) {
+                             const double* ys, double* pt, int n_save, int isave, int ik, int lane,
+                             const double* sv) {
   BG b;
-  bg_eval(c, tables, lna, b);
+  if (sv) bg_load(sv, b);               // computed ahead for this save point
+  else bg_eval(c, tables, lna, b);
   const double a = b.a, aH = b.aH;
   double srd = b.rho_cdm * ys[1] + b.rho_b * ys[2] + b.rho_g * ys[L.i_g] + b.rho_nu * ys[L.i_nu];
   double srt = (b.rho_b + 0.) * ys[3] + (b.rho_g + b.rho_g / 3.) * ys[L.i_g + 1] +
@@ -708,6 +743,7 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
     Layout L;
     make_layout(c, L);
     const int n = L.ny;
+    const double inv_n = 1. / (double)n;
     const bool ncdm = c.has_ncdm != 0;
     // a descriptor this launch cannot hold is reported, never indexed
     {
@@ -784,7 +820,8 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
           Pb[2] = ns / 2. * fac;
         }
       }
-      stage_basis(c, P.tables, k, lna_start, m.SB());
+      stage_basis(c, P.tables, k, lna_start, m.SB(), nullptr);
+      m.SV()[16] = -1.;                                      // no save background computed yet
     }
     __syncwarp();
 
@@ -794,7 +831,7 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
     int isave = 0, nsteps = 0, nacc = 0, nrej = 0, nnewton = 0, status = ABCMB_STATUS_OK;
     CoreRow cr;
     core_row_at(L, R, m, m.SB(), lane, cr);
-    apply_A(L, m, R, cr, m.SB(), m.y0(), m.F(), ncdm, lane);     // FSAL stage 1
+    apply_A(L, m, R, cr, m.SB(), m.y0(), m.F(), nullptr, ncdm, lane);   // FSAL stage 1
 
     while (t0 < 0.0) {
       if (nsteps >= S.max_steps) { status = ABCMB_STATUS_MAX_STEPS; break; }
@@ -802,7 +839,16 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
       const double h = t1 - t0;
       const double hg = h * KV_G;
       // background of the five distinct stage times, one lane each
-      if (lane < NSLOT - 1) stage_basis(c, P.tables, k, t0 + KV_C[lane + 1] * h, m.SB() + (lane + 1) * NB);
+      {
+        // lanes 0-4: the five distinct stage times; lane 5: the next save
+        // point if this step's candidate end covers it
+        const double tsn = isave < nsave ? linspace_at(lts, 0.0, nsave, isave) : 1.0;
+        const bool want_sv = lane == NSLOT - 1 && tsn <= t1 && (double)isave != m.SV()[16];
+        if (lane < NSLOT - 1 || want_sv)
+          stage_basis(c, P.tables, k, want_sv ? tsn : t0 + KV_C[lane + 1] * h, m.SB() + (lane + 1) * NB,
+                      want_sv ? m.SV() : nullptr);
+        if (want_sv) m.SV()[16] = (double)isave;
+      }
       __syncwarp();
       factor_newton(L, m, R, m.SB() + NB, hg, ncdm, lane);
       bool ok = true;
@@ -822,29 +868,29 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
         for (int it = 1; it <= root_max; ++it) {
           for (int e = lane; e < n; e += WARP) m.v()[e] = m.base()[e] + hg * fi[e];
           __syncwarp();
-          apply_A(L, m, R, cr, B, m.v(), m.r(), ncdm, lane);
-          for (int e = lane; e < n; e += WARP) m.r()[e] = m.r()[e] - fi[e];
-          __syncwarp();
+          apply_A(L, m, R, cr, B, m.v(), m.r(), fi, ncdm, lane);    // residual A v - f
           solve_newton(L, m, m.r(), lane);
           double ss = 0.;
           for (int e = lane; e < n; e += WARP) {
             double x = m.r()[e];
             double fnew = fi[e] + x;
             fi[e] = fnew;
-            double q = x / (atol + rtol * fabs(fnew));
+            double q = x * pos_rcp(atol + rtol * fabs(fnew));
             ss += q * q;
           }
           ss = warp_sum(ss);
-          __syncwarp();
           diffsize_prev = diffsize;
-          diffsize = sqrt(ss / n);
+          diffsize = sqrt(ss * inv_n);
           ++nnewton;
           if (it >= 2) {
-            double rate = diffsize / diffsize_prev;
-            double factor = diffsize * rate / (1. - rate);
-            bool small = diffsize < small_res;
-            bool diverged = !isfinite(rate) || rate > 2.;
-            bool converged = factor > 0. && factor < kappa;
+            // optimistix very-chord termination, without divisions:
+            // rate = d/dp; converged <=> 0 < rate < 1 and d rate / (1 - rate) < kappa
+            //                        <=> 0 < d < dp and d^2 < kappa (dp - d);
+            // diverged <=> rate not finite or rate > 2 <=> !(d <= 2 dp)
+            const double d = diffsize, dp = diffsize_prev;
+            const bool small = d < small_res;
+            const bool converged = d > 0. && d < dp && d * d < kappa * (dp - d);
+            const bool diverged = !(d <= 2. * dp);
             if (small || converged) { conv = true; break; }
             if (diverged) break;
           }
@@ -868,11 +914,11 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
           double y1e = y0e + h * acc;
           m.y1()[e] = y1e;
           double err = h * acce;
-          double q = err / (atol + fmax(fabs(y0e), fabs(y1e)) * rtol);
+          double q = err * pos_rcp(atol + fmax(fabs(y0e), fabs(y1e)) * rtol);
           ss += q * q;
         }
         ss = warp_sum(ss);
-        scaled = sqrt(ss / n);
+        scaled = sqrt(ss * inv_n);
         if (!isfinite(scaled)) scaled = INFINITY;
       }
       __syncwarp();
@@ -897,7 +943,8 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
             m.v()[e] = y0e + th * (k0 + th * ((3. * (y1e - y0e) - 2. * k0 - k1) + th * (2. * (y0e - y1e) + k0 + k1)));
           }
           __syncwarp();
-          write_fields(c, L, P.tables, k, ts, m.v(), P.pt, nsave, isave, ik, lane);
+          write_fields(c, L, P.tables, k, ts, m.v(), P.pt, nsave, isave, ik, lane,
+                       m.SV()[16] == (double)isave ? m.SV() : nullptr);
           __syncwarp();
           ++isave;
         }
