@@ -129,8 +129,9 @@ struct WarpMem {
   __device__ __forceinline__ double* m3() const { return SB() + 6 * 32; }     // M_{2,3} / d_3 per chain
   __device__ __forceinline__ double* SV() const { return m3() + NCHAIN; }     // background at the next save time
   __device__ __forceinline__ int* cmap() const { return reinterpret_cast<int*>(SV() + NSV); }
-  __device__ __forceinline__ int* perm() const { return cmap() + ncm; }
-  __device__ __forceinline__ int* rstate() const { return perm() + ncm; }    // 5 ncm
+  __device__ __forceinline__ int* perm() const { return cmap() + ncm; }      // pivot row of column k
+  __device__ __forceinline__ int* iperm() const { return perm() + ncm; }     // column whose pivot row is j
+  __device__ __forceinline__ int* rstate() const { return iperm() + ncm; }   // 5 ncm
   __device__ __forceinline__ int* chs() const { return rstate() + 5 * ncm; }  // 8
   __device__ __forceinline__ int* chL() const { return chs() + 8; }           // 8
   __device__ __forceinline__ int* tinfo() const { return chL() + 8; }         // max_ny
@@ -167,7 +168,7 @@ enum {
 __device__ __forceinline__ int chain_speed_bid(int chn) { return chn < 3 ? B_KIAH : B_NCDM + 3 * (chn - 3) + 1; }
 
 __host__ __device__ inline size_t warp_mem_doubles(int max_ny, int ncm) {
-  const size_t ints = (size_t)ncm * 7 + (size_t)max_ny + 16;
+  const size_t ints = (size_t)ncm * 8 + (size_t)max_ny + 16;
   return (size_t)14 * max_ny + (size_t)ncm * (ncm + 1) + (size_t)ncm + NSLOT * NB + NCHAIN + NSV + (ints + 1) / 2;
 }
 
@@ -454,7 +455,7 @@ __device__ void factor_newton(const Layout& L, WarpMem& m, const RowTab& R, cons
         sup = hg * s * R.tg[li];
         sb = -hg * s * R.ta[li];
       }
-      double inv = 1. / (diag - sup * sub_next * inv_next);
+      double inv = pos_rcp(diag - sup * sub_next * inv_next);    // pivots are >= 1
       m.invd()[e] = inv;
       m.mult()[e] = sup * inv_next;
       m.sub()[e] = sb;
@@ -468,42 +469,34 @@ __device__ void factor_newton(const Layout& L, WarpMem& m, const RowTab& R, cons
     m.m3()[chn] = M23 * inv_next;
   }
   __syncwarp();
-  // in-place Gauss-Jordan inverse of the core with partial (row) pivoting
+  // In-place Gauss-Jordan inverse of the core with partial pivoting and no
+  // row exchanges: the pivot of column p is the not-yet-used row q_p of
+  // largest |M[.][p]| (compared on the high 32 bits of the IEEE pattern,
+  // monotonic in magnitude; ties -> lowest row), recorded in perm[p] and left
+  // in place.  Afterwards A^{-1}[i][j] = Mc[q_i][k] with q_k = j, which
+  // solve_newton applies as x_i = sum_k Mc[q_i][k] b[q_k].
+  unsigned used = 0u;
   for (int p = 0; p < nc; ++p) {
-    // pivot = row p..nc-1 of largest |M[.][p]|, compared on the high 32 bits
-    // of the IEEE representation (monotonic in magnitude; ties -> lowest row)
-    const bool elig = lane >= p && lane < nc;
+    const bool elig = lane < nc && !((used >> lane) & 1u);
     const unsigned key = elig ? (unsigned)(__double_as_longlong(fabs(m.Mc()[lane * CS + p])) >> 32) : 0u;
     const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
     const unsigned hit = __ballot_sync(0xffffffffu, elig && key == kmax);
-    const int q = hit ? __ffs(hit) - 1 : p;
-    if (lane == 0) m.perm()[p] = q;
-    if (q != p && lane < nc) {
-      double a = m.Mc()[p * CS + lane], bq = m.Mc()[q * CS + lane];
-      m.Mc()[p * CS + lane] = bq;
-      m.Mc()[q * CS + lane] = a;
+    const int q = __ffs(hit) - 1;
+    used |= 1u << q;
+    if (lane == 0) {
+      m.perm()[p] = q;
+      m.iperm()[q] = p;
     }
+    const double pinv = 1. / m.Mc()[q * CS + p];
     __syncwarp();
-    const double pinv = 1. / m.Mc()[p * CS + p];
+    if (lane < nc) m.Mc()[q * CS + lane] = (lane == p ? 1. : m.Mc()[q * CS + lane]) * pinv;
     __syncwarp();
-    if (lane < nc) m.Mc()[p * CS + lane] = (lane == p ? 1. : m.Mc()[p * CS + lane]) * pinv;
-    __syncwarp();
-    if (lane < nc && lane != p) {
+    if (lane < nc && lane != q) {
       double* row = m.Mc() + lane * CS;
-      const double* prow = m.Mc() + p * CS;
+      const double* prow = m.Mc() + q * CS;
       double f = row[p];
       row[p] = 0.;
       for (int j = 0; j < nc; ++j) row[j] = fma(-f, prow[j], row[j]);
-    }
-    __syncwarp();
-  }
-  for (int p = nc - 1; p >= 0; --p) {
-    int q = m.perm()[p];
-    if (q != p && lane < nc) {
-      double* row = m.Mc() + lane * CS;
-      double a = row[p];
-      row[p] = row[q];
-      row[q] = a;
     }
     __syncwarp();
   }
@@ -534,15 +527,19 @@ __device__ void solve_newton(const Layout& L, WarpMem& m, double* r, int lane) {
       r[e] = nxt;
     }
     const int cc = chain_core_l2(chn);
-    m.vc()[cc] = r[m.cmap()[cc]] - m.m3()[chn] * nxt;
+    m.vc()[m.iperm()[cc]] = r[m.cmap()[cc]] - m.m3()[chn] * nxt;
   }
   // every other core row gathers its right-hand side directly
-  if (lane < nc && !(lane >= 4 && (lane - 4) % 3 == 2)) m.vc()[lane] = r[m.cmap()[lane]];
+  // (vc is stored permuted: the entry for core row j goes to slot iperm[j])
+  if (lane < nc && !(lane >= 4 && (lane - 4) % 3 == 2)) m.vc()[m.iperm()[lane]] = r[m.cmap()[lane]];
   __syncwarp();
   double xc = 0.;
   if (lane < nc) {
-    const double* row = m.Mc() + lane * m.cs;
-    for (int j = 0; j < nc; ++j) xc = fma(row[j], m.vc()[j], xc);
+    // x_i = sum_k Mc[q_i][k] b[q_k] (pivot rows left in place, see
+    // factor_newton); vc already holds b[q_k] in slot k
+    const double* row = m.Mc() + m.perm()[lane] * m.cs;
+    const double* vc = m.vc();
+    for (int j = 0; j < nc; ++j) xc = fma(row[j], vc[j], xc);
   }
   __syncwarp();
   if (lane < nc) r[m.cmap()[lane]] = xc;
@@ -865,9 +862,9 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
         __syncwarp();
         double diffsize = INFINITY, diffsize_prev;
         bool conv = false;
+        for (int e = lane; e < n; e += WARP) m.v()[e] = m.base()[e] + hg * fi[e];
+        __syncwarp();
         for (int it = 1; it <= root_max; ++it) {
-          for (int e = lane; e < n; e += WARP) m.v()[e] = m.base()[e] + hg * fi[e];
-          __syncwarp();
           apply_A(L, m, R, cr, B, m.v(), m.r(), fi, ncdm, lane);    // residual A v - f
           solve_newton(L, m, m.r(), lane);
           double ss = 0.;
@@ -875,10 +872,12 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
             double x = m.r()[e];
             double fnew = fi[e] + x;
             fi[e] = fnew;
+            m.v()[e] = m.base()[e] + hg * fnew;                 // the next iteration's argument
             double q = x * pos_rcp(atol + rtol * fabs(fnew));
             ss += q * q;
           }
           ss = warp_sum(ss);
+          __syncwarp();
           diffsize_prev = diffsize;
           diffsize = sqrt(ss * inv_n);
           ++nnewton;
