@@ -32,6 +32,9 @@ SIGNATURES = [
                                          _vp]),
     ("abcmb_pk_lin", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _d, ctypes.c_int, _vp, ctypes.c_int,
                                     _vp, _vp, _vp]),
+    ("abcmb_lens_workspace_size", _i64, [ctypes.c_int, _vp]),
+    ("abcmb_lens_forward", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                          _i64, _vp]),
     ("abcmb_set_pert_warps_per_block", ctypes.c_int, [ctypes.c_int]),
     ("abcmb_last_pert_grid", ctypes.c_int, []),
     ("abcmb_probe_fp64_tflops", ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.c_int, _vp]),

@@ -41,12 +41,14 @@ class Workload:
     has_ncdm: list
     kgrids: list
     l_max: int
+    lensing: bool = False
     bgs: list = field(default_factory=list)
     layouts: list = field(default_factory=list)
     batch: packing.Batch = None
     kt: np.ndarray = None
     idx_min: int = 0
     idx_max: int = 0
+    l_los: int = 0               # last ell of the line-of-sight output (l_max, + 500 when lensing)
 
     def build(self, n_save: int = 500):
         self.bgs = []
@@ -60,20 +62,27 @@ class Workload:
         sp.get_k_axis_perturbations(ks)
         self.kt = sp.get_k_axis_transfer(ks)
         B = bessel_mod.load()
-        self.idx_min, self.idx_max, _ = sp.ell_index_range(B.l_tab, int(self.specs["l_min"]), self.l_max, False)
+        self.idx_min, self.idx_max, self.l_los = sp.ell_index_range(B.l_tab, int(self.specs["l_min"]), self.l_max,
+                                                                    self.lensing)
         return self
 
     def pert_settings(self):
         return packing.pert_settings(self.specs, self.batch.n_save, self.batch)
 
     def los_settings(self, precision: int = 0):
-        return packing.los_settings(self.specs, self.idx_min, self.idx_max, len(self.kt), self.l_max,
+        return packing.los_settings(self.specs, self.idx_min, self.idx_max, len(self.kt), self.l_los,
                                     precision=precision, n_save=self.batch.n_save)
 
+    def lens_settings(self):
+        """Settings of abcmb_lens_forward (lensed output to l_max, input to l_max + 500)."""
+        from . import lensing
+        return lensing.lens_settings(self.l_max, self.specs["k_pivot"], self.batch.n_save,
+                                     int(self.batch.cosmo["nk"].max()))
 
-def c1(nk: int = 200, l_max: int = 1500) -> Workload:
-    specs = sp.load_specs(dict(l_max=l_max, lensing=False, l_max_g=12, l_max_pol_g=12, l_max_massless_nu=12))
-    return Workload("C1", specs, [dict(FIDUCIAL)], [False], [np.geomspace(1e-4, 0.5, nk)], l_max)
+
+def c1(nk: int = 200, l_max: int = 1500, lensing: bool = False) -> Workload:
+    specs = sp.load_specs(dict(l_max=l_max, lensing=lensing, l_max_g=12, l_max_pol_g=12, l_max_massless_nu=12))
+    return Workload("C1", specs, [dict(FIDUCIAL)], [False], [np.geomspace(1e-4, 0.5, nk)], l_max, lensing)
 
 
 def c2(nk: int = 600, l_max: int = 2500, lmax_h: int = 30) -> Workload:

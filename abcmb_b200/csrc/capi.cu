@@ -20,6 +20,11 @@ cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_co
 cudaError_t launch_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* kbuf, const double* pt,
                           int n_save, double k_pivot, int n_kout, const double* kout, int n_z, const double* z,
                           double* pk, cudaStream_t stream);
+int64_t lens_workspace_bytes(int n_cosmo, const abcmb_lens_settings& s);
+cudaError_t launch_lens(int n_cosmo, const abcmb_cosmo* cosmo, const abcmb_lens_cosmo* lens, const double* tables,
+                        const double* kbuf, const double* pt, const double* mu, const double* w,
+                        const double* cl_unl, const abcmb_lens_settings& s, double* clpp, double* cl, void* ws,
+                        cudaStream_t stream);
 }  // namespace abcmb
 
 namespace {
@@ -184,6 +189,35 @@ int abcmb_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* k_dev,
   cudaError_t e = abcmb::launch_pk_lin(n_cosmo, cosmo_dev, k_dev, pt_dev, n_save, k_pivot, n_kout, kout_dev, n_z,
                                        z_dev, pk_dev, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "abcmb_pk_lin");
+  return ABCMB_OK;
+}
+
+static bool lens_settings_ok(int n_cosmo, const abcmb_lens_settings* s) {
+  return s && n_cosmo > 0 && n_cosmo <= 65535 && s->l_max >= 2 && s->l_lens >= s->l_max && s->n_mu >= 2 &&
+         s->n_lna >= 3 && s->n_save >= 2 && s->max_nk >= 1;
+}
+
+int64_t abcmb_lens_workspace_size(int n_cosmo, const abcmb_lens_settings* settings) {
+  if (!lens_settings_ok(n_cosmo, settings)) return fail(ABCMB_ERR_ARG, "abcmb_lens_workspace_size: bad settings");
+  return abcmb::lens_workspace_bytes(n_cosmo, *settings);
+}
+
+int abcmb_lens_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_lens_cosmo* lens_dev,
+                       const double* tables_dev, const double* k_dev, const double* pt_dev, const double* mu_dev,
+                       const double* w_dev, const double* cl_unlensed_dev, const abcmb_lens_settings* settings,
+                       double* clpp_dev, double* cl_dev, void* workspace_dev, int64_t workspace_bytes,
+                       void* stream) {
+  if (!cosmo_dev || !lens_dev || !tables_dev || !k_dev || !pt_dev || !mu_dev || !w_dev || !cl_unlensed_dev ||
+      !clpp_dev || !cl_dev)
+    return fail(ABCMB_ERR_ARG, "abcmb_lens_forward: null argument");
+  if (!lens_settings_ok(n_cosmo, settings))
+    return fail(ABCMB_ERR_ARG, "abcmb_lens_forward: settings (need 2 <= l_max <= l_lens, n_mu >= 2, n_lna >= 3)");
+  const int64_t need = abcmb::lens_workspace_bytes(n_cosmo, *settings);
+  if (!workspace_dev || workspace_bytes < need) return fail(ABCMB_ERR_WORKSPACE, "abcmb_lens_forward: workspace");
+  cudaError_t e = abcmb::launch_lens(n_cosmo, cosmo_dev, lens_dev, tables_dev, k_dev, pt_dev, mu_dev, w_dev,
+                                     cl_unlensed_dev, *settings, clpp_dev, cl_dev, workspace_dev,
+                                     static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "abcmb_lens_forward");
   return ABCMB_OK;
 }
 

@@ -52,6 +52,13 @@ class CKStat(ctypes.Structure):
                 ("n_newton", ctypes.c_int32), ("lna_start", ctypes.c_double)]
 
 
+class CLensSettings(ctypes.Structure):
+    _fields_ = [("k_pivot", ctypes.c_double)] + \
+               [(n, ctypes.c_int32) for n in ["l_max", "l_lens", "n_mu", "n_lna", "n_save", "max_nk"]]
+
+
+LENS_DTYPE = np.dtype([("lna_rec", "<f8"), ("omega_m", "<f8")], align=True)
+
 KSTAT_DTYPE = np.dtype([("status", "<i4"), ("n_accepted", "<i4"), ("n_rejected", "<i4"),
                         ("n_newton", "<i4"), ("lna_start", "<f8")], align=True)
 

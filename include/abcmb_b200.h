@@ -283,6 +283,60 @@ int abcmb_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* k_dev,
                  double* pk_dev, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Lensing: SpectrumSolver.lensing_Cl / lensed_Cls (spectrum.py:349-572)    */
+/* ------------------------------------------------------------------------ */
+
+/* Per-cosmology lensing inputs. */
+typedef struct abcmb_lens_cosmo {
+  double lna_rec;     /* BG.lna_rec: argmax of the visibility on
+                         linspace(-8, -4, 1500) (abcmb/background.py:555-557) */
+  double omega_m;     /* params["omega_m"] (abcmb/main.py:569-574)           */
+} abcmb_lens_cosmo;
+
+/* Lensing settings (SpectrumSolver.__init__, abcmb/spectrum.py:219-236). */
+typedef struct abcmb_lens_settings {
+  double k_pivot;
+  int32_t l_max;      /* lensed output ells 2..l_max                          */
+  int32_t l_lens;     /* lensing_ellmax = l_max + 500: unlensed input and
+                         C_l^phiphi on ells 2..l_lens                         */
+  int32_t n_mu;       /* quadrature nodes: the l_lens + 70 Gauss-Legendre
+                         nodes plus mu = 1 with weight 0, mu ascending        */
+  int32_t n_lna;      /* Limber quadrature points (500, spectrum.py:419)     */
+  int32_t n_save;     /* PT save points (500)                                */
+  int32_t max_nk;     /* largest perturbation k grid in the batch            */
+} abcmb_lens_settings;
+
+/* Bytes of device workspace abcmb_lens_forward needs. */
+int64_t abcmb_lens_workspace_size(int n_cosmo, const abcmb_lens_settings* settings);
+
+/*
+ * Lensed TT, TE, EE (no BB, like the reference) for every cosmology:
+ * C_l^phiphi in the Limber approximation (lensing_Cl, spectrum.py:386-435,
+ * with lensing_power_spectrum :349-384 and Pk_lin :268-302), the lensing
+ * correlation functions on the mu nodes from the Wigner-d recursions
+ * (lensed_Cls :437-572; ABCMBTools.wigner_d_matrix and d00..d4n,
+ * ABCMBTools.py:16-186, evaluated on the fly rather than stored), and the
+ * Gauss-Legendre quadrature back to C_l.
+ *   lens_dev        [n_cosmo]                    lna_rec, omega_m
+ *   mu_dev, w_dev   [n_mu]                       nodes and weights
+ *   cl_unlensed_dev [n_cosmo x 3 x (l_lens-1)]   unlensed TT, TE, EE on
+ *                   ells 2..l_lens (abcmb_los_forward with l_max = l_lens)
+ *   clpp_dev        [n_cosmo x (l_lens-1)]       C_l^phiphi on 2..l_lens
+ *   cl_dev          [n_cosmo x 3 x (l_max-1)]    lensed TT, TE, EE
+ * Replaces: the lensing branch of get_Cl (spectrum.py:603-612).
+ */
+int abcmb_lens_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev,
+                       const abcmb_lens_cosmo* lens_dev,
+                       const double* tables_dev, const double* k_dev,
+                       const double* pt_dev,
+                       const double* mu_dev, const double* w_dev,
+                       const double* cl_unlensed_dev,
+                       const abcmb_lens_settings* settings,
+                       double* clpp_dev, double* cl_dev,
+                       void* workspace_dev, int64_t workspace_bytes,
+                       void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Tuning and diagnostics                                                   */
 /* ------------------------------------------------------------------------ */
 

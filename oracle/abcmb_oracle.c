@@ -34,6 +34,9 @@
  *   k quadrature         abcmb/spectrum.py:789-796 (trapezoid)
  *   l spline             abcmb/spectrum.py:594-608
  *   Pk_lin               abcmb/spectrum.py:250-302
+ *   lensing              abcmb/spectrum.py:349-572 (Limber C_l^phiphi, the
+ *                        correlation-function lensed spectra) with the
+ *                        Wigner-d recursion of abcmb/ABCMBTools.py:16-186
  */
 #include <math.h>
 #include <stdint.h>
@@ -1157,6 +1160,235 @@ int oracle_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* kbuf, con
   return ABCMB_OK;
 }
 
+/* ---------------------------------------------------------------------- */
+/* lensing (spectrum.py:349-572, ABCMBTools.py:16-186)                     */
+/* ---------------------------------------------------------------------- */
+
+static double nan_to_zero(double x) { return isnan(x) ? 0. : x; }
+
+static double factorial_int(int n) {
+  double f = 1.;
+  for (int i = 2; i <= n; ++i) f *= (double)i;
+  return f;
+}
+
+static double ipow(double x, int p) {
+  double r = 1.;
+  for (int i = 0; i < p; ++i) r *= x;
+  return r;
+}
+
+/* ABCMBTools.wigner_d_matrix (ABCMBTools.py:16-65) for one mu: d^l_{mn}(mu)
+ * for l = m..l_end into out[l - m].  The recursion variable is normalised by
+ * sqrt((2l+1)/2); the coefficients' 0/0 at l = 0 (d00) become 0 exactly as
+ * jnp.nan_to_num does there (no coefficient is ever infinite). */
+void oracle_wigner_d(int m, int n, double mu, int l_end, double* out) {
+  double beta = acos(mu);
+  double norm = sqrt((2. * m + 1.) / 2.) * sqrt(factorial_int(2 * m) / (factorial_int(m + n) * factorial_int(m - n)));
+  double D = norm * ipow(cos(beta / 2.), m + n) * ipow(-sin(beta / 2.), m - n);
+  double Dm1 = 0.;
+  for (int l = m; l <= l_end; ++l) {
+    double L = (double)l;
+    out[l - m] = D * sqrt(2. / (2. * L + 1.));
+    double normA = sqrt((2. * L + 3.) / (2. * L + 1.));
+    double normC = sqrt((2. * L + 3.) / (2. * L - 1.));
+    double denom = sqrt((L + 1.) * (L + 1.) - (double)(m * m)) * sqrt((L + 1.) * (L + 1.) - (double)(n * n));
+    double A = nan_to_zero(normA * (L + 1.) * (2. * L + 1.) / denom);
+    double B = nan_to_zero(-A * m * n / L / (L + 1.));
+    double C = nan_to_zero(-normC * sqrt(L * L - (double)(m * m)) * sqrt(L * L - (double)(n * n)) / denom * (L + 1.) / L);
+    double Dn = A * mu * D + B * D + C * Dm1;
+    Dm1 = D;
+    D = Dn;
+  }
+}
+
+/* d^l_{mn}(mu) on ells 2..l_lens as the d00/d1n/d2n/d3n/d4n wrappers return
+ * them (ABCMBTools.py:67-186): rows for m < 2 drop the patched l < 2, rows
+ * for m > 2 are zero below l = m.  row[l - 2]. */
+static void wigner_row(int m, int n, double mu, int l_lens, double* row, double* tmp) {
+  oracle_wigner_d(m, n, mu, l_lens, tmp);
+  for (int l = 2; l <= l_lens; ++l) row[l - 2] = (l >= m) ? tmp[l - m] : 0.;
+}
+
+/* SpectrumSolver.lensing_Cl (spectrum.py:386-435) with
+ * lensing_power_spectrum (:349-384) and Pk_lin (:268-302). */
+static void lensing_cl(const abcmb_cosmo* c, const abcmb_lens_cosmo* lc, const double* tables, const double* kbuf,
+                       const double* pt, const abcmb_lens_settings* s, double* clpp) {
+  const int n_lna = s->n_lna, n_save = s->n_save, nk = c->nk, L = s->l_lens;
+  const double* kp = kbuf + c->off_k;
+  const double* dm = pt + c->off_pt + (size_t)ABCMB_F_DELTA_M * n_save * nk;
+  double* ptl = (double*)malloc(sizeof(double) * n_save);
+  double* col = (double*)malloc(sizeof(double) * n_save);
+  double* dml = (double*)malloc(sizeof(double) * (size_t)n_lna * nk);   /* delta_m(lna_i) per PT k */
+  double* fac = (double*)malloc(sizeof(double) * n_lna);                /* everything but Pk/k     */
+  double* chi = (double*)malloc(sizeof(double) * n_lna);
+  double* x = (double*)malloc(sizeof(double) * n_lna);
+  for (int i = 0; i < n_save; ++i) ptl[i] = linspace_at(c->lna_transfer_start, 0., n_save, i);
+  const double chi_rec = c->tau0 - oracle_tau(c, tables, lc->lna_rec);
+  const double lna_floor = linspace_at(lc->lna_rec, 0., n_lna, n_lna - 2);
+  const double Omega_m = lc->omega_m / (c->h * c->h);
+  const double Omega_L = c->omega_Lambda / (c->h * c->h);
+  for (int i = 0; i < n_lna; ++i) {
+    double lna = linspace_at(lc->lna_rec, 0., n_lna, i);
+    x[i] = lna;
+    double ls = lna < 0. ? lna : lna_floor;
+    double chs = c->tau0 - oracle_tau(c, tables, ls);
+    chi[i] = chs;
+    double window = (chi_rec - chs) / chi_rec / chs;
+    double aH = oracle_aH(c, ls);
+    double a = exp(ls);
+    double z = 1. / a - 1.;
+    double zp3 = (1. + z) * (1. + z) * (1. + z);
+    double Om = (Omega_m * zp3) / ((Omega_m * zp3) + Omega_L);
+    double aH2 = aH * aH;
+    fac[i] = lna < 0. ? chs / aH * window * window * (9. / 8. / (PI * PI) * (Om * Om) * (aH2 * aH2)) : 0.;
+    double lnap = -log(1. + z);
+    for (int j = 0; j < nk; ++j) {
+      for (int t = 0; t < n_save; ++t) col[t] = dm[(size_t)t * nk + j];
+      dml[(size_t)i * nk + j] = oracle_np_interp(lnap, ptl, col, n_save);
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (int l = 2; l <= L; ++l) {
+    double acc = 0., yprev = 0.;
+    for (int i = 0; i < n_lna; ++i) {
+      double k = ((double)l + 0.5) / chi[i];
+      double d = oracle_np_interp(k, kp, dml + (size_t)i * nk, nk);
+      double Pk = d * d * (c->A_s * pow(k / s->k_pivot, c->n_s - 1.) * (2 * PI * PI / (k * k * k)));
+      double y = fac[i] * Pk / k;
+      if (i > 0) acc += (x[i] - x[i - 1]) * (y + yprev);
+      yprev = y;
+    }
+    double lh = (double)l + 0.5;
+    clpp[l - 2] = 8. * PI * PI / (lh * lh * lh) * (0.5 * acc);
+  }
+  free(ptl); free(col); free(dml); free(fac); free(chi); free(x);
+}
+
+enum { W00, W11, W1M1, W2M2, W22, W20, W31, W3M3, W3M1, W40, W4M4, W4M2, NWROW };
+static const int WROW_M[NWROW] = {0, 1, 1, 2, 2, 2, 3, 3, 3, 4, 4, 4};
+static const int WROW_N[NWROW] = {0, 1, -1, -2, 2, 0, 1, -3, -1, 0, -4, -2};
+
+/* SpectrumSolver.lensed_Cls (spectrum.py:437-572) for one cosmology, one mu
+ * row of the 12 distinct d matrices at a time. */
+static void lensed_cls(const abcmb_lens_settings* s, const double* mu, const double* w, const double* clpp,
+                       const double* cl_unl, double* cl_out) {
+  const int L = s->l_lens, nl = L - 1, n_mu = s->n_mu;
+  const double* ClTT = cl_unl;
+  const double* ClTE = cl_unl + nl;
+  const double* ClEE = cl_unl + 2 * nl;
+  double* Cgl = (double*)malloc(sizeof(double) * n_mu);
+  double* Cgl2 = (double*)malloc(sizeof(double) * n_mu);
+  /* lensing angular correlation functions (spectrum.py:497-506) */
+#pragma omp parallel
+  {
+    double* r11 = (double*)malloc(sizeof(double) * nl);
+    double* r1m1 = (double*)malloc(sizeof(double) * nl);
+    double* tmp = (double*)malloc(sizeof(double) * (L + 2));
+#pragma omp for schedule(static)
+    for (int im = 0; im < n_mu; ++im) {
+      wigner_row(1, 1, mu[im], L, r11, tmp);
+      wigner_row(1, -1, mu[im], L, r1m1, tmp);
+      double a = 0., b = 0.;
+      for (int l = 2; l <= L; ++l) {
+        double c0 = (2. * l + 1) * l * (l + 1) * clpp[l - 2];
+        a += c0 * r11[l - 2];
+        b += c0 * r1m1[l - 2];
+      }
+      Cgl[im] = 1. / 4. / PI * a;
+      Cgl2[im] = 1. / 4. / PI * b;
+    }
+    free(r11); free(r1m1); free(tmp);
+  }
+  int nthr = 1;
+#ifdef _OPENMP
+  nthr = omp_get_max_threads();
+#endif
+  double* acc = (double*)calloc((size_t)nthr * 3 * nl, sizeof(double));
+#pragma omp parallel
+  {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    double* my = acc + (size_t)tid * 3 * nl;
+    double* d = (double*)malloc(sizeof(double) * NWROW * nl);
+    double* tmp = (double*)malloc(sizeof(double) * (L + 2));
+#pragma omp for schedule(static)
+    for (int im = 0; im < n_mu; ++im) {
+      for (int r = 0; r < NWROW; ++r) wigner_row(WROW_M[r], WROW_N[r], mu[im], L, d + (size_t)r * nl, tmp);
+      const double sigma2 = Cgl[n_mu - 1] - Cgl[im];
+      const double cg = Cgl2[im];
+      double ksi = 0., ksip = 0., ksim = 0., ksix = 0.;
+      for (int l = 2; l <= L; ++l) {
+        const int i = l - 2;
+        const double llp1 = (double)l * (l + 1);
+        const double X000 = exp(-llp1 * sigma2 / 4);
+        const double X000p = -llp1 / 4. * X000;
+        const double X220 = 1. / 4. * sqrt((double)(l + 2) * (l - 1) * l * (l + 1)) * exp(-(llp1 - 2) * sigma2 / 4.);
+        const double X022 = exp(-(llp1 - 4) * sigma2 / 4);
+        const double X022p = -(llp1 - 4) / 4 * X022;
+        const double X121 = -1. / 2. * sqrt((double)(l + 2) * (l - 1)) * exp(-(llp1 - 8. / 3.) * sigma2 / 4.);
+        const double X132 = -1. / 2. * sqrt((double)(l + 3) * (l - 2)) * exp(-(llp1 - 20. / 3.) * sigma2 / 4.);
+        const double X242 = 1. / 4. * sqrt((double)(l + 4) * (l + 3) * (l - 2) * (l - 3)) *
+                            exp(-(llp1 - 10.) * sigma2 / 4.);
+        const double d00 = d[W00 * nl + i], d11 = d[W11 * nl + i], d1m1 = d[W1M1 * nl + i];
+        const double d2m2 = d[W2M2 * nl + i], d22 = d[W22 * nl + i], d20 = d[W20 * nl + i];
+        const double d31 = d[W31 * nl + i], d3m3 = d[W3M3 * nl + i], d3m1 = d[W3M1 * nl + i];
+        const double d40 = d[W40 * nl + i], d4m4 = d[W4M4 * nl + i], d4m2 = d[W4M2 * nl + i];
+        const double tl = 2. * l + 1;
+        ksi += tl * ClTT[i] * (X000 * X000 * d00 + 8. / l / (l + 1) * cg * X000p * X000p * d1m1 +
+                               cg * cg * (X000p * X000p * d00 + X220 * X220 * d2m2));
+        ksip += tl * ClEE[i] * (X022 * X022 * d22 + 2 * cg * X132 * X121 * d31 +
+                                cg * cg * (X022p * X022p * d22 + X242 * X220 * d40));
+        ksim += tl * ClEE[i] * (X022 * X022 * d2m2 + cg * (X121 * X121 * d1m1 + X132 * X132 * d3m3) +
+                                1. / 2. * cg * cg * (2 * X022p * X022p * d2m2 + X220 * X220 * d00 + X242 * X242 * d4m4));
+        ksix += tl * ClTE[i] * (X022 * X000 * d20 + cg * 2 * X000p / sqrt(llp1) * (X121 * d11 + X132 * d3m1) +
+                                1. / 2. * cg * cg * ((2 * X022p * X000p + X220 * X220) * d20 + X220 * X242 * d4m2));
+      }
+      ksi *= 1. / 4. / PI; ksip *= 1. / 4. / PI; ksim *= 1. / 4. / PI; ksix *= 1. / 4. / PI;
+      /* Gauss-Legendre quadrature back to C_l (spectrum.py:563-570) */
+      for (int i = 0; i < nl; ++i) {
+        my[i] += ksi * d[W00 * nl + i] * w[im];
+        my[nl + i] += ksix * d[W20 * nl + i] * w[im];
+        my[2 * nl + i] += (ksip * d[W22 * nl + i] + ksim * d[W2M2 * nl + i]) * w[im];
+      }
+    }
+    free(d); free(tmp);
+  }
+  const int n_out = s->l_max - 1;
+  for (int i = 0; i < n_out; ++i) {
+    double tt = 0., te = 0., ee = 0.;
+    for (int t = 0; t < nthr; ++t) {
+      tt += acc[(size_t)t * 3 * nl + i];
+      te += acc[(size_t)t * 3 * nl + nl + i];
+      ee += acc[(size_t)t * 3 * nl + 2 * nl + i];
+    }
+    cl_out[i] = 2 * PI * tt;
+    cl_out[n_out + i] = 2 * PI * te;
+    cl_out[2 * n_out + i] = 1. / 2. * 2 * PI * ee;
+  }
+  free(acc); free(Cgl); free(Cgl2);
+}
+
+/* The lensing branch of get_Cl (spectrum.py:603-612): C_l^phiphi, then the
+ * lensed spectra on ells 2..l_max. */
+int oracle_lens_forward(int n_cosmo, const abcmb_cosmo* cosmo, const abcmb_lens_cosmo* lens, const double* tables,
+                        const double* kbuf, const double* pt, const double* mu, const double* w,
+                        const double* cl_unl, const abcmb_lens_settings* s, double* clpp, double* cl,
+                        int n_threads) {
+#ifdef _OPENMP
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+#endif
+  if (s->l_max < 2 || s->l_lens < s->l_max || s->n_mu < 2 || s->n_lna < 3) return ABCMB_ERR_ARG;
+  const int nl = s->l_lens - 1;
+  for (int ci = 0; ci < n_cosmo; ++ci) {
+    lensing_cl(&cosmo[ci], &lens[ci], tables, kbuf, pt, s, clpp + (size_t)ci * nl);
+    lensed_cls(s, mu, w, clpp + (size_t)ci * nl, cl_unl + (size_t)ci * 3 * nl, cl + (size_t)ci * 3 * (s->l_max - 1));
+  }
+  return ABCMB_OK;
+}
+
 /* sizeof of the C-ABI records, so tests can check the Python layouts. */
 int oracle_sizeof(int which) {
   switch (which) {
@@ -1164,6 +1396,8 @@ int oracle_sizeof(int which) {
     case 1: return (int)sizeof(abcmb_pert_settings);
     case 2: return (int)sizeof(abcmb_kstat);
     case 3: return (int)sizeof(abcmb_los_settings);
+    case 4: return (int)sizeof(abcmb_lens_cosmo);
+    case 5: return (int)sizeof(abcmb_lens_settings);
   }
   return -1;
 }

@@ -47,6 +47,11 @@ int oracle_los_forward(int n_cosmo, const abcmb_cosmo* cosmo, const double* tabl
                        const double* pt, const double* kt, const abcmb_los_settings* ls, int n_save,
                        const oracle_bessel* B, double* cl_raw, double* cl, int n_threads);
 int oracle_sizeof(int which);
+void oracle_wigner_d(int m, int n, double mu, int l_end, double* out);
+int oracle_lens_forward(int n_cosmo, const abcmb_cosmo* cosmo, const abcmb_lens_cosmo* lens, const double* tables,
+                        const double* kbuf, const double* pt, const double* mu, const double* w,
+                        const double* cl_unl, const abcmb_lens_settings* s, double* clpp, double* cl,
+                        int n_threads);
 int oracle_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* kbuf, const double* pt, int n_save,
                   double k_pivot, int n_kout, const double* kout, int n_z, const double* z, double* pk);
 

@@ -66,6 +66,10 @@ def lib():
         L.oracle_pk_lin.restype = ctypes.c_int
         L.oracle_pk_lin.argtypes = [ctypes.c_int, vp, _dp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                     _dp, ctypes.c_int, _dp, _dp]
+        L.oracle_wigner_d.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp]
+        L.oracle_lens_forward.restype = ctypes.c_int
+        L.oracle_lens_forward.argtypes = [ctypes.c_int, vp, vp, _dp, _dp, _dp, _dp, _dp, _dp, vp, _dp, _dp,
+                                          ctypes.c_int]
         _lib = L
     return _lib
 
@@ -132,3 +136,26 @@ def pk_lin(batch, pt, k_pivot, kout, z):
     lib().oracle_pk_lin(batch.n_cosmo, vptr(batch.cosmo), dptr(batch.kbuf), dptr(pt), batch.n_save,
                         float(k_pivot), len(kout), dptr(kout), len(z), dptr(z), dptr(pk))
     return pk.reshape(batch.n_cosmo, len(z), len(kout))
+
+
+def wigner_d(m: int, n: int, mu: float, l_end: int) -> np.ndarray:
+    """d^l_{mn}(mu) for l = m..l_end (ABCMBTools.wigner_d_matrix for one mu)."""
+    out = np.zeros(l_end - m + 1)
+    lib().oracle_wigner_d(int(m), int(n), float(mu), int(l_end), dptr(out))
+    return out
+
+
+def lens_forward(batch, pt, lens, mu, w, cl_unl, settings, n_threads: int = 0):
+    """Oracle lensing branch of get_Cl: (rc, clpp [n, l_lens-1], cl [n, 3, l_max-1])."""
+    n = batch.n_cosmo
+    nl = settings.l_lens - 1
+    clpp = np.zeros(n * nl)
+    cl = np.zeros(n * 3 * (settings.l_max - 1))
+    mu = np.ascontiguousarray(mu, dtype=np.float64)
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    cl_unl = np.ascontiguousarray(cl_unl, dtype=np.float64).reshape(-1)
+    lens = np.ascontiguousarray(lens)
+    rc = lib().oracle_lens_forward(n, vptr(batch.cosmo), vptr(lens), dptr(batch.tables), dptr(batch.kbuf),
+                                   dptr(pt), dptr(mu), dptr(w), dptr(cl_unl), ctypes.byref(settings),
+                                   dptr(clpp), dptr(cl), n_threads)
+    return rc, clpp.reshape(n, nl), cl.reshape(n, 3, settings.l_max - 1)
