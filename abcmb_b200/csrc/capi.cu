@@ -12,7 +12,7 @@ int64_t pert_workspace_bytes(int n_cosmo);
 cudaError_t launch_pert(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
                         int n_items, const int32_t* items, const abcmb_pert_settings& s, double* pt,
                         abcmb_kstat* kstat, void* ws, cudaStream_t stream, int warps_per_block, int* grid_out);
-int64_t los_workspace_bytes(int max_nk, int nkt, int n_ell_tab, int n_save, int precision);
+int64_t los_workspace_bytes(int n_cosmo, int max_nk, int nkt, int n_ell_tab, int n_save, int precision);
 cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_cosmo* cosmo_host,
                        const double* tables, const double* kbuf, const double* pt, const double* kt,
                        const abcmb_los_settings& ls, int n_save, const BesselDev& B, double* cl_raw,
@@ -140,8 +140,7 @@ int abcmb_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* 
 }
 
 int64_t abcmb_los_workspace_size(int n_cosmo, int max_nk, int nkt, int n_ell_tab, int n_save, int precision) {
-  (void)n_cosmo;
-  return abcmb::los_workspace_bytes(max_nk, nkt, n_ell_tab, n_save, precision);
+  return abcmb::los_workspace_bytes(n_cosmo, max_nk, nkt, n_ell_tab, n_save, precision);
 }
 
 int abcmb_los_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_cosmo* cosmo_host,
@@ -173,7 +172,7 @@ int abcmb_los_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_cos
   for (const auto& c : host) max_nk = c.nk > max_nk ? c.nk : max_nk;
   const int n_save = ls.n_save;
   if (n_save < 3) return fail(ABCMB_ERR_ARG, "abcmb_los_forward: n_save");
-  int64_t need = abcmb::los_workspace_bytes(max_nk, ls.nkt, ls.idx_max - ls.idx_min + 1, n_save, ls.precision);
+  int64_t need = abcmb::los_workspace_bytes(n_cosmo, max_nk, ls.nkt, ls.idx_max - ls.idx_min + 1, n_save, ls.precision);
   if (!workspace_dev || workspace_bytes < need) return fail(ABCMB_ERR_WORKSPACE, "abcmb_los_forward: workspace");
   e = abcmb::launch_los(n_cosmo, cosmo_dev, host.data(), tables_dev, k_dev, pt_dev, kt_dev, ls, n_save, bc->dev,
                         cl_raw_dev, cl_dev, dcl_dns_dev, workspace_dev, st);

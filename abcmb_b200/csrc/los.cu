@@ -1,17 +1,18 @@
 // los.cu -- line-of-sight C_l projection (SpectrumSolver.get_Cl).
 //
-// Per cosmology, five launches:
+// Cosmologies are processed in chunks of up to LOS_CHUNK; five launches per
+// chunk:
 //   spline_prep   not-a-knot cubic-spline factorisation in log10 k of the
 //                 perturbation k grid (interpax CubicSpline, spectrum.py:664)
 //                 and the interval of every transfer k;
 //   spline_slopes the spline slopes of the 10 source fields on every lna row;
 //   sources       the splined fields at the transfer k and the T0/T1/T2/E
 //                 sources (spectrum.py:681-696);
-//   los           one CTA per (tabulated l, k tile): the l column of the
-//                 phi0/phi1/phi2 Bessel tables is staged in shared memory and
-//                 every thread accumulates the four lna integrals of one
-//                 transfer k (spectrum.py:755-786), then the block reduces its
-//                 share of the k trapezoid (spectrum.py:789-796);
+//   los           one CTA per (tabulated l, k tile, cosmology): the l column
+//                 of the phi0/phi1/phi2 Bessel tables is staged in shared
+//                 memory and the four lna integrals of every transfer k are
+//                 accumulated (spectrum.py:755-786), then the block reduces
+//                 its share of the k trapezoid (spectrum.py:789-796);
 //   cl_final      fixed-order sum of the tile partials and the cubic spline
 //                 over tabulated l onto the integer ells (spectrum.py:597-608).
 #include "common.cuh"
@@ -105,46 +106,77 @@ __device__ __forceinline__ int spline_interval(const double* x, int n, double xq
   return min(max(lo, 1), n - 1) - 1;
 }
 
-__global__ void spline_prep_kernel(const double* __restrict__ kp, int nk, const double* __restrict__ kt, int nkt,
-                                   double* xk, double* dinv, double* mlo, double* up, int* kidx) {
-  // xk = log10(PT.k); one block: threads fill x, thread 0 factorises, all map kt
+// Chunked launches: every kernel below covers a chunk of up to LOS_CHUNK
+// cosmologies (blockIdx.z, or blockIdx.x for the one-block-per-cosmology
+// kernels); per-cosmology scratch lives at a fixed stride in the workspace.
+constexpr int LOS_CHUNK = 8;
+
+struct LosScratch {
+  double* xk;        // [C][max_nk] log10 of the perturbation k grid
+  double* dinv;      // [C][max_nk] not-a-knot factorisation
+  double* mlo;
+  double* up;
+  int* kidx;         // [C][nkt] spline interval of every transfer k
+  double* slopes;    // [C][NSRC_FIELDS][nl][max_nk]
+  void* S;           // [C][4][nl][nkt] sources (double or float)
+  double* partial;   // [C][n_ell_tab][ntile][6]
+  double* lscr;      // [C][16 n_ell_tab] l-spline scratch
+  int max_nk;
+};
+
+__global__ void spline_prep_kernel(const abcmb_cosmo* __restrict__ cosmo, int c0, const double* __restrict__ kbuf,
+                                   const double* __restrict__ kt, int nkt, LosScratch W) {
+  // one block per cosmology: threads fill x = log10(PT.k), thread 0
+  // factorises, all threads locate the transfer k
+  const int cz = blockIdx.x;
+  const abcmb_cosmo& c = cosmo[c0 + cz];
+  const int nk = c.nk;
+  const double* kp = kbuf + c.off_k;
+  double* xk = W.xk + (int64_t)cz * W.max_nk;
   for (int i = threadIdx.x; i < nk; i += blockDim.x) xk[i] = log10(kp[i]);
   __syncthreads();
-  if (threadIdx.x == 0) nak_factor(xk, nk, dinv, mlo, up);
-  for (int j = threadIdx.x; j < nkt; j += blockDim.x) kidx[j] = spline_interval(xk, nk, log10(kt[j]));
+  if (threadIdx.x == 0)
+    nak_factor(xk, nk, W.dinv + (int64_t)cz * W.max_nk, W.mlo + (int64_t)cz * W.max_nk, W.up + (int64_t)cz * W.max_nk);
+  for (int j = threadIdx.x; j < nkt; j += blockDim.x) W.kidx[(int64_t)cz * nkt + j] = spline_interval(xk, nk, log10(kt[j]));
 }
 
-__global__ void spline_slopes_kernel(const double* __restrict__ ptc, int n_save, int nk, int nl,
-                                     const double* __restrict__ xk, const double* __restrict__ dinv,
-                                     const double* __restrict__ mlo, const double* __restrict__ up,
-                                     double* __restrict__ slopes) {
-  int col = blockIdx.x * blockDim.x + threadIdx.x;    // f * nl + il
+__global__ void spline_slopes_kernel(const abcmb_cosmo* __restrict__ cosmo, int c0, const double* __restrict__ pt,
+                                     int n_save, int nl, LosScratch W) {
+  const int cz = blockIdx.y;
+  const abcmb_cosmo& c = cosmo[c0 + cz];
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;    // f * nl + il
   if (col >= NSRC_FIELDS * nl) return;
-  int f = col / nl, il = col % nl;
-  const double* y = ptc + ((int64_t)SRC_FIELDS[f] * n_save + il) * nk;
-  nak_solve(xk, y, nk, dinv, mlo, up, slopes + (int64_t)col * nk);
+  const int nk = c.nk;
+  const int f = col / nl, il = col % nl;
+  const double* y = pt + c.off_pt + ((int64_t)SRC_FIELDS[f] * n_save + il) * nk;
+  const int64_t o = (int64_t)cz * W.max_nk;
+  nak_solve(W.xk + o, y, nk, W.dinv + o, W.mlo + o, W.up + o,
+            W.slopes + ((int64_t)cz * NSRC_FIELDS * nl + col) * W.max_nk);
 }
 
 template <typename SrcT>
-__global__ void sources_kernel(const abcmb_cosmo* __restrict__ cosmo, int ci, const double* __restrict__ tables,
-                               const double* __restrict__ ptc, int n_save, int nk, int nl,
-                               const double* __restrict__ xk, const double* __restrict__ slopes,
-                               const int* __restrict__ kidx, const double* __restrict__ kt, int nkt,
-                               abcmb_los_settings ls, SrcT* __restrict__ S) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  int il = blockIdx.y;
+__global__ void sources_kernel(const abcmb_cosmo* __restrict__ cosmo, int c0, const double* __restrict__ tables,
+                               const double* __restrict__ pt, int n_save, int nl, const double* __restrict__ kt,
+                               int nkt, abcmb_los_settings ls, LosScratch W) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int il = blockIdx.y;
+  const int cz = blockIdx.z;
   if (j >= nkt) return;
-  const abcmb_cosmo& c = cosmo[ci];
+  const abcmb_cosmo& c = cosmo[c0 + cz];
+  const int nk = c.nk;
+  const double* ptc = pt + c.off_pt;
   const double* los = tables + c.off_los;
+  const double* xk = W.xk + (int64_t)cz * W.max_nk;
+  const double* slopes = W.slopes + (int64_t)cz * NSRC_FIELDS * nl * W.max_nk;
   const double k = kt[j];
-  const int i = kidx[j];
+  const int i = W.kidx[(int64_t)cz * nkt + j];
   const double dx = xk[i + 1] - xk[i];
   const double u = log10(k) - xk[i];
   double v[NSRC_FIELDS];
 #pragma unroll
   for (int f = 0; f < NSRC_FIELDS; ++f) {
     const double* y = ptc + ((int64_t)SRC_FIELDS[f] * n_save + il) * nk;
-    const double* s = slopes + ((int64_t)f * nl + il) * nk;
+    const double* s = slopes + ((int64_t)f * nl + il) * W.max_nk;
     v[f] = spline_piece(y[i], y[i + 1], s[i], s[i + 1], dx, u);
   }
   const double dg = v[0], thb = v[1], thbp = v[2], sg = v[3], G0 = v[4], G2 = v[5];
@@ -158,6 +190,7 @@ __global__ void sources_kernel(const abcmb_cosmo* __restrict__ cosmo, int ci, co
   double sT2 = ls.scale_pol * g * (2 * sg + G0 + G2) / 8.;
   double sE = sqrt(6.) * g * (2 * sg + G0 + G2) / 8.;
   const int64_t plane = (int64_t)nl * nkt;
+  SrcT* S = static_cast<SrcT*>(W.S) + (int64_t)cz * 4 * plane;
   const int64_t o = (int64_t)il * nkt + j;
   S[o] = (SrcT)sT0;
   S[plane + o] = (SrcT)sT1;
@@ -165,16 +198,31 @@ __global__ void sources_kernel(const abcmb_cosmo* __restrict__ cosmo, int ci, co
   S[3 * plane + o] = (SrcT)sE;
 }
 
-// large-x asymptotic spherical Bessel j_l (spectrum.py:48-51)
-__device__ __forceinline__ double jasym(double l, double x) {
-  double nu = l + 0.5;
-  double r = sqrt(x * x - nu * nu);
-  double Q = r - nu * PI / 2 + nu * asin(nu / x);
-  double J = sqrt(2 / PI / r) * cos(Q - PI / 4);
-  return sqrt(PI / 2 / x) * J;
+// Large-x asymptotic spherical Bessel j_l (spectrum.py:48-51):
+//   r = sqrt(x^2 - nu^2), Q = r - nu pi/2 + nu asin(nu/x),
+//   j = sqrt(2/(pi r)) cos(Q - pi/4) sqrt(pi/(2x)) = cos(Q - pi/4) / sqrt(r x)
+// with nu = l + 1/2 and 1/x supplied by the caller (no division).
+__device__ __forceinline__ double jasym(double nu, double nusq, double x, double ix) {
+  const double r = sqrt(fma(x, x, -nusq));
+  const double Q = r - nu * (PI / 2) + nu * asin(nu * ix);
+  return rsqrt(r * x) * cos(Q - PI / 4);
 }
 
-constexpr int LOS_THREADS = 256;
+// fast_interp (ABCMBTools.py:268-308) with the scale (n-1)/(xp_max-xp_min)
+// precomputed; the table is in shared memory.
+__device__ __forceinline__ double lerp_tab(double x, double xmin, double scale, const double* fp, int n) {
+  const double eps = 1.e-6;
+  double i = (x - xmin) * scale;
+  i = fmin(fmax(i, eps), (double)(n - 1) - eps);
+  const int il = (int)i;
+  const int iu = min(il + 1, n - 1);
+  const double wu = i - (double)il;
+  return (1.0 - wu) * fp[il] + wu * fp[iu];
+}
+
+constexpr int LOS_TX = 256;   // transfer k per CTA (one per thread column)
+constexpr int LOS_TY = 3;     // lna segments: thread row y sums segment y
+constexpr int LOS_THREADS = LOS_TX * LOS_TY;
 
 // Kahan-compensated accumulator for the FP32 path.
 struct KahanF {
@@ -187,86 +235,106 @@ struct KahanF {
   }
 };
 
+// One CTA per (tabulated l, 256-wide transfer-k tile, cosmology of the
+// chunk).  The l column of the three Bessel tables and the per-lna factors
+// (tau0 - tau, its reciprocal, w / aH) sit in shared memory; each thread
+// column owns one transfer k and each of the LOS_TY thread rows sums one
+// contiguous third of the lna points; the rows' sums are added in segment
+// order.  Shared memory (~148 KB) admits one CTA per SM: 24 resident warps.
 template <int PREC>
-__global__ void __launch_bounds__(LOS_THREADS) los_kernel(const abcmb_cosmo* __restrict__ cosmo, int ci,
-                                                          const double* __restrict__ tables, int nl,
-                                                          double delta_lna, const void* __restrict__ Sv,
-                                                          const double* __restrict__ kt, int nkt,
-                                                          BesselDev B, int idx_min, double A_s, double n_s,
-                                                          double k_pivot, double* __restrict__ partial) {
+__global__ void __launch_bounds__(LOS_THREADS, 1) los_kernel(const abcmb_cosmo* __restrict__ cosmo, int c0,
+                                                             const double* __restrict__ tables, int nl, int n_save,
+                                                             const double* __restrict__ kt, int nkt, BesselDev B,
+                                                             int idx_min, double k_pivot, LosScratch W) {
   extern __shared__ double sm[];
-  const int ie = blockIdx.x;
+  const int ie = blockIdx.x, tile = blockIdx.y, cz = blockIdx.z;
+  const int n_ell = gridDim.x, ntile = gridDim.y;
   const int idx = idx_min + ie;
-  const int tile = blockIdx.y;
-  const int ntile = gridDim.y;
   const int nx = B.n_x;
   double* ph0 = sm;
-  double* ph1 = sm + nx;
-  double* ph2 = sm + 2 * nx;
-  double* stau = sm + 3 * nx;
-  double* sinv = stau + nl;
-  const abcmb_cosmo& c = cosmo[ci];
+  double* ph1 = ph0 + nx;
+  double* ph2 = ph1 + nx;
+  double* sdt = ph2 + nx;          // tau0 - tau_i
+  double* sidt = sdt + nl;         // 1 / (tau0 - tau_i)
+  double* swa = sidt + nl;         // w_i / aH_i
+  double* seg = swa + nl;          // [LOS_TY - 1][4][LOS_TX] segment sums of rows 1..
+  const int tid = threadIdx.y * LOS_TX + threadIdx.x;
+  const abcmb_cosmo& c = cosmo[c0 + cz];
   const double* los = tables + c.off_los;
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+  for (int i = tid; i < nx; i += LOS_THREADS) {
     ph0[i] = B.phi[((int64_t)0 * B.n_l + idx) * nx + i];
     ph1[i] = B.phi[((int64_t)1 * B.n_l + idx) * nx + i];
     ph2[i] = B.phi[((int64_t)2 * B.n_l + idx) * nx + i];
   }
-  for (int i = threadIdx.x; i < nl; i += blockDim.x) {
-    stau[i] = los[i];
-    sinv[i] = 1.0 / los[3 * nl + i];
+  const double lts = c.lna_transfer_start;
+  const double delta_lna = linspace_at(lts, 0., n_save, n_save - 1) - linspace_at(lts, 0., n_save, n_save - 2);
+  for (int i = tid; i < nl; i += LOS_THREADS) {
+    const double d = c.tau0 - los[i];
+    sdt[i] = d;
+    sidt[i] = 1.0 / d;
+    swa[i] = ((i == 0) ? 0.5 * delta_lna : delta_lna) * (1.0 / los[3 * nl + i]);
   }
   __syncthreads();
   const double l = (double)B.l_tab[idx];
   const double x0min = B.xmin[idx], x0max = B.xmax[idx];
   const double x1min = B.xmin[B.n_l + idx], x1max = B.xmax[B.n_l + idx];
   const double x2min = B.xmin[2 * B.n_l + idx], x2max = B.xmax[2 * B.n_l + idx];
+  const double s0 = (double)(nx - 1) / (x0max - x0min);
+  const double s1 = (double)(nx - 1) / (x1max - x1min);
+  const double s2 = (double)(nx - 1) / (x2max - x2min);
   const double ef = sqrt(3. / 8. * (l + 2) * (l + 1) * l * (l - 1));
-  const double tau0 = c.tau0;
-  const int j = tile * blockDim.x + threadIdx.x;
-  double contrib[3] = {0., 0., 0.};
+  const double nu0 = l + 0.5, nu1 = l + 1.5;
+  const double nu0sq = nu0 * nu0, nu1sq = nu1 * nu1;
+  const double c2 = 3 * l * (l - 1);
+  const int j = tile * LOS_TX + threadIdx.x;
+  const int iy = threadIdx.y;
+  const int i0 = iy * nl / LOS_TY, i1 = (iy + 1) * nl / LOS_TY;
+  double a0 = 0., a1 = 0., a2 = 0., aE = 0.;
+  double k = 0.;
   if (j < nkt) {
-    const double k = kt[j];
+    k = kt[j];
+    const double invk = 1.0 / k;
     const int64_t plane = (int64_t)nl * nkt;
-    double a0 = 0., a1 = 0., a2 = 0., aE = 0.;
     KahanF f0{0.f, 0.f}, f1{0.f, 0.f}, f2{0.f, 0.f}, fE{0.f, 0.f};
-    for (int il = 0; il < nl; ++il) {
-      const double w = (il == 0) ? 0.5 * delta_lna : delta_lna;
-      const double chi = (tau0 - stau[il]) * k;
+    for (int il = i0; il < i1; ++il) {
+      const double chi = sdt[il] * k;
+      const double ichi = sidt[il] * invk;
       // phi0/phi1/phi2 (spectrum.py:719-753): 0 below the table, table
       // lerp inside, asymptotic j_l above; only the taken branch is evaluated
       double p0;
       if (chi < x0min) p0 = 0.;
-      else if (chi >= x0max) p0 = jasym(l, chi);
-      else p0 = fast_interp_smem(chi, x0min, x0max, ph0, nx);
+      else if (chi >= x0max) p0 = jasym(nu0, nu0sq, chi, ichi);
+      else p0 = lerp_tab(chi, x0min, s0, ph0, nx);
       const bool as1 = chi >= x1max, as2 = chi >= x2max;
       double jl = 0., jl1 = 0.;
       if (as1 || as2) {
-        jl = (chi >= x0max) ? p0 : jasym(l, chi);
-        jl1 = jasym(l + 1, chi);
+        jl = (chi >= x0max) ? p0 : jasym(nu0, nu0sq, chi, ichi);
+        jl1 = jasym(nu1, nu1sq, chi, ichi);
       }
       double p1, p2;
       if (chi < x1min) p1 = 0.;
-      else if (as1) p1 = l / chi * jl - jl1;
-      else p1 = fast_interp_smem(chi, x1min, x1max, ph1, nx);
+      else if (as1) p1 = l * ichi * jl - jl1;
+      else p1 = lerp_tab(chi, x1min, s1, ph1, nx);
+      const double ichi2 = ichi * ichi;
       if (chi < x2min) p2 = 0.;
-      else if (as2) p2 = ((3 * l * (l - 1) - 2 * chi * chi) * jl + 6 * chi * jl1) / 2 / (chi * chi);
-      else p2 = fast_interp_smem(chi, x2min, x2max, ph2, nx);
-      const double eps = p0 / (chi * chi) * ef;
-      const double wi = w * sinv[il];
+      else if (as2) p2 = ((c2 - 2 * chi * chi) * jl + 6 * chi * jl1) * 0.5 * ichi2;
+      else p2 = lerp_tab(chi, x2min, s2, ph2, nx);
+      const double eps = p0 * ichi2 * ef;
+      const double wa = swa[il];
       const int64_t o = (int64_t)il * nkt + j;
       if (PREC == 0) {
-        const double* S = static_cast<const double*>(Sv);
-        a0 = a0 + w * S[o] * sinv[il] * p0;
-        a1 = a1 + w * S[plane + o] * sinv[il] * p1;
-        a2 = a2 + w * S[2 * plane + o] * sinv[il] * p2;
-        aE = aE + w * S[3 * plane + o] * sinv[il] * eps;
+        const double* S = static_cast<const double*>(W.S) + (int64_t)cz * 4 * plane;
+        a0 = fma(wa * S[o], p0, a0);
+        a1 = fma(wa * S[plane + o], p1, a1);
+        a2 = fma(wa * S[2 * plane + o], p2, a2);
+        aE = fma(wa * S[3 * plane + o], eps, aE);
       } else {
-        const float* S = static_cast<const float*>(Sv);
-        f0.add((float)wi * S[o] * (float)p0);
-        f1.add((float)wi * S[plane + o] * (float)p1);
-        f2.add((float)wi * S[2 * plane + o] * (float)p2);
-        fE.add((float)wi * S[3 * plane + o] * (float)eps);
+        const float* S = static_cast<const float*>(W.S) + (int64_t)cz * 4 * plane;
+        const float wf = (float)wa;
+        f0.add(wf * S[o] * (float)p0);
+        f1.add(wf * S[plane + o] * (float)p1);
+        f2.add(wf * S[2 * plane + o] * (float)p2);
+        fE.add(wf * S[3 * plane + o] * (float)eps);
       }
     }
     if (PREC != 0) {
@@ -275,9 +343,28 @@ __global__ void __launch_bounds__(LOS_THREADS) los_kernel(const abcmb_cosmo* __r
       a2 = (double)f2.s - (double)f2.c;
       aE = (double)fE.s - (double)fE.c;
     }
+  }
+  if (iy > 0) {
+    double* sg = seg + (int64_t)(iy - 1) * 4 * LOS_TX + threadIdx.x;
+    sg[0] = a0;
+    sg[LOS_TX] = a1;
+    sg[2 * LOS_TX] = a2;
+    sg[3 * LOS_TX] = aE;
+  }
+  __syncthreads();
+  if (iy != 0) return;
+  double contrib[6] = {0., 0., 0., 0., 0., 0.};
+  if (j < nkt) {
+    for (int y = 1; y < LOS_TY; ++y) {
+      const double* sg = seg + (int64_t)(y - 1) * 4 * LOS_TX + threadIdx.x;
+      a0 += sg[0];
+      a1 += sg[LOS_TX];
+      a2 += sg[2 * LOS_TX];
+      aE += sg[3 * LOS_TX];
+    }
     const double T = a0 + a1 + a2;
     const double E = aE;
-    const double pr = 4. * PI * A_s * pow(k / k_pivot, n_s - 1.) / k;
+    const double pr = 4. * PI * c.A_s * pow(k / k_pivot, c.n_s - 1.) / k;
     // trapezoid weight of node j
     double wj;
     if (nkt == 1) wj = 0.;
@@ -293,8 +380,9 @@ __global__ void __launch_bounds__(LOS_THREADS) los_kernel(const abcmb_cosmo* __r
     contrib[4] = contrib[1] * lk;
     contrib[5] = contrib[2] * lk;
   }
-  // block reduction (fixed order: deterministic)
-  __shared__ double red[6][LOS_THREADS / 32];
+  // reduction over the LOS_TX columns (fixed order: deterministic); rows
+  // y > 0 have returned, so only named warps of row 0 take part
+  __shared__ double red[6][LOS_TX / 32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int X = 0; X < 6; ++X) {
@@ -303,22 +391,27 @@ __global__ void __launch_bounds__(LOS_THREADS) los_kernel(const abcmb_cosmo* __r
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     if (lane == 0) red[X][wid] = v;
   }
-  __syncthreads();
+  asm volatile("bar.sync 1, %0;" ::"r"(LOS_TX));
   if (threadIdx.x < 6) {
     double s = 0.;
-    for (int w = 0; w < (int)(blockDim.x / 32); ++w) s += red[threadIdx.x][w];
-    partial[((int64_t)ie * ntile + tile) * 6 + threadIdx.x] = s;
+    for (int w = 0; w < LOS_TX / 32; ++w) s += red[threadIdx.x][w];
+    W.partial[(((int64_t)cz * n_ell + ie) * ntile + tile) * 6 + threadIdx.x] = s;
   }
 }
 
-__global__ void cl_final_kernel(const double* __restrict__ partial, int n_ell_tab, int ntile, BesselDev B,
-                                int idx_min, int l_min, int n_out, double* __restrict__ cl_raw,
-                                double* __restrict__ cl, double* __restrict__ dcl_dns,
-                                double* __restrict__ scratch) {
-  // scratch: x[n], y[6][n], s[6][n], dinv, mlo, up  (n = n_ell_tab); series 3..5 are dC/dn_s
+__global__ void cl_final_kernel(int c0, int n_ell_tab, int ntile, BesselDev B, int idx_min, int l_min, int n_out,
+                                LosScratch W, double* __restrict__ cl_raw, double* __restrict__ cl,
+                                double* __restrict__ dcl_dns) {
+  // one block per cosmology of the chunk; scratch: x[n], y[6][n], s[6][n],
+  // dinv, mlo, up (n = n_ell_tab); series 3..5 are dC/dn_s
+  const int cz = blockIdx.x, ci = c0 + cz;
+  const double* partial = W.partial + (int64_t)cz * n_ell_tab * ntile * 6;
+  cl_raw += (int64_t)ci * n_ell_tab * 3;
+  cl += (int64_t)ci * 3 * n_out;
+  if (dcl_dns) dcl_dns += (int64_t)ci * 3 * n_out;
   const int n = n_ell_tab;
   const int nser = dcl_dns ? 6 : 3;
-  double* x = scratch;
+  double* x = W.lscr + (int64_t)cz * 16 * n;
   double* y = x + n;
   double* s = y + 6 * n;
   double* dinv = s + 6 * n;
@@ -407,41 +500,62 @@ __global__ void pk_lin_kernel(const abcmb_cosmo* __restrict__ cosmo, const doubl
 // ---------------------------------------------------------------------------
 static int64_t al256(int64_t b) { return (b + 255) / 256 * 256; }
 
-int64_t los_workspace_bytes(int max_nk, int nkt, int n_ell_tab, int n_save, int precision) {
-  const int nl = n_save - 1;
-  const int ntile = (nkt + LOS_THREADS - 1) / LOS_THREADS;
+struct LosLayout {
+  int chunk, max_nk, nkt, n_ell_tab, nl, ntile;
+  int64_t o_xk, o_dinv, o_mlo, o_up, o_kidx, o_slopes, o_S, o_partial, o_lscr, total;
+};
+
+static LosLayout los_layout(int n_cosmo, int max_nk, int nkt, int n_ell_tab, int n_save, int precision) {
+  LosLayout L{};
+  L.chunk = n_cosmo < LOS_CHUNK ? (n_cosmo > 0 ? n_cosmo : 1) : LOS_CHUNK;
+  L.max_nk = max_nk;
+  L.nkt = nkt;
+  L.n_ell_tab = n_ell_tab;
+  L.nl = n_save - 1;
+  L.ntile = (nkt + LOS_TX - 1) / LOS_TX;
+  const int64_t C = L.chunk;
   int64_t b = 0;
-  b += 4 * al256((int64_t)max_nk * 8);                         // xk, dinv, mlo, up
-  b += al256((int64_t)nkt * 4);                                // kidx
-  b += al256((int64_t)NSRC_FIELDS * nl * max_nk * 8);          // slopes
-  b += al256((int64_t)4 * nl * nkt * (precision ? 4 : 8));     // sources
-  b += al256((int64_t)n_ell_tab * ntile * 6 * 8);              // partials
-  b += al256((int64_t)16 * n_ell_tab * 8);                     // l-spline scratch
-  return b;
+  L.o_xk = b;      b += al256(C * max_nk * 8);
+  L.o_dinv = b;    b += al256(C * max_nk * 8);
+  L.o_mlo = b;     b += al256(C * max_nk * 8);
+  L.o_up = b;      b += al256(C * max_nk * 8);
+  L.o_kidx = b;    b += al256(C * nkt * 4);
+  L.o_slopes = b;  b += al256(C * NSRC_FIELDS * L.nl * max_nk * 8);
+  L.o_S = b;       b += al256(C * 4 * L.nl * nkt * (precision ? 4 : 8));
+  L.o_partial = b; b += al256(C * n_ell_tab * L.ntile * 6 * 8);
+  L.o_lscr = b;    b += al256(C * 16 * n_ell_tab * 8);
+  L.total = b;
+  return L;
+}
+
+int64_t los_workspace_bytes(int n_cosmo, int max_nk, int nkt, int n_ell_tab, int n_save, int precision) {
+  return los_layout(n_cosmo, max_nk, nkt, n_ell_tab, n_save, precision).total;
 }
 
 cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_cosmo* cosmo_host,
                        const double* tables, const double* kbuf, const double* pt, const double* kt,
                        const abcmb_los_settings& ls, int n_save, const BesselDev& B, double* cl_raw,
                        double* cl, double* dcl_dns, void* ws, cudaStream_t stream) {
-  const int nl = n_save - 1;
   const int nkt = ls.nkt;
   const int n_ell_tab = ls.idx_max - ls.idx_min + 1;
   const int n_out = ls.l_max - ls.l_min + 1;
-  const int ntile = (nkt + LOS_THREADS - 1) / LOS_THREADS;
   int max_nk = 0;
   for (int c = 0; c < n_cosmo; ++c) max_nk = cosmo_host[c].nk > max_nk ? cosmo_host[c].nk : max_nk;
+  const LosLayout L = los_layout(n_cosmo, max_nk, nkt, n_ell_tab, n_save, ls.precision);
+  const int nl = L.nl;
   char* w = static_cast<char*>(ws);
-  double* xk = reinterpret_cast<double*>(w); w += al256((int64_t)max_nk * 8);
-  double* dinv = reinterpret_cast<double*>(w); w += al256((int64_t)max_nk * 8);
-  double* mlo = reinterpret_cast<double*>(w); w += al256((int64_t)max_nk * 8);
-  double* up = reinterpret_cast<double*>(w); w += al256((int64_t)max_nk * 8);
-  int* kidx = reinterpret_cast<int*>(w); w += al256((int64_t)nkt * 4);
-  double* slopes = reinterpret_cast<double*>(w); w += al256((int64_t)NSRC_FIELDS * nl * max_nk * 8);
-  void* S = w; w += al256((int64_t)4 * nl * nkt * (ls.precision ? 4 : 8));
-  double* partial = reinterpret_cast<double*>(w); w += al256((int64_t)n_ell_tab * ntile * 6 * 8);
-  double* lscr = reinterpret_cast<double*>(w);
-  const size_t smem = (size_t)(3 * B.n_x + 2 * nl) * sizeof(double);
+  LosScratch W;
+  W.xk = reinterpret_cast<double*>(w + L.o_xk);
+  W.dinv = reinterpret_cast<double*>(w + L.o_dinv);
+  W.mlo = reinterpret_cast<double*>(w + L.o_mlo);
+  W.up = reinterpret_cast<double*>(w + L.o_up);
+  W.kidx = reinterpret_cast<int*>(w + L.o_kidx);
+  W.slopes = reinterpret_cast<double*>(w + L.o_slopes);
+  W.S = w + L.o_S;
+  W.partial = reinterpret_cast<double*>(w + L.o_partial);
+  W.lscr = reinterpret_cast<double*>(w + L.o_lscr);
+  W.max_nk = max_nk;
+  const size_t smem = (size_t)(3 * B.n_x + 3 * nl + (LOS_TY - 1) * 4 * LOS_TX) * sizeof(double);
   cudaError_t e;
   if (ls.precision == 0) {
     e = cudaFuncSetAttribute(los_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -449,33 +563,23 @@ cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_co
     e = cudaFuncSetAttribute(los_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   }
   if (e != cudaSuccess) return e;
-  for (int ci = 0; ci < n_cosmo; ++ci) {
-    const abcmb_cosmo& ch = cosmo_host[ci];
-    const int nk = ch.nk;
-    const double* kp = kbuf + ch.off_k;
-    const double* ptc = pt + ch.off_pt;
-    spline_prep_kernel<<<1, 256, 0, stream>>>(kp, nk, kt, nkt, xk, dinv, mlo, up, kidx);
-    const int ncol = NSRC_FIELDS * nl;
-    spline_slopes_kernel<<<(ncol + 127) / 128, 128, 0, stream>>>(ptc, n_save, nk, nl, xk, dinv, mlo, up, slopes);
-    dim3 gs((nkt + 127) / 128, nl);
+  for (int c0 = 0; c0 < n_cosmo; c0 += L.chunk) {
+    const int nc = (n_cosmo - c0) < L.chunk ? (n_cosmo - c0) : L.chunk;
+    spline_prep_kernel<<<nc, 256, 0, stream>>>(cosmo_dev, c0, kbuf, kt, nkt, W);
+    spline_slopes_kernel<<<dim3((NSRC_FIELDS * nl + 127) / 128, nc), 128, 0, stream>>>(cosmo_dev, c0, pt, n_save, nl, W);
+    dim3 gs((nkt + 127) / 128, nl, nc);
     if (ls.precision == 0)
-      sources_kernel<double><<<gs, 128, 0, stream>>>(cosmo_dev, ci, tables, ptc, n_save, nk, nl, xk, slopes, kidx,
-                                                     kt, nkt, ls, static_cast<double*>(S));
+      sources_kernel<double><<<gs, 128, 0, stream>>>(cosmo_dev, c0, tables, pt, n_save, nl, kt, nkt, ls, W);
     else
-      sources_kernel<float><<<gs, 128, 0, stream>>>(cosmo_dev, ci, tables, ptc, n_save, nk, nl, xk, slopes, kidx,
-                                                    kt, nkt, ls, static_cast<float*>(S));
-    const double lts = ch.lna_transfer_start;
-    const double dl = 0.0 - (lts + (double)(n_save - 2) * ((0.0 - lts) / (double)(n_save - 1)));
-    dim3 gl(n_ell_tab, ntile);
+      sources_kernel<float><<<gs, 128, 0, stream>>>(cosmo_dev, c0, tables, pt, n_save, nl, kt, nkt, ls, W);
+    dim3 gl(n_ell_tab, L.ntile, nc);
+    dim3 bl(LOS_TX, LOS_TY);
     if (ls.precision == 0)
-      los_kernel<0><<<gl, LOS_THREADS, smem, stream>>>(cosmo_dev, ci, tables, nl, dl, S, kt, nkt, B, ls.idx_min,
-                                                       ch.A_s, ch.n_s, ls.k_pivot, partial);
+      los_kernel<0><<<gl, bl, smem, stream>>>(cosmo_dev, c0, tables, nl, n_save, kt, nkt, B, ls.idx_min, ls.k_pivot, W);
     else
-      los_kernel<1><<<gl, LOS_THREADS, smem, stream>>>(cosmo_dev, ci, tables, nl, dl, S, kt, nkt, B, ls.idx_min,
-                                                       ch.A_s, ch.n_s, ls.k_pivot, partial);
-    cl_final_kernel<<<1, 256, 0, stream>>>(partial, n_ell_tab, ntile, B, ls.idx_min, ls.l_min, n_out,
-                                           cl_raw + (int64_t)ci * n_ell_tab * 3, cl + (int64_t)ci * 3 * n_out,
-                                           dcl_dns ? dcl_dns + (int64_t)ci * 3 * n_out : nullptr, lscr);
+      los_kernel<1><<<gl, bl, smem, stream>>>(cosmo_dev, c0, tables, nl, n_save, kt, nkt, B, ls.idx_min, ls.k_pivot, W);
+    cl_final_kernel<<<nc, 256, 0, stream>>>(c0, n_ell_tab, L.ntile, B, ls.idx_min, ls.l_min, n_out, W, cl_raw, cl,
+                                            dcl_dns);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
