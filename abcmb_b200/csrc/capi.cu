@@ -220,9 +220,10 @@ int abcmb_lens_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_le
   return ABCMB_OK;
 }
 
-/* Tuning knob: warps per block of the perturbation kernel (1..8). */
+/* Tuning knob: warps per block of the perturbation kernel (1..4; the
+ * kernel is compiled for at most 128 threads per block). */
 int abcmb_set_pert_warps_per_block(int w) {
-  if (w < 1 || w > 8) return fail(ABCMB_ERR_ARG, "warps per block must be 1..8");
+  if (w < 1 || w > 4) return fail(ABCMB_ERR_ARG, "warps per block must be 1..4");
   g_warps_per_block = w;
   return ABCMB_OK;
 }

@@ -406,6 +406,50 @@ __device__ PERT_APPLY_ATTR void apply_A(const Layout& L, const WarpMem& m, const
 }
 
 // Factor M = I - hg A(t_lin) (basis B): tails bottom-up, then the core inverse.
+// The Gauss-Jordan sweep of factor_newton on NC x NC core rows held in
+// registers (lane r owns row r; the pivot row travels by shuffle).  Same
+// operations in the same order as a shared-memory row sweep, so the inverse
+// is bit-identical to it; the pivot index p stays a loop variable (the row
+// entry it selects is picked with compares, not by register indexing).
+template <int NC>
+__device__ __forceinline__ void gauss_jordan_regs(WarpMem& m, int lane) {
+  const unsigned FULL = 0xffffffffu;
+  const int CS = m.cs;
+  double row[NC];
+#pragma unroll
+  for (int j = 0; j < NC; ++j) row[j] = lane < NC ? m.Mc()[lane * CS + j] : 0.;
+  unsigned used = 0u;
+  for (int p = 0; p < NC; ++p) {
+    double f = 0.;
+#pragma unroll
+    for (int j = 0; j < NC; ++j) f = (j == p) ? row[j] : f;
+    const bool elig = lane < NC && !((used >> lane) & 1u);
+    const unsigned key = elig ? (unsigned)(__double_as_longlong(fabs(f)) >> 32) : 0u;
+    const unsigned kmax = __reduce_max_sync(FULL, key);
+    const unsigned hit = __ballot_sync(FULL, elig && key == kmax);
+    const int q = __ffs(hit) - 1;
+    used |= 1u << q;
+    if (lane == 0) {
+      m.perm()[p] = q;
+      m.iperm()[q] = p;
+    }
+    const double pinv = 1. / __shfl_sync(FULL, f, q);
+    const bool isq = lane == q;
+#pragma unroll
+    for (int j = 0; j < NC; ++j) {
+      const double pj = __shfl_sync(FULL, row[j], q);
+      const bool jp = j == p;
+      const double sj = (jp ? 1. : pj) * pinv;                 // pivot row, scaled
+      row[j] = isq ? sj : fma(-f, sj, jp ? 0. : row[j]);
+    }
+  }
+  if (lane < NC) {
+#pragma unroll
+    for (int j = 0; j < NC; ++j) m.Mc()[lane * CS + j] = row[j];
+  }
+  __syncwarp();
+}
+
 __device__ void factor_newton(const Layout& L, WarpMem& m, const RowTab& R, const double* B, double hg,
                               bool ncdm, int lane) {
   const int nc = L.nc;
@@ -475,31 +519,8 @@ __device__ void factor_newton(const Layout& L, WarpMem& m, const RowTab& R, cons
   // monotonic in magnitude; ties -> lowest row), recorded in perm[p] and left
   // in place.  Afterwards A^{-1}[i][j] = Mc[q_i][k] with q_k = j, which
   // solve_newton applies as x_i = sum_k Mc[q_i][k] b[q_k].
-  unsigned used = 0u;
-  for (int p = 0; p < nc; ++p) {
-    const bool elig = lane < nc && !((used >> lane) & 1u);
-    const unsigned key = elig ? (unsigned)(__double_as_longlong(fabs(m.Mc()[lane * CS + p])) >> 32) : 0u;
-    const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
-    const unsigned hit = __ballot_sync(0xffffffffu, elig && key == kmax);
-    const int q = __ffs(hit) - 1;
-    used |= 1u << q;
-    if (lane == 0) {
-      m.perm()[p] = q;
-      m.iperm()[q] = p;
-    }
-    const double pinv = 1. / m.Mc()[q * CS + p];
-    __syncwarp();
-    if (lane < nc) m.Mc()[q * CS + lane] = (lane == p ? 1. : m.Mc()[q * CS + lane]) * pinv;
-    __syncwarp();
-    if (lane < nc && lane != q) {
-      double* row = m.Mc() + lane * CS;
-      const double* prow = m.Mc() + q * CS;
-      double f = row[p];
-      row[p] = 0.;
-      for (int j = 0; j < nc; ++j) row[j] = fma(-f, prow[j], row[j]);
-    }
-    __syncwarp();
-  }
+  if (nc == 13) gauss_jordan_regs<13>(m, lane);
+  else gauss_jordan_regs<MAXC>(m, lane);
 }
 
 // Solve M x = r in place (r holds the right-hand side on entry).
@@ -692,10 +713,17 @@ struct PertArgs {
   abcmb_pert_settings s;
 };
 
-#ifndef PERT_MIN_BLOCKS
-#define PERT_MIN_BLOCKS 2   // 250 registers, no spills: faster than 3 or 4 blocks/SM (measured on C2, C4)
-#endif
-__global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) {
+// Two instantiations of the same kernel, differing only in the register cap:
+// 2 blocks of 4 warps per SM (250 registers, no spills: the shortest time per
+// item) and 3 blocks per SM (168 registers, 12 warps: the shared-memory limit
+// at ny = 100, the most items per second once the queue is long).
+constexpr int PERT_BLOCKS_LATENCY = 2;
+constexpr int PERT_BLOCKS_THROUGHPUT = 3;
+constexpr int PERT_THREADS_MAX = 128;
+// queue length per warp (at 2 blocks/SM) from which the throughput variant wins
+constexpr int PERT_THROUGHPUT_ITEMS_PER_WARP = 16;
+
+__device__ __forceinline__ void pert_body(const PertArgs& P) {
   extern __shared__ double smem[];
   __shared__ RowTab R;
   const int lane = threadIdx.x & 31;
@@ -852,29 +880,45 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
       for (int i = 1; i < 7 && ok; ++i) {
         const double* B = m.SB() + (i == 6 ? 5 : i) * NB;
         double* fi = m.F() + i * n;
-        for (int e = lane; e < n; e += WARP) {
-          double acc = 0.;
-          for (int j = 0; j < i; ++j) acc = fma(KV_A[i][j], m.F()[j * n + e], acc);
-          m.base()[e] = m.y0()[e] + h * acc;
-          fi[e] = m.F()[(i - 1) * n + e];
+        {
+          // F rows 0..i-1 are read, row i (fi), base and v written: disjoint
+          const double* __restrict__ Fr = m.F();
+          const double* __restrict__ y0 = m.y0();
+          double* __restrict__ bw = m.base();
+          double* __restrict__ fw = fi;
+          double* __restrict__ vw = m.v();
+          for (int e = lane; e < n; e += WARP) {
+            double acc = 0.;
+            for (int j = 0; j < i; ++j) acc = fma(KV_A[i][j], Fr[j * n + e], acc);
+            const double be = y0[e] + h * acc;
+            const double fe = Fr[(i - 1) * n + e];              // predictor: the previous stage's f
+            bw[e] = be;
+            fw[e] = fe;
+            vw[e] = be + hg * fe;                               // first chord argument
+          }
         }
         if (i != 6) core_row_at(L, R, m, B, lane, cr);       // stage 7 shares stage 6's time
         __syncwarp();
         double diffsize = INFINITY, diffsize_prev;
         bool conv = false;
-        for (int e = lane; e < n; e += WARP) m.v()[e] = m.base()[e] + hg * fi[e];
-        __syncwarp();
         for (int it = 1; it <= root_max; ++it) {
           apply_A(L, m, R, cr, B, m.v(), m.r(), fi, ncdm, lane);    // residual A v - f
           solve_newton(L, m, m.r(), lane);
           double ss = 0.;
-          for (int e = lane; e < n; e += WARP) {
-            double x = m.r()[e];
-            double fnew = fi[e] + x;
-            fi[e] = fnew;
-            m.v()[e] = m.base()[e] + hg * fnew;                 // the next iteration's argument
-            double q = x * pos_rcp(atol + rtol * fabs(fnew));
-            ss += q * q;
+          {
+            // disjoint regions of the warp's scratch: no load waits on a store
+            const double* __restrict__ rr = m.r();
+            const double* __restrict__ bb = m.base();
+            double* __restrict__ ff = fi;
+            double* __restrict__ vv = m.v();
+            for (int e = lane; e < n; e += WARP) {
+              double x = rr[e];
+              double fnew = ff[e] + x;
+              ff[e] = fnew;
+              vv[e] = bb[e] + hg * fnew;                        // the next iteration's argument
+              double q = x * pos_rcp(atol + rtol * fabs(fnew));
+              ss += q * q;
+            }
           }
           ss = warp_sum(ss);
           __syncwarp();
@@ -986,6 +1030,11 @@ __global__ void __launch_bounds__(128, PERT_MIN_BLOCKS) pert_kernel(PertArgs P) 
 // ---------------------------------------------------------------------------
 namespace abcmb {
 
+template <int MIN_BLOCKS>
+__global__ void __launch_bounds__(PERT_THREADS_MAX, MIN_BLOCKS) pert_kernel(PertArgs P) {
+  pert_body(P);
+}
+
 int64_t pert_workspace_bytes(int n_cosmo) {
   int64_t b = 256;                                        // queue counter
   b += ((int64_t)n_cosmo * 8 + 255) / 256 * 256;          // lna1
@@ -1027,14 +1076,22 @@ cudaError_t launch_pert(int n_cosmo, const abcmb_cosmo* cosmo, const double* tab
   A.lna1 = lna1;
   A.queue = queue;
   A.s = s;
+  if (warps_per_block < 1 || 32 * warps_per_block > PERT_THREADS_MAX) return cudaErrorInvalidConfiguration;
   const int threads = 32 * warps_per_block;
   const size_t smem = (size_t)warps_per_block * pert_smem_per_warp(s.max_ny, A.ncm);
-  e = cudaFuncSetAttribute(pert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  int dev = 0, nsm = 0, per_sm = 0;
+  int dev = 0, nsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pert_kernel, threads, smem);
+  // a long queue (many items per warp) favours more resident warps; a short
+  // one is bounded by its slowest items and favours the uncapped registers
+  const bool throughput =
+      (int64_t)n_items >= (int64_t)PERT_THROUGHPUT_ITEMS_PER_WARP * nsm * PERT_BLOCKS_LATENCY * warps_per_block;
+  const void* fn = throughput ? (const void*)pert_kernel<PERT_BLOCKS_THROUGHPUT>
+                              : (const void*)pert_kernel<PERT_BLOCKS_LATENCY>;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   int grid = nsm * per_sm;
@@ -1042,7 +1099,8 @@ cudaError_t launch_pert(int n_cosmo, const abcmb_cosmo* cosmo, const double* tab
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
   if (grid_out) *grid_out = grid;
-  pert_kernel<<<grid, threads, smem, stream>>>(A);
+  if (throughput) pert_kernel<PERT_BLOCKS_THROUGHPUT><<<grid, threads, smem, stream>>>(A);
+  else pert_kernel<PERT_BLOCKS_LATENCY><<<grid, threads, smem, stream>>>(A);
   return cudaGetLastError();
 }
 

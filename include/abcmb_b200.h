@@ -340,7 +340,7 @@ int abcmb_lens_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev,
 /* Tuning and diagnostics                                                   */
 /* ------------------------------------------------------------------------ */
 
-/* Warps per block of the perturbation kernel (1..8; default 4). */
+/* Warps per block of the perturbation kernel (1..4; default 4). */
 int abcmb_set_pert_warps_per_block(int warps);
 
 /* Grid size (blocks) of the last perturbation launch on this process. */
