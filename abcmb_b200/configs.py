@@ -48,7 +48,6 @@ class Workload:
     kt: np.ndarray = None
     idx_min: int = 0
     idx_max: int = 0
-    l_los: int = 0               # last ell of the line-of-sight output (l_max, + 500 when lensing)
 
     def build(self, n_save: int = 500):
         self.bgs = []
@@ -62,9 +61,14 @@ class Workload:
         sp.get_k_axis_perturbations(ks)
         self.kt = sp.get_k_axis_transfer(ks)
         B = bessel_mod.load()
-        self.idx_min, self.idx_max, self.l_los = sp.ell_index_range(B.l_tab, int(self.specs["l_min"]), self.l_max,
-                                                                    self.lensing)
+        self.idx_min, self.idx_max, _ = sp.ell_index_range(B.l_tab, int(self.specs["l_min"]), self.l_max,
+                                                           self.lensing)
         return self
+
+    @property
+    def l_los(self) -> int:
+        """Last ell of the line-of-sight output: l_max, or l_max + 500 when lensing."""
+        return self.l_max + 500 if self.lensing else self.l_max
 
     def pert_settings(self):
         return packing.pert_settings(self.specs, self.batch.n_save, self.batch)

@@ -17,6 +17,10 @@ from .packing import Batch, NFIELDS, CPertSettings, CLosSettings
 
 _uploaded_devices: set = set()
 
+# cosmologies per line-of-sight launch group (LOS_CHUNK in csrc/los.cu): each
+# group costs five kernel launches
+LOS_CHUNK = 8
+
 
 def _ptr(t: torch.Tensor) -> ctypes.c_void_p:
     return ctypes.c_void_p(t.data_ptr())

@@ -91,6 +91,7 @@ def expand(w: Workload, n_save: int = 500, processes: int = 0, rel_step: float =
         sp.get_k_axis_perturbations(ks)
         w.kt = sp.get_k_axis_transfer(ks)
         from . import bessel as bessel_mod
-        w.idx_min, w.idx_max, _ = sp.ell_index_range(bessel_mod.load().l_tab, int(w.specs["l_min"]), w.l_max, False)
+        w.idx_min, w.idx_max, _ = sp.ell_index_range(bessel_mod.load().l_tab, int(w.specs["l_min"]), w.l_max,
+                                                        w.lensing)
     w.batch = batch
     return GradWorkload(base=w, variants=variants, batch=batch, n_var=len(variants[0]))

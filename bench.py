@@ -119,9 +119,13 @@ def cpu_sample(gw, stride: int, n_threads: int):
     sub = packing.Batch(cosmo=b.cosmo, tables=b.tables, kbuf=b.kbuf, items=b.items[sel].copy(), pt_size=b.pt_size,
                         n_save=b.n_save, bgs=b.bgs, layouts=b.layouts)
     st = gw.base.pert_settings()
-    t0 = time.perf_counter()
-    rc, pt, ks = oracle.pert_forward(sub, st, n_threads)
-    t_ode = (time.perf_counter() - t0) * n_full / len(sel)
+    # the host is shared: the faster of two identical runs
+    t_runs = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        rc, pt, ks = oracle.pert_forward(sub, st, n_threads)
+        t_runs.append(time.perf_counter() - t0)
+    t_ode = min(t_runs) * n_full / len(sel)
     one = packing.Batch(cosmo=b.cosmo[:1].copy(), tables=b.tables, kbuf=b.kbuf, items=b.items[:0], pt_size=b.pt_size,
                         n_save=b.n_save, bgs=b.bgs[:1], layouts=b.layouts[:1])
     ls = gw.base.los_settings()
@@ -132,7 +136,8 @@ def cpu_sample(gw, stride: int, n_threads: int):
     return {"value": 1.0 / total, "unit": UNIT, "cores": n_threads, "kind": "port",
             "sample": f"oracle (C, FP64, OpenMP) on 1 cosmology's 9 gradient variants: every {stride}th k mode of "
                       f"the ODE ({len(sel)}/{n_full} items, scaled) + 1 full line-of-sight run (x{nvar}); "
-                      f"s per cosmology+grad: ode {t_ode:.2f} los {t_los:.2f}"}
+                      f"s per cosmology+grad: ode {t_ode:.2f} (faster of 2 runs; the other "
+                      f"{max(t_runs) * n_full / len(sel):.2f}) los {t_los:.2f}"}
 
 
 def run_reference(args, rank, world):
@@ -316,8 +321,9 @@ def main():
                                "MEASURED_PEAKS.json has no FP64 figure",
                 "flops_def": "sum_k steps_k * 7 * (8 Ny + 200 + 20 Ny)", "launch_ms": pert_avg,
                 "hbm_gbs_peak_measured": _peak_hbm()}
-    # our kernel launches per step: pert (memset + 2 start kernels + persistent) + 5 per LOS cosmology
-    launches = 3 + 5 * b.n_cosmo
+    # our kernel launches per step: pert (2 start kernels + the persistent
+    # kernel) + 5 per line-of-sight chunk of engine.LOS_CHUNK cosmologies
+    launches = 3 + 5 * ((b.n_cosmo + engine.LOS_CHUNK - 1) // engine.LOS_CHUNK)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",

@@ -125,3 +125,15 @@ def test_gradient_variants_and_assembly():
         np.testing.assert_allclose(grad[0, names.index(n)], s, rtol=1e-6)
     np.testing.assert_allclose(grad[0, names.index("n_s")], 5.0)
     np.testing.assert_allclose(grad[0, names.index("A_s")], cl_base[0] / w.params_in[0]["A_s"])
+
+
+def test_expanded_workload_los_settings():
+    """The gradient-expanded workload (what bench.py runs) carries a valid
+    line-of-sight range without a separate build()."""
+    from abcmb_b200 import configs, gradients
+    w = configs.c4(n_cosmo=2, nk_range=(30, 40))
+    gradients.expand(w, processes=1)
+    ls = w.los_settings()
+    assert ls.l_max == w.l_max == 2500 and ls.idx_max > ls.idx_min >= 0 and ls.nkt > 100
+    w.lensing = True
+    assert w.los_settings().l_max == 3000
