@@ -140,13 +140,17 @@ struct WarpMem {
 // Static sparsity of the core rows, shared by the block (filled once).
 constexpr int MAXC = 22;
 constexpr int LMAXT = 63;           // largest hierarchy l_max the kernel supports
+// Byte-sized index tables: with ny = 100 the 3-blocks/SM instantiation needs
+// 3 x (4 x 18 320 B of warp scratch + this table + 1 KB reserved) to fit in
+// the SM's 228 KB, which leaves this table about 2.4 KB.
 struct RowTab {
-  int n[MAXC];
-  int bid[MAXC * 5];
-  int col[MAXC * 5];
-  int tch[MAXC];
+  int8_t n[MAXC];
+  uint8_t bid[MAXC * 5];     // basis slot (< NB)
+  uint8_t col[MAXC * 5];     // core column (< MAXC)
+  int8_t tch[MAXC];          // chain hanging off the row, -1 for none
   double cst[MAXC * 5];
   double uh[MAXC], ue[MAXC], tco[MAXC];
+  double ncdm_w[9];   // massive-neutrino bin weights of write_fields
   // tail coefficients of v[l-1] and v[l+1] per unit chain speed, by l:
   // l / (2l+1) and (l+1) / (2l+1); slot 1 holds the l = 3 pair of the F and
   // N hierarchies (6/7, 4/7: their l = 2 slot stores sigma = F_2 / 2)
@@ -433,7 +437,7 @@ __device__ __forceinline__ void gauss_jordan_regs(WarpMem& m, int lane) {
       m.perm()[p] = q;
       m.iperm()[q] = p;
     }
-    const double pinv = 1. / __shfl_sync(FULL, f, q);
+    const double pinv = __drcp_rn(__shfl_sync(FULL, f, q));    // == 1. / pivot, correctly rounded
     const bool isq = lane == q;
 #pragma unroll
     for (int j = 0; j < NC; ++j) {
@@ -587,13 +591,25 @@ __device__ void solve_newton(const Layout& L, WarpMem& m, double* r, int lane) {
 }
 
 // Fields of make_output_table at one save point from the interpolated state ys.
+// Massive-neutrino perturbation sums of write_fields: 4/pi^2 / (hbar c)^3
+constexpr double NCDM_K = 4. / (PI * PI) / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
+constexpr double G4C = 4. * PI * GN / (C_MPC * C_MPC);
+
+// PerturbationTable fields at one save point (make_output_table,
+// perturbations.py:318-404, with each species' output_perturbations).  Lane f
+// (< ABCMB_NFIELDS) writes field f.  Reciprocals are taken once (1/aH, 1/k^2,
+// the massive-neutrino bin constants come from the block table) so the metric
+// fields are products rather than chains of divisions; output-only, the
+// integration never reads them.
 __device__ __noinline__ void write_fields(const abcmb_cosmo& c, const Layout& L, const double* tables, double k, double lna,
                              const double* ys, double* pt, int n_save, int isave, int ik, int lane,
-                             const double* sv) {
+                             const double* sv, const double* ncdm_w) {
   BG b;
   if (sv) bg_load(sv, b);               // computed ahead for this save point
   else bg_eval(c, tables, lna, b);
   const double a = b.a, aH = b.aH;
+  const double iaH = 1. / aH;
+  const double ik2 = 1. / (k * k);
   double srd = b.rho_cdm * ys[1] + b.rho_b * ys[2] + b.rho_g * ys[L.i_g] + b.rho_nu * ys[L.i_nu];
   double srt = (b.rho_b + 0.) * ys[3] + (b.rho_g + b.rho_g / 3.) * ys[L.i_g + 1] +
                (b.rho_nu + b.rho_nu / 3.) * ys[L.i_nu + 1];
@@ -602,41 +618,40 @@ __device__ __noinline__ void write_fields(const abcmb_cosmo& c, const Layout& L,
   double rm = b.rho_cdm + b.rho_b;
   double nd = 0., nt = 0., ns = 0.;
   if (c.has_ncdm) {
+    // ncdm_w[3 i + {0,1,2}] = w_i (1 + e^-q_i) / q_i^2, / q_i, * 1
     double r0 = 0., r1 = 0., r2 = 0.;
     for (int i = 0; i < 3; ++i) {
-      double q = Q3[i], w = W3[i];
       const double* P = ys + L.i_ncdm + i * L.nM;
-      r0 += w * (1. + exp(-q)) * b.eps[i] / (q * q) * P[0];
-      r1 += w * (1. + exp(-q)) / q * P[1];
-      r2 += w * (1. + exp(-q)) / b.eps[i] * P[2];
+      r0 += ncdm_w[3 * i] * b.eps[i] * P[0];
+      r1 += ncdm_w[3 * i + 1] * P[1];
+      r2 += ncdm_w[3 * i + 2] / b.eps[i] * P[2];
     }
-    double T = c.T_nu_massive * c.TCMB0 / a;
-    double T4 = T * T * T * T;
-    double rd = c.N_nu_massive * r0 * 4. / (PI * PI) * T4 / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
-    double rt = c.N_nu_massive * r1 * 4. / (PI * PI) * T4 / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
-    double rs = c.N_nu_massive * r2 * 8. / 3. / (PI * PI) * T4 / (HBAR * HBAR * HBAR) / (C_CM * C_CM * C_CM);
+    const double T = c.T_nu_massive * c.TCMB0 / a;
+    const double f = c.N_nu_massive * NCDM_K * (T * T) * (T * T);
+    const double rd = f * r0, rt = f * r1, rs = (2. / 3.) * f * r2;
     srd += rd; srt += rt; srs += rs;
     rdm += rd; rm += b.rho_ncdm;
-    double rhoP = b.rho_ncdm + b.P_ncdm;
-    nd = rd / b.rho_ncdm; nt = rt / rhoP; ns = rs / rhoP;
+    const double irhoP = 1. / (b.rho_ncdm + b.P_ncdm);
+    nd = rd / b.rho_ncdm; nt = rt * irhoP; ns = rs * irhoP;
   }
   if (lane < ABCMB_NFIELDS) {
     const double eta = ys[0];
-    const double hp = 2. / (aH * aH) * (k * k * eta + 4. * PI * GN * a * a / (C_MPC * C_MPC) * srd);
-    const double etap = 4. * PI * GN * a * a / aH * srt / (C_MPC * C_MPC) / (k * k);
-    const double alpha = aH * (hp + 6. * etap) / 2. / (k * k);
+    const double a2 = a * a;
+    const double hp = 2. * (iaH * iaH) * (k * k * eta + G4C * a2 * srd);
+    const double etap = G4C * a2 * iaH * srt * ik2;
+    const double alpha = aH * (hp + 6. * etap) * 0.5 * ik2;
     double val = 0.;
     switch (lane) {
       case ABCMB_F_DELTA_M: val = rdm / rm; break;
       case ABCMB_F_THETA_B_PRIME:
-        val = -ys[3] + b.cs2 / aH * (k * k * ys[2]) + b.R / aH / b.tau_c * (ys[L.i_g + 1] - ys[3]);
+        val = -ys[3] + b.cs2 * iaH * (k * k * ys[2]) + b.R * iaH / b.tau_c * (ys[L.i_g + 1] - ys[3]);
         break;
       case ABCMB_F_ETA: val = eta; break;
       case ABCMB_F_H_PRIME: val = hp; break;
       case ABCMB_F_ETA_PRIME: val = etap; break;
       case ABCMB_F_ALPHA: val = alpha; break;
       case ABCMB_F_ALPHA_PRIME:
-        val = eta / aH - 2. * alpha - 12. * PI * GN * a * a / aH * srs / (C_MPC * C_MPC) / (k * k);
+        val = eta * iaH - 2. * alpha - 3. * G4C * a2 * iaH * srs * ik2;
         break;
       case ABCMB_F_CDM_DELTA: val = ys[1]; break;
       case ABCMB_F_B_DELTA: val = ys[2]; break;
@@ -742,6 +757,13 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
       R.col[r * 5 + t] = t < d.n ? d.col[t] : 0;
       R.cst[r * 5 + t] = t < d.n ? d.cst[t] : 0.;
     }
+  }
+  if (threadIdx.x < 3) {
+    const int i = threadIdx.x;
+    const double q = Q3[i], wq = W3[i] * (1. + exp(-q));
+    R.ncdm_w[3 * i] = wq / (q * q);
+    R.ncdm_w[3 * i + 1] = wq / q;
+    R.ncdm_w[3 * i + 2] = wq;
   }
   for (int l = threadIdx.x; l <= LMAXT; l += blockDim.x) {
     R.ta[l] = (l == 1) ? 6. / 7. : (double)l / (2. * l + 1.);
@@ -987,7 +1009,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
           }
           __syncwarp();
           write_fields(c, L, P.tables, k, ts, m.v(), P.pt, nsave, isave, ik, lane,
-                       m.SV()[16] == (double)isave ? m.SV() : nullptr);
+                       m.SV()[16] == (double)isave ? m.SV() : nullptr, R.ncdm_w);
           __syncwarp();
           ++isave;
         }

@@ -206,3 +206,18 @@ def test_torch_ops_match_engine(gpu, c1_small):
                                       db.ws_pert)
     torch.cuda.synchronize()
     assert torch.equal(ref, pt2)
+
+
+def test_long_queue_runs_three_blocks_per_sm(gpu):
+    """A long queue with the largest state (ny = 100, massive neutrinos) gets
+    the 3-blocks/SM instantiation: its shared memory must still fit 3 blocks."""
+    import torch
+    from abcmb_b200 import configs, engine, _lib
+    w = configs.c4(n_cosmo=40, nk_range=(500, 520)).build()
+    assert int(w.batch.cosmo["ny"].max()) == 100
+    db = engine.DeviceBatch.upload(w.batch)
+    db.pert_forward(w.pert_settings())
+    torch.cuda.synchronize()
+    nsm = torch.cuda.get_device_properties(0).multi_processor_count
+    assert _lib.load().abcmb_last_pert_grid() == 3 * nsm
+    db.check_status()
