@@ -380,8 +380,11 @@ __device__ __forceinline__ void core_row_at(const Layout& L, const RowTab& R, co
 #define PERT_APPLY_ATTR
 #endif
 // out = A v - fsub (fsub may be null): the RHS, or the chord residual directly.
+// B (a basis slot), v, out and fsub are disjoint regions of the warp's
+// scratch in every call (fsub may be null).
 __device__ PERT_APPLY_ATTR void apply_A(const Layout& L, const WarpMem& m, const RowTab& R, const CoreRow& cr,
-                                       const double* B, const double* v, double* out, const double* fsub,
+                                       const double* __restrict__ B, const double* __restrict__ v,
+                                       double* __restrict__ out, const double* __restrict__ fsub,
                                        bool ncdm, int lane) {
   double hp, etap;
   metric(L, B, v, ncdm, hp, etap);
@@ -410,25 +413,20 @@ __device__ PERT_APPLY_ATTR void apply_A(const Layout& L, const WarpMem& m, const
 }
 
 // Factor M = I - hg A(t_lin) (basis B): tails bottom-up, then the core inverse.
-// The Gauss-Jordan sweep of factor_newton on NC x NC core rows held in
-// registers (lane r owns row r; the pivot row travels by shuffle).  Same
-// operations in the same order as a shared-memory row sweep, so the inverse
-// is bit-identical to it; the pivot index p stays a loop variable (the row
-// entry it selects is picked with compares, not by register indexing).
+// The Gauss-Jordan sweep of factor_newton on the NC x NC core in shared
+// memory, one row per lane.  NC is a compile-time size (13, or 22 with
+// massive neutrinos) so the row loops unroll; the row a lane updates and the
+// pivot row are disjoint, declared __restrict__, so all loads of a pivot step
+// issue before its stores.
 template <int NC>
-__device__ __forceinline__ void gauss_jordan_regs(WarpMem& m, int lane) {
+__device__ __forceinline__ void gauss_jordan(WarpMem& m, int lane) {
   const unsigned FULL = 0xffffffffu;
   const int CS = m.cs;
-  double row[NC];
-#pragma unroll
-  for (int j = 0; j < NC; ++j) row[j] = lane < NC ? m.Mc()[lane * CS + j] : 0.;
+  double* Mc = m.Mc();
   unsigned used = 0u;
   for (int p = 0; p < NC; ++p) {
-    double f = 0.;
-#pragma unroll
-    for (int j = 0; j < NC; ++j) f = (j == p) ? row[j] : f;
     const bool elig = lane < NC && !((used >> lane) & 1u);
-    const unsigned key = elig ? (unsigned)(__double_as_longlong(fabs(f)) >> 32) : 0u;
+    const unsigned key = elig ? (unsigned)(__double_as_longlong(fabs(Mc[lane * CS + p])) >> 32) : 0u;
     const unsigned kmax = __reduce_max_sync(FULL, key);
     const unsigned hit = __ballot_sync(FULL, elig && key == kmax);
     const int q = __ffs(hit) - 1;
@@ -437,21 +435,25 @@ __device__ __forceinline__ void gauss_jordan_regs(WarpMem& m, int lane) {
       m.perm()[p] = q;
       m.iperm()[q] = p;
     }
-    const double pinv = __drcp_rn(__shfl_sync(FULL, f, q));    // == 1. / pivot, correctly rounded
-    const bool isq = lane == q;
+    const double pinv = __drcp_rn(Mc[q * CS + p]);          // == 1. / pivot, correctly rounded
+    __syncwarp();
+    if (lane < NC) Mc[q * CS + lane] = (lane == p ? 1. : Mc[q * CS + lane]) * pinv;
+    __syncwarp();
+    if (lane < NC && lane != q) {
+      double* __restrict__ row = Mc + lane * CS;
+      const double* __restrict__ prow = Mc + q * CS;
+      const double f = row[p];
+      double pr[NC], rw[NC];
 #pragma unroll
-    for (int j = 0; j < NC; ++j) {
-      const double pj = __shfl_sync(FULL, row[j], q);
-      const bool jp = j == p;
-      const double sj = (jp ? 1. : pj) * pinv;                 // pivot row, scaled
-      row[j] = isq ? sj : fma(-f, sj, jp ? 0. : row[j]);
+      for (int c = 0; c < NC; ++c) {
+        pr[c] = prow[c];
+        rw[c] = (c == p) ? 0. : row[c];
+      }
+#pragma unroll
+      for (int c = 0; c < NC; ++c) row[c] = fma(-f, pr[c], rw[c]);
     }
+    __syncwarp();
   }
-  if (lane < NC) {
-#pragma unroll
-    for (int j = 0; j < NC; ++j) m.Mc()[lane * CS + j] = row[j];
-  }
-  __syncwarp();
 }
 
 __device__ void factor_newton(const Layout& L, WarpMem& m, const RowTab& R, const double* B, double hg,
@@ -523,8 +525,8 @@ __device__ void factor_newton(const Layout& L, WarpMem& m, const RowTab& R, cons
   // monotonic in magnitude; ties -> lowest row), recorded in perm[p] and left
   // in place.  Afterwards A^{-1}[i][j] = Mc[q_i][k] with q_k = j, which
   // solve_newton applies as x_i = sum_k Mc[q_i][k] b[q_k].
-  if (nc == 13) gauss_jordan_regs<13>(m, lane);
-  else gauss_jordan_regs<MAXC>(m, lane);
+  if (nc == 13) gauss_jordan<13>(m, lane);
+  else gauss_jordan<MAXC>(m, lane);
 }
 
 // Solve M x = r in place (r holds the right-hand side on entry).
@@ -965,19 +967,22 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
       double scaled = INFINITY;
       if (ok) {
         double ss = 0.;
+        const double* __restrict__ Fr = m.F();
+        const double* __restrict__ y0 = m.y0();
+        double* __restrict__ y1 = m.y1();
         for (int e = lane; e < n; e += WARP) {
           double acc = 0., acce = 0.;
 #pragma unroll
           for (int j = 0; j < 6; ++j) {
-            double fj = m.F()[j * n + e];
+            double fj = Fr[j * n + e];
             acc = fma(KV_A[6][j], fj, acc);
             acce = fma(KV_A[6][j] - KV_A[5][j], fj, acce);
           }
-          acc = fma(KV_G, m.F()[6 * n + e], acc);
-          acce += -KV_G * m.F()[5 * n + e] + KV_G * m.F()[6 * n + e];
-          double y0e = m.y0()[e];
+          acc = fma(KV_G, Fr[6 * n + e], acc);
+          acce += -KV_G * Fr[5 * n + e] + KV_G * Fr[6 * n + e];
+          double y0e = y0[e];
           double y1e = y0e + h * acc;
-          m.y1()[e] = y1e;
+          y1[e] = y1e;
           double err = h * acce;
           double q = err * pos_rcp(atol + fmax(fabs(y0e), fabs(y1e)) * rtol);
           ss += q * q;
@@ -1002,10 +1007,16 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
           double ts = linspace_at(lts, 0.0, nsave, isave);
           if (!(ts <= t1)) break;
           double th = (ts - t0) / h;
-          for (int e = lane; e < n; e += WARP) {
-            double y0e = m.y0()[e], y1e = m.y1()[e];
-            double k0 = h * m.F()[e], k1 = h * m.F()[6 * n + e];
-            m.v()[e] = y0e + th * (k0 + th * ((3. * (y1e - y0e) - 2. * k0 - k1) + th * (2. * (y0e - y1e) + k0 + k1)));
+          {
+            const double* __restrict__ y0 = m.y0();
+            const double* __restrict__ y1 = m.y1();
+            const double* __restrict__ Fr = m.F();
+            double* __restrict__ vv = m.v();
+            for (int e = lane; e < n; e += WARP) {
+              double y0e = y0[e], y1e = y1[e];
+              double k0 = h * Fr[e], k1 = h * Fr[6 * n + e];
+              vv[e] = y0e + th * (k0 + th * ((3. * (y1e - y0e) - 2. * k0 - k1) + th * (2. * (y0e - y1e) + k0 + k1)));
+            }
           }
           __syncwarp();
           write_fields(c, L, P.tables, k, ts, m.v(), P.pt, nsave, isave, ik, lane,
