@@ -221,3 +221,59 @@ def test_long_queue_runs_three_blocks_per_sm(gpu):
     nsm = torch.cuda.get_device_properties(0).multi_processor_count
     assert _lib.load().abcmb_last_pert_grid() == 3 * nsm
     db.check_status()
+
+
+def test_gradients_match_oracle(gpu):
+    """The batched gradient (9 variants in one launch: central differences in
+    h, omega_b, omega_cdm, tau_reion; exact A_s) agrees with the same gradient
+    from the oracle."""
+    from abcmb_b200 import configs, engine, gradients, bessel
+    from oracle import oracle
+    w = configs.c1(nk=40, l_max=400)
+    gw = gradients.expand(w, processes=1)
+    ls = w.los_settings()
+    db = engine.DeviceBatch.upload(gw.batch)
+    db.pert_forward(w.pert_settings())
+    db.check_status()
+    lr = engine.LosRunner(db, w.kt, ls, want_dns=True)
+    lr.run()
+    n_out = ls.l_max - 1
+    cl = lr.cl_host()
+    dns = lr.dcl_dns.cpu().numpy().reshape(-1, 3, n_out)
+    cl_b, grad = gw.assemble(cl, dns)
+    rc, pt_o, _ = oracle.pert_forward(gw.batch, w.pert_settings())
+    assert rc == 0
+    _, _, cl_o = oracle.los_forward(gw.batch, pt_o, w.kt, ls, bessel.load())
+    cl_bo, grad_o = gw.assemble(cl_o, dns)           # the n_s row is compared on its own below
+    names = configs.GRAD_PARAMS
+    for name in ("h", "omega_b", "omega_cdm", "A_s", "tau_reion"):
+        gi = names.index(name)
+        for X in (0, 2):
+            g, go = grad[0, gi, X], grad_o[0, gi, X]
+            assert np.abs(g - go).max() / np.abs(go).max() < 1e-4, (name, X)
+
+
+def test_dcl_dns_matches_central_difference(gpu, c1_small, c1_oracle):
+    """dC_l/dn_s from the ln(k/k_pivot)-weighted quadrature equals a central
+    difference of C_l in n_s (the perturbations do not depend on n_s)."""
+    import torch
+    from abcmb_b200 import engine
+    w = c1_small
+    db = engine.DeviceBatch.upload(w.batch)
+    db.pert_forward(w.pert_settings())
+    lr = engine.LosRunner(db, w.kt, w.los_settings(), want_dns=True)
+    lr.run()
+    dns = lr.dcl_dns.cpu().numpy().reshape(1, 3, -1)
+    n_s = float(w.batch.cosmo["n_s"][0])
+    dn = 1e-4 * n_s
+    out = []
+    for sgn in (+1, -1):
+        cos = w.batch.cosmo.copy()
+        cos["n_s"] = n_s + sgn * dn
+        db.cosmo.copy_(torch.from_numpy(cos.view(np.uint8)))
+        lr.cosmo_host = np.ascontiguousarray(cos)
+        lr.run()
+        out.append(lr.cl_host().copy())
+    fd = (out[0] - out[1]) / (2 * dn)
+    for X in (0, 1, 2):
+        assert np.abs(fd[0, X] - dns[0, X]).max() / np.abs(dns[0, X]).max() < 1e-6, X
