@@ -21,6 +21,8 @@ from __future__ import annotations
 
 from dataclasses import dataclass, field
 
+import math
+
 import numpy as np
 
 from . import background_tables as bt
@@ -113,3 +115,46 @@ def c4(n_cosmo: int = 64, l_max: int = 2500, nk_range=(400, 800), seed: int = SE
         ncdm.append(nnu > 0)
         kgrids.append(np.geomspace(1e-5, 1.0, nk))
     return Workload("C4", specs, params, ncdm, kgrids, l_max)
+
+
+# three massive species already carry N_eff = 3 x 1.0132 (T_nu_massive =
+# 0.71611); below that the massless density would be negative
+NEFF_MIN_THREE_MASSIVE = 3.05
+
+
+C5_MAX_STEPS = 16384
+
+
+def c5(n_cosmo: int = 256, l_max: int = 3000, nk_range=(400, 800), seed: int = SEED, k_max: float = 5.0) -> Workload:
+    """Lensed batch: C4's parameter draws plus N_eff uniform in 2.8..3.4
+    (3.05..3.4 with three massive species), lensed TT/TE/EE to l_max with the
+    line of sight to l_max + 500, k grids geomspace(1e-5, k_max, Nk') with Nk'
+    scaled so the density per decade matches C4's, for P(k) to k_max."""
+    rng = np.random.default_rng(seed)
+    # k to 5 / Mpc takes ~5x the steps of k = 1 (C4 peaks at 1833 of the
+    # default 2048): max_steps_PE raised as the reference's error asks
+    specs = sp.load_specs(dict(l_max=l_max, lensing=True, max_steps_PE=C5_MAX_STEPS))
+    params, ncdm, kgrids = [], [], []
+    dec = math.log10(k_max / 1e-5) / math.log10(1.0 / 1e-5)
+    for _ in range(n_cosmo):
+        p = dict(FIDUCIAL)
+        for name in GRAD_PARAMS:
+            p[name] = FIDUCIAL[name] * rng.uniform(0.95, 1.05)
+        nnu = int(rng.choice([0, 1, 3]))
+        if nnu:
+            p.update(N_nu_massive=nnu, m_nu_massive=0.06)
+        nk = int(rng.integers(nk_range[0], nk_range[1] + 1))
+        lo = NEFF_MIN_THREE_MASSIVE if nnu == 3 else 2.8
+        p["Neff"] = float(rng.uniform(lo, 3.4))
+        params.append(p)
+        ncdm.append(nnu > 0)
+        kgrids.append(np.geomspace(1e-5, k_max, int(round(nk * dec))))
+    return Workload("C5", specs, params, ncdm, kgrids, l_max, lensing=True)
+
+
+# P(k) of the lensed batch: z in {0, 1, 2, 3}, k to 5 / Mpc
+C5_PK_Z = (0.0, 1.0, 2.0, 3.0)
+
+
+def c5_pk_k(k_max: float = 5.0, n: int = 200) -> np.ndarray:
+    return np.geomspace(1e-4, k_max, n)

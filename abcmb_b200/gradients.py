@@ -7,6 +7,13 @@ h, omega_b, omega_cdm and tau_reion change the background and the
 perturbations; their derivatives are central differences with relative step
 1e-4 (the finite-difference check of the gradient configuration), all
 variants of all cosmologies integrated in one batched launch.
+
+With lensing, A_s and n_s also set C_l^phiphi (lensing_power_spectrum goes
+through Pk_lin, spectrum.py:349-384), so the lensed spectra are not linear in
+A_s: their derivatives are central differences too, from four extra
+descriptors per cosmology that share the base cosmology's perturbations (the
+perturbations do not depend on A_s or n_s) and cost only line-of-sight and
+lensing work.
 """
 from __future__ import annotations
 
@@ -57,10 +64,11 @@ class GradWorkload:
         grad = np.zeros((nb, len(GRAD_PARAMS)) + cl.shape[2:])
         for i in range(nb):
             var = self.variants[i]
+            fd_names = {v[0] for v in var}
             for gi, name in enumerate(GRAD_PARAMS):
-                if name == "A_s":
+                if name == "A_s" and name not in fd_names:
                     grad[i, gi] = cl[i, 0] / self.base.params_in[i]["A_s"]
-                elif name == "n_s":
+                elif name == "n_s" and name not in fd_names:
                     grad[i, gi] = dns[i, 0]
                 else:
                     jp = next(j for j, v in enumerate(var) if v[0] == name and v[1] > 0)
@@ -69,23 +77,53 @@ class GradWorkload:
         return cl[:, 0], grad
 
 
-def expand(w: Workload, n_save: int = 500, processes: int = 0, rel_step: float = REL_STEP) -> GradWorkload:
-    """Background tables for every variant (host, optionally in a spawn pool)."""
-    jobs, variants, layouts, kgrids = [], [], [], []
+PRIMORDIAL_PARAMS = ("A_s", "n_s")
+
+
+def expand(w: Workload, n_save: int = 500, processes: int = 0, rel_step: float = REL_STEP,
+           primordial_fd: bool = None) -> GradWorkload:
+    """Background tables for every variant (host, optionally in a spawn pool).
+
+    primordial_fd (default: the workload's lensing flag) adds the A_s and n_s
+    +- descriptors that share their base cosmology's perturbations."""
+    if primordial_fd is None:
+        primordial_fd = bool(w.lensing)
+    jobs, variants, layouts, kgrids, alias, overrides = [], [], [], [], [], []
     for p_in, ncdm, kg in zip(w.params_in, w.has_ncdm, w.kgrids):
         var = fd_variants(p_in, rel_step)
-        variants.append([(v[0], v[1], v[2]) for v in var])
+        entries = [(v[0], v[1], v[2]) for v in var]
+        base_index = len(jobs)
         for v in var:
             jobs.append((v[3], ncdm, w.specs))
             layouts.append(sp.state_layout(w.specs, ncdm))
             kgrids.append(kg)
+            alias.append(None)
+            overrides.append(None)
+        if primordial_fd:
+            for name in PRIMORDIAL_PARAMS:
+                hstep = rel_step * p_in[name]
+                for sgn in (+1, -1):
+                    entries.append((name, sgn, hstep))
+                    jobs.append(None)
+                    layouts.append(sp.state_layout(w.specs, ncdm))
+                    kgrids.append(kg)
+                    alias.append(base_index)
+                    overrides.append({name: p_in[name] + sgn * hstep})
+        variants.append(entries)
+    real = [j for j in jobs if j is not None]
     if processes and processes > 1:
         import multiprocessing as mp
         with mp.get_context("spawn").Pool(processes) as pool:
-            bgs = pool.map(_bg_job, jobs, chunksize=max(1, len(jobs) // (4 * processes)))
+            bgs_real = pool.map(_bg_job, real, chunksize=max(1, len(real) // (4 * processes)))
     else:
-        bgs = [_bg_job(j) for j in jobs]
-    batch = packing.pack(bgs, layouts, kgrids, n_save=n_save)
+        bgs_real = [_bg_job(j) for j in real]
+    it = iter(bgs_real)
+    bgs = [next(it) if j is not None else None for j in jobs]
+    for i, a in enumerate(alias):
+        if a is not None:
+            bgs[i] = bgs[a]
+    batch = packing.pack(bgs, layouts, kgrids, n_save=n_save, alias_of=alias if primordial_fd else None,
+                         overrides=overrides if primordial_fd else None)
     if w.kt is None:
         ks = dict(w.specs)
         sp.get_k_axis_perturbations(ks)

@@ -112,12 +112,19 @@ class Batch:
         return self.kbuf[int(c["off_k"]):int(c["off_k"]) + int(c["nk"])]
 
 
-def pack(bgs, layouts, kgrids, n_save: int = 500, order: str = "cost") -> Batch:
+def pack(bgs, layouts, kgrids, n_save: int = 500, order: str = "cost", alias_of=None,
+         overrides=None) -> Batch:
     """Pack cosmologies (BackgroundTables, StateLayout, k grid) into a Batch.
 
     order="cost" hands the persistent queue the expensive items first:
     large k (many steps) and large state vectors, which keeps the tail of
     the launch short.
+
+    alias_of[i] = j (< i) makes entry i a descriptor of entry j's tables, k
+    grid and PerturbationTable with no work items of its own; overrides[i]
+    (a dict) then changes parameters that only the line of sight reads
+    (A_s, n_s): the primordial finite-difference variants, which share their
+    base cosmology's perturbations.
     """
     n = len(bgs)
     rec = np.zeros(n, dtype=COSMO_DTYPE)
@@ -128,6 +135,16 @@ def pack(bgs, layouts, kgrids, n_save: int = 500, order: str = "cost") -> Batch:
     ptoff = 0
     nl = n_save - 1
     for i, (bg, lay, kg) in enumerate(zip(bgs, layouts, kgrids)):
+        if alias_of is not None and alias_of[i] is not None:
+            j = alias_of[i]
+            if not 0 <= j < i or (alias_of[j] is not None):
+                raise ValueError("alias_of must point to an earlier, non-alias entry")
+            rec[i] = rec[j]
+            for name, val in (overrides[i] if overrides is not None and overrides[i] else {}).items():
+                if name not in ("A_s", "n_s"):
+                    raise ValueError("an alias entry may only change A_s and n_s")
+                rec[i][name] = float(val)
+            continue
         p = bg.params
         r = rec[i]
         for name in ["h", "omega_b", "omega_cdm", "omega_Lambda", "A_s", "n_s", "TCMB0", "YHe",
@@ -177,7 +194,8 @@ def pack(bgs, layouts, kgrids, n_save: int = 500, order: str = "cost") -> Batch:
         r["has_ncdm"] = int(lay.has_ncdm)
         r["ny"] = lay.ny
         r["nk"] = kg.shape[0]
-    items = [(i, j) for i in range(n) for j in range(int(rec[i]["nk"]))]
+    items = [(i, j) for i in range(n) for j in range(int(rec[i]["nk"]))
+             if alias_of is None or alias_of[i] is None]
     if order == "cost":
         items.sort(key=lambda it: (-rec[it[0]]["ny"], -kgrids[it[0]][it[1]]))
     return Batch(cosmo=rec, tables=np.concatenate(chunks), kbuf=np.concatenate(kchunks),

@@ -137,3 +137,38 @@ def test_expanded_workload_los_settings():
     assert ls.l_max == w.l_max == 2500 and ls.idx_max > ls.idx_min >= 0 and ls.nkt > 100
     w.lensing = True
     assert w.los_settings().l_max == 3000
+
+
+def test_lensed_expansion_shares_perturbations():
+    """With lensing the A_s / n_s +- variants are descriptors of their base
+    cosmology's tables and PerturbationTable with no work items, and the
+    assembly takes central differences for them."""
+    from abcmb_b200 import configs, gradients
+    w = configs.c5(n_cosmo=2, l_max=300, nk_range=(30, 40))
+    gw = gradients.expand(w, processes=1)
+    b = gw.batch
+    assert gw.n_var == 13 and b.n_cosmo == 26
+    c = b.cosmo
+    for i in range(2):
+        base = 13 * i
+        for j in range(9, 13):
+            for f in ("off_pt", "off_tau", "off_k", "nk", "ny", "tau0", "h", "omega_b"):
+                assert c[base + j][f] == c[base][f], f
+        var = gw.variants[i]
+        assert [v[0] for v in var[9:]] == ["A_s", "A_s", "n_s", "n_s"]
+        assert c[base + 9]["A_s"] > c[base]["A_s"] > c[base + 10]["A_s"]
+        assert c[base + 11]["n_s"] > c[base]["n_s"] > c[base + 12]["n_s"]
+    assert set(int(x) % 13 for x in b.items[:, 0]) == set(range(9))
+    # assembly: C_l linear in every parameter recovers the slopes
+    slope = {"h": 2.0, "omega_b": -3.0, "omega_cdm": 0.5, "A_s": 4e8, "n_s": -1.5, "tau_reion": 7.0}
+    cl = np.zeros((26, 3, 5))
+    for i in range(2):
+        p0 = w.params_in[i]
+        for j, (name, sgn, hstep) in enumerate(gw.variants[i]):
+            val = 1.0
+            if name is not None:
+                val += slope[name] * sgn * hstep
+            cl[13 * i + j] = val
+    _, grad = gw.assemble(cl, np.zeros_like(cl))
+    for gi, name in enumerate(configs.GRAD_PARAMS):
+        np.testing.assert_allclose(grad[:, gi], slope[name], rtol=1e-6)

@@ -213,3 +213,42 @@ def test_dropin_lensed_get_cl(lensed_c1):
     assert np.abs(lt[: w.l_max - 1] - cll_o[0, 0]).max() / np.abs(cll_o[0, 0]).max() < 1e-6
     with pytest.raises(ValueError):
         SS.lensed_Cls(SS.ells, tt, te, ee, PT)
+
+
+@pytest.mark.gpu
+def test_c5_lensed_batch_gradient_and_pk_match_oracle():
+    """The lensed batch (C5 shape, reduced): lensed C_l, the 6-parameter
+    gradient (13 variants, A_s / n_s sharing their base's perturbations) and
+    P(k) at z = 0..3 against the oracle."""
+    from abcmb_b200 import gradients, pipeline
+    w = configs.c5(n_cosmo=2, l_max=300, nk_range=(40, 60))
+    gw = gradients.expand(w, processes=1)
+    kout = configs.c5_pk_k(n=40)
+    z = np.array(configs.C5_PK_Z)
+    cl, grad, pk, cl_var = pipeline.run_cl_grad(gw, "cuda:0", kout, z, return_variants=True)
+    rc, pt, _ = oracle.pert_forward(gw.batch, w.pert_settings())
+    assert rc == 0
+    rc, _, cl_unl = oracle.los_forward(gw.batch, pt, w.kt, w.los_settings(), bessel.load())
+    assert rc == 0
+    mu, wt = lensing.lensing_nodes(w.l_max)
+    rc, _, cll = oracle.lens_forward(gw.batch, pt, lensing.lens_descriptors(gw.batch), mu, wt, cl_unl,
+                                     w.lens_settings())
+    assert rc == 0
+    cl_o, grad_o = gw.assemble(cll, np.zeros_like(cll))
+    pk_o = oracle.pk_lin(gw.batch, pt, w.specs["k_pivot"], kout, z)[::gw.n_var]
+    # every variant's lensed C_l (the quantities the differences are taken of)
+    for i in range(cl_var.shape[0]):
+        for X in range(3):
+            assert np.abs(cl_var[i, X] - cll[i, X]).max() / np.abs(cll[i, X]).max() < 1e-6, (i, X)
+    # a central difference with relative step 1e-4 divides C_l-level
+    # differences by ~1e-4 |dlnC/dln theta|: at l = 2, where dC/dtau_reio
+    # peaks, 1e-9 of C_2 becomes ~1e-3 of the derivative, so the gradients
+    # are held to 1e-2 of each series' maximum
+    for ci in range(2):
+        for X in range(3):
+            assert np.abs(cl[ci, X] - cl_o[ci, X]).max() / np.abs(cl_o[ci, X]).max() < 1e-6
+            for gi in range(6):
+                g, go = grad[ci, gi, X], grad_o[ci, gi, X]
+                assert np.abs(g - go).max() / np.abs(go).max() < 1e-2, (ci, X, gi)
+    # GPU and oracle perturbations agree to ~3e-6 of each field; P ~ delta_m^2
+    np.testing.assert_allclose(pk, pk_o, rtol=1e-5)
