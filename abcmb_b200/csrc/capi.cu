@@ -20,6 +20,8 @@ cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_co
 cudaError_t launch_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* kbuf, const double* pt,
                           int n_save, double k_pivot, int n_kout, const double* kout, int n_z, const double* z,
                           double* pk, cudaStream_t stream);
+cudaError_t launch_cl_spline(int n_cosmo, const double* cl_raw, int idx_min, int n_ell_tab, int l_min, int l_max,
+                             const BesselDev& B, double* cl, cudaStream_t stream);
 int64_t lens_workspace_bytes(int n_cosmo, const abcmb_lens_settings& s);
 cudaError_t launch_lens(int n_cosmo, const abcmb_cosmo* cosmo, const abcmb_lens_cosmo* lens, const double* tables,
                         const double* kbuf, const double* pt, const double* mu, const double* w,
@@ -188,6 +190,21 @@ int abcmb_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* k_dev,
   cudaError_t e = abcmb::launch_pk_lin(n_cosmo, cosmo_dev, k_dev, pt_dev, n_save, k_pivot, n_kout, kout_dev, n_z,
                                        z_dev, pk_dev, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "abcmb_pk_lin");
+  return ABCMB_OK;
+}
+
+int abcmb_cl_spline(int n_cosmo, const double* cl_raw_dev, int idx_min, int n_ell_tab, int l_min, int l_max,
+                    double* cl_dev, void* stream) {
+  if (n_cosmo <= 0 || n_cosmo > 65535 || !cl_raw_dev || !cl_dev)
+    return fail(ABCMB_ERR_ARG, "abcmb_cl_spline: bad argument");
+  if (l_min != 2 || l_max < l_min || n_ell_tab < 4)
+    return fail(ABCMB_ERR_ARG, "abcmb_cl_spline: need l_min == 2 <= l_max and at least 4 tabulated l");
+  BesselCache* bc = bessel_for_current_device();
+  if (!bc || !bc->ready) return fail(ABCMB_ERR_TABLES, "abcmb_cl_spline: Bessel tables not uploaded");
+  if (idx_min < 0 || idx_min + n_ell_tab > bc->dev.n_l) return fail(ABCMB_ERR_ARG, "abcmb_cl_spline: l index range");
+  cudaError_t e = abcmb::launch_cl_spline(n_cosmo, cl_raw_dev, idx_min, n_ell_tab, l_min, l_max, bc->dev, cl_dev,
+                                          static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "abcmb_cl_spline");
   return ABCMB_OK;
 }
 

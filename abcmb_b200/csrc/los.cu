@@ -441,6 +441,39 @@ __global__ void cl_final_kernel(int c0, int n_ell_tab, int ntile, BesselDev B, i
   }
 }
 
+// The l spline of cl_final_kernel on C_l already summed at the tabulated l
+// (cl_raw [n_cosmo][n_ell_tab][3]): one block per cosmology, scratch in
+// dynamic shared memory (13 n_ell_tab doubles).  Same operations as
+// cl_final_kernel, so the results are identical to the single-call path.
+__global__ void cl_spline_kernel(const double* __restrict__ cl_raw, int n_ell_tab, BesselDev B, int idx_min,
+                                 int l_min, int n_out, double* __restrict__ cl) {
+  extern __shared__ double sp[];
+  const int ci = blockIdx.x;
+  const int n = n_ell_tab;
+  double* x = sp;
+  double* y = x + n;
+  double* s = y + 3 * n;
+  double* dinv = s + 3 * n;
+  double* mlo = dinv + n;
+  double* up = mlo + n;
+  const double* raw = cl_raw + (int64_t)ci * n * 3;
+  for (int i = threadIdx.x; i < n * 3; i += blockDim.x) y[(i % 3) * n + i / 3] = raw[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = (double)B.l_tab[idx_min + i];
+  __syncthreads();
+  if (threadIdx.x == 0) nak_factor(x, n, dinv, mlo, up);
+  __syncthreads();
+  if (threadIdx.x < 3) nak_solve(x, y + threadIdx.x * n, n, dinv, mlo, up, s + threadIdx.x * n);
+  __syncthreads();
+  double* out = cl + (int64_t)ci * 3 * n_out;
+  for (int i = threadIdx.x; i < 3 * n_out; i += blockDim.x) {
+    const int X = i / n_out, o = i % n_out;
+    const double xq = (double)(l_min + o);
+    const int iv = spline_interval(x, n, xq);
+    out[(int64_t)X * n_out + o] = spline_piece(y[X * n + iv], y[X * n + iv + 1], s[X * n + iv], s[X * n + iv + 1],
+                                               x[iv + 1] - x[iv], xq - x[iv]);
+  }
+}
+
 // jnp.interp(x, xp, fp) for increasing xp
 __device__ double np_interp(double x, const double* xp, const double* fp, int n, int stride) {
   int lo = 0, hi = n;
@@ -584,6 +617,13 @@ cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_co
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+cudaError_t launch_cl_spline(int n_cosmo, const double* cl_raw, int idx_min, int n_ell_tab, int l_min, int l_max,
+                             const BesselDev& B, double* cl, cudaStream_t stream) {
+  const size_t smem = (size_t)13 * n_ell_tab * sizeof(double);
+  cl_spline_kernel<<<n_cosmo, 256, smem, stream>>>(cl_raw, n_ell_tab, B, idx_min, l_min, l_max - l_min + 1, cl);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* kbuf, const double* pt,

@@ -272,6 +272,18 @@ int abcmb_los_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev,
                       void* stream);
 
 /*
+ * The last stage of abcmb_los_forward on its own: the cubic spline in l of
+ * C_l given at the tabulated l (spectrum.py:597-608) onto the integer ells
+ * l_min..l_max (l_min == 2), for callers that assemble cl_raw themselves --
+ * e.g. one cosmology whose tabulated l were shared out over several GPUs and
+ * gathered.  Same arithmetic as abcmb_los_forward's own spline.
+ *   cl_raw_dev [n_cosmo x n_ell_tab x 3]  C_l at bessel_l_tab[idx_min + i]
+ *   cl_dev     [n_cosmo x 3 x (l_max-l_min+1)]
+ */
+int abcmb_cl_spline(int n_cosmo, const double* cl_raw_dev, int idx_min, int n_ell_tab,
+                    int l_min, int l_max, double* cl_dev, void* stream);
+
+/*
  * Linear matter power spectrum P(k, z) (SpectrumSolver.Pk_lin,
  * spectrum.py:268-302): delta_m interpolated linearly in lna to z, then
  * linearly in k (clamped), times the primordial spectrum.

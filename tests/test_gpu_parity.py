@@ -277,3 +277,27 @@ def test_dcl_dns_matches_central_difference(gpu, c1_small, c1_oracle):
     fd = (out[0] - out[1]) / (2 * dn)
     for X in (0, 1, 2):
         assert np.abs(fd[0, X] - dns[0, X]).max() / np.abs(dns[0, X]).max() < 1e-6, X
+
+
+def test_one_cosmology_in_two_shares_matches_one_call(gpu):
+    """The stages of a two-rank split of one cosmology (k modes, then
+    tabulated l), run one after the other on this GPU, give the same C_l bits
+    as one abcmb_los_forward call."""
+    from abcmb_b200 import configs, engine, sharding
+    w = configs.c2(nk=60, l_max=400).build()
+    db = engine.DeviceBatch.upload(w.batch)
+    db.pert_forward(w.pert_settings())
+    db.check_status()
+    lr = engine.LosRunner(db, w.kt, w.los_settings())
+    lr.run()
+    ref = lr.cl_host()[0]
+    nk = int(w.batch.cosmo["nk"][0])
+    n_ell = w.idx_max - w.idx_min + 1
+    ranks = [sharding.GpuCompute(w) for _ in range(2)]
+    pieces = [sharding.pert_piece(c, nk, r, 2) for r, c in enumerate(ranks)]
+    full = sharding.place_pieces(pieces, nk, 2)
+    for c in ranks:
+        c.set_pt(full)
+    raws = [sharding.los_piece(c, n_ell, r, 2) for r, c in enumerate(ranks)]
+    cl = ranks[1].spline(sharding.place_raw(raws, n_ell, 2)).cpu().numpy()
+    np.testing.assert_array_equal(cl, ref)
