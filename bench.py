@@ -140,6 +140,44 @@ def cpu_sample(gw, stride: int, n_threads: int):
                       f"{max(t_runs) * n_full / len(sel):.2f}) los {t_los:.2f}"}
 
 
+def plain_gpu_fwd_fd(gw, w, dev, stream, want_dns=True):
+    """The metric's comparison path, on this library's kernels (the
+    reference's JAX GPU path is not installable here): one cosmology's C_l and
+    gradient with every finite-difference variant run on its own -- its own
+    perturbation launch over its k modes, its own line of sight, C_l copied
+    back -- one after another, as a caller without batching would."""
+    import torch
+    from abcmb_b200 import engine, packing
+    b = gw.batch
+    runs = []
+    for v in range(gw.n_var):
+        sub = packing.pack([b.bgs[v]], [b.layouts[v]], [w.kgrids[0]], n_save=b.n_save)
+        db = engine.DeviceBatch.upload(sub, dev)
+        lr = engine.LosRunner(db, w.kt, w.los_settings(), want_dns=want_dns)
+        runs.append((db, lr))
+    st = w.pert_settings()
+
+    def once():
+        for db, lr in runs:
+            db.pert_forward(st, stream)
+            lr.run(stream)
+            lr.cl.cpu()                      # the caller reads each variant's C_l
+
+    once()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    once()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    return {"value": 1000.0 / ms, "unit": UNIT, "ms_per_cosmology": ms,
+            "sample": f"first cosmology of the batch, its {gw.n_var} variants each run alone (own perturbation "
+                      f"launch over its {int(b.cosmo['nk'][0])} k modes + own line of sight + C_l read back), "
+                      f"this library's kernels"}
+
+
 def run_reference(args, rank, world):
     """Reference arm: the CPU restatement of the path on the host cores."""
     if rank != 0:
@@ -332,6 +370,9 @@ def main():
             "clocks": clk.summary(), "items_per_step": int(b.n_items),
             "ode_steps_mean": float(steps_k.mean()), "host_build_s": t_build}
     if rank == 0 and world == 1:
+        plain = plain_gpu_fwd_fd(gw, w, dev, stream)
+        plain["batched_over_plain"] = value / plain["value"]
+        line["plain_gpu_fwd_fd"] = plain
         line["cpu_baseline"] = cpu_sample(gw, args.cpu_sample_stride, os.cpu_count() or 1)
     if rank == 0:
         print(json.dumps(line), flush=True)

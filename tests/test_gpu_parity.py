@@ -301,3 +301,34 @@ def test_one_cosmology_in_two_shares_matches_one_call(gpu):
     raws = [sharding.los_piece(c, n_ell, r, 2) for r, c in enumerate(ranks)]
     cl = ranks[1].spline(sharding.place_raw(raws, n_ell, 2)).cpu().numpy()
     np.testing.assert_array_equal(cl, ref)
+
+
+def test_step_captures_in_a_cuda_graph(gpu, c1_small):
+    """The perturbation launch and the line of sight (descriptors passed from
+    the host, so no call synchronises) capture into one CUDA graph whose
+    replay reproduces the eager results bit for bit."""
+    import torch
+    from abcmb_b200 import engine
+    w = c1_small
+    st = w.pert_settings()
+    db = engine.DeviceBatch.upload(w.batch)
+    lr = engine.LosRunner(db, w.kt, w.los_settings(), want_dns=True)
+    db.pert_forward(st)
+    lr.run()
+    torch.cuda.synchronize()
+    pt_ref, cl_ref = db.pt.clone(), lr.cl.clone()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        db.pert_forward(st, s)                   # warm the stream once outside capture
+        lr.run(s)
+        with torch.cuda.graph(g, stream=s, capture_error_mode="relaxed"):
+            db.pert_forward(st, s)
+            lr.run(s)
+    torch.cuda.current_stream().wait_stream(s)
+    db.pt.zero_()
+    lr.cl.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(db.pt, pt_ref) and torch.equal(lr.cl, cl_ref)
