@@ -32,6 +32,8 @@ SIGNATURES = [
                                          _vp]),
     ("abcmb_pk_lin", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _d, ctypes.c_int, _vp, ctypes.c_int,
                                     _vp, _vp, _vp]),
+    ("abcmb_los_vjp_workspace_size", _i64, [ctypes.c_int, ctypes.c_int, _vp]),
+    ("abcmb_los_vjp", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp]),
     ("abcmb_cl_spline", ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        _vp, _vp]),
     ("abcmb_lens_workspace_size", _i64, [ctypes.c_int, _vp]),

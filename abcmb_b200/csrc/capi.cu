@@ -22,6 +22,11 @@ cudaError_t launch_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* k
                           double* pk, cudaStream_t stream);
 cudaError_t launch_cl_spline(int n_cosmo, const double* cl_raw, int idx_min, int n_ell_tab, int l_min, int l_max,
                              const BesselDev& B, double* cl, cudaStream_t stream);
+int64_t los_vjp_workspace_bytes(int n_cosmo, int max_nk, int nkt, int n_ell_tab, int n_save, int n_out);
+cudaError_t launch_los_vjp(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_cosmo* cosmo_host,
+                           const double* tables, const double* kbuf, const double* pt, const double* kt,
+                           const abcmb_los_settings& ls, int n_save, const BesselDev& B, const double* cl_bar,
+                           double* pt_bar, double* param_bar, void* ws, cudaStream_t stream);
 int64_t lens_workspace_bytes(int n_cosmo, const abcmb_lens_settings& s);
 cudaError_t launch_lens(int n_cosmo, const abcmb_cosmo* cosmo, const abcmb_lens_cosmo* lens, const double* tables,
                         const double* kbuf, const double* pt, const double* mu, const double* w,
@@ -190,6 +195,40 @@ int abcmb_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* k_dev,
   cudaError_t e = abcmb::launch_pk_lin(n_cosmo, cosmo_dev, k_dev, pt_dev, n_save, k_pivot, n_kout, kout_dev, n_z,
                                        z_dev, pk_dev, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "abcmb_pk_lin");
+  return ABCMB_OK;
+}
+
+int64_t abcmb_los_vjp_workspace_size(int n_cosmo, int max_nk, const abcmb_los_settings* settings) {
+  if (n_cosmo <= 0 || max_nk < 4 || !settings) return fail(ABCMB_ERR_ARG, "abcmb_los_vjp_workspace_size: bad argument");
+  const abcmb_los_settings& ls = *settings;
+  return abcmb::los_vjp_workspace_bytes(n_cosmo, max_nk, ls.nkt, ls.idx_max - ls.idx_min + 1, ls.n_save,
+                                        ls.l_max - ls.l_min + 1);
+}
+
+int abcmb_los_vjp(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_cosmo* cosmo_host, const double* tables_dev,
+                  const double* k_dev, const double* pt_dev, const double* kt_dev, const abcmb_los_settings* settings,
+                  const double* cl_bar_dev, double* pt_bar_dev, double* param_bar_dev, void* workspace_dev,
+                  int64_t workspace_bytes, void* stream) {
+  if (n_cosmo <= 0 || !cosmo_dev || !cosmo_host || !tables_dev || !k_dev || !pt_dev || !kt_dev || !settings ||
+      !cl_bar_dev || !pt_bar_dev || !param_bar_dev)
+    return fail(ABCMB_ERR_ARG, "abcmb_los_vjp: null argument");
+  const abcmb_los_settings& ls = *settings;
+  if (ls.l_min != 2 || ls.idx_max - ls.idx_min + 1 < 4 || ls.nkt < 2 || ls.n_save < 3 || ls.l_max < ls.l_min)
+    return fail(ABCMB_ERR_ARG, "abcmb_los_vjp: settings");
+  if (ls.precision != 0) return fail(ABCMB_ERR_ARG, "abcmb_los_vjp: the adjoint is FP64 (precision 0)");
+  BesselCache* bc = bessel_for_current_device();
+  if (!bc || !bc->ready) return fail(ABCMB_ERR_TABLES, "abcmb_los_vjp: Bessel tables not uploaded");
+  if (ls.idx_min < 0 || ls.idx_max >= bc->dev.n_l) return fail(ABCMB_ERR_ARG, "abcmb_los_vjp: l index range");
+  int max_nk = 0;
+  for (int c = 0; c < n_cosmo; ++c) max_nk = cosmo_host[c].nk > max_nk ? cosmo_host[c].nk : max_nk;
+  if (max_nk < 4) return fail(ABCMB_ERR_ARG, "abcmb_los_vjp: k grid");
+  const int64_t need = abcmb::los_vjp_workspace_bytes(n_cosmo, max_nk, ls.nkt, ls.idx_max - ls.idx_min + 1, ls.n_save,
+                                                      ls.l_max - ls.l_min + 1);
+  if (!workspace_dev || workspace_bytes < need) return fail(ABCMB_ERR_WORKSPACE, "abcmb_los_vjp: workspace");
+  cudaError_t e = abcmb::launch_los_vjp(n_cosmo, cosmo_dev, cosmo_host, tables_dev, k_dev, pt_dev, kt_dev, ls,
+                                        ls.n_save, bc->dev, cl_bar_dev, pt_bar_dev, param_bar_dev, workspace_dev,
+                                        static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "abcmb_los_vjp");
   return ABCMB_OK;
 }
 

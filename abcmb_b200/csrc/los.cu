@@ -121,6 +121,7 @@ struct LosScratch {
   void* S;           // [C][4][nl][nkt] sources (double or float)
   double* partial;   // [C][n_ell_tab][ntile][6]
   double* lscr;      // [C][16 n_ell_tab] l-spline scratch
+  double* te;        // null, or [C][n_ell_tab][2][nkt]: T and E of every (l, k) (the adjoint reads them)
   int max_nk;
 };
 
@@ -364,6 +365,11 @@ __global__ void __launch_bounds__(LOS_THREADS, 1) los_kernel(const abcmb_cosmo* 
     }
     const double T = a0 + a1 + a2;
     const double E = aE;
+    if (W.te) {
+      double* te = W.te + (((int64_t)cz * n_ell + ie) * 2) * nkt;
+      te[j] = T;
+      te[nkt + j] = E;
+    }
     const double pr = 4. * PI * c.A_s * pow(k / k_pivot, c.n_s - 1.) / k;
     // trapezoid weight of node j
     double wj;
@@ -531,6 +537,297 @@ __global__ void pk_lin_kernel(const abcmb_cosmo* __restrict__ cosmo, const doubl
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// adjoint (vector-Jacobian product) of the line of sight
+// ---------------------------------------------------------------------------
+// d piece / d(y0, y1, s0, s1) of spline_piece at offset u in an interval dx
+struct PieceGrad {
+  double y0, y1, s0, s1;
+};
+__device__ __forceinline__ PieceGrad piece_grad(double dx, double u) {
+  const double idx = 1.0 / dx;
+  const double u2 = u * u, u3 = u2 * u;
+  const double dsl = -2. * u3 * idx * idx + 3. * u2 * idx;   // d piece / d slope (y1 - y0) / dx
+  PieceGrad g;
+  g.y1 = dsl * idx;
+  g.y0 = 1. - g.y1;
+  g.s0 = u3 * idx * idx - 2. * u2 * idx + u;
+  g.s1 = u3 * idx * idx - u2 * idx;
+  return g;
+}
+
+// ybar += R^T z, R the not-a-knot right-hand side operator of nak_rhs
+__device__ void nak_rhs_adjoint(const double* x, int n, const double* z, double* ybar, int64_t ystride) {
+  for (int i = 0; i < n; ++i) {
+    const double zi = z[i];
+    if (i == 0) {
+      const double dx0 = x[1] - x[0], dx1 = x[2] - x[1], d = x[2] - x[0];
+      const double c0 = zi * (dx0 + 2. * d) * dx1 / d / dx0;   // via s0 = (y1 - y0) / dx0
+      const double c1 = zi * dx0 * dx0 / d / dx1;              // via s1 = (y2 - y1) / dx1
+      ybar[0] -= c0;
+      ybar[ystride] += c0 - c1;
+      ybar[2 * ystride] += c1;
+    } else if (i == n - 1) {
+      const double dxa = x[n - 2] - x[n - 3], dxb = x[n - 1] - x[n - 2], d = x[n - 1] - x[n - 3];
+      const double ca = zi * dxb * dxb / d / dxa;
+      const double cb = zi * (2. * d + dxb) * dxa / d / dxb;
+      ybar[(int64_t)(n - 3) * ystride] -= ca;
+      ybar[(int64_t)(n - 2) * ystride] += ca - cb;
+      ybar[(int64_t)(n - 1) * ystride] += cb;
+    } else {
+      const double dxm = x[i] - x[i - 1], dxp = x[i + 1] - x[i];
+      const double cm = zi * 3. * dxp / dxm, cp = zi * 3. * dxm / dxp;
+      ybar[(int64_t)(i - 1) * ystride] -= cm;
+      ybar[(int64_t)i * ystride] += cm - cp;
+      ybar[(int64_t)(i + 1) * ystride] += cp;
+    }
+  }
+}
+
+// z = T^{-T} sbar in place, T = L U the factorisation of nak_factor
+// (L unit lower with sub-diagonal mlo, U upper with diagonal 1/dinv and
+// super-diagonal up): U^T w = sbar forward, then L^T z = w backward.
+__device__ void nak_solve_transposed(int n, const double* dinv, const double* mlo, const double* up, double* v,
+                                     int64_t vstride) {
+  double wprev = 0.;
+  for (int i = 0; i < n; ++i) {
+    const double w = (v[(int64_t)i * vstride] - (i > 0 ? up[i - 1] * wprev : 0.)) * dinv[i];
+    v[(int64_t)i * vstride] = w;
+    wprev = w;
+  }
+  double znext = v[(int64_t)(n - 1) * vstride];
+  for (int i = n - 2; i >= 0; --i) {
+    znext = v[(int64_t)i * vstride] - mlo[i + 1] * znext;
+    v[(int64_t)i * vstride] = znext;
+  }
+}
+
+// C_l cotangent at the integer ells -> at the tabulated l (transposed l
+// spline), and the A_s / n_s cotangents.  One block, three threads.
+__global__ void cl_spline_adjoint_kernel(int ci, int n_ell_tab, int ntile, BesselDev B, int idx_min, int l_min,
+                                         int n_out, const double* __restrict__ cl_bar, const double* __restrict__ cl_raw,
+                                         const abcmb_cosmo* __restrict__ cosmo, LosScratch W,
+                                         double* __restrict__ rbar, double* __restrict__ param_bar) {
+  const int n = n_ell_tab;
+  double* x = W.lscr;
+  double* dinv = x + n;
+  double* mlo = dinv + n;
+  double* up = mlo + n;
+  double* sb = up + n;                      // 3 n
+  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = (double)B.l_tab[idx_min + i];
+  __syncthreads();
+  if (threadIdx.x == 0) nak_factor(x, n, dinv, mlo, up);
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int X = threadIdx.x;
+    double* yb = rbar + X;                  // rbar [n][3]
+    double* s = sb + X * n;
+    for (int i = 0; i < n; ++i) {
+      yb[(int64_t)i * 3] = 0.;
+      s[i] = 0.;
+    }
+    const double* cb = cl_bar + (int64_t)ci * 3 * n_out + (int64_t)X * n_out;
+    for (int o = 0; o < n_out; ++o) {
+      const double xq = (double)(l_min + o);
+      const int iv = spline_interval(x, n, xq);
+      const PieceGrad g = piece_grad(x[iv + 1] - x[iv], xq - x[iv]);
+      const double c = cb[o];
+      yb[(int64_t)iv * 3] += c * g.y0;
+      yb[(int64_t)(iv + 1) * 3] += c * g.y1;
+      s[iv] += c * g.s0;
+      s[iv + 1] += c * g.s1;
+    }
+    nak_solve_transposed(n, dinv, mlo, up, s, 1);
+    nak_rhs_adjoint(x, n, s, yb, 3);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // C_raw is linear in A_s; dC_raw/dn_s is the ln(k/k_pivot)-weighted quadrature (series 3..5)
+    const double* raw = cl_raw + (int64_t)ci * n * 3;
+    double as = 0., ns = 0.;
+    for (int ie = 0; ie < n; ++ie) {
+      for (int X = 0; X < 3; ++X) {
+        double d = 0.;
+        for (int t = 0; t < ntile; ++t) d += W.partial[((int64_t)ie * ntile + t) * 6 + 3 + X];
+        as += rbar[ie * 3 + X] * raw[ie * 3 + X];
+        ns += rbar[ie * 3 + X] * d;
+      }
+    }
+    param_bar[2 * ci] = as / cosmo[ci].A_s;
+    param_bar[2 * ci + 1] = ns;
+  }
+}
+
+// T, E (stored by los_kernel) -> their cotangents in place:
+// Tbar = w_k pr_k (2 Cbar_TT T + Cbar_TE E), Ebar = w_k pr_k (Cbar_TE T + 2 Cbar_EE E)
+__global__ void te_adjoint_kernel(const abcmb_cosmo* __restrict__ cosmo, int ci, int n_ell, const double* __restrict__ kt,
+                                  int nkt, double k_pivot, const double* __restrict__ rbar, double* __restrict__ te) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ie = blockIdx.y;
+  if (j >= nkt) return;
+  const abcmb_cosmo& c = cosmo[ci];
+  const double k = kt[j];
+  const double pr = 4. * PI * c.A_s * pow(k / k_pivot, c.n_s - 1.) / k;
+  double wj;
+  if (nkt == 1) wj = 0.;
+  else if (j == 0) wj = 0.5 * (kt[1] - kt[0]);
+  else if (j == nkt - 1) wj = 0.5 * (kt[nkt - 1] - kt[nkt - 2]);
+  else wj = 0.5 * (kt[j + 1] - kt[j - 1]);
+  const double f = wj * pr;
+  double* t = te + ((int64_t)ie * 2) * nkt;
+  const double T = t[j], E = t[nkt + j];
+  const double btt = rbar[ie * 3], bte = rbar[ie * 3 + 1], bee = rbar[ie * 3 + 2];
+  t[j] = f * (2. * btt * T + bte * E);
+  t[nkt + j] = f * (bte * T + 2. * bee * E);
+}
+
+// Source cotangents: Sbar_X(i, k) = sum_l Xbar(l, k) w_i / aH_i phi_X(l, k chi_i)
+// (the line-of-sight sum taken over l instead of lna).  Thread per transfer
+// k, ADJ_TAU lna points per block; the Bessel columns are read through L1.
+constexpr int ADJ_TAU = 8;
+__global__ void __launch_bounds__(128) los_adjoint_kernel(const abcmb_cosmo* __restrict__ cosmo, int ci,
+                                                          const double* __restrict__ tables, int nl, int n_save,
+                                                          const double* __restrict__ kt, int nkt, BesselDev B,
+                                                          int idx_min, int n_ell, const double* __restrict__ te,
+                                                          double* __restrict__ sbar) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i0 = blockIdx.y * ADJ_TAU;
+  if (j >= nkt) return;
+  const abcmb_cosmo& c = cosmo[ci];
+  const double* los = tables + c.off_los;
+  const double lts = c.lna_transfer_start;
+  const double delta_lna = linspace_at(lts, 0., n_save, n_save - 1) - linspace_at(lts, 0., n_save, n_save - 2);
+  double dt[ADJ_TAU], idt[ADJ_TAU], wa[ADJ_TAU];
+#pragma unroll
+  for (int u = 0; u < ADJ_TAU; ++u) {
+    const int i = min(i0 + u, nl - 1);
+    dt[u] = c.tau0 - los[i];
+    idt[u] = 1.0 / dt[u];
+    wa[u] = (i0 + u < nl) ? ((i == 0) ? 0.5 * delta_lna : delta_lna) * (1.0 / los[3 * nl + i]) : 0.;
+  }
+  const double k = kt[j], invk = 1.0 / k;
+  const int nx = B.n_x;
+  double a0[ADJ_TAU], a1[ADJ_TAU], a2[ADJ_TAU], aE[ADJ_TAU];
+#pragma unroll
+  for (int u = 0; u < ADJ_TAU; ++u) a0[u] = a1[u] = a2[u] = aE[u] = 0.;
+  for (int ie = 0; ie < n_ell; ++ie) {
+    const int idx = idx_min + ie;
+    const double Tb = te[((int64_t)ie * 2) * nkt + j], Eb = te[((int64_t)ie * 2 + 1) * nkt + j];
+    const double l = (double)B.l_tab[idx];
+    const double x0min = B.xmin[idx], x0max = B.xmax[idx];
+    const double x1min = B.xmin[B.n_l + idx], x1max = B.xmax[B.n_l + idx];
+    const double x2min = B.xmin[2 * B.n_l + idx], x2max = B.xmax[2 * B.n_l + idx];
+    const double s0 = (double)(nx - 1) / (x0max - x0min);
+    const double s1 = (double)(nx - 1) / (x1max - x1min);
+    const double s2 = (double)(nx - 1) / (x2max - x2min);
+    const double* ph0 = B.phi + ((int64_t)0 * B.n_l + idx) * nx;
+    const double* ph1 = B.phi + ((int64_t)1 * B.n_l + idx) * nx;
+    const double* ph2 = B.phi + ((int64_t)2 * B.n_l + idx) * nx;
+    const double ef = sqrt(3. / 8. * (l + 2) * (l + 1) * l * (l - 1));
+    const double nu0 = l + 0.5, nu1 = l + 1.5, nu0sq = nu0 * nu0, nu1sq = nu1 * nu1;
+    const double c2 = 3 * l * (l - 1);
+#pragma unroll
+    for (int u = 0; u < ADJ_TAU; ++u) {
+      const double chi = dt[u] * k;
+      const double ichi = idt[u] * invk;
+      double p0;
+      if (chi < x0min) p0 = 0.;
+      else if (chi >= x0max) p0 = jasym(nu0, nu0sq, chi, ichi);
+      else p0 = lerp_tab(chi, x0min, s0, ph0, nx);
+      const bool as1 = chi >= x1max, as2 = chi >= x2max;
+      double jl = 0., jl1 = 0.;
+      if (as1 || as2) {
+        jl = (chi >= x0max) ? p0 : jasym(nu0, nu0sq, chi, ichi);
+        jl1 = jasym(nu1, nu1sq, chi, ichi);
+      }
+      double p1, p2;
+      if (chi < x1min) p1 = 0.;
+      else if (as1) p1 = l * ichi * jl - jl1;
+      else p1 = lerp_tab(chi, x1min, s1, ph1, nx);
+      const double ichi2 = ichi * ichi;
+      if (chi < x2min) p2 = 0.;
+      else if (as2) p2 = ((c2 - 2 * chi * chi) * jl + 6 * chi * jl1) * 0.5 * ichi2;
+      else p2 = lerp_tab(chi, x2min, s2, ph2, nx);
+      const double eps = p0 * ichi2 * ef;
+      const double tw = Tb * wa[u], ew = Eb * wa[u];
+      a0[u] = fma(tw, p0, a0[u]);
+      a1[u] = fma(tw, p1, a1[u]);
+      a2[u] = fma(tw, p2, a2[u]);
+      aE[u] = fma(ew, eps, aE[u]);
+    }
+  }
+  const int64_t plane = (int64_t)nl * nkt;
+#pragma unroll
+  for (int u = 0; u < ADJ_TAU; ++u) {
+    if (i0 + u < nl) {
+      const int64_t o = (int64_t)(i0 + u) * nkt + j;
+      sbar[o] = a0[u];
+      sbar[plane + o] = a1[u];
+      sbar[2 * plane + o] = a2[u];
+      sbar[3 * plane + o] = aE[u];
+    }
+  }
+}
+
+// PT cotangent of one (source field, lna row) column: the transposed source
+// combination (sources_kernel) and the transposed k spline (spline_slopes /
+// spline_piece), accumulated in a fixed order.
+__global__ void spline_adjoint_kernel(const abcmb_cosmo* __restrict__ cosmo, int ci, const double* __restrict__ tables,
+                                      int n_save, int nl, const double* __restrict__ kt, int nkt,
+                                      abcmb_los_settings ls, LosScratch W, const double* __restrict__ sbar,
+                                      double* __restrict__ pt_bar) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;    // f * nl + il
+  if (col >= NSRC_FIELDS * nl) return;
+  const abcmb_cosmo& c = cosmo[ci];
+  const int nk = c.nk;
+  const int f = col / nl, il = col % nl;
+  const double* los = tables + c.off_los;
+  const double g = los[1 * nl + il], gp = los[2 * nl + il], aH = los[3 * nl + il];
+  const double em = los[4 * nl + il], aHd = los[5 * nl + il];
+  const double* xk = W.xk;
+  double* yb = pt_bar + c.off_pt + ((int64_t)SRC_FIELDS[f] * n_save + il) * nk;
+  double* s = W.slopes + (int64_t)col * W.max_nk;
+  for (int m = 0; m < nk; ++m) {
+    yb[m] = 0.;
+    s[m] = 0.;
+  }
+  const int64_t plane = (int64_t)nl * nkt;
+  for (int j = 0; j < nkt; ++j) {
+    const double k = kt[j];
+    const int64_t o = (int64_t)il * nkt + j;
+    const double b0 = sbar[o], b1 = sbar[plane + o], b2 = sbar[2 * plane + o], bE = sbar[3 * plane + o];
+    // d(sT0, sT1, sT2, sE) / d field f (sources_kernel)
+    double fb;
+    switch (f) {
+      case 0: fb = b0 * (ls.scale_sw * g / 4.); break;                                          // delta_g
+      case 1: fb = b0 * (ls.scale_dop * aH * gp / (k * k)); break;                              // theta_b
+      case 2: fb = b0 * (ls.scale_dop * aH * g / (k * k)); break;                               // theta_b'
+      case 3: fb = b2 * (ls.scale_pol * g * 2. / 8.) + bE * (sqrt(6.) * g * 2. / 8.); break;    // sigma_g
+      case 4:
+      case 5: fb = b2 * (ls.scale_pol * g / 8.) + bE * (sqrt(6.) * g / 8.); break;              // G0, G2
+      case 6: fb = b0 * (ls.scale_isw * g) - b1 * (ls.scale_isw * em * k); break;               // eta
+      case 7: fb = b0 * (ls.scale_isw * 2. * em * aH); break;                                   // eta'
+      case 8:                                                                                   // alpha
+        fb = b0 * (-ls.scale_isw * 2. * g * aH - ls.scale_isw * 2. * em * aHd + ls.scale_dop * aH * gp) +
+             b1 * (ls.scale_isw * em * 2. * aH * k);
+        break;
+      default:                                                                                  // alpha'
+        fb = b0 * (ls.scale_sw * g * aH - ls.scale_isw * g * aH - ls.scale_isw * 2. * em * aH * aH +
+                   ls.scale_dop * aH * g) +
+             b1 * (ls.scale_isw * em * aH * k);
+        break;
+    }
+    const int m = W.kidx[j];
+    const PieceGrad pg = piece_grad(xk[m + 1] - xk[m], log10(k) - xk[m]);
+    yb[m] += fb * pg.y0;
+    yb[m + 1] += fb * pg.y1;
+    s[m] += fb * pg.s0;
+    s[m + 1] += fb * pg.s1;
+  }
+  nak_solve_transposed(nk, W.dinv, W.mlo, W.up, s, 1);
+  nak_rhs_adjoint(xk, nk, s, yb, 1);
+}
+
 static int64_t al256(int64_t b) { return (b + 255) / 256 * 256; }
 
 struct LosLayout {
@@ -587,6 +884,7 @@ cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_co
   W.S = w + L.o_S;
   W.partial = reinterpret_cast<double*>(w + L.o_partial);
   W.lscr = reinterpret_cast<double*>(w + L.o_lscr);
+  W.te = nullptr;
   W.max_nk = max_nk;
   const size_t smem = (size_t)(3 * B.n_x + 3 * nl + (LOS_TY - 1) * 4 * LOS_TX) * sizeof(double);
   cudaError_t e;
@@ -613,6 +911,90 @@ cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_co
       los_kernel<1><<<gl, bl, smem, stream>>>(cosmo_dev, c0, tables, nl, n_save, kt, nkt, B, ls.idx_min, ls.k_pivot, W);
     cl_final_kernel<<<nc, 256, 0, stream>>>(c0, n_ell_tab, L.ntile, B, ls.idx_min, ls.l_min, n_out, W, cl_raw, cl,
                                             dcl_dns);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+struct LosVjpLayout {
+  LosLayout f;
+  int n_out;
+  int64_t o_te, o_raw, o_cl, o_rbar, total;
+};
+
+static LosVjpLayout los_vjp_layout(int n_cosmo, int max_nk, int nkt, int n_ell_tab, int n_save, int n_out) {
+  LosVjpLayout L{};
+  L.f = los_layout(1, max_nk, nkt, n_ell_tab, n_save, 0);
+  L.n_out = n_out;
+  int64_t b = L.f.total;
+  L.o_te = b;   b += al256((int64_t)n_ell_tab * 2 * nkt * 8);
+  L.o_raw = b;  b += al256((int64_t)n_cosmo * n_ell_tab * 3 * 8);
+  L.o_cl = b;   b += al256((int64_t)n_cosmo * 3 * n_out * 8);
+  L.o_rbar = b; b += al256((int64_t)n_ell_tab * 3 * 8);
+  L.total = b;
+  return L;
+}
+
+int64_t los_vjp_workspace_bytes(int n_cosmo, int max_nk, int nkt, int n_ell_tab, int n_save, int n_out) {
+  return los_vjp_layout(n_cosmo, max_nk, nkt, n_ell_tab, n_save, n_out).total;
+}
+
+// Vector-Jacobian product of launch_los (FP64), one cosmology after another:
+// the forward pieces again (storing T and E), then the adjoint kernels.
+cudaError_t launch_los_vjp(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_cosmo* cosmo_host,
+                           const double* tables, const double* kbuf, const double* pt, const double* kt,
+                           const abcmb_los_settings& ls, int n_save, const BesselDev& B, const double* cl_bar,
+                           double* pt_bar, double* param_bar, void* ws, cudaStream_t stream) {
+  const int nkt = ls.nkt;
+  const int n_ell_tab = ls.idx_max - ls.idx_min + 1;
+  const int n_out = ls.l_max - ls.l_min + 1;
+  int max_nk = 0;
+  for (int c = 0; c < n_cosmo; ++c) max_nk = cosmo_host[c].nk > max_nk ? cosmo_host[c].nk : max_nk;
+  const LosVjpLayout L = los_vjp_layout(n_cosmo, max_nk, nkt, n_ell_tab, n_save, n_out);
+  const int nl = L.f.nl;
+  char* w = static_cast<char*>(ws);
+  LosScratch W;
+  W.xk = reinterpret_cast<double*>(w + L.f.o_xk);
+  W.dinv = reinterpret_cast<double*>(w + L.f.o_dinv);
+  W.mlo = reinterpret_cast<double*>(w + L.f.o_mlo);
+  W.up = reinterpret_cast<double*>(w + L.f.o_up);
+  W.kidx = reinterpret_cast<int*>(w + L.f.o_kidx);
+  W.slopes = reinterpret_cast<double*>(w + L.f.o_slopes);
+  W.S = w + L.f.o_S;
+  W.partial = reinterpret_cast<double*>(w + L.f.o_partial);
+  W.lscr = reinterpret_cast<double*>(w + L.f.o_lscr);
+  W.te = reinterpret_cast<double*>(w + L.o_te);
+  W.max_nk = max_nk;
+  double* raw = reinterpret_cast<double*>(w + L.o_raw);
+  double* clf = reinterpret_cast<double*>(w + L.o_cl);
+  double* rbar = reinterpret_cast<double*>(w + L.o_rbar);
+  const size_t smem = (size_t)(3 * B.n_x + 3 * nl + (LOS_TY - 1) * 4 * LOS_TX) * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(los_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  for (int ci = 0; ci < n_cosmo; ++ci) {
+    const abcmb_cosmo& ch = cosmo_host[ci];
+    e = cudaMemsetAsync(pt_bar + ch.off_pt, 0, (size_t)ABCMB_NFIELDS * n_save * ch.nk * sizeof(double), stream);
+    if (e != cudaSuccess) return e;
+    // forward, one cosmology (chunk of one: scratch index 0)
+    spline_prep_kernel<<<1, 256, 0, stream>>>(cosmo_dev, ci, kbuf, kt, nkt, W);
+    spline_slopes_kernel<<<dim3((NSRC_FIELDS * nl + 127) / 128, 1), 128, 0, stream>>>(cosmo_dev, ci, pt, n_save, nl, W);
+    sources_kernel<double><<<dim3((nkt + 127) / 128, nl, 1), 128, 0, stream>>>(cosmo_dev, ci, tables, pt, n_save, nl,
+                                                                              kt, nkt, ls, W);
+    los_kernel<0><<<dim3(n_ell_tab, L.f.ntile, 1), dim3(LOS_TX, LOS_TY), smem, stream>>>(
+        cosmo_dev, ci, tables, nl, n_save, kt, nkt, B, ls.idx_min, ls.k_pivot, W);
+    cl_final_kernel<<<1, 256, 0, stream>>>(ci, n_ell_tab, L.f.ntile, B, ls.idx_min, ls.l_min, n_out, W, raw, clf,
+                                           nullptr);
+    // adjoint
+    cl_spline_adjoint_kernel<<<1, 32, 0, stream>>>(ci, n_ell_tab, L.f.ntile, B, ls.idx_min, ls.l_min, n_out, cl_bar,
+                                                   raw, cosmo_dev, W, rbar, param_bar);
+    te_adjoint_kernel<<<dim3((nkt + 127) / 128, n_ell_tab), 128, 0, stream>>>(cosmo_dev, ci, n_ell_tab, kt, nkt,
+                                                                               ls.k_pivot, rbar, W.te);
+    double* sbar = static_cast<double*>(W.S);
+    los_adjoint_kernel<<<dim3((nkt + 127) / 128, (nl + ADJ_TAU - 1) / ADJ_TAU), 128, 0, stream>>>(
+        cosmo_dev, ci, tables, nl, n_save, kt, nkt, B, ls.idx_min, n_ell_tab, W.te, sbar);
+    spline_adjoint_kernel<<<(NSRC_FIELDS * nl + 127) / 128, 128, 0, stream>>>(cosmo_dev, ci, tables, n_save, nl, kt,
+                                                                               nkt, ls, W, sbar, pt_bar);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

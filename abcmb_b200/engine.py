@@ -143,6 +143,27 @@ class LosRunner:
                                    _ptr(self.ws), self.ws.numel(), ctypes.c_void_p(st.cuda_stream))
         _lib.check(rc, "abcmb_los_forward")
 
+    def vjp(self, cl_bar: torch.Tensor, stream=None):
+        """Cotangents (pt_bar, param_bar[n_cosmo, 2] = dL/dA_s, dL/dn_s) of
+        L = <cl_bar, C_l> through the line of sight (abcmb_los_vjp, FP64)."""
+        lib = _lib.load()
+        db = self.db
+        n = db.batch.n_cosmo
+        if cl_bar.numel() != n * 3 * self.n_out or cl_bar.dtype != torch.float64 or cl_bar.device != self.cl.device:
+            raise ValueError("cl_bar must be a float64 tensor on the batch's device shaped like C_l")
+        cl_bar = cl_bar.contiguous()
+        max_nk = int(db.batch.cosmo["nk"].max())
+        nws = int(lib.abcmb_los_vjp_workspace_size(n, max_nk, ctypes.byref(self.ls)))
+        ws = torch.empty(max(nws, 1), dtype=torch.uint8, device=db.device)
+        pt_bar = torch.zeros_like(db.pt)
+        param_bar = torch.zeros(n * 2, dtype=torch.float64, device=db.device)
+        st = stream if stream is not None else torch.cuda.current_stream(db.device)
+        rc = lib.abcmb_los_vjp(n, _ptr(db.cosmo), ctypes.c_void_p(self.cosmo_host.ctypes.data), _ptr(db.tables),
+                               _ptr(db.kbuf), _ptr(db.pt), _ptr(self.kt), ctypes.byref(self.ls), _ptr(cl_bar),
+                               _ptr(pt_bar), _ptr(param_bar), _ptr(ws), ws.numel(), ctypes.c_void_p(st.cuda_stream))
+        _lib.check(rc, "abcmb_los_vjp")
+        return pt_bar, param_bar.view(n, 2)
+
     def cl_host(self) -> np.ndarray:
         return self.cl.cpu().numpy().reshape(self.db.batch.n_cosmo, 3, self.n_out)
 

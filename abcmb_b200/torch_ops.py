@@ -5,6 +5,9 @@
   ``abcmb_los_forward``; they write into caller-provided CUDA tensors on the
   current stream (device memory and stream are torch's; every kernel is the
   library's).
+* ``torch.ops.abcmb_b200.los_vjp`` over ``abcmb_los_vjp``, and ``ClFromPT``:
+  a ``torch.autograd.Function`` PerturbationTable -> C_l whose backward is
+  the hand-written line-of-sight adjoint.
 * ``ClWithGrad``: a ``torch.autograd.Function`` mapping parameters
   theta = (h, omega_b, omega_cdm, A_s, n_s, tau_reion) of a batch of
   cosmologies to C_l^{TT,TE,EE}; its backward contracts the incoming
@@ -57,8 +60,44 @@ def los_forward(cosmo: Tensor, cosmo_host: Tensor, tables: Tensor, kbuf: Tensor,
     _lib.check(rc, "abcmb_los_forward")
 
 
+@torch.library.custom_op("abcmb_b200::los_vjp", mutates_args=("pt_bar", "param_bar", "workspace"))
+def los_vjp(cosmo: Tensor, cosmo_host: Tensor, tables: Tensor, kbuf: Tensor, pt: Tensor, kt: Tensor,
+            settings: Tensor, cl_bar: Tensor, pt_bar: Tensor, param_bar: Tensor, workspace: Tensor) -> None:
+    """abcmb_los_vjp: cotangent of the PerturbationTable (and of A_s, n_s) for a C_l cotangent."""
+    ls = packing.CLosSettings.from_buffer_copy(settings.numpy().tobytes())
+    n_cosmo = cosmo.numel() // packing.COSMO_DTYPE.itemsize
+    hc = cosmo_host.contiguous()
+    rc = _lib.load().abcmb_los_vjp(n_cosmo, _p(cosmo), ctypes.c_void_p(hc.data_ptr()), _p(tables), _p(kbuf), _p(pt),
+                                   _p(kt), ctypes.byref(ls), _p(cl_bar.contiguous()), _p(pt_bar), _p(param_bar),
+                                   _p(workspace), workspace.numel(), _stream())
+    _lib.check(rc, "abcmb_los_vjp")
+
+
 def settings_bytes(s) -> Tensor:
     return torch.frombuffer(bytearray(bytes(s)), dtype=torch.uint8)
+
+
+class ClFromPT(torch.autograd.Function):
+    """PerturbationTable -> C_l (abcmb_los_forward) with the hand-written
+    adjoint (abcmb_los_vjp) as its backward: ``ClFromPT.apply(pt, runner)``
+    with ``runner`` an engine.LosRunner over the batch whose table ``pt``
+    replaces.  Returns C_l [n_cosmo, 3, n_l]; the gradient flows to ``pt``."""
+
+    @staticmethod
+    def forward(ctx, pt: Tensor, runner) -> Tensor:
+        runner.db.pt.copy_(pt)
+        runner.run()
+        ctx.runner = runner
+        ctx.save_for_backward(pt)
+        return runner.cl.view(runner.db.batch.n_cosmo, 3, runner.n_out).clone()
+
+    @staticmethod
+    def backward(ctx, grad_cl: Tensor):
+        (pt,) = ctx.saved_tensors
+        r = ctx.runner
+        r.db.pt.copy_(pt)
+        pt_bar, _ = r.vjp(grad_cl.contiguous().view(-1))
+        return pt_bar, None
 
 
 class ClWithGrad(torch.autograd.Function):

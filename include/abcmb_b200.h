@@ -272,6 +272,26 @@ int abcmb_los_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev,
                       void* stream);
 
 /*
+ * Vector-Jacobian product of abcmb_los_forward (FP64): given cl_bar, the
+ * cotangent of cl (same layout), writes
+ *   pt_bar_dev     cotangent of the PerturbationTable (layout of pt; the ten
+ *                  fields the line of sight reads get their cotangent on the
+ *                  lna rows it uses, everything else 0)
+ *   param_bar_dev  [n_cosmo x 2] cotangents of A_s and n_s.
+ * The background arrays and the transfer k grid are held fixed.  The
+ * hand-written adjoint of Cl_one_ell / get_Cl (spectrum.py:574-797): the
+ * transposed l spline, the k-quadrature and line-of-sight sums taken in
+ * reverse (over l instead of lna), the transposed source combination and
+ * the transposed not-a-knot k spline.  cosmo_host is required.
+ */
+int64_t abcmb_los_vjp_workspace_size(int n_cosmo, int max_nk, const abcmb_los_settings* settings);
+int abcmb_los_vjp(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_cosmo* cosmo_host,
+                  const double* tables_dev, const double* k_dev, const double* pt_dev,
+                  const double* kt_dev, const abcmb_los_settings* settings,
+                  const double* cl_bar_dev, double* pt_bar_dev, double* param_bar_dev,
+                  void* workspace_dev, int64_t workspace_bytes, void* stream);
+
+/*
  * The last stage of abcmb_los_forward on its own: the cubic spline in l of
  * C_l given at the tabulated l (spectrum.py:597-608) onto the integer ells
  * l_min..l_max (l_min == 2), for callers that assemble cl_raw themselves --

@@ -332,3 +332,77 @@ def test_step_captures_in_a_cuda_graph(gpu, c1_small):
     g.replay()
     torch.cuda.synchronize()
     assert torch.equal(db.pt, pt_ref) and torch.equal(lr.cl, cl_ref)
+
+
+def test_los_vjp_matches_directional_differences(gpu):
+    """abcmb_los_vjp against central differences of <cl_bar, C_l>.  C_l is
+    exactly quadratic in the PerturbationTable (splines, sources and the line
+    of sight are linear, the k quadrature is quadratic), so the central
+    difference along any direction equals the directional derivative up to
+    rounding; A_s enters linearly, n_s through (k/k_pivot)^(n_s-1)."""
+    import torch
+    from abcmb_b200 import configs, engine
+    w = configs.c4(n_cosmo=2, l_max=400, nk_range=(40, 60)).build()
+    db = engine.DeviceBatch.upload(w.batch)
+    db.pert_forward(w.pert_settings())
+    db.check_status()
+    lr = engine.LosRunner(db, w.kt, w.los_settings())
+    lr.run()
+    cl0 = lr.cl.clone()
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    cl_bar = torch.randn(cl0.shape, generator=gen, device="cuda", dtype=torch.float64) / cl0.abs().clamp_min(1e-30)
+    pt_bar, param_bar = lr.vjp(cl_bar)
+
+    def L():
+        lr.run()
+        return float((cl_bar * lr.cl).sum())
+
+    pt0 = db.pt.clone()
+    # entry-relative perturbation: the linear term dominates, so lp - lm keeps its digits
+    delta = torch.randn(pt0.shape, generator=gen, device="cuda", dtype=torch.float64) * 1e-4 * pt0.abs()
+    db.pt.copy_(pt0 + delta)
+    lp = L()
+    db.pt.copy_(pt0 - delta)
+    lm = L()
+    db.pt.copy_(pt0)
+    fd = (lp - lm) / 2.0
+    ad = float((pt_bar * delta).sum())
+    assert abs(fd - ad) <= 1e-8 * max(abs(fd), abs(ad)), (fd, ad)
+    # pt_bar is zero on every field the line of sight does not read
+    from abcmb_b200.packing import F
+    c0 = w.batch.cosmo[0]
+    v = pt_bar[int(c0["off_pt"]):int(c0["off_pt"]) + 21 * 500 * int(c0["nk"])].view(21, 500, -1)
+    for name in ("delta_m", "metric_h_prime", "cdm_delta", "b_delta", "nu_delta", "ncdm_delta"):
+        assert float(v[F[name]].abs().max()) == 0.0, name
+    # A_s (linear) and n_s (central difference)
+    cos0 = w.batch.cosmo.copy()
+    for p, (name, rel) in enumerate((("A_s", 1e-3), ("n_s", 1e-5))):
+        vals = []
+        for sgn in (+1, -1):
+            cos = cos0.copy()
+            cos[name] = cos0[name] * (1 + sgn * rel)
+            db.cosmo.copy_(torch.from_numpy(cos.view(np.uint8)))
+            lr.cosmo_host = np.ascontiguousarray(cos)
+            vals.append(L())
+        db.cosmo.copy_(torch.from_numpy(cos0.view(np.uint8)))
+        lr.cosmo_host = np.ascontiguousarray(cos0)
+        # both cosmologies move together: compare with the sum of their cotangents times the steps
+        fdp = (vals[0] - vals[1]) / 2.0
+        adp = float(sum(param_bar[ci, p].item() * cos0[name][ci] * rel for ci in range(2)))
+        assert abs(fdp - adp) <= 1e-6 * max(abs(fdp), abs(adp)), (name, fdp, adp)
+
+
+def test_cl_from_pt_autograd_uses_the_adjoint(gpu, c1_small):
+    """torch autograd through ClFromPT returns abcmb_los_vjp's cotangent."""
+    import torch
+    from abcmb_b200 import engine, torch_ops
+    w = c1_small
+    db = engine.DeviceBatch.upload(w.batch)
+    db.pert_forward(w.pert_settings())
+    lr = engine.LosRunner(db, w.kt, w.los_settings())
+    pt = db.pt.clone().requires_grad_(True)
+    cl = torch_ops.ClFromPT.apply(pt, lr)
+    weights = 1.0 / cl.detach().abs().clamp_min(1e-30)
+    (cl * weights).sum().backward()
+    ref, _ = lr.vjp(weights.reshape(-1))
+    assert torch.equal(pt.grad, ref)

@@ -92,6 +92,7 @@ def test_torch_ops_registered_and_settings_roundtrip():
     import torch
     from abcmb_b200 import torch_ops, packing
     assert hasattr(torch.ops.abcmb_b200, "pert_forward") and hasattr(torch.ops.abcmb_b200, "los_forward")
+    assert hasattr(torch.ops.abcmb_b200, "los_vjp")
     st = packing.CPertSettings(max_ny=77, rtol_large=1e-4, n_save=500)
     back = packing.CPertSettings.from_buffer_copy(torch_ops.settings_bytes(st).numpy().tobytes())
     assert (back.max_ny, back.rtol_large, back.n_save) == (77, 1e-4, 500)
