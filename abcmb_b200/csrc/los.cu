@@ -239,9 +239,8 @@ struct KahanF {
 // One CTA per (tabulated l, 256-wide transfer-k tile, cosmology of the
 // chunk).  The l column of the three Bessel tables and the per-lna factors
 // (tau0 - tau, its reciprocal, w / aH) sit in shared memory; each thread
-// column owns one transfer k and each of the LOS_TY thread rows sums one
-// contiguous third of the lna points; the rows' sums are added in segment
-// order.  Shared memory (~148 KB) admits one CTA per SM: 24 resident warps.
+// column owns one transfer k and each of the LOS_TY thread rows sums every
+// LOS_TY-th lna point; the rows' sums are added in row order.  Shared memory (~148 KB) admits one CTA per SM: 24 resident warps.
 template <int PREC>
 __global__ void __launch_bounds__(LOS_THREADS, 1) los_kernel(const abcmb_cosmo* __restrict__ cosmo, int c0,
                                                              const double* __restrict__ tables, int nl, int n_save,
@@ -289,7 +288,6 @@ __global__ void __launch_bounds__(LOS_THREADS, 1) los_kernel(const abcmb_cosmo* 
   const double c2 = 3 * l * (l - 1);
   const int j = tile * LOS_TX + threadIdx.x;
   const int iy = threadIdx.y;
-  const int i0 = iy * nl / LOS_TY, i1 = (iy + 1) * nl / LOS_TY;
   double a0 = 0., a1 = 0., a2 = 0., aE = 0.;
   double k = 0.;
   if (j < nkt) {
@@ -297,7 +295,9 @@ __global__ void __launch_bounds__(LOS_THREADS, 1) los_kernel(const abcmb_cosmo* 
     const double invk = 1.0 / k;
     const int64_t plane = (int64_t)nl * nkt;
     KahanF f0{0.f, 0.f}, f1{0.f, 0.f}, f2{0.f, 0.f}, fE{0.f, 0.f};
-    for (int il = i0; il < i1; ++il) {
+    // row iy takes lna points iy, iy + LOS_TY, ...: the costly early points
+    // (large k chi: asymptotic j_l) are shared evenly between the rows
+    for (int il = iy; il < nl; il += LOS_TY) {
       const double chi = sdt[il] * k;
       const double ichi = sidt[il] * invk;
       // phi0/phi1/phi2 (spectrum.py:719-753): 0 below the table, table
