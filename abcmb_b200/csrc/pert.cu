@@ -150,7 +150,7 @@ struct RowTab {
   int8_t tch[MAXC];          // chain hanging off the row, -1 for none
   double cst[MAXC * 5];
   double uh[MAXC], ue[MAXC], tco[MAXC];
-  double ncdm_w[9];   // massive-neutrino bin weights of write_fields
+  double ncdm_w[9];   // massive-neutrino bin weights of stage_basis and write_fields
   // tail coefficients of v[l-1] and v[l+1] per unit chain speed, by l:
   // l / (2l+1) and (l+1) / (2l+1); slot 1 holds the l = 3 pair of the F and
   // N hierarchies (6/7, 4/7: their l = 2 slot stores sigma = F_2 / 2)
@@ -219,8 +219,11 @@ __device__ __forceinline__ void bg_load(const double* s, BG& b) {
 // Background basis of one stage time; with sv != null the same lane instead
 // stores the full background of a save time (lanes 0-4 stage times, lane 5
 // the next save point: one instruction stream, no divergence).
+// ik2 = 1/k^2 of the item; ncdm_w the block table's massive-neutrino bin
+// weights w_b (1 + e^-q_b) / q_b^2 and / q_b (constants, not recomputed here)
 __device__ __noinline__ void stage_basis(const abcmb_cosmo& c, const double* __restrict__ tables, double k,
-                                         double lna, double* B, double* sv) {
+                                         double ik2, const double* __restrict__ ncdm_w, double lna, double* B,
+                                         double* sv) {
   BG b;
   bg_eval(c, tables, lna, b);
   if (sv) {
@@ -247,7 +250,7 @@ __device__ __noinline__ void stage_basis(const abcmb_cosmo& c, const double* __r
   // metric functionals (perturbations.py:238-239)
   const double Ca2 = 4. * PI * GN * b.a * b.a / (C_MPC * C_MPC);
   const double whf = 2. * iaH * iaH * Ca2;
-  const double wef = Ca2 * iaH / (k * k);
+  const double wef = Ca2 * iaH * ik2;
   B[B_WH + 0] = 2. * iaH * iaH * k * k;
   B[B_WH + 1] = whf * b.rho_cdm;
   B[B_WH + 2] = whf * b.rho_b;
@@ -257,10 +260,8 @@ __device__ __noinline__ void stage_basis(const abcmb_cosmo& c, const double* __r
   B[B_WE + 1] = wef * (b.rho_g + b.rho_g / 3.);
   B[B_WE + 2] = wef * (b.rho_nu + b.rho_nu / 3.);
   for (int bb = 0; bb < 3; ++bb) {
-    double q = Q3[bb], w = W3[bb];
-    double g = w * (1. + exp(-q));
-    B[B_WH + 5 + bb] = whf * b.ncdm_fac * (g * b.eps[bb] / (q * q));
-    B[B_WE + 3 + bb] = wef * b.ncdm_fac * (g / q);
+    B[B_WH + 5 + bb] = whf * b.ncdm_fac * (ncdm_w[3 * bb] * b.eps[bb]);
+    B[B_WE + 3 + bb] = wef * b.ncdm_fac * ncdm_w[3 * bb + 1];
   }
   B[31] = 0.;
 }
@@ -807,6 +808,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
       }
     }
     const double k = P.kbuf[c.off_k + ik];
+    const double ik2 = 1. / (k * k);
     const double rtol = k > S.k_split ? S.rtol_large : S.rtol_small;
     const double atol = k > S.k_split ? S.atol_large : S.atol_small;
     const int nsave = S.n_save;
@@ -869,7 +871,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
           Pb[2] = ns / 2. * fac;
         }
       }
-      stage_basis(c, P.tables, k, lna_start, m.SB(), nullptr);
+      stage_basis(c, P.tables, k, ik2, R.ncdm_w, lna_start, m.SB(), nullptr);
       m.SV()[16] = -1.;                                      // no save background computed yet
     }
     __syncwarp();
@@ -894,7 +896,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
         const double tsn = isave < nsave ? linspace_at(lts, 0.0, nsave, isave) : 1.0;
         const bool want_sv = lane == NSLOT - 1 && tsn <= t1 && (double)isave != m.SV()[16];
         if (lane < NSLOT - 1 || want_sv)
-          stage_basis(c, P.tables, k, want_sv ? tsn : t0 + KV_C[lane + 1] * h, m.SB() + (lane + 1) * NB,
+          stage_basis(c, P.tables, k, ik2, R.ncdm_w, want_sv ? tsn : t0 + KV_C[lane + 1] * h, m.SB() + (lane + 1) * NB,
                       want_sv ? m.SV() : nullptr);
         if (want_sv) m.SV()[16] = (double)isave;
       }
