@@ -141,7 +141,7 @@ struct BesselDev {
 
 // Every background scalar the perturbation equations use at one lna.
 struct BG {
-  double a, aH, tau, tau_c, cs2, R;
+  double a, aH, tau, itau_c, cs2, R;   // itau_c = 1 / tau_c
   double rho_cdm, rho_b, rho_g, rho_nu, rho_ncdm, P_ncdm;
   double ncdm_fac;   // N * 4/pi^2 * T^4 / hbar^3 / c^3
   double eps[3];     // sqrt(q^2 + (m/T)^2) for the 3 perturbation q-bins
@@ -164,14 +164,33 @@ static __constant__ double R5[5] = {0.03720333831716864, 0.19567702290257588, 0.
 static __constant__ double P5[5] = {0.012652164020403861, 0.7827080916103035, 2.857699177413455,
                                     2.052994097538504, 0.1268102866323721};
 
+// Constant factors of bg_eval, folded at compile time (a division by a
+// constant at run time costs a full FP64 division sequence).
+constexpr double BG_RHOG = PI * PI / 15. / CHB3;
+constexpr double BG_RHONU = (2. * 7. / 8. * PI * PI / 30.) / CHB3;
+constexpr double BG_NCDM = 1. / (PI * PI) / HB3C3;
+constexpr double BG_NH = 3. * H0H * H0H / 8. / PI / GN / MH;
+constexpr double BG_ITAUC = SIGT * C_CM / C_MPC;           // 1/tau_c = n_e a sigma_T c (in Mpc units)
+constexpr double BG_IMH = 1. / MH;
+constexpr double BG_IME = 1. / ME;
+constexpr double BG_ICMPC = 1. / C_MPC;
+constexpr double BG_TAU_SCALE = (double)(ABCMB_NTAU_TAB - 1) / (ABCMB_LNA_TAU_MAX - ABCMB_LNA_TAU_MIN);
+
 // Every background scalar at one lna.  Same formulas as the reference; the
 // three table reads are issued before the density sums so their latencies
-// overlap, and powers of 1/a replace repeated divisions.
+// overlap, powers of 1/a replace repeated divisions, and constants are
+// folded (this changes only rounding).
 __device__ __forceinline__ void bg_eval(const abcmb_cosmo& c, const double* __restrict__ tables, double lna,
                                         BG& b) {
   int t0, t1, x0, x1, m0, m1;
   double tw, xw, mw;
-  lerp_index(lna, ABCMB_LNA_TAU_MIN, ABCMB_LNA_TAU_MAX, ABCMB_NTAU_TAB, t0, t1, tw);
+  {
+    double i = (lna - ABCMB_LNA_TAU_MIN) * BG_TAU_SCALE;
+    i = fmin(fmax(i, 1.e-6), (double)(ABCMB_NTAU_TAB - 1) - 1.e-6);
+    t0 = (int)floor(i);
+    t1 = min(t0 + 1, ABCMB_NTAU_TAB - 1);
+    tw = i - (double)t0;
+  }
   lerp_index(lna, c.lna_xe0, c.lna_xe_max, c.n_xe, x0, x1, xw);
   lerp_index(lna, c.lna_tm0, c.lna_tm_max, c.n_tm, m0, m1, mw);
   const double* tt = tables + c.off_tau;
@@ -189,8 +208,8 @@ __device__ __forceinline__ void bg_eval(const abcmb_cosmo& c, const double* __re
   const double rde = c.omega_Lambda * RHO_CRIT_UNIT;
   b.rho_cdm = c.omega_cdm * RHO_CRIT_UNIT * ia3;
   b.rho_b = c.omega_b * RHO_CRIT_UNIT * ia3;
-  b.rho_g = PI * PI / 15. * T04 * ia4 / CHB3;
-  b.rho_nu = c.N_nu_massless * (2. * 7. / 8. * PI * PI / 30.) * (tn * tn * tn * tn) * T04 * ia4 / CHB3;
+  b.rho_g = BG_RHOG * T04 * ia4;
+  b.rho_nu = c.N_nu_massless * BG_RHONU * (tn * tn * tn * tn) * T04 * ia4;
   b.rho_ncdm = 0.;
   b.P_ncdm = 0.;
   double x = 0.;
@@ -201,23 +220,24 @@ __device__ __forceinline__ void bg_eval(const abcmb_cosmo& c, const double* __re
     double ir = 0., ip = 0.;
 #pragma unroll
     for (int j = 0; j < 5; ++j) {
-      const double e = sqrt(Q5[j] * Q5[j] + x * x);
-      ir = fma(R5[j], e, ir);
-      ip += P5[j] / e;
+      const double e2 = Q5[j] * Q5[j] + x * x;
+      const double ie = rsqrt(e2);
+      ir = fma(R5[j], e2 * ie, ir);
+      ip = fma(P5[j], ie, ip);
     }
     const double T4 = T * T * T * T;
-    const double f = c.N_nu_massive * T4 / (PI * PI) / HB3C3;
+    const double f = c.N_nu_massive * T4 * BG_NCDM;
     b.rho_ncdm = 4. * f * ir;
     b.P_ncdm = 4. / 3. * f * ip;
     b.ncdm_fac = 4. * f;
   }
   const double tot = rde + b.rho_cdm + b.rho_b + b.rho_g + b.rho_nu + b.rho_ncdm;
   const double H = sqrt(8. * PI * GN / 3. * tot);
-  b.aH = a * H / C_MPC;
+  b.aH = a * H * BG_ICMPC;
   b.tau = (1. - tw) * ta + tw * tb;
   const double xe = (lna < c.lna_xe0) ? c.xe_first : (lna >= c.lna_xe_last) ? c.xe_last : (1. - xw) * xa + xw * xb;
-  const double ne = nH_of(c, a) * xe;
-  b.tau_c = ia / ne * (C_MPC / (SIGT * C_CM));
+  const double ne = (1. - c.YHe) * c.omega_b * BG_NH * ia3 * xe;
+  b.itau_c = ne * a * BG_ITAUC;
   const double TCMB = c.TCMB0 * ia;
   double Tm;
   if (lna < c.lna_tm0) Tm = TCMB * (1. - H / gamma_compton(xe, TCMB, c.YHe));
@@ -226,7 +246,8 @@ __device__ __forceinline__ void bg_eval(const abcmb_cosmo& c, const double* __re
   const double denom = (1. + xe) * (1. - c.YHe) + MH / MHE * c.YHe;
   const double mu = MH / denom;
   b.R = 4. / 3. * b.rho_g / b.rho_b;
-  b.cs2 = Tm / mu * (5. / 3. - 2. / 3. * mu * b.R / ME / b.aH / b.tau_c * (TCMB / Tm - 1.));
+  const double iaH = 1. / b.aH;
+  b.cs2 = Tm * denom * BG_IMH * (5. / 3. - 2. / 3. * mu * b.R * BG_IME * iaH * b.itau_c * (TCMB / Tm - 1.));
   if (c.has_ncdm) {
 #pragma unroll
     for (int i = 0; i < 3; ++i) b.eps[i] = sqrt(Q3[i] * Q3[i] + x * x);

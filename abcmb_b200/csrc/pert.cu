@@ -206,12 +206,12 @@ __device__ __forceinline__ double warp_sum(double v) {
 // ---------------------------------------------------------------------------
 // BG <-> shared memory (the background of a save point computed ahead)
 __device__ __forceinline__ void bg_store(const BG& b, double* s) {
-  s[0] = b.a; s[1] = b.aH; s[2] = b.tau; s[3] = b.tau_c; s[4] = b.cs2; s[5] = b.R;
+  s[0] = b.a; s[1] = b.aH; s[2] = b.tau; s[3] = b.itau_c; s[4] = b.cs2; s[5] = b.R;
   s[6] = b.rho_cdm; s[7] = b.rho_b; s[8] = b.rho_g; s[9] = b.rho_nu; s[10] = b.rho_ncdm; s[11] = b.P_ncdm;
   s[12] = b.ncdm_fac; s[13] = b.eps[0]; s[14] = b.eps[1]; s[15] = b.eps[2];
 }
 __device__ __forceinline__ void bg_load(const double* s, BG& b) {
-  b.a = s[0]; b.aH = s[1]; b.tau = s[2]; b.tau_c = s[3]; b.cs2 = s[4]; b.R = s[5];
+  b.a = s[0]; b.aH = s[1]; b.tau = s[2]; b.itau_c = s[3]; b.cs2 = s[4]; b.R = s[5];
   b.rho_cdm = s[6]; b.rho_b = s[7]; b.rho_g = s[8]; b.rho_nu = s[9]; b.rho_ncdm = s[10]; b.P_ncdm = s[11];
   b.ncdm_fac = s[12]; b.eps[0] = s[13]; b.eps[1] = s[14]; b.eps[2] = s[15];
 }
@@ -232,7 +232,7 @@ __device__ __noinline__ void stage_basis(const abcmb_cosmo& c, const double* __r
   }
   const double aH = b.aH;
   const double iaH = 1. / aH;
-  const double kap = iaH / b.tau_c;                          // 1/(aH tau_c)
+  const double kap = iaH * b.itau_c;                         // 1/(aH tau_c)
   B[B_ONE] = 1.;
   B[B_IAH] = iaH;
   B[B_KIAH] = k * iaH;
@@ -241,14 +241,14 @@ __device__ __noinline__ void stage_basis(const abcmb_cosmo& c, const double* __r
   B[B_RKAP] = b.R * kap;
   B[B_CS2K2IAH] = b.cs2 * k * k * iaH;
   for (int bb = 0; bb < 3; ++bb) {
-    double s = Q3[bb] / b.eps[bb] * iaH;                     // q/(eps aH)
+    double s = Q3[bb] * rsqrt(b.eps[bb] * b.eps[bb]) * iaH;  // q/(eps aH)
     B[B_NCDM + 3 * bb] = s;
     B[B_NCDM + 3 * bb + 1] = s * k;
     B[B_NCDM + 3 * bb + 2] = s * k * k;
   }
   B[B_TRUNC] = iaH / b.tau;
   // metric functionals (perturbations.py:238-239)
-  const double Ca2 = 4. * PI * GN * b.a * b.a / (C_MPC * C_MPC);
+  const double Ca2 = (4. * PI * GN / (C_MPC * C_MPC)) * b.a * b.a;
   const double whf = 2. * iaH * iaH * Ca2;
   const double wef = Ca2 * iaH * ik2;
   B[B_WH + 0] = 2. * iaH * iaH * k * k;
@@ -647,7 +647,7 @@ __device__ __noinline__ void write_fields(const abcmb_cosmo& c, const Layout& L,
     switch (lane) {
       case ABCMB_F_DELTA_M: val = rdm / rm; break;
       case ABCMB_F_THETA_B_PRIME:
-        val = -ys[3] + b.cs2 * iaH * (k * k * ys[2]) + b.R * iaH / b.tau_c * (ys[L.i_g + 1] - ys[3]);
+        val = -ys[3] + b.cs2 * iaH * (k * k * ys[2]) + b.R * iaH * b.itau_c * (ys[L.i_g + 1] - ys[3]);
         break;
       case ABCMB_F_ETA: val = eta; break;
       case ABCMB_F_H_PRIME: val = hp; break;
