@@ -142,6 +142,7 @@ struct BesselDev {
 // Every background scalar the perturbation equations use at one lna.
 struct BG {
   double a, aH, tau, itau_c, cs2, R;   // itau_c = 1 / tau_c
+  double iaH;                          // 1 / aH
   double rho_cdm, rho_b, rho_g, rho_nu, rho_ncdm, P_ncdm;
   double ncdm_fac;   // N * 4/pi^2 * T^4 / hbar^3 / c^3
   double eps[3];     // sqrt(q^2 + (m/T)^2) for the 3 perturbation q-bins
@@ -176,12 +177,37 @@ constexpr double BG_IME = 1. / ME;
 constexpr double BG_ICMPC = 1. / C_MPC;
 constexpr double BG_TAU_SCALE = (double)(ABCMB_NTAU_TAB - 1) / (ABCMB_LNA_TAU_MAX - ABCMB_LNA_TAU_MIN);
 
+// Per-cosmology constants of bg_eval, computed once per (cosmology, k) item:
+// the x_e and T_m table scales (n - 1) / (lna_max - lna_0) of fast_interp and
+// R a = (4/3) rho_g a^4 / (rho_b a^3).
+struct BGK {
+  double sxe, stm, rfac;
+};
+__device__ __forceinline__ BGK bg_constants(const abcmb_cosmo& c) {
+  BGK k;
+  k.sxe = (double)(c.n_xe - 1) / (c.lna_xe_max - c.lna_xe0);
+  k.stm = (double)(c.n_tm - 1) / (c.lna_tm_max - c.lna_tm0);
+  const double T04 = c.TCMB0 * c.TCMB0 * c.TCMB0 * c.TCMB0;
+  k.rfac = 4. / 3. * BG_RHOG * T04 / (c.omega_b * RHO_CRIT_UNIT);
+  return k;
+}
+
+// fast_interp index with a precomputed scale
+__device__ __forceinline__ void lerp_index_scaled(double x, double xp_min, double scale, int n, int& il, int& iu,
+                                                  double& wu) {
+  double i = (x - xp_min) * scale;
+  i = fmin(fmax(i, 1.e-6), (double)(n - 1) - 1.e-6);
+  il = (int)floor(i);
+  iu = min(il + 1, n - 1);
+  wu = i - (double)il;
+}
+
 // Every background scalar at one lna.  Same formulas as the reference; the
 // three table reads are issued before the density sums so their latencies
 // overlap, powers of 1/a replace repeated divisions, and constants are
 // folded (this changes only rounding).
-__device__ __forceinline__ void bg_eval(const abcmb_cosmo& c, const double* __restrict__ tables, double lna,
-                                        BG& b) {
+__device__ __forceinline__ void bg_eval(const abcmb_cosmo& c, const BGK& K, const double* __restrict__ tables,
+                                        double lna, BG& b) {
   int t0, t1, x0, x1, m0, m1;
   double tw, xw, mw;
   {
@@ -191,8 +217,8 @@ __device__ __forceinline__ void bg_eval(const abcmb_cosmo& c, const double* __re
     t1 = min(t0 + 1, ABCMB_NTAU_TAB - 1);
     tw = i - (double)t0;
   }
-  lerp_index(lna, c.lna_xe0, c.lna_xe_max, c.n_xe, x0, x1, xw);
-  lerp_index(lna, c.lna_tm0, c.lna_tm_max, c.n_tm, m0, m1, mw);
+  lerp_index_scaled(lna, c.lna_xe0, K.sxe, c.n_xe, x0, x1, xw);
+  lerp_index_scaled(lna, c.lna_tm0, K.stm, c.n_tm, m0, m1, mw);
   const double* tt = tables + c.off_tau;
   const double* tx = tables + c.off_xe;
   const double* tm = tables + c.off_tm;
@@ -245,8 +271,9 @@ __device__ __forceinline__ void bg_eval(const abcmb_cosmo& c, const double* __re
   else Tm = (1. - mw) * ma + mw * mb;
   const double denom = (1. + xe) * (1. - c.YHe) + MH / MHE * c.YHe;
   const double mu = MH / denom;
-  b.R = 4. / 3. * b.rho_g / b.rho_b;
+  b.R = K.rfac * ia;
   const double iaH = 1. / b.aH;
+  b.iaH = iaH;
   b.cs2 = Tm * denom * BG_IMH * (5. / 3. - 2. / 3. * mu * b.R * BG_IME * iaH * b.itau_c * (TCMB / Tm - 1.));
   if (c.has_ncdm) {
 #pragma unroll

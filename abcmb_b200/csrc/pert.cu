@@ -27,7 +27,7 @@ namespace abcmb {
 
 constexpr int WARP = 32;
 constexpr int NCHAIN = 6;            // F, G, N, Psi(q0), Psi(q1), Psi(q2)
-constexpr int NSV = 18;              // saved background: 16 BG values + save-index tag
+constexpr int NSV = 18;              // saved background: 16 BG values, the save-index tag, 1/aH
 constexpr int NSTART = 10000;        // get_starting_time grid
 
 // Kvaerno5 tableau (Kvaerno, BIT 44 (2004) 489-502), ESDIRK 5(4), 7 stages.
@@ -209,11 +209,13 @@ __device__ __forceinline__ void bg_store(const BG& b, double* s) {
   s[0] = b.a; s[1] = b.aH; s[2] = b.tau; s[3] = b.itau_c; s[4] = b.cs2; s[5] = b.R;
   s[6] = b.rho_cdm; s[7] = b.rho_b; s[8] = b.rho_g; s[9] = b.rho_nu; s[10] = b.rho_ncdm; s[11] = b.P_ncdm;
   s[12] = b.ncdm_fac; s[13] = b.eps[0]; s[14] = b.eps[1]; s[15] = b.eps[2];
+  s[17] = b.iaH;                        // s[16] is the save-index tag
 }
 __device__ __forceinline__ void bg_load(const double* s, BG& b) {
   b.a = s[0]; b.aH = s[1]; b.tau = s[2]; b.itau_c = s[3]; b.cs2 = s[4]; b.R = s[5];
   b.rho_cdm = s[6]; b.rho_b = s[7]; b.rho_g = s[8]; b.rho_nu = s[9]; b.rho_ncdm = s[10]; b.P_ncdm = s[11];
   b.ncdm_fac = s[12]; b.eps[0] = s[13]; b.eps[1] = s[14]; b.eps[2] = s[15];
+  b.iaH = s[17];
 }
 
 // Background basis of one stage time; with sv != null the same lane instead
@@ -221,17 +223,16 @@ __device__ __forceinline__ void bg_load(const double* s, BG& b) {
 // the next save point: one instruction stream, no divergence).
 // ik2 = 1/k^2 of the item; ncdm_w the block table's massive-neutrino bin
 // weights w_b (1 + e^-q_b) / q_b^2 and / q_b (constants, not recomputed here)
-__device__ __noinline__ void stage_basis(const abcmb_cosmo& c, const double* __restrict__ tables, double k,
-                                         double ik2, const double* __restrict__ ncdm_w, double lna, double* B,
+__device__ __noinline__ void stage_basis(const abcmb_cosmo& c, const BGK& K, const double* __restrict__ tables,
+                                         double k, double ik2, const double* __restrict__ ncdm_w, double lna, double* B,
                                          double* sv) {
   BG b;
-  bg_eval(c, tables, lna, b);
+  bg_eval(c, K, tables, lna, b);
   if (sv) {
     bg_store(b, sv);
     return;
   }
-  const double aH = b.aH;
-  const double iaH = 1. / aH;
+  const double iaH = b.iaH;
   const double kap = iaH * b.itau_c;                         // 1/(aH tau_c)
   B[B_ONE] = 1.;
   B[B_IAH] = iaH;
@@ -257,8 +258,8 @@ __device__ __noinline__ void stage_basis(const abcmb_cosmo& c, const double* __r
   B[B_WH + 3] = whf * b.rho_g;
   B[B_WH + 4] = whf * b.rho_nu;
   B[B_WE + 0] = wef * b.rho_b;
-  B[B_WE + 1] = wef * (b.rho_g + b.rho_g / 3.);
-  B[B_WE + 2] = wef * (b.rho_nu + b.rho_nu / 3.);
+  B[B_WE + 1] = wef * ((4. / 3.) * b.rho_g);
+  B[B_WE + 2] = wef * ((4. / 3.) * b.rho_nu);
   for (int bb = 0; bb < 3; ++bb) {
     B[B_WH + 5 + bb] = whf * b.ncdm_fac * (ncdm_w[3 * bb] * b.eps[bb]);
     B[B_WE + 3 + bb] = wef * b.ncdm_fac * ncdm_w[3 * bb + 1];
@@ -609,14 +610,14 @@ __device__ __noinline__ void write_fields(const abcmb_cosmo& c, const Layout& L,
                              const double* sv, const double* ncdm_w) {
   BG b;
   if (sv) bg_load(sv, b);               // computed ahead for this save point
-  else bg_eval(c, tables, lna, b);
+  else bg_eval(c, bg_constants(c), tables, lna, b);
   const double a = b.a, aH = b.aH;
-  const double iaH = 1. / aH;
+  const double iaH = b.iaH;
   const double ik2 = 1. / (k * k);
   double srd = b.rho_cdm * ys[1] + b.rho_b * ys[2] + b.rho_g * ys[L.i_g] + b.rho_nu * ys[L.i_nu];
-  double srt = (b.rho_b + 0.) * ys[3] + (b.rho_g + b.rho_g / 3.) * ys[L.i_g + 1] +
-               (b.rho_nu + b.rho_nu / 3.) * ys[L.i_nu + 1];
-  double srs = (b.rho_g + b.rho_g / 3.) * ys[L.i_g + 2] + (b.rho_nu + b.rho_nu / 3.) * ys[L.i_nu + 2];
+  const double pg = (4. / 3.) * b.rho_g, pn = (4. / 3.) * b.rho_nu;   // rho + P of photons, massless nu
+  double srt = b.rho_b * ys[3] + pg * ys[L.i_g + 1] + pn * ys[L.i_nu + 1];
+  double srs = pg * ys[L.i_g + 2] + pn * ys[L.i_nu + 2];
   double rdm = b.rho_cdm * ys[1] + b.rho_b * ys[2];
   double rm = b.rho_cdm + b.rho_b;
   double nd = 0., nt = 0., ns = 0.;
@@ -809,6 +810,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
     }
     const double k = P.kbuf[c.off_k + ik];
     const double ik2 = 1. / (k * k);
+    const BGK K = bg_constants(c);
     const double rtol = k > S.k_split ? S.rtol_large : S.rtol_small;
     const double atol = k > S.k_split ? S.atol_large : S.atol_small;
     const int nsave = S.n_save;
@@ -871,7 +873,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
           Pb[2] = ns / 2. * fac;
         }
       }
-      stage_basis(c, P.tables, k, ik2, R.ncdm_w, lna_start, m.SB(), nullptr);
+      stage_basis(c, K, P.tables, k, ik2, R.ncdm_w, lna_start, m.SB(), nullptr);
       m.SV()[16] = -1.;                                      // no save background computed yet
     }
     __syncwarp();
@@ -896,7 +898,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
         const double tsn = isave < nsave ? linspace_at(lts, 0.0, nsave, isave) : 1.0;
         const bool want_sv = lane == NSLOT - 1 && tsn <= t1 && (double)isave != m.SV()[16];
         if (lane < NSLOT - 1 || want_sv)
-          stage_basis(c, P.tables, k, ik2, R.ncdm_w, want_sv ? tsn : t0 + KV_C[lane + 1] * h, m.SB() + (lane + 1) * NB,
+          stage_basis(c, K, P.tables, k, ik2, R.ncdm_w, want_sv ? tsn : t0 + KV_C[lane + 1] * h, m.SB() + (lane + 1) * NB,
                       want_sv ? m.SV() : nullptr);
         if (want_sv) m.SV()[16] = (double)isave;
       }
