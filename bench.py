@@ -358,7 +358,7 @@ def main():
                 "peak_source": "measured in this run: FP64 FMA probe (abcmb_probe_fp64_tflops); "
                                "MEASURED_PEAKS.json has no FP64 figure",
                 "flops_def": "sum_k steps_k * 7 * (8 Ny + 200 + 20 Ny)", "launch_ms": pert_avg,
-                "hbm_gbs_peak_measured": _peak_hbm()}
+                "hbm_gbs_peak": _peak_hbm()[0], "hbm_gbs_peak_source": _peak_hbm()[1]}
     # our kernel launches per step: pert (2 start kernels + the persistent
     # kernel) + 5 per line-of-sight chunk of engine.LOS_CHUNK cosmologies
     launches = 3 + 5 * ((b.n_cosmo + engine.LOS_CHUNK - 1) // engine.LOS_CHUNK)
@@ -380,12 +380,19 @@ def main():
         dist.destroy_process_group()
 
 
+HBM_GBS_FALLBACK = 6650.0     # copy bandwidth measured earlier on this pool's B200s
+
+
 def _peak_hbm():
+    """(HBM GB/s, source): the measured copy bandwidth, or the fallback figure."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
-        return json.load(open(p)).get("hbm_gbs")
+        v = json.load(open(p)).get("hbm_gbs")
+        if v:
+            return float(v), "MEASURED_PEAKS.json"
     except (OSError, ValueError):
-        return None
+        pass
+    return HBM_GBS_FALLBACK, "fallback (MEASURED_PEAKS.json absent)"
 
 
 if __name__ == "__main__":
