@@ -1,0 +1,119 @@
+"""Model-level entry point and output formats.
+
+* ``Output`` mirrors ``abcmb.main.Output`` (abcmb/main.py:614-650): C_l^TT,
+  C_l^TE, C_l^EE at ells ``l``, P(k) at ``k`` (z = 0), the background, the
+  PerturbationTable and the parameter dictionary.
+* ``B200Model(user_species=None, **specs)(params) -> Output`` mirrors
+  ``Model.__init__`` / ``Model.__call__`` (main.py:84-184, 289-298): specs
+  with the reference's defaults, the reference's k grids, the perturbation and
+  spectrum stages on the CUDA kernels.  The background and recombination
+  history come from ``background_tables.make_background`` (the host model
+  that stands in for the reference's JAX background and HyRex here).
+* ``write_class_cl`` / ``read_class_cl``: C_l files in CLASS's ``cl.dat``
+  layout (dimensionless l(l+1)/2pi C_l, columns l, TT, EE, TE, BB, phiphi),
+  the format the reference's example notebooks compare against
+  (example_notebooks/data/idr0*_cl.dat).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import background_tables as bt
+from . import cosmology
+from . import specs as sp
+from .perturbations import B200PerturbationEvolver, PerturbationTable
+from .spectrum import B200SpectrumSolver
+
+LCDM_SPECIES = ("DarkEnergy", "ColdDarkMatter", "Baryon", "Photon", "MasslessNeutrino")
+
+
+@dataclass
+class Output:
+    """Results of one cosmology (abcmb/main.py:614-650)."""
+    ClTT: np.ndarray
+    ClTE: np.ndarray
+    ClEE: np.ndarray
+    Pk: np.ndarray
+    l: np.ndarray
+    k: np.ndarray
+    BG: bt.BackgroundTables
+    PT: PerturbationTable
+    params: dict
+
+
+def _species_names(user_species) -> tuple:
+    names = []
+    for s in (user_species or ()):
+        names.append(s if isinstance(s, str) else getattr(s, "name", type(s).__name__))
+    return LCDM_SPECIES + tuple(n for n in names if n not in LCDM_SPECIES)
+
+
+class B200Model:
+    """Model(**specs)(params) on the CUDA path (abcmb/main.py:84-184)."""
+
+    def __init__(self, user_species=None, device=None, **kwargs):
+        specs = sp.load_specs(kwargs)
+        self.specs = specs
+        self.species = _species_names(user_species)
+        self.has_ncdm = "MassiveNeutrino" in self.species
+        k_pert, k_pk = sp.get_k_axis_perturbations(specs)         # also sets k_min / k_max_cmb
+        self.k_axis_Pk_output = np.asarray(k_pk, dtype=np.float64)
+        self.PE = B200PerturbationEvolver(self.species, k_pert, specs, device=device)
+        self.SS = B200SpectrumSolver(int(specs["l_min"]), int(specs["l_max"]), bool(specs["lensing"]),
+                                     sp.get_k_axis_transfer(specs), self.k_axis_Pk_output,
+                                     k_pivot=specs["k_pivot"], scale_sw=specs["scale_sw"],
+                                     scale_isw=specs["scale_isw"], scale_dop=specs["scale_dop"],
+                                     scale_pol=specs["scale_pol"])
+
+    def add_derived_parameters(self, params: dict) -> dict:
+        return cosmology.add_derived_parameters(params, self.has_ncdm, self.specs)
+
+    def __call__(self, params: dict) -> Output:
+        p = self.add_derived_parameters(params)
+        BG = bt.make_background(p, self.has_ncdm)
+        PT = self.PE.full_evolution((BG, p))
+        tt, te, ee = self.SS.get_Cl(PT, BG, p)
+        Pk = self.SS.Pk_lin(self.k_axis_Pk_output, 0.0, PT, p)
+        return Output(tt, te, ee, Pk, self.SS.ells, self.k_axis_Pk_output, BG, PT, p)
+
+
+CLASS_COLUMNS = ("l", "TT", "EE", "TE", "BB", "phiphi")
+
+
+def write_class_cl(path, l, ClTT, ClTE, ClEE, Clpp=None, ClBB=None):
+    """C_l in CLASS's cl.dat layout: dimensionless l(l+1)/2pi C_l per column
+    (phiphi scaled the same way); BB and phiphi are zero when not given."""
+    l = np.asarray(l, dtype=np.float64)
+    d = l * (l + 1.0) / (2.0 * np.pi)
+    zero = np.zeros_like(l)
+    cols = [l, d * np.asarray(ClTT), d * np.asarray(ClEE), d * np.asarray(ClTE),
+            d * np.asarray(ClBB) if ClBB is not None else zero,
+            d * np.asarray(Clpp) if Clpp is not None else zero]
+    header = ("dimensionless total [l(l+1)/2pi] C_l's\n"
+              f"for l={int(l[0])} to {int(l[-1])}, i.e. number of multipoles equal to {len(l)}\n"
+              "\n" + "     ".join(f"{i + 1}:{name}" for i, name in enumerate(CLASS_COLUMNS)))
+    np.savetxt(path, np.column_stack(cols), fmt=["%5d"] + ["%24.12e"] * 5, header=header)
+
+
+def read_class_cl(path) -> dict:
+    """A CLASS cl.dat file as {'l': ..., 'TT': C_l, 'EE': ..., ...}: the
+    columns named in its last header line, l(l+1)/2pi removed."""
+    names = None
+    with open(path) as fh:
+        for line in fh:
+            if not line.startswith("#"):
+                break
+            toks = [t.split(":", 1)[1] for t in line[1:].split() if ":" in t and t.split(":", 1)[0].isdigit()]
+            if toks:
+                names = toks
+    data = np.loadtxt(path, comments="#")
+    if names is None or len(names) != data.shape[1]:
+        raise ValueError(f"{path}: no column header matching the {data.shape[1]} columns")
+    l = data[:, 0]
+    d = l * (l + 1.0) / (2.0 * np.pi)
+    out = {"l": l.astype(int)}
+    for i, name in enumerate(names[1:], start=1):
+        out[name] = data[:, i] / d
+    return out

@@ -406,3 +406,23 @@ def test_cl_from_pt_autograd_uses_the_adjoint(gpu, c1_small):
     (cl * weights).sum().backward()
     ref, _ = lr.vjp(weights.reshape(-1))
     assert torch.equal(pt.grad, ref)
+
+
+def test_model_output_matches_oracle(gpu):
+    """B200Model(**specs)(params) -> Output: C_l and P(k) against the oracle on
+    the same background and k grid."""
+    from abcmb_b200 import configs, packing, bessel
+    from abcmb_b200.output import B200Model
+    from oracle import oracle
+    m = B200Model(l_max=400, l_max_g=12, l_max_pol_g=12, l_max_massless_nu=12)
+    out = m(dict(configs.FIDUCIAL))
+    assert out.ClTT.shape == (399,) and out.l[0] == 2 and out.Pk.shape == out.k.shape
+    batch = packing.pack([out.BG], [m.PE.layout], [m.PE.k_axis_perturbations])
+    rc, pt, _ = oracle.pert_forward(batch, packing.pert_settings(m.specs, 500, batch))
+    assert rc == 0
+    ls = packing.los_settings(m.specs, m.SS.idx_min, m.SS.idx_max, len(m.SS.k_axis_transfer), m.SS.l_out_max,
+                              n_save=500)
+    _, _, cl_o = oracle.los_forward(batch, pt, m.SS.k_axis_transfer, ls, bessel.load())
+    assert np.max(np.abs(out.ClTT - cl_o[0, 0]) / cl_o[0, 0]) < 1e-5
+    pk_o = oracle.pk_lin(batch, pt, m.specs["k_pivot"], out.k, np.array([0.0]))[0, 0]
+    np.testing.assert_allclose(out.Pk, pk_o, rtol=1e-5)

@@ -173,3 +173,34 @@ def test_lensed_expansion_shares_perturbations():
     _, grad = gw.assemble(cl, np.zeros_like(cl))
     for gi, name in enumerate(configs.GRAD_PARAMS):
         np.testing.assert_allclose(grad[:, gi], slope[name], rtol=1e-6)
+
+
+def test_class_cl_file_round_trip(tmp_path):
+    """write_class_cl / read_class_cl keep CLASS's layout (l(l+1)/2pi C_l,
+    columns l TT EE TE BB phiphi) and invert each other."""
+    from abcmb_b200.output import write_class_cl, read_class_cl, CLASS_COLUMNS
+    l = np.arange(2, 51)
+    rng = np.random.default_rng(3)
+    tt, te, ee, pp = (rng.uniform(0.5, 2.0, l.size) * 1e-10 / (l * (l + 1.0)) for _ in range(4))
+    f = tmp_path / "cl.dat"
+    write_class_cl(f, l, tt, te, ee, Clpp=pp)
+    text = f.read_text()
+    assert "[l(l+1)/2pi] C_l" in text and "1:l" in text and "6:phiphi" in text
+    first = np.loadtxt(f)[0]
+    np.testing.assert_allclose(first[1], 2 * 3 / (2 * np.pi) * tt[0], rtol=1e-11)
+    back = read_class_cl(f)
+    assert list(back) == list(CLASS_COLUMNS)
+    np.testing.assert_array_equal(back["l"], l)
+    for name, ref in (("TT", tt), ("TE", te), ("EE", ee), ("phiphi", pp)):
+        np.testing.assert_allclose(back[name], ref, rtol=1e-11)
+    assert np.all(back["BB"] == 0)
+
+
+def test_model_setup_mirrors_reference_defaults():
+    from abcmb_b200.output import B200Model
+    m = B200Model(l_max=800)
+    assert m.specs["l_max"] == 800 and not m.has_ncdm
+    assert m.SS.ells[0] == 2 and m.SS.ells[-1] == 800
+    assert len(m.PE.k_axis_perturbations) > 50 and m.k_axis_Pk_output[-1] <= m.specs["k_max"]
+    m2 = B200Model(user_species=("MassiveNeutrino",), l_max=800)
+    assert m2.has_ncdm and m2.PE.layout.has_ncdm
