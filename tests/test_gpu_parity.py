@@ -3,7 +3,7 @@
 Tolerances (stated per test): the GPU kernels run the same algorithm as the
 oracle (Kvaerno5 + very-chord + PID, same tableau, same dense output) in
 FP64, so step sequences coincide and results agree far below the 1e-4
-relative C_l budget of the north star; the FP32 + compensated line of sight
+relative C_l accuracy the path is specified to; the FP32 + compensated line of sight
 is checked against the FP64 path at its own stated bound.
 """
 import numpy as np
