@@ -8,8 +8,12 @@ and Background adds reionisation, replaces the inf padding by the last
 value and integrates the optical depth (abcmb/background.py:501-564,
 682-768).  ``BackgroundTables.from_background`` packs such a Background.
 
-For standalone runs (tests, benchmarks) ``make_background`` produces tables
-of the same format from a compact recombination model: helium by Saha
+For standalone runs (tests, benchmarks) ``make_recombination`` produces x_e
+and T_m tables of the same format from a compact recombination model, and
+``complete_on_host`` adds the conformal-time table, optical depth and
+line-of-sight arrays on the host (``make_background`` does both); without
+``complete_on_host`` the CUDA path produces those with the reference's own
+solves (abcmb_bg_forward).  The recombination model: helium by Saha
 equilibrium and hydrogen by the Peebles three-level atom with the RECFAST
 fudge factor 1.14 (Seager, Sasselov & Scott 1999), and the matter
 temperature from Compton heating.  These are realistic synthetic inputs,
@@ -78,6 +82,22 @@ class BackgroundTables:
     z_reion: float
     kappa_lna: np.ndarray = field(repr=False, default=None)   # fine grid on [-10, 0]
     kappa_val: np.ndarray = field(repr=False, default=None)
+    los: np.ndarray = field(repr=False, default=None)         # (6, n_save - 1) from abcmb_bg_forward
+
+    @property
+    def on_device(self) -> bool:
+        """True while the conformal-time table, optical depth and
+        line-of-sight arrays are still to be produced by abcmb_bg_forward."""
+        return self.tau_tab is None
+
+    def set_device_result(self, tau_tab, los, stat):
+        """Take the tables and scalars abcmb_bg_forward produced for this
+        cosmology (stat: one BGSTAT_DTYPE record)."""
+        self.tau_tab = np.asarray(tau_tab, dtype=np.float64).copy() if tau_tab is not None else None
+        self.los = np.asarray(los, dtype=np.float64).copy() if los is not None else None
+        self.tau0 = float(stat["tau0"])
+        self.lna_rec = float(stat["lna_rec"])
+        self.lna_transfer_start = float(stat["lna_transfer_start"])
 
     # -- evaluators with the reference's exact semantics --------------------
     def tau(self, lna):
@@ -115,6 +135,9 @@ class BackgroundTables:
         return cosmo.aH_prime(lna, self.params, self.has_ncdm)
 
     def kappa(self, lna):
+        if self.kappa_lna is None:
+            raise ValueError("this background's optical depth was produced on the GPU (abcmb_bg_forward): "
+                             "exp(-kappa) at the line-of-sight points is los[4]")
         return np.interp(lna, self.kappa_lna, self.kappa_val)
 
     def expmkappa(self, lna):
@@ -132,6 +155,8 @@ class BackgroundTables:
 
     def los_arrays(self, n_save: int = 500) -> np.ndarray:
         """The six 1-D arrays of Cl_one_ell on PT.lna[:-1] (spectrum.py:640-651)."""
+        if self.los is not None and self.los.shape == (6, n_save - 1):
+            return self.los
         lna = np.linspace(self.lna_transfer_start, 0.0, n_save)[:-1]
         aH = self.aH(lna)
         return np.stack([
@@ -283,12 +308,12 @@ def _tabulate_tau(p, has_ncdm):
     return tab
 
 
-def make_background(params: dict, has_ncdm: bool, xe_pad: int = 37, tm_pad: int = 29) -> BackgroundTables:
-    """Synthetic Background for one cosmology (derived params dict in)."""
+def make_recombination(params: dict, has_ncdm: bool, xe_pad: int = 37, tm_pad: int = 29) -> BackgroundTables:
+    """The recombination and reionisation part of the synthetic background:
+    x_e (with reionisation) and T_m tables in HyRex's padded format and
+    z_reion.  The conformal-time table, the optical depth and the
+    line-of-sight arrays are left to abcmb_bg_forward (tau_tab is None)."""
     p = params
-    tau_tab = _tabulate_tau(p, has_ncdm)
-    tau0 = float(fast_interp(0.0, -33.0, 0.0, tau_tab))
-
     # x_e grid: HyRex lna_axis_full = arange(-log(1+8000), 0, 5e-4)
     dx = 5.0e-4
     lna_full = np.arange(-math.log(1 + 8000.0), -math.log(1 + 0.0), dx)
@@ -307,14 +332,24 @@ def make_background(params: dict, has_ncdm: bool, xe_pad: int = 37, tm_pad: int 
     lna_tm = lna_full[i_tm:]
     tm_arr = np.concatenate([tm_rec[i_tm:], np.full(tm_pad, tm_rec[-1])])
 
-    bg = BackgroundTables(
-        params=p, has_ncdm=has_ncdm, tau_tab=tau_tab, tau0=tau0,
+    return BackgroundTables(
+        params=p, has_ncdm=has_ncdm, tau_tab=None, tau0=float("nan"),
         xe_arr=xe_arr, lna_xe0=float(lna_xe_arr[0]), lna_xe_dx=float(lna_xe_arr[1] - lna_xe_arr[0]),
         lna_xe_last=float(lna_xe_arr[-1]), xe_last=float(xe_full[-1]),
         tm_arr=tm_arr, lna_tm0=float(lna_tm[0]), lna_tm_dx=float(lna_tm[1] - lna_tm[0]),
         lna_tm_last=float(lna_tm[-1]), tm_last=float(tm_rec[-1]),
-        lna_transfer_start=0.0, lna_rec=0.0, z_reion=float(z_re))
+        lna_transfer_start=float("nan"), lna_rec=float("nan"), z_reion=float(z_re))
 
+
+def complete_on_host(bg: BackgroundTables) -> BackgroundTables:
+    """The host model of the rest of the background: conformal time by
+    DOP853 (rtol 1e-12), the optical depth by the trapezoid rule on 400 001
+    points, lna_rec and lna_transfer_start as background.py:552-564 finds
+    them.  abcmb_bg_forward produces the same quantities on the GPU with the
+    reference's own Kvaerno5 solves."""
+    p = bg.params
+    bg.tau_tab = _tabulate_tau(p, bg.has_ncdm)
+    bg.tau0 = float(fast_interp(0.0, -33.0, 0.0, bg.tau_tab))
     # optical depth kappa(lna) = int_lna^0 dl / (tau_c aH), on a fine grid
     lk = np.linspace(-10.0, 0.0, 400001)
     integrand = 1.0 / (bg.tau_c(lk) * bg.aH(lk))
@@ -328,3 +363,9 @@ def make_background(params: dict, has_ncdm: bool, xe_pad: int = 37, tm_pad: int 
     lt = np.linspace(-15.0, -6.0, 5000)
     bg.lna_transfer_start = float(lt[np.argmin((bg.aH(lt) * bg.tau_c(lt) - 0.008) ** 2)])
     return bg
+
+
+def make_background(params: dict, has_ncdm: bool, xe_pad: int = 37, tm_pad: int = 29) -> BackgroundTables:
+    """Synthetic Background for one cosmology (derived params dict in), all
+    of it on the host."""
+    return complete_on_host(make_recombination(params, has_ncdm, xe_pad, tm_pad))

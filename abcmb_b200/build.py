@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libabcmb_b200.so")
-SOURCES = ["capi.cu", "pert.cu", "los.cu", "lens.cu", "probe.cu", "pert_noalloc.cu"]
+SOURCES = ["capi.cu", "bg.cu", "pert.cu", "los.cu", "lens.cu", "probe.cu", "pert_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

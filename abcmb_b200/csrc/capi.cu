@@ -28,6 +28,9 @@ cudaError_t launch_los_vjp(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcm
                            const abcmb_los_settings& ls, int n_save, const BesselDev& B, const double* cl_bar,
                            double* pt_bar, double* param_bar, void* ws, cudaStream_t stream);
 int64_t lens_workspace_bytes(int n_cosmo, const abcmb_lens_settings& s);
+int64_t bg_workspace_bytes(int n_cosmo, const abcmb_bg_settings& s);
+cudaError_t launch_bg(int n_cosmo, abcmb_cosmo* cosmo, double* tables, const abcmb_bg_settings& s,
+                      abcmb_bgstat* stat, void* ws, cudaStream_t stream);
 cudaError_t launch_lens(int n_cosmo, const abcmb_cosmo* cosmo, const abcmb_lens_cosmo* lens, const double* tables,
                         const double* kbuf, const double* pt, const double* mu, const double* w,
                         const double* cl_unl, const abcmb_lens_settings& s, double* clpp, double* cl, void* ws,
@@ -121,6 +124,34 @@ int abcmb_upload_bessel(int n_l, int n_x, const int32_t* l_tab, const double* xm
   bc->mem = mem;
   bc->dev = abcmb::BesselDev{n_l, n_x, dl, dxmin, dxmax, dphi};
   bc->ready = true;
+  return ABCMB_OK;
+}
+
+// the two solves' step limits: positive and small enough that the node
+// buffers stay a modest workspace (diffrax accepts any positive max_steps)
+constexpr int BG_MAX_STEPS_LIMIT = 1 << 20;
+
+static bool bg_settings_ok(const abcmb_bg_settings* s) {
+  return s && s->n_save >= 3 && s->max_steps_tau >= 1 && s->max_steps_kappa >= 1 &&
+         s->max_steps_tau <= BG_MAX_STEPS_LIMIT && s->max_steps_kappa <= BG_MAX_STEPS_LIMIT;
+}
+
+int64_t abcmb_bg_workspace_size(int n_cosmo, const abcmb_bg_settings* settings) {
+  if (n_cosmo <= 0 || !bg_settings_ok(settings)) return -1;
+  return abcmb::bg_workspace_bytes(n_cosmo, *settings);
+}
+
+int abcmb_bg_forward(int n_cosmo, abcmb_cosmo* cosmo_dev, double* tables_dev, const abcmb_bg_settings* settings,
+                     abcmb_bgstat* stat_dev, void* workspace_dev, int64_t workspace_bytes, void* stream) {
+  if (n_cosmo <= 0 || !cosmo_dev || !tables_dev || !stat_dev)
+    return fail(ABCMB_ERR_ARG, "abcmb_bg_forward: null argument or n_cosmo <= 0");
+  if (!bg_settings_ok(settings))
+    return fail(ABCMB_ERR_ARG, "abcmb_bg_forward: settings need n_save >= 3 and 1 <= max_steps <= 2^20");
+  const int64_t need = abcmb::bg_workspace_bytes(n_cosmo, *settings);
+  if (!workspace_dev || workspace_bytes < need) return fail(ABCMB_ERR_WORKSPACE, "abcmb_bg_forward: workspace");
+  cudaError_t e = abcmb::launch_bg(n_cosmo, cosmo_dev, tables_dev, *settings, stat_dev, workspace_dev,
+                                   static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "abcmb_bg_forward");
   return ABCMB_OK;
 }
 

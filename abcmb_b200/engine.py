@@ -13,7 +13,7 @@ import torch
 
 from . import _lib
 from . import bessel as bessel_mod
-from .packing import Batch, NFIELDS, CPertSettings, CLosSettings
+from .packing import Batch, NFIELDS, NTAU_TAB, CPertSettings, CLosSettings
 
 _uploaded_devices: set = set()
 
@@ -93,6 +93,54 @@ class DeviceBatch:
                                     _ptr(self.kstat), _ptr(self.ws_pert), self.ws_pert.numel(),
                                     ctypes.c_void_p(st.cuda_stream))
         _lib.check(rc, "abcmb_pert_forward")
+
+    def bg_forward(self, settings=None, stream=None, fetch_tables: bool = False) -> np.ndarray:
+        """abcmb_bg_forward on the whole batch: the conformal-time tables,
+        tau0, lna_transfer_start and line-of-sight arrays of every cosmology,
+        written into the device descriptors and tables.  Reads the
+        per-cosmology results back (one synchronisation), raises like diffrax
+        when a solve hit its step limit, and updates the host descriptors and
+        the batch's BackgroundTables (their tau table and line-of-sight
+        arrays too when fetch_tables is set).  Returns the BGSTAT_DTYPE
+        records."""
+        from .packing import BGSTAT_DTYPE, bg_settings
+        lib = _lib.load()
+        b = self.batch
+        s = settings if settings is not None else bg_settings(b.n_save)
+        if s.n_save != b.n_save:
+            raise ValueError("bg settings n_save differs from the batch's")
+        nws = int(lib.abcmb_bg_workspace_size(b.n_cosmo, ctypes.byref(s)))
+        if nws < 0:
+            raise ValueError("invalid abcmb_bg_settings")
+        ws = torch.empty(nws, dtype=torch.uint8, device=self.device)
+        stat = torch.zeros(b.n_cosmo * BGSTAT_DTYPE.itemsize, dtype=torch.uint8, device=self.device)
+        st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        rc = lib.abcmb_bg_forward(b.n_cosmo, _ptr(self.cosmo), _ptr(self.tables), ctypes.byref(s), _ptr(stat),
+                                  _ptr(ws), ws.numel(), ctypes.c_void_p(st.cuda_stream))
+        _lib.check(rc, "abcmb_bg_forward")
+        res = stat.cpu().numpy().view(BGSTAT_DTYPE).copy()
+        bad = np.nonzero(res["status"] != 0)[0]
+        if bad.size:
+            i = int(bad[0])
+            raise _lib.ABCMBError(
+                f"background of {bad.size} cosmologies failed; first: cosmology {i} status {int(res['status'][i])} "
+                f"after {int(res['n_steps_tau'][i])} conformal-time and {int(res['n_steps_kappa'][i])} "
+                f"optical-depth steps (1 = max_steps reached: raise max_steps_kappa / max_steps_tau, as for "
+                f"diffrax)")
+        b.cosmo["tau0"] = res["tau0"]
+        b.cosmo["lna_transfer_start"] = res["lna_transfer_start"]
+        tables = self.tables.cpu().numpy() if fetch_tables else None
+        nl = b.n_save - 1
+        for i, bg in enumerate(b.bgs):
+            if bg is None:
+                continue
+            c = b.cosmo[i]
+            tau_tab = los = None
+            if tables is not None:
+                tau_tab = tables[int(c["off_tau"]):int(c["off_tau"]) + NTAU_TAB]
+                los = tables[int(c["off_los"]):int(c["off_los"]) + 6 * nl].reshape(6, nl)
+            bg.set_device_result(tau_tab, los, res[i])
+        return res
 
     def kstat_host(self) -> np.ndarray:
         from .packing import KSTAT_DTYPE

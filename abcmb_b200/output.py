@@ -6,9 +6,13 @@
 * ``B200Model(user_species=None, **specs)(params) -> Output`` mirrors
   ``Model.__init__`` / ``Model.__call__`` (main.py:84-184, 289-298): specs
   with the reference's defaults, the reference's k grids, the perturbation and
-  spectrum stages on the CUDA kernels.  The background and recombination
-  history come from ``background_tables.make_background`` (the host model
-  that stands in for the reference's JAX background and HyRex here).
+  spectrum stages on the CUDA kernels.  The recombination history (x_e, T_m,
+  z_reion) comes from ``background_tables.make_recombination``, the host
+  model that stands in for HyRex here; the conformal-time table, optical
+  depth, visibility and line-of-sight arrays are then produced on the GPU by
+  abcmb_bg_forward with the reference's own Kvaerno5 solves
+  (``background="device"``, the default), or by the host model
+  (``background="host"``).
 * ``write_class_cl`` / ``read_class_cl``: C_l files in CLASS's ``cl.dat``
   layout (dimensionless l(l+1)/2pi C_l, columns l, TT, EE, TE, BB, phiphi),
   the format the reference's example notebooks compare against
@@ -53,7 +57,10 @@ def _species_names(user_species) -> tuple:
 class B200Model:
     """Model(**specs)(params) on the CUDA path (abcmb/main.py:84-184)."""
 
-    def __init__(self, user_species=None, device=None, **kwargs):
+    def __init__(self, user_species=None, device=None, background: str = "device", **kwargs):
+        if background not in ("device", "host"):
+            raise ValueError("background must be 'device' or 'host'")
+        self.background = background
         specs = sp.load_specs(kwargs)
         self.specs = specs
         self.species = _species_names(user_species)
@@ -72,7 +79,7 @@ class B200Model:
 
     def __call__(self, params: dict) -> Output:
         p = self.add_derived_parameters(params)
-        BG = bt.make_background(p, self.has_ncdm)
+        BG = (bt.make_recombination if self.background == "device" else bt.make_background)(p, self.has_ncdm)
         PT = self.PE.full_evolution((BG, p))
         tt, te, ee = self.SS.get_Cl(PT, BG, p)
         Pk = self.SS.Pk_lin(self.k_axis_Pk_output, 0.0, PT, p)

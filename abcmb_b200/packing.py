@@ -13,6 +13,7 @@ import numpy as np
 from .specs import StateLayout
 
 NFIELDS = 21
+NTAU_TAB = 10000        # ABCMB_NTAU_TAB
 FIELD_NAMES = (
     "delta_m", "theta_b_prime", "metric_eta", "metric_h_prime", "metric_eta_prime",
     "metric_alpha", "metric_alpha_prime", "cdm_delta", "b_delta", "b_theta",
@@ -58,6 +59,25 @@ class CLensSettings(ctypes.Structure):
 
 
 LENS_DTYPE = np.dtype([("lna_rec", "<f8"), ("omega_m", "<f8")], align=True)
+
+
+class CBgSettings(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in ["n_save", "max_steps_tau", "max_steps_kappa", "pad_"]]
+
+
+BGSTAT_DTYPE = np.dtype([("status", "<i4"), ("n_steps_tau", "<i4"), ("n_steps_kappa", "<i4"),
+                         ("n_accepted_kappa", "<i4"), ("tau0", "<f8"), ("lna_rec", "<f8"),
+                         ("lna_transfer_start", "<f8"), ("kappa_rec", "<f8")], align=True)
+
+# diffeqsolve's default max_steps (the conformal-time solve passes none,
+# background.py:286-297) and the optical-depth solve's own (background.py:714)
+BG_MAX_STEPS_TAU = 4096
+BG_MAX_STEPS_KAPPA = 2048
+
+
+def bg_settings(n_save: int = 500, max_steps_tau: int = BG_MAX_STEPS_TAU,
+                max_steps_kappa: int = BG_MAX_STEPS_KAPPA) -> CBgSettings:
+    return CBgSettings(n_save=n_save, max_steps_tau=max_steps_tau, max_steps_kappa=max_steps_kappa, pad_=0)
 
 KSTAT_DTYPE = np.dtype([("status", "<i4"), ("n_accepted", "<i4"), ("n_rejected", "<i4"),
                         ("n_newton", "<i4"), ("lna_start", "<f8")], align=True)
@@ -151,8 +171,11 @@ def pack(bgs, layouts, kgrids, n_save: int = 500, order: str = "cost", alias_of=
                      "N_nu_massless", "T_nu_massless", "N_nu_massive", "T_nu_massive", "m_nu_massive",
                      "R_nu", "R_b", "om"]:
             r[name] = float(p[name])
-        r["tau0"] = bg.tau0
-        r["lna_transfer_start"] = bg.lna_transfer_start
+        # a background without its conformal-time table is completed on the
+        # device (abcmb_bg_forward): zero placeholders until then
+        pending = bg.tau_tab is None
+        r["tau0"] = 0.0 if pending else bg.tau0
+        r["lna_transfer_start"] = 0.0 if pending else bg.lna_transfer_start
         nxe = bg.xe_arr.shape[0]
         ntm = bg.tm_arr.shape[0]
         r["lna_xe0"] = bg.lna_xe0
@@ -164,9 +187,10 @@ def pack(bgs, layouts, kgrids, n_save: int = 500, order: str = "cost", alias_of=
         r["lna_tm_max"] = bg.lna_tm0 + ntm * bg.lna_tm_dx
         r["lna_tm_last"] = bg.lna_tm_last
         r["tm_last"] = bg.tm_last
-        los = bg.los_arrays(n_save)
+        los = np.zeros((6, nl)) if pending else bg.los_arrays(n_save)
+        tau_tab = np.zeros(NTAU_TAB) if pending else bg.tau_tab
         r["off_tau"] = off
-        chunks.append(bg.tau_tab); off += bg.tau_tab.shape[0]
+        chunks.append(tau_tab); off += tau_tab.shape[0]
         r["off_xe"] = off
         chunks.append(bg.xe_arr); off += nxe
         r["off_tm"] = off

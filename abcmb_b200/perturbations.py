@@ -7,7 +7,10 @@ theta_b_prime, metric_eta, metric_h_prime, metric_eta_prime, metric_alpha,
 metric_alpha_prime and species_perturbations -- computed by the CUDA kernels
 (abcmb_pert_forward).  The background comes in as a
 `background_tables.BackgroundTables` (the tables the reference's
-BackgroundPreRecomb / HyRex / Background produce).  Only the six shipped
+BackgroundPreRecomb / HyRex / Background produce); one that carries only the
+x_e / T_m history (``background_tables.make_recombination``) is completed on
+the GPU first (abcmb_bg_forward: conformal time, optical depth, visibility,
+line-of-sight arrays).  Only the six shipped
 species are supported; any other species tuple raises, as the CUDA path
 cannot compile arbitrary Python right-hand sides.
 """
@@ -85,6 +88,9 @@ class B200PerturbationEvolver:
         self.k_axis_perturbations = np.asarray(k_axis_perturbations, dtype=np.float64)
         self.layout = sp.state_layout(self.specs, self.has_ncdm)
         self.device = device
+        # step limits of the two background solves run on the GPU when BG
+        # carries only x_e / T_m (background.py:286-297 default, :714)
+        self.bg_max_steps = dict(max_steps_tau=packing.BG_MAX_STEPS_TAU, max_steps_kappa=packing.BG_MAX_STEPS_KAPPA)
 
     def full_evolution(self, args, n_save: int = 500) -> PerturbationTable:
         """args = (BG, params): BG a BackgroundTables; params unused beyond BG.params."""
@@ -92,6 +98,10 @@ class B200PerturbationEvolver:
         batch = packing.pack([BG], [self.layout], [self.k_axis_perturbations], n_save=n_save)
         st = packing.pert_settings(self.specs, n_save, batch)
         db = engine.DeviceBatch.upload(batch, self.device)
+        if getattr(BG, "on_device", False):
+            # x_e / T_m only: conformal time, optical depth and the
+            # line-of-sight arrays come from abcmb_bg_forward
+            db.bg_forward(packing.bg_settings(n_save, **self.bg_max_steps), fetch_tables=True)
         db.pert_forward(st)
         ks = db.check_status()
         fields = batch.pt_view(db.pt.cpu().numpy(), 0)

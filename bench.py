@@ -18,6 +18,7 @@ produced on the host before timing (they are inputs of this path).
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -176,6 +177,52 @@ def plain_gpu_fwd_fd(gw, w, dev, stream, want_dns=True):
             "sample": f"first cosmology of the batch, its {gw.n_var} variants each run alone (own perturbation "
                       f"launch over its {int(b.cosmo['nk'][0])} k modes + own line of sight + C_l read back), "
                       f"this library's kernels"}
+
+
+def bg_forward_timing(gw, db, dev, stream):
+    """The GPU background producer (abcmb_bg_forward: conformal-time table,
+    optical depth, visibility, line-of-sight arrays by the reference's
+    Kvaerno5 solves) over every cosmology of the batch, outside the timed
+    step: on clones of the descriptors and tables, so the step's inputs stay
+    those of the host model.  Beside it, the host model of the same
+    quantities (complete_on_host) on two cosmologies."""
+    import ctypes
+    import torch
+    from abcmb_b200 import _lib, background_tables as bt, packing
+    lib = _lib.load()
+    n = db.batch.n_cosmo
+    # one C4 cosmology in 64 needs 2084 optical-depth steps with this
+    # recombination history, above the reference's 2048
+    s = packing.bg_settings(db.batch.n_save, max_steps_kappa=4096)
+    cos = db.cosmo.clone()
+    tab = db.tables.clone()
+    ws = torch.empty(int(lib.abcmb_bg_workspace_size(n, ctypes.byref(s))), dtype=torch.uint8, device=dev)
+    stat = torch.zeros(n * packing.BGSTAT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+
+    def once():
+        _lib.check(lib.abcmb_bg_forward(n, ctypes.c_void_p(cos.data_ptr()), ctypes.c_void_p(tab.data_ptr()),
+                                        ctypes.byref(s), ctypes.c_void_p(stat.data_ptr()),
+                                        ctypes.c_void_p(ws.data_ptr()), ws.numel(),
+                                        ctypes.c_void_p(stream.cuda_stream)), "abcmb_bg_forward")
+
+    once()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(3):
+        once()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / 3
+    res = stat.cpu().numpy().view(packing.BGSTAT_DTYPE)
+    t = time.perf_counter()
+    for bg in gw.batch.bgs[:2]:
+        bt.complete_on_host(dataclasses.replace(bg))
+    host_ms = (time.perf_counter() - t) * 1000.0 / 2
+    return {"ms": ms, "cosmologies": n, "us_per_cosmology": 1000.0 * ms / n, "max_steps_kappa": 4096,
+            "ok": int((res["status"] == 0).sum()), "kappa_steps_max": int(res["n_steps_kappa"].max()),
+            "tau_steps_max": int(res["n_steps_tau"].max()), "host_model_ms_per_cosmology": host_ms}
 
 
 def run_reference(args, rank, world):
@@ -370,6 +417,7 @@ def main():
             "clocks": clk.summary(), "items_per_step": int(b.n_items),
             "ode_steps_mean": float(steps_k.mean()), "host_build_s": t_build}
     if rank == 0 and world == 1:
+        line["bg_forward"] = bg_forward_timing(gw, db, dev, stream)
         plain = plain_gpu_fwd_fd(gw, w, dev, stream)
         plain["batched_over_plain"] = value / plain["value"]
         line["plain_gpu_fwd_fd"] = plain

@@ -182,6 +182,73 @@ int abcmb_upload_bessel(int n_l, int n_x, const int32_t* l_tab,
                         const double* xmin2, const double* xmax2, const double* phi2);
 
 /* ------------------------------------------------------------------------ */
+/* Background tables: Background / BackgroundPreRecomb (background.py)      */
+/* ------------------------------------------------------------------------ */
+
+/* Settings of abcmb_bg_forward. */
+typedef struct abcmb_bg_settings {
+  int32_t n_save;           /* PT save points (500): the line-of-sight arrays
+                               are written on linspace(lna_transfer_start, 0,
+                               n_save)[:-1] (spectrum.py:638-651)            */
+  int32_t max_steps_tau;    /* step attempts of the conformal-time solve
+                               (diffeqsolve's default 4096,
+                               background.py:285-296)                        */
+  int32_t max_steps_kappa;  /* step attempts of the optical-depth solve
+                               (2048, background.py:708-719)                 */
+  int32_t pad_;
+} abcmb_bg_settings;
+
+/* Per-cosmology result of abcmb_bg_forward. */
+typedef struct abcmb_bgstat {
+  int32_t status;           /* ABCMB_STATUS_* of both solves (MAX_STEPS when
+                               either reached its limit, as diffrax raises) */
+  int32_t n_steps_tau;      /* step attempts of the conformal-time solve     */
+  int32_t n_steps_kappa;    /* step attempts of the optical-depth solve      */
+  int32_t n_accepted_kappa;
+  double tau0;              /* BG.tau0 = BG.tau(0.) (background.py:89)       */
+  double lna_rec;           /* BG.lna_rec (background.py:554-557)            */
+  double lna_transfer_start;/* BG.lna_transfer_start (background.py:561-564) */
+  double kappa_rec;         /* optical depth at lna_rec                      */
+} abcmb_bgstat;
+
+/* Bytes of device workspace abcmb_bg_forward needs (the dense-output nodes
+ * of both solves, (max_steps + 1) x 3 doubles each per cosmology). */
+int64_t abcmb_bg_workspace_size(int n_cosmo, const abcmb_bg_settings* settings);
+
+/*
+ * Everything the perturbation and line-of-sight kernels read about the
+ * background that the reference derives from the x_e history, for every
+ * cosmology of the batch, from the descriptor parameters and the x_e / T_m
+ * tables already in tables_dev:
+ *  - the conformal-time table (ABCMB_NTAU_TAB values at off_tau): dtau/dlna =
+ *    1/aH integrated from lna = -16.1 (analytic radiation-era value before)
+ *    to 0 by Kvaerno5 + PIDController(rtol = atol = 1e-8), dt0 = 1e-5, dense
+ *    output (BackgroundPreRecomb._tabulate_conformal_time,
+ *    background.py:252-319), and tau0 = BG.tau(0.);
+ *  - the optical depth: dkappa/dlna = -1/(tau_c aH) from 0 down to -10 by
+ *    Kvaerno5 + PIDController(pcoeff 0.4, icoeff 0.3, rtol = atol = 1e-10),
+ *    dt0 = -1e-3, dense output (Background._tabulate_optical_depth,
+ *    background.py:682-720);
+ *  - lna_rec and lna_transfer_start (background.py:554-564);
+ *  - the six line-of-sight arrays at off_los: tau, g, dg/dlna (the derivative
+ *    of the visibility through the dense optical-depth solution, as jax.grad
+ *    takes it), aH, exp(-kappa), d(aH)/dtau (spectrum.py:640-651).
+ * Both right-hand sides are independent of the state, so each implicit stage
+ * of the very-chord solve settles on f(t_i) at its first iteration; the
+ * kernels take f(t_i) directly.
+ *   cosmo_dev  [n_cosmo]  in: parameters, x_e / T_m fields and offsets;
+ *                         out: tau0 and lna_transfer_start
+ *   tables_dev            in: x_e and T_m tables; out: tau table, LOS arrays
+ *   stat_dev   [n_cosmo]  per-cosmology status and scalars
+ * Replaces: the pre-recombination conformal-time table and the
+ * Background.__init__ steps after reionisation (background.py:88-89,
+ * 552-564) for the shipped species.
+ */
+int abcmb_bg_forward(int n_cosmo, abcmb_cosmo* cosmo_dev, double* tables_dev,
+                     const abcmb_bg_settings* settings, abcmb_bgstat* stat_dev,
+                     void* workspace_dev, int64_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Perturbations: PerturbationEvolver.full_evolution (perturbations.py:75)  */
 /* ------------------------------------------------------------------------ */
 

@@ -17,6 +17,10 @@
  *   background           abcmb/background.py:101-187 (rho_tot, H, aH,
  *                        aH_prime), 321-387 (tau, nH, TCMB), 568-680 (xe, Tm,
  *                        tau_c), hyrex/recomb_functions.py:127-153
+ *   background tables    abcmb/background.py:252-319 (conformal-time table,
+ *                        Kvaerno5 + PID, dense output), 682-720 (optical
+ *                        depth), 552-564 (lna_rec, lna_transfer_start),
+ *                        spectrum.py:640-651 (line-of-sight arrays)
  *   start time           abcmb/perturbations.py:119-159, 279
  *   initial conditions   abcmb/perturbations.py:161-199 + species y_ini
  *   RHS                  abcmb/perturbations.py:201-248 + species y_prime
@@ -1389,6 +1393,252 @@ int oracle_lens_forward(int n_cosmo, const abcmb_cosmo* cosmo, const abcmb_lens_
   return ABCMB_OK;
 }
 
+/* ---------------------------------------------------------------------- */
+/* background producer: conformal-time table, optical depth, visibility    */
+/* ---------------------------------------------------------------------- */
+
+/* Dense output of a scalar solve: the accepted points (s_j, y_j, f_j) in the
+ * solver's own time s = d t (d = -1 for a backward solve, as diffrax flips
+ * time), f = dy/ds. */
+typedef struct {
+  int n;
+  double* s;
+  double* y;
+  double* f;
+} dense_t;
+
+typedef double (*bg_rhs_fn)(const abcmb_cosmo* c, const double* tables, double lna);
+
+static double rhs_dtau(const abcmb_cosmo* c, const double* tables, double lna) {
+  (void)tables;
+  return 1. / oracle_aH(c, lna);                               /* background.py:231-250 */
+}
+
+static double rhs_dkappa(const abcmb_cosmo* c, const double* tables, double lna) {
+  return -1. / oracle_tau_c(c, tables, lna) / oracle_aH(c, lna); /* background.py:704 */
+}
+
+/* diffeqsolve(ODETerm(f), Kvaerno5(), t0, t1, dt0, y0, PIDController(...),
+ * SaveAt(dense=True), max_steps) for a right-hand side f(t) that does not
+ * depend on y (background.py:286-297, 708-719).  With a constant Jacobian
+ * of zero the very-chord iteration of every implicit stage returns f(t_i)
+ * (its second iteration finds a zero update), so each stage derivative is f
+ * at the stage time; the step, error estimate, PID controller and end
+ * clipping are those of solve_k.  Returns an ABCMB_STATUS_* code; *nsteps =
+ * step attempts, d->n = accepted points (including the initial one). */
+static int quad_solve(bg_rhs_fn f, const abcmb_cosmo* c, const double* tables, double t0, double t1,
+                      double y0, double dt0, double rtol, double atol, double pcoeff, double icoeff,
+                      double dcoeff, int max_steps, dense_t* d, int* nsteps_out) {
+  const double dir = t1 < t0 ? -1. : 1.;
+  const double err_order = 5.0, safety = 0.9, factormin = 0.2, factormax = 10.0;
+  const double coeff1 = (icoeff + pcoeff + dcoeff) / err_order;
+  const double coeff2 = -(pcoeff + 2. * dcoeff) / err_order;
+  const double coeff3 = dcoeff / err_order;
+  const double s_end = dir * t1;
+  double s0 = dir * t0;
+  double s1 = s0 + dir * dt0;
+  if (s1 > s_end) s1 = s_end;
+  double y = y0;
+  double F[7];
+  F[0] = dir * f(c, tables, dir * s0);
+  double prev_inv = 1.0, prev_prev_inv = 1.0;
+  int status = ABCMB_STATUS_OK, nsteps = 0;
+  d->n = 1;
+  d->s[0] = s0; d->y[0] = y; d->f[0] = F[0];
+  while (s0 < s_end) {
+    if (nsteps >= max_steps) { status = ABCMB_STATUS_MAX_STEPS; break; }
+    nsteps++;
+    const double h = s1 - s0;
+    for (int i = 1; i < 7; ++i) F[i] = dir * f(c, tables, dir * (s0 + KV_C[i] * h));
+    double acc = 0., acce = 0.;
+    for (int j = 0; j < 6; ++j) {
+      acc += KV_A[6][j] * F[j];
+      acce += (KV_A[6][j] - KV_A[5][j]) * F[j];
+    }
+    acc += KV_GAMMA * F[6];
+    acce += -KV_GAMMA * F[5] + KV_GAMMA * F[6];
+    const double y1 = y + h * acc;
+    const double err = h * acce;
+    const double sc_y = fabs(y) > fabs(y1) ? fabs(y) : fabs(y1);
+    double scaled = fabs(err / (atol + rtol * sc_y));
+    if (!isfinite(scaled)) scaled = INFINITY;
+    const int keep = scaled < 1.0;
+    double inv = 1.0 / scaled;
+    double f1v = (coeff1 == 0.) ? 1. : pow(inv, coeff1);
+    double f2v = (coeff2 == 0.) ? 1. : pow(prev_inv, coeff2);
+    double f3v = (coeff3 == 0.) ? 1. : pow(prev_prev_inv, coeff3);
+    double fmn = keep ? 1.0 : factormin;
+    double factor = safety * f1v * f2v * f3v;
+    if (factor < fmn) factor = fmn;
+    if (factor > factormax) factor = factormax;
+    const double dt_new = h * factor;
+    if (inv == 0. || isinf(inv)) inv = 1.;
+    if (keep) {
+      d->s[d->n] = s1; d->y[d->n] = y1; d->f[d->n] = F[6];
+      d->n++;
+      prev_prev_inv = prev_inv;
+      prev_inv = inv;
+      y = y1;
+      F[0] = F[6];                                        /* FSAL */
+      s0 = s1;
+    }
+    if (s0 >= s_end) break;
+    double sn = s0 + dt_new;
+    if (sn > s_end - 1e-10) sn = keep ? s_end : s0 + 0.5 * (s_end - s0);
+    s1 = sn;
+    if (!(h > 1e-14) || !isfinite(s1)) { status = ABCMB_STATUS_DT_UNDERFLOW; break; }
+  }
+  *nsteps_out = nsteps;
+  return status;
+}
+
+/* sol.evaluate(t) and its t-derivative: the cubic Hermite interpolation
+ * (ThirdOrderHermitePolynomialInterpolation, coefficients [a, b, k0, y0] in
+ * the step fraction, k = h f) of the step interval holding t, chosen as
+ * DenseInterpolation does: the first point s_i >= s (searchsorted, side
+ * left) closes the interval, clipped to the first and last intervals. */
+static double dense_eval(const dense_t* d, double dir, double t, double* dydt) {
+  const double s = dir * t;
+  int lo = 0, hi = d->n;                         /* first index with s_i >= s */
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (d->s[mid] < s) lo = mid + 1; else hi = mid;
+  }
+  int j = lo - 1;
+  if (j < 0) j = 0;
+  if (j > d->n - 2) j = d->n - 2;
+  const double h = d->s[j + 1] - d->s[j];
+  const double y0 = d->y[j], y1 = d->y[j + 1];
+  const double k0 = h * d->f[j], k1 = h * d->f[j + 1];
+  const double a = k0 + k1 + 2. * y0 - 2. * y1;
+  const double b = -2. * k0 - k1 - 3. * y0 + 3. * y1;
+  const double th = (s - d->s[j]) / h;
+  if (dydt) *dydt = dir * ((3. * a * th + 2. * b) * th + k0) / h;
+  return ((a * th + b) * th + k0) * th + y0;
+}
+
+/* d x_e / d lna as jax.grad takes it through BG.xe (background.py:593-603)
+ * and fast_interp (ABCMBTools.py:300-308): zero outside the table and where
+ * the index is clipped. */
+static double xe_slope(const abcmb_cosmo* c, const double* tables, double lna) {
+  if (lna < c->lna_xe0 || lna >= c->lna_xe_last) return 0.;
+  const int n = c->n_xe;
+  const double di = 1. / (c->lna_xe_max - c->lna_xe0) * (double)(n - 1);
+  double i = (lna - c->lna_xe0) * di;
+  if (!(i > 1.e-6 && i < (double)(n - 1) - 1.e-6)) return 0.;
+  int il = (int)floor(i);
+  int iu = il + 1 < n - 1 ? il + 1 : n - 1;
+  const double* fp = tables + c->off_xe;
+  return (fp[iu] - fp[il]) * di;
+}
+
+/* omega_r (main.py:581-586): every species' density at a = e^-23 times a^4. */
+static double omega_r_of(const abcmb_cosmo* c) {
+  const double lna = -23.0, a = exp(lna);
+  double rt, pt;
+  rho_P_tot(c, lna, &rt, &pt, 0, 0, 0, 0, 0, 0);
+  return rt * a * a * a * a / RHO_CRIT_UNIT;
+}
+
+/* One cosmology of abcmb_bg_forward: conformal-time table and tau0
+ * (background.py:252-319, 88-89), optical depth (682-720), lna_rec and
+ * lna_transfer_start (552-564), the line-of-sight arrays of Cl_one_ell
+ * (spectrum.py:640-651). */
+static int bg_one(abcmb_cosmo* c, double* tables, const abcmb_bg_settings* s, abcmb_bgstat* st,
+                  dense_t* dt, dense_t* dk) {
+  memset(st, 0, sizeof(*st));
+  const double lna_cut = -16.1;
+  const double tscale = H0H / C_MPC;                 /* H0_over_h / c_Mpc_over_s */
+  const double sq_or = sqrt(omega_r_of(c));
+  /* conformal time: analytic before lna_cut, Kvaerno5 after */
+  const double tau_cut = exp(lna_cut) / tscale / sq_or;
+  int st_tau = quad_solve(rhs_dtau, c, tables, lna_cut, 0.0, tau_cut, 1e-5, 1e-8, 1e-8, 0., 1., 0.,
+                          s->max_steps_tau, dt, &st->n_steps_tau);
+  int st_kap = quad_solve(rhs_dkappa, c, tables, 0.0, -10.0, 0.0, -1e-3, 1e-10, 1e-10, 0.4, 0.3, 0.,
+                          s->max_steps_kappa, dk, &st->n_steps_kappa);
+  st->n_accepted_kappa = dk->n - 1;
+  st->status = st_tau != ABCMB_STATUS_OK ? st_tau : st_kap;
+  if (st->status != ABCMB_STATUS_OK) return st->status;
+  double* tab = tables + c->off_tau;
+  for (int i = 0; i < ABCMB_NTAU_TAB; ++i) {
+    const double l = linspace_at(ABCMB_LNA_TAU_MIN, ABCMB_LNA_TAU_MAX, ABCMB_NTAU_TAB, i);
+    const double ap = exp(l) / tscale / sq_or;
+    double v = l > lna_cut ? dense_eval(dt, 1., l, 0) : ap;
+    tab[i] = isfinite(v) ? v : ap;
+  }
+  c->tau0 = oracle_tau(c, tables, 0.);
+  st->tau0 = c->tau0;
+  /* visibility maximum (first index of the max) on linspace(-8, -4, 1500) */
+  int imax = 0;
+  double vmax = -INFINITY;
+  for (int i = 0; i < 1500; ++i) {
+    const double l = linspace_at(-8.0, -4.0, 1500, i);
+    const double g = exp(-dense_eval(dk, -1., l, 0)) / oracle_tau_c(c, tables, l);
+    if (g > vmax) { vmax = g; imax = i; }
+  }
+  st->lna_rec = linspace_at(-8.0, -4.0, 1500, imax);
+  st->kappa_rec = dense_eval(dk, -1., st->lna_rec, 0);
+  /* first lna of linspace(-15, -6, 5000) minimising (aH tau_c - 0.008)^2 */
+  int imin = 0;
+  double vmin = INFINITY;
+  for (int i = 0; i < 5000; ++i) {
+    const double l = linspace_at(-15.0, -6.0, 5000, i);
+    const double q = oracle_aH(c, l) * oracle_tau_c(c, tables, l) - 0.008;
+    if (q * q < vmin) { vmin = q * q; imin = i; }
+  }
+  c->lna_transfer_start = linspace_at(-15.0, -6.0, 5000, imin);
+  st->lna_transfer_start = c->lna_transfer_start;
+  /* the six 1-D arrays of Cl_one_ell on PT.lna[:-1] */
+  const int nl = s->n_save - 1;
+  double* los = tables + c->off_los;
+  for (int i = 0; i < nl; ++i) {
+    const double l = linspace_at(c->lna_transfer_start, 0.0, s->n_save, i);
+    const double aH = oracle_aH(c, l);
+    const double tc = oracle_tau_c(c, tables, l);
+    double em = 0., g = 0., gp = 0.;
+    if (!(l < -10.)) {
+      double dkap;
+      const double kap = dense_eval(dk, -1., l, &dkap);
+      em = exp(-kap);
+      g = em / tc;
+      gp = g * (-dkap - 2. + xe_slope(c, tables, l) / oracle_xe(c, tables, l));
+    }
+    los[0 * nl + i] = oracle_tau(c, tables, l);
+    los[1 * nl + i] = g;
+    los[2 * nl + i] = gp;
+    los[3 * nl + i] = aH;
+    los[4 * nl + i] = em;
+    los[5 * nl + i] = oracle_aH_prime(c, l) * aH;
+  }
+  return ABCMB_STATUS_OK;
+}
+
+int oracle_bg_forward(int n_cosmo, abcmb_cosmo* cosmo, double* tables, const abcmb_bg_settings* s,
+                      abcmb_bgstat* stat, int n_threads) {
+  if (n_cosmo <= 0 || !cosmo || !tables || !s || !stat || s->n_save < 3 || s->max_steps_tau < 1 ||
+      s->max_steps_kappa < 1)
+    return ABCMB_ERR_ARG;
+#ifdef _OPENMP
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+#else
+  (void)n_threads;
+#endif
+  int bad = 0;
+#pragma omp parallel reduction(+ : bad)
+  {
+    dense_t dt, dk;
+    const int nt = s->max_steps_tau + 1, nk = s->max_steps_kappa + 1;
+    dt.s = (double*)malloc(sizeof(double) * 3 * nt); dt.y = dt.s + nt; dt.f = dt.y + nt;
+    dk.s = (double*)malloc(sizeof(double) * 3 * nk); dk.y = dk.s + nk; dk.f = dk.y + nk;
+#pragma omp for schedule(dynamic, 1)
+    for (int ci = 0; ci < n_cosmo; ++ci)
+      if (bg_one(&cosmo[ci], tables, s, &stat[ci], &dt, &dk) != ABCMB_STATUS_OK) bad++;
+    free(dt.s);
+    free(dk.s);
+  }
+  return bad ? ABCMB_ERR_SOLVER : ABCMB_OK;
+}
+
 /* sizeof of the C-ABI records, so tests can check the Python layouts. */
 int oracle_sizeof(int which) {
   switch (which) {
@@ -1398,6 +1648,8 @@ int oracle_sizeof(int which) {
     case 3: return (int)sizeof(abcmb_los_settings);
     case 4: return (int)sizeof(abcmb_lens_cosmo);
     case 5: return (int)sizeof(abcmb_lens_settings);
+    case 6: return (int)sizeof(abcmb_bg_settings);
+    case 7: return (int)sizeof(abcmb_bgstat);
   }
   return -1;
 }

@@ -63,6 +63,8 @@ def lib():
         L.oracle_los_forward.restype = ctypes.c_int
         L.oracle_los_forward.argtypes = [ctypes.c_int, vp, _dp, _dp, _dp, _dp, vp, ctypes.c_int,
                                          ctypes.POINTER(COracleBessel), _dp, _dp, ctypes.c_int]
+        L.oracle_bg_forward.restype = ctypes.c_int
+        L.oracle_bg_forward.argtypes = [ctypes.c_int, vp, _dp, vp, vp, ctypes.c_int]
         L.oracle_pk_lin.restype = ctypes.c_int
         L.oracle_pk_lin.argtypes = [ctypes.c_int, vp, _dp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                     _dp, ctypes.c_int, _dp, _dp]
@@ -159,3 +161,16 @@ def lens_forward(batch, pt, lens, mu, w, cl_unl, settings, n_threads: int = 0):
                                    dptr(pt), dptr(mu), dptr(w), dptr(cl_unl), ctypes.byref(settings),
                                    dptr(clpp), dptr(cl), n_threads)
     return rc, clpp.reshape(n, nl), cl.reshape(n, 3, settings.l_max - 1)
+
+
+def bg_forward(batch, settings, n_threads: int = 0):
+    """Oracle background producer on a packed Batch whose x_e / T_m tables are
+    filled: (rc, cosmo, tables, stat) with new copies of the descriptors and
+    tables (tau table, tau0, lna_transfer_start, line-of-sight arrays)."""
+    from abcmb_b200.packing import BGSTAT_DTYPE
+    cosmo = np.ascontiguousarray(batch.cosmo).copy()
+    tables = np.ascontiguousarray(batch.tables, dtype=np.float64).copy()
+    stat = np.zeros(batch.n_cosmo, dtype=BGSTAT_DTYPE)
+    rc = lib().oracle_bg_forward(batch.n_cosmo, vptr(cosmo), dptr(tables), ctypes.byref(settings), vptr(stat),
+                                 n_threads)
+    return rc, cosmo, tables, stat

@@ -1,0 +1,201 @@
+"""Background producer: conformal-time table, optical depth, visibility and
+the line-of-sight arrays (abcmb_bg_forward against the oracle's restatement of
+background.py:252-319, 552-564, 682-768 and spectrum.py:640-651).
+
+CPU tests pin the oracle against the host model, an independent method
+(DOP853 at rtol 1e-12 for the conformal time, a 400 001-point trapezoid for
+the optical depth); GPU tests compare the kernel with the oracle."""
+import ctypes
+import dataclasses
+
+import numpy as np
+import pytest
+
+from abcmb_b200 import background_tables as bt, configs, cosmology, packing
+from abcmb_b200 import specs as sp
+
+
+def _recombination_batch(n_cosmo=3, nk=12):
+    """C4 draws (both with and without massive neutrinos), x_e / T_m only."""
+    w = configs.c4(n_cosmo=n_cosmo, nk_range=(nk, nk))
+    recs, lays, hosts = [], [], []
+    for p_in, ncdm in zip(w.params_in, w.has_ncdm):
+        p = cosmology.add_derived_parameters(p_in, ncdm, w.specs)
+        recs.append(bt.make_recombination(p, ncdm))
+        hosts.append(bt.complete_on_host(bt.make_recombination(p, ncdm)))
+        lays.append(sp.state_layout(w.specs, ncdm))
+    return w, packing.pack(recs, lays, w.kgrids), hosts, lays
+
+
+@pytest.fixture(scope="module")
+def rec_batch():
+    return _recombination_batch()
+
+
+def test_bg_record_sizes_match_the_header():
+    from oracle import oracle
+    assert oracle.lib().oracle_sizeof(6) == ctypes.sizeof(packing.CBgSettings) == 16
+    assert oracle.lib().oracle_sizeof(7) == packing.BGSTAT_DTYPE.itemsize == 48
+
+
+def test_pending_background_packs_placeholders(rec_batch):
+    w, b, hosts, _ = rec_batch
+    assert all(bg.on_device for bg in b.bgs)
+    assert (b.cosmo["tau0"] == 0).all() and (b.cosmo["lna_transfer_start"] == 0).all()
+    c = b.cosmo[0]
+    assert not b.tables[int(c["off_tau"]):int(c["off_tau"]) + packing.NTAU_TAB].any()
+    with pytest.raises(ValueError):
+        b.bgs[0].kappa(-5.0)
+
+
+def test_oracle_background_matches_host_model(rec_batch):
+    """The oracle's Kvaerno5 solves against the host model: the conformal-time
+    table agrees within the dense-output error of an rtol = 1e-8 solve
+    (cubic Hermite over steps of ~0.2 in lna: 2.6e-5 at the largest, just
+    after lna = -16.1), the scalars and line-of-sight arrays within the
+    optical-depth solve's tolerance."""
+    from oracle import oracle
+    w, b, hosts, _ = rec_batch
+    rc, cos, tab, st = oracle.bg_forward(b, packing.bg_settings(max_steps_kappa=4096))
+    assert rc == 0 and (st["status"] == 0).all()
+    # ~80 conformal-time steps; 1500-2100 optical-depth steps (the
+    # reference's own limit is 2048)
+    assert (st["n_steps_tau"] > 50).all() and (st["n_steps_tau"] < 200).all()
+    assert (st["n_steps_kappa"] > 1000).all() and (st["n_steps_kappa"] < 2600).all()
+    nl = b.n_save - 1
+    for i, h in enumerate(hosts):
+        c = cos[i]
+        tt = tab[int(c["off_tau"]):int(c["off_tau"]) + packing.NTAU_TAB]
+        np.testing.assert_allclose(tt, h.tau_tab, rtol=4e-5)
+        assert c["tau0"] == pytest.approx(h.tau0, rel=1e-8)
+        assert c["lna_transfer_start"] == h.lna_transfer_start
+        assert st[i]["lna_rec"] == h.lna_rec
+        assert st[i]["kappa_rec"] == pytest.approx(float(h.kappa(h.lna_rec)), rel=1e-6)
+        los = tab[int(c["off_los"]):int(c["off_los"]) + 6 * nl].reshape(6, nl)
+        ref = h.los_arrays(b.n_save)
+        tol = [5e-6, 1e-6, 1e-5, 1e-13, 1e-6, 1e-13]     # tau, g, g', aH, exp(-kappa), aH_dot
+        for j in range(6):
+            err = np.max(np.abs(los[j] - ref[j])) / np.max(np.abs(ref[j]))
+            assert err < tol[j], (i, j, err)
+
+
+def test_oracle_background_reports_max_steps(rec_batch):
+    from oracle import oracle
+    w, b, hosts, _ = rec_batch
+    rc, cos, tab, st = oracle.bg_forward(b, packing.bg_settings(max_steps_kappa=100))
+    assert rc == -5                                        # ABCMB_ERR_SOLVER
+    assert (st["status"] == 1).all() and (st["n_steps_kappa"] == 100).all()
+
+
+def test_bg_argument_errors_without_gpu():
+    from abcmb_b200 import _lib
+    lib = _lib.load()
+    s = packing.bg_settings(n_save=2)
+    assert lib.abcmb_bg_workspace_size(4, ctypes.byref(s)) == -1
+    s = packing.bg_settings()
+    assert lib.abcmb_bg_workspace_size(4, ctypes.byref(s)) == 4 * 3 * (4097 + 2049) * 8
+    rc = lib.abcmb_bg_forward(1, ctypes.c_void_p(8), ctypes.c_void_p(8), ctypes.byref(s), ctypes.c_void_p(8),
+                              ctypes.c_void_p(8), 0, None)
+    assert rc == -3 and b"workspace" in lib.abcmb_last_error()
+    bad = packing.bg_settings(max_steps_kappa=0)
+    rc = lib.abcmb_bg_forward(1, ctypes.c_void_p(8), ctypes.c_void_p(8), ctypes.byref(bad), ctypes.c_void_p(8),
+                              ctypes.c_void_p(8), 1 << 30, None)
+    assert rc == -1
+
+
+# --------------------------------------------------------------------------
+# GPU
+# --------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def gpu():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from abcmb_b200 import engine
+    return engine
+
+
+@pytest.mark.gpu
+def test_bg_forward_matches_oracle(gpu, rec_batch):
+    """abcmb_bg_forward against the oracle on the same x_e / T_m tables: the
+    same step sequences (step counts equal), tables and scalars to rounding."""
+    from oracle import oracle
+    w, b0, _, lays = rec_batch
+    b = packing.pack([dataclasses.replace(bg) for bg in b0.bgs], lays, w.kgrids)
+    s = packing.bg_settings(max_steps_kappa=4096)
+    rc, cos_o, tab_o, st_o = oracle.bg_forward(b, s)
+    assert rc == 0
+    db = gpu.DeviceBatch.upload(b)
+    st = db.bg_forward(s, fetch_tables=True)
+    for f in ("status", "n_steps_tau", "n_steps_kappa", "n_accepted_kappa"):
+        np.testing.assert_array_equal(st[f], st_o[f])
+    np.testing.assert_array_equal(st["lna_rec"], st_o["lna_rec"])
+    np.testing.assert_array_equal(st["lna_transfer_start"], st_o["lna_transfer_start"])
+    np.testing.assert_allclose(st["tau0"], st_o["tau0"], rtol=1e-13)
+    np.testing.assert_allclose(st["kappa_rec"], st_o["kappa_rec"], rtol=1e-12)
+    cos_d = db.cosmo.cpu().numpy().view(packing.COSMO_DTYPE)
+    np.testing.assert_allclose(cos_d["tau0"], cos_o["tau0"], rtol=1e-13)
+    np.testing.assert_array_equal(cos_d["lna_transfer_start"], cos_o["lna_transfer_start"])
+    tab_d = db.tables.cpu().numpy()
+    nl = b.n_save - 1
+    for i in range(b.n_cosmo):
+        c = cos_o[i]
+        sl = slice(int(c["off_tau"]), int(c["off_tau"]) + packing.NTAU_TAB)
+        np.testing.assert_allclose(tab_d[sl], tab_o[sl], rtol=1e-12)
+        lo = int(c["off_los"])
+        d = tab_d[lo:lo + 6 * nl].reshape(6, nl)
+        o = tab_o[lo:lo + 6 * nl].reshape(6, nl)
+        err = np.max(np.abs(d - o), axis=1) / np.max(np.abs(o), axis=1)
+        assert (err < 1e-10).all(), (i, err)
+        # x_e and T_m tables untouched
+        xo = int(c["off_xe"])
+        np.testing.assert_array_equal(tab_d[xo:xo + int(c["n_xe"])], b.tables[xo:xo + int(c["n_xe"])])
+    assert all(not bg.on_device for bg in b.bgs)
+
+
+@pytest.mark.gpu
+def test_bg_forward_step_limit_raises(gpu, rec_batch):
+    """A solve that reaches max_steps is reported per cosmology and raised,
+    like diffrax's max_steps error; the kernel stops at the limit."""
+    from abcmb_b200 import _lib
+    w, b0, _, lays = rec_batch
+    b = packing.pack([dataclasses.replace(bg) for bg in b0.bgs], lays, w.kgrids)
+    db = gpu.DeviceBatch.upload(b)
+    with pytest.raises(_lib.ABCMBError, match="max_steps"):
+        db.bg_forward(packing.bg_settings(max_steps_kappa=100))
+
+
+@pytest.mark.gpu
+def test_device_background_pipeline_matches_oracle(gpu):
+    """x_e / T_m in, C_l out, all on the GPU (abcmb_bg_forward, then the
+    perturbation and line-of-sight kernels) against the oracle's background,
+    perturbations and line of sight on the same recombination history."""
+    from abcmb_b200 import bessel
+    from oracle import oracle
+    w = configs.c1(nk=40, l_max=400)
+    p = cosmology.add_derived_parameters(w.params_in[0], False, w.specs)
+    lay = sp.state_layout(w.specs, False)
+    b = packing.pack([bt.make_recombination(p, False)], [lay], w.kgrids)
+    rc, cos_o, tab_o, _ = oracle.bg_forward(b, packing.bg_settings())
+    assert rc == 0
+    bo = packing.pack([bt.make_recombination(p, False)], [lay], w.kgrids)
+    bo.cosmo[:] = cos_o
+    bo.tables = tab_o
+    rc, pt_o, _ = oracle.pert_forward(bo, packing.pert_settings(w.specs, 500, bo))
+    assert rc == 0
+    ks = dict(w.specs)
+    sp.get_k_axis_perturbations(ks)
+    kt = sp.get_k_axis_transfer(ks)
+    B = bessel.load()
+    i0, i1, _ = sp.ell_index_range(B.l_tab, 2, 400, False)
+    ls = packing.los_settings(w.specs, i0, i1, len(kt), 400, n_save=500)
+    _, _, cl_o = oracle.los_forward(bo, pt_o, kt, ls, B)
+    db = gpu.DeviceBatch.upload(b)
+    db.bg_forward()
+    db.pert_forward(packing.pert_settings(w.specs, 500, b))
+    db.check_status()
+    lr = gpu.LosRunner(db, kt, ls)
+    lr.run()
+    cl = lr.cl_host()
+    err = np.max(np.abs(cl - cl_o) / np.abs(cl_o).max(axis=2, keepdims=True))
+    assert err < 1e-8, err
