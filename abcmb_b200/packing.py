@@ -72,7 +72,13 @@ BGSTAT_DTYPE = np.dtype([("status", "<i4"), ("n_steps_tau", "<i4"), ("n_steps_ka
 # diffeqsolve's default max_steps (the conformal-time solve passes none,
 # background.py:286-297) and the optical-depth solve's own (background.py:714)
 BG_MAX_STEPS_TAU = 4096
-BG_MAX_STEPS_KAPPA = 2048
+BG_MAX_STEPS_KAPPA_REFERENCE = 2048
+# The default here is twice the reference's: with the host recombination
+# history the optical-depth solve takes 1500-2200 steps, and its step
+# sequence changes with rounding-level differences of the integrand (the
+# kinks of the piecewise-linear x_e table drive the error estimate), so a
+# 2048 limit is within reach of rounding alone.
+BG_MAX_STEPS_KAPPA = 4096
 
 
 def bg_settings(n_save: int = 500, max_steps_tau: int = BG_MAX_STEPS_TAU,

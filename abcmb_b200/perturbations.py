@@ -89,7 +89,9 @@ class B200PerturbationEvolver:
         self.layout = sp.state_layout(self.specs, self.has_ncdm)
         self.device = device
         # step limits of the two background solves run on the GPU when BG
-        # carries only x_e / T_m (background.py:286-297 default, :714)
+        # carries only x_e / T_m (packing.BG_MAX_STEPS_TAU and
+        # BG_MAX_STEPS_KAPPA; the reference's optical-depth limit is
+        # BG_MAX_STEPS_KAPPA_REFERENCE = 2048, background.py:714)
         self.bg_max_steps = dict(max_steps_tau=packing.BG_MAX_STEPS_TAU, max_steps_kappa=packing.BG_MAX_STEPS_KAPPA)
 
     def full_evolution(self, args, n_save: int = 500) -> PerturbationTable:

@@ -194,7 +194,8 @@ typedef struct abcmb_bg_settings {
                                (diffeqsolve's default 4096,
                                background.py:285-296)                        */
   int32_t max_steps_kappa;  /* step attempts of the optical-depth solve
-                               (2048, background.py:708-719)                 */
+                               (the reference passes 2048,
+                               background.py:708-719)                        */
   int32_t pad_;
 } abcmb_bg_settings;
 

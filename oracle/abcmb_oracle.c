@@ -1613,6 +1613,30 @@ static int bg_one(abcmb_cosmo* c, double* tables, const abcmb_bg_settings* s, ab
   return ABCMB_STATUS_OK;
 }
 
+/* The optical-depth solve alone with its right-hand side scaled by
+ * rhs_scale: how far the reference's step sequence moves under a rounding-
+ * level change of the integrand.  Returns the status; *nsteps = attempts,
+ * *kappa_end = kappa(-10). */
+static double g_rhs_scale = 1.0;
+static double rhs_dkappa_scaled(const abcmb_cosmo* c, const double* tables, double lna) {
+  return g_rhs_scale * rhs_dkappa(c, tables, lna);
+}
+
+int oracle_kappa_solve(const abcmb_cosmo* c, const double* tables, double rhs_scale, int max_steps,
+                       int* nsteps, double* kappa_end) {
+  dense_t d;
+  d.s = (double*)malloc(sizeof(double) * 3 * (size_t)(max_steps + 1));
+  d.y = d.s + max_steps + 1;
+  d.f = d.y + max_steps + 1;
+  g_rhs_scale = rhs_scale;
+  int st = quad_solve(rhs_dkappa_scaled, c, tables, 0.0, -10.0, 0.0, -1e-3, 1e-10, 1e-10, 0.4, 0.3, 0.,
+                      max_steps, &d, nsteps);
+  g_rhs_scale = 1.0;
+  *kappa_end = d.y[d.n - 1];
+  free(d.s);
+  return st;
+}
+
 int oracle_bg_forward(int n_cosmo, abcmb_cosmo* cosmo, double* tables, const abcmb_bg_settings* s,
                       abcmb_bgstat* stat, int n_threads) {
   if (n_cosmo <= 0 || !cosmo || !tables || !s || !stat || s->n_save < 3 || s->max_steps_tau < 1 ||

@@ -54,6 +54,8 @@ int oracle_lens_forward(int n_cosmo, const abcmb_cosmo* cosmo, const abcmb_lens_
                         int n_threads);
 int oracle_bg_forward(int n_cosmo, abcmb_cosmo* cosmo, double* tables, const abcmb_bg_settings* s,
                       abcmb_bgstat* stat, int n_threads);
+int oracle_kappa_solve(const abcmb_cosmo* c, const double* tables, double rhs_scale, int max_steps,
+                       int* nsteps, double* kappa_end);
 int oracle_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* kbuf, const double* pt, int n_save,
                   double k_pivot, int n_kout, const double* kout, int n_z, const double* z, double* pk);
 

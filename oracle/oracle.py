@@ -65,6 +65,8 @@ def lib():
                                          ctypes.POINTER(COracleBessel), _dp, _dp, ctypes.c_int]
         L.oracle_bg_forward.restype = ctypes.c_int
         L.oracle_bg_forward.argtypes = [ctypes.c_int, vp, _dp, vp, vp, ctypes.c_int]
+        L.oracle_kappa_solve.restype = ctypes.c_int
+        L.oracle_kappa_solve.argtypes = [vp, _dp, ctypes.c_double, ctypes.c_int, _ip, _dp]
         L.oracle_pk_lin.restype = ctypes.c_int
         L.oracle_pk_lin.argtypes = [ctypes.c_int, vp, _dp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                     _dp, ctypes.c_int, _dp, _dp]
@@ -174,3 +176,14 @@ def bg_forward(batch, settings, n_threads: int = 0):
     rc = lib().oracle_bg_forward(batch.n_cosmo, vptr(cosmo), dptr(tables), ctypes.byref(settings), vptr(stat),
                                  n_threads)
     return rc, cosmo, tables, stat
+
+
+def kappa_solve(batch, ci: int, rhs_scale: float = 1.0, max_steps: int = 100000):
+    """(status, step attempts, kappa(-10)) of the optical-depth solve of
+    cosmology ci with its right-hand side scaled by rhs_scale."""
+    cos = np.ascontiguousarray(batch.cosmo[ci:ci + 1]).copy()
+    n = ctypes.c_int32(0)
+    k = np.zeros(1)
+    st = lib().oracle_kappa_solve(vptr(cos), dptr(batch.tables), float(rhs_scale), int(max_steps),
+                                  ctypes.byref(n), dptr(k))
+    return st, int(n.value), float(k[0])

@@ -87,13 +87,32 @@ def test_oracle_background_reports_max_steps(rec_batch):
     assert (st["status"] == 1).all() and (st["n_steps_kappa"] == 100).all()
 
 
+def test_optical_depth_solve_is_chaotic_under_rounding(rec_batch):
+    """The reference's optical-depth solve (Kvaerno5 + PID at rtol = atol =
+    1e-10 over the piecewise-linear x_e table, whose kinks every 5e-4 in lna
+    dominate the embedded error estimate) has no stable step sequence: a
+    relative change of the integrand at the rounding level moves the step
+    count by hundreds and kappa(-10) by ~1e-6 relative.  Two correct
+    implementations (or the reference on two backends) therefore agree on
+    the optical depth to that spread, not to rounding; the conformal-time
+    solve (smooth integrand) keeps its step sequence."""
+    from oracle import oracle
+    w, b, hosts, _ = rec_batch
+    st0, n0, k0 = oracle.kappa_solve(b, 0)
+    assert st0 == 0
+    runs = [oracle.kappa_solve(b, 0, 1.0 + e) for e in (2e-16, -2e-16, 1e-15, -1e-15)]
+    assert all(r[0] == 0 for r in runs)
+    assert max(abs(r[1] - n0) for r in runs) > 50
+    assert max(abs(r[2] / k0 - 1.0) for r in runs) < 1e-5
+
+
 def test_bg_argument_errors_without_gpu():
     from abcmb_b200 import _lib
     lib = _lib.load()
     s = packing.bg_settings(n_save=2)
     assert lib.abcmb_bg_workspace_size(4, ctypes.byref(s)) == -1
     s = packing.bg_settings()
-    assert lib.abcmb_bg_workspace_size(4, ctypes.byref(s)) == 4 * 3 * (4097 + 2049) * 8
+    assert lib.abcmb_bg_workspace_size(4, ctypes.byref(s)) == 4 * 3 * (4097 + 4097) * 8
     rc = lib.abcmb_bg_forward(1, ctypes.c_void_p(8), ctypes.c_void_p(8), ctypes.byref(s), ctypes.c_void_p(8),
                               ctypes.c_void_p(8), 0, None)
     assert rc == -3 and b"workspace" in lib.abcmb_last_error()
@@ -117,8 +136,12 @@ def gpu():
 
 @pytest.mark.gpu
 def test_bg_forward_matches_oracle(gpu, rec_batch):
-    """abcmb_bg_forward against the oracle on the same x_e / T_m tables: the
-    same step sequences (step counts equal), tables and scalars to rounding."""
+    """abcmb_bg_forward against the oracle on the same x_e / T_m tables.  The
+    conformal-time solve follows the same step sequence (step counts equal,
+    table to rounding); the optical-depth solve is chaotic under rounding
+    (test_optical_depth_solve_is_chaotic_under_rounding), so its step count
+    and the quantities drawn from it agree to that spread: exp(-kappa) and g
+    within 1e-6 of their maxima, g' within 2e-5, kappa(lna_rec) within 5e-6."""
     from oracle import oracle
     w, b0, _, lays = rec_batch
     b = packing.pack([dataclasses.replace(bg) for bg in b0.bgs], lays, w.kgrids)
@@ -127,12 +150,13 @@ def test_bg_forward_matches_oracle(gpu, rec_batch):
     assert rc == 0
     db = gpu.DeviceBatch.upload(b)
     st = db.bg_forward(s, fetch_tables=True)
-    for f in ("status", "n_steps_tau", "n_steps_kappa", "n_accepted_kappa"):
+    for f in ("status", "n_steps_tau"):
         np.testing.assert_array_equal(st[f], st_o[f])
+    assert (np.abs(st["n_steps_kappa"] / st_o["n_steps_kappa"] - 1.0) < 0.3).all()
     np.testing.assert_array_equal(st["lna_rec"], st_o["lna_rec"])
     np.testing.assert_array_equal(st["lna_transfer_start"], st_o["lna_transfer_start"])
     np.testing.assert_allclose(st["tau0"], st_o["tau0"], rtol=1e-13)
-    np.testing.assert_allclose(st["kappa_rec"], st_o["kappa_rec"], rtol=1e-12)
+    np.testing.assert_allclose(st["kappa_rec"], st_o["kappa_rec"], rtol=5e-6)
     cos_d = db.cosmo.cpu().numpy().view(packing.COSMO_DTYPE)
     np.testing.assert_allclose(cos_d["tau0"], cos_o["tau0"], rtol=1e-13)
     np.testing.assert_array_equal(cos_d["lna_transfer_start"], cos_o["lna_transfer_start"])
@@ -146,7 +170,8 @@ def test_bg_forward_matches_oracle(gpu, rec_batch):
         d = tab_d[lo:lo + 6 * nl].reshape(6, nl)
         o = tab_o[lo:lo + 6 * nl].reshape(6, nl)
         err = np.max(np.abs(d - o), axis=1) / np.max(np.abs(o), axis=1)
-        assert (err < 1e-10).all(), (i, err)
+        tol = np.array([1e-12, 1e-6, 2e-5, 1e-13, 1e-6, 1e-13])   # tau, g, g', aH, exp(-kappa), aH_dot
+        assert (err < tol).all(), (i, err)
         # x_e and T_m tables untouched
         xo = int(c["off_xe"])
         np.testing.assert_array_equal(tab_d[xo:xo + int(c["n_xe"])], b.tables[xo:xo + int(c["n_xe"])])
@@ -169,7 +194,8 @@ def test_bg_forward_step_limit_raises(gpu, rec_batch):
 def test_device_background_pipeline_matches_oracle(gpu):
     """x_e / T_m in, C_l out, all on the GPU (abcmb_bg_forward, then the
     perturbation and line-of-sight kernels) against the oracle's background,
-    perturbations and line of sight on the same recombination history."""
+    perturbations and line of sight on the same recombination history,
+    within the optical depth's rounding-level spread."""
     from abcmb_b200 import bessel
     from oracle import oracle
     w = configs.c1(nk=40, l_max=400)
@@ -197,5 +223,6 @@ def test_device_background_pipeline_matches_oracle(gpu):
     lr = gpu.LosRunner(db, kt, ls)
     lr.run()
     cl = lr.cl_host()
+    # the optical depth's rounding-level chaos moves C_l by ~1e-6
     err = np.max(np.abs(cl - cl_o) / np.abs(cl_o).max(axis=2, keepdims=True))
-    assert err < 1e-8, err
+    assert err < 2e-5, err
