@@ -36,6 +36,7 @@ SIGNATURES = [
     ("abcmb_los_vjp", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp]),
     ("abcmb_cl_spline", ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        _vp, _vp]),
+    ("abcmb_pert_phase_clocks", ctypes.c_int, [_vp, ctypes.c_int]),
     ("abcmb_bg_workspace_size", _i64, [ctypes.c_int, _vp]),
     ("abcmb_bg_forward", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _i64, _vp]),
     ("abcmb_lens_workspace_size", _i64, [ctypes.c_int, _vp]),

@@ -9,6 +9,7 @@
 
 namespace abcmb {
 int64_t pert_workspace_bytes(int n_cosmo);
+int pert_phase_clocks(unsigned long long* out, int reset);
 cudaError_t launch_pert(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
                         int n_items, const int32_t* items, const abcmb_pert_settings& s, double* pt,
                         abcmb_kstat* kstat, void* ws, cudaStream_t stream, int warps_per_block, int* grid_out);
@@ -316,6 +317,14 @@ int abcmb_set_pert_warps_per_block(int w) {
 }
 
 /* Grid size of the last perturbation launch (diagnostics). */
+int abcmb_pert_phase_clocks(uint64_t* cycles, int reset) {
+  if (!cycles) return fail(ABCMB_ERR_ARG, "abcmb_pert_phase_clocks: null argument");
+  const int rc = abcmb::pert_phase_clocks(reinterpret_cast<unsigned long long*>(cycles), reset);
+  if (rc == -1) return fail(ABCMB_ERR_ARG, "abcmb_pert_phase_clocks: library built without ABCMB_PHASE_CLOCKS");
+  if (rc != 0) return fail(ABCMB_ERR_CUDA, "abcmb_pert_phase_clocks: device read");
+  return ABCMB_OK;
+}
+
 int abcmb_last_pert_grid(void) { return g_last_grid; }
 
 }  // extern "C"

@@ -742,6 +742,31 @@ constexpr int PERT_THREADS_MAX = 128;
 // queue length per warp (at 2 blocks/SM) from which the throughput variant wins
 constexpr int PERT_THROUGHPUT_ITEMS_PER_WARP = 16;
 
+// Optional per-phase cycle accounting, compiled in only with
+// -DABCMB_PHASE_CLOCKS (python -m abcmb_b200.build --phase-clocks): every
+// warp adds the clock64() cycles it spends in each phase of its steps to its
+// own slot of g_pert_phase with reductions whose result nobody waits for;
+// abcmb_pert_phase_clocks sums the slots.  Phases: 0 stage-time background,
+// 1 Newton-matrix factorisation, 2 stage set-up, 3 residual (apply_A),
+// 4 structured solve, 5 chord update and convergence test, 6 error estimate
+// and step-size control, 7 the rest (dense output and PerturbationTable
+// writes, item start and end, queue).
+#ifdef ABCMB_PHASE_CLOCKS
+constexpr int PHASE_N = 8;
+constexpr int PHASE_SLOTS = 8192;
+__device__ unsigned long long g_pert_phase[PHASE_SLOTS * PHASE_N];
+#define PERT_PHASE(k)                                                                      \
+  do {                                                                                    \
+    const long long ph_now = clock64();                                                   \
+    if (lane == 0 && ph_slot) atomicAdd(ph_slot + (k), (unsigned long long)(ph_now - ph_t)); \
+    ph_t = ph_now;                                                                        \
+  } while (0)
+#else
+#define PERT_PHASE(k) \
+  do {                \
+  } while (0)
+#endif
+
 __device__ __forceinline__ void pert_body(const PertArgs& P) {
   extern __shared__ double smem[];
   __shared__ RowTab R;
@@ -776,6 +801,11 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
   __syncthreads();
   WarpMem m;
   carve(smem + (size_t)wib * warp_mem_doubles(P.max_ny, P.ncm), P.max_ny, P.ncm, m);
+#ifdef ABCMB_PHASE_CLOCKS
+  const int ph_index = blockIdx.x * (blockDim.x >> 5) + wib;
+  unsigned long long* ph_slot = ph_index < PHASE_SLOTS ? g_pert_phase + (size_t)ph_index * PHASE_N : nullptr;
+  long long ph_t = clock64();
+#endif
   const abcmb_pert_settings& S = P.s;
   const double err_order = 5.0, safety = 0.9, factormin = 0.2, factormax = 10.0;
   const double coeff1 = (S.icoeff + S.pcoeff + S.dcoeff) / err_order;
@@ -887,6 +917,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
     apply_A(L, m, R, cr, m.SB(), m.y0(), m.F(), nullptr, ncdm, lane);   // FSAL stage 1
 
     while (t0 < 0.0) {
+      PERT_PHASE(7);
       if (nsteps >= S.max_steps) { status = ABCMB_STATUS_MAX_STEPS; break; }
       ++nsteps;
       const double h = t1 - t0;
@@ -903,7 +934,9 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
         if (want_sv) m.SV()[16] = (double)isave;
       }
       __syncwarp();
+      PERT_PHASE(0);
       factor_newton(L, m, R, m.SB() + NB, hg, ncdm, lane);
+      PERT_PHASE(1);
       bool ok = true;
       for (int i = 1; i < 7 && ok; ++i) {
         const double* B = m.SB() + (i == 6 ? 5 : i) * NB;
@@ -927,11 +960,14 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
         }
         if (i != 6) core_row_at(L, R, m, B, lane, cr);       // stage 7 shares stage 6's time
         __syncwarp();
+        PERT_PHASE(2);
         double diffsize = INFINITY, diffsize_prev;
         bool conv = false;
         for (int it = 1; it <= root_max; ++it) {
           apply_A(L, m, R, cr, B, m.v(), m.r(), fi, ncdm, lane);    // residual A v - f
+          PERT_PHASE(3);
           solve_newton(L, m, m.r(), lane);
+          PERT_PHASE(4);
           double ss = 0.;
           {
             // disjoint regions of the warp's scratch: no load waits on a store
@@ -953,6 +989,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
           diffsize_prev = diffsize;
           diffsize = sqrt(ss * inv_n);
           ++nnewton;
+          PERT_PHASE(5);
           if (it >= 2) {
             // optimistix very-chord termination, without divisions:
             // rate = d/dp; converged <=> 0 < rate < 1 and d rate / (1 - rate) < kappa
@@ -1004,6 +1041,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
       double factor = fmin(fmax(safety * f1v * f2v * f3v, keep ? 1.0 : factormin), factormax);
       double dt_new = h * factor;
       if (inv == 0. || isinf(inv)) inv = 1.;
+      PERT_PHASE(6);
       if (keep) {
         ++nacc;
         // cubic Hermite dense output on [t0, t1] at every save point it covers
@@ -1070,6 +1108,27 @@ namespace abcmb {
 template <int MIN_BLOCKS>
 __global__ void __launch_bounds__(PERT_THREADS_MAX, MIN_BLOCKS) pert_kernel(PertArgs P) {
   pert_body(P);
+}
+
+int pert_phase_clocks(unsigned long long* out, int reset) {
+#ifdef ABCMB_PHASE_CLOCKS
+  static unsigned long long h[PHASE_SLOTS * PHASE_N];
+  cudaError_t e = cudaMemcpyFromSymbol(h, g_pert_phase, sizeof(h));
+  if (e != cudaSuccess) return -2;
+  for (int k = 0; k < PHASE_N; ++k) out[k] = 0;
+  for (int i = 0; i < PHASE_SLOTS; ++i)
+    for (int k = 0; k < PHASE_N; ++k) out[k] += h[(size_t)i * PHASE_N + k];
+  if (reset) {
+    static const unsigned long long zero[PHASE_SLOTS * PHASE_N] = {};
+    e = cudaMemcpyToSymbol(g_pert_phase, zero, sizeof(zero));
+    if (e != cudaSuccess) return -2;
+  }
+  return 0;
+#else
+  (void)out;
+  (void)reset;
+  return -1;
+#endif
 }
 
 int64_t pert_workspace_bytes(int n_cosmo) {

@@ -4,6 +4,8 @@
     python -m abcmb_b200.profile_case c2        # the 600-k massive-neutrino cosmology
     python -m abcmb_b200.profile_case c1 --los  # C1 with the line of sight
     python -m abcmb_b200.profile_case c4 64 --bg-only   # the background producer alone
+    ABCMB_B200_LIB=abcmb_b200/libabcmb_b200_phase.so \
+        python -m abcmb_b200.profile_case c4 40 --phases  # cycles per phase of pert_kernel
 
 Runs the perturbation launch twice (warm-up + measured) and, with --los, the
 line of sight twice, then checks the per-k status.  With --bg-only the batch
@@ -14,12 +16,26 @@ from __future__ import annotations
 import argparse
 
 
+PHASES = ("stage-time background (stage_basis)", "Newton-matrix factorisation", "stage set-up",
+          "residual (apply_A)", "structured solve (solve_newton)", "chord update + convergence test",
+          "error estimate + step-size control", "rest (dense output, table writes, item start/end)")
+
+
+def _phase_clocks(reset: bool):
+    import ctypes
+    from . import _lib
+    cyc = (ctypes.c_uint64 * 8)()
+    _lib.check(_lib.load().abcmb_pert_phase_clocks(cyc, 1 if reset else 0), "abcmb_pert_phase_clocks")
+    return [int(c) for c in cyc]
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["c1", "c2", "c4"])
     ap.add_argument("n", nargs="?", type=int, default=4)
     ap.add_argument("--los", action="store_true")
     ap.add_argument("--bg-only", action="store_true")
+    ap.add_argument("--phases", action="store_true")
     a = ap.parse_args()
     import torch
     from . import configs, engine
@@ -38,8 +54,26 @@ def main():
     w.build()
     st = w.pert_settings()
     db = engine.DeviceBatch.upload(w.batch)
-    for _ in range(2):
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for i in range(2):
+        if a.phases and i == 1:
+            _phase_clocks(reset=True)
+        if i == 1:
+            e0.record()
         db.pert_forward(st)
+    e1.record()
+    torch.cuda.synchronize()
+    print(f"perturbation launch {e0.elapsed_time(e1):.1f} ms")
+    if a.phases:
+        torch.cuda.synchronize()
+        cyc = _phase_clocks(reset=False)
+        ks = db.kstat_host()
+        steps = float((ks["n_accepted"] + ks["n_rejected"]).sum())
+        tot = float(sum(cyc))
+        for name, c in zip(PHASES, cyc):
+            print(f"{name:44s} {c / tot * 100:6.2f} %  {c / steps:9.0f} cycles per step and warp")
+        print(f"steps {steps:.0f}  chord iterations per stage {float(ks['n_newton'].sum()) / (6 * steps):.3f}")
     if a.los:
         lr = engine.LosRunner(db, w.kt, w.los_settings())
         for _ in range(2):

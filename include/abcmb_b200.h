@@ -443,6 +443,15 @@ int abcmb_lens_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev,
 /* Warps per block of the perturbation kernel (1..4; default 4). */
 int abcmb_set_pert_warps_per_block(int warps);
 
+/* Cycles the perturbation kernel's warps spent per phase since the last
+ * reset, summed over warps: cycles[8] = stage-time background, Newton-matrix
+ * factorisation, stage set-up, residual, structured solve, chord update and
+ * convergence test, error estimate and step-size control, the rest.  Only a
+ * library built with ABCMB_PHASE_CLOCKS counts (python -m abcmb_b200.build
+ * --phase-clocks); others return ABCMB_ERR_ARG.  reset != 0 zeroes the
+ * counters after reading. */
+int abcmb_pert_phase_clocks(uint64_t* cycles, int reset);
+
 /* Grid size (blocks) of the last perturbation launch on this process. */
 int abcmb_last_pert_grid(void);
 

@@ -78,6 +78,15 @@ def test_c_abi_library_exports_every_declared_symbol():
     assert lib.abcmb_pert_workspace_size(2, 10) > 2 * 10000 * 8
 
 
+def test_phase_clocks_only_in_the_phase_build():
+    from abcmb_b200 import _lib
+    lib = _lib.load()
+    cyc = (ctypes.c_uint64 * 8)()
+    if "phase" not in _lib.LIB_PATH:
+        assert lib.abcmb_pert_phase_clocks(cyc, 0) == -1 and b"ABCMB_PHASE_CLOCKS" in lib.abcmb_last_error()
+    assert lib.abcmb_pert_phase_clocks(None, 0) == -1
+
+
 def test_los_argument_errors_without_gpu():
     from abcmb_b200 import _lib, packing
     lib = _lib.load()
