@@ -339,13 +339,14 @@ __device__ __noinline__ void make_row(int r, RowDesc& d) {
 // h' and eta' of the state v (perturbations.py:238-239) with basis B.
 __device__ __forceinline__ void metric(const Layout& L, const double* B, const double* v, bool ncdm, double& hp,
                                        double& etap) {
-  hp = B[B_WH] * v[0] + B[B_WH + 1] * v[1] + B[B_WH + 2] * v[2] + B[B_WH + 3] * v[L.i_g] + B[B_WH + 4] * v[L.i_nu];
-  etap = B[B_WE] * v[3] + B[B_WE + 1] * v[L.i_g + 1] + B[B_WE + 2] * v[L.i_nu + 1];
+  // sums split into independent partial sums: short dependency chains
+  hp = fma(B[B_WH], v[0], B[B_WH + 1] * v[1]) + fma(B[B_WH + 2], v[2], fma(B[B_WH + 3], v[L.i_g], B[B_WH + 4] * v[L.i_nu]));
+  etap = fma(B[B_WE], v[3], B[B_WE + 1] * v[L.i_g + 1]) + B[B_WE + 2] * v[L.i_nu + 1];
   if (ncdm) {
-    for (int bb = 0; bb < 3; ++bb) {
-      hp += B[B_WH + 5 + bb] * v[L.i_ncdm + bb * L.nM];
-      etap += B[B_WE + 3 + bb] * v[L.i_ncdm + bb * L.nM + 1];
-    }
+    const double* p0 = v + L.i_ncdm;
+    const int nM = L.nM;
+    hp += fma(B[B_WH + 5], p0[0], fma(B[B_WH + 6], p0[nM], B[B_WH + 7] * p0[2 * nM]));
+    etap += fma(B[B_WE + 3], p0[1], fma(B[B_WE + 4], p0[nM + 1], B[B_WE + 5] * p0[2 * nM + 1]));
   }
 }
 
@@ -531,6 +532,22 @@ __device__ void factor_newton(const Layout& L, WarpMem& m, const RowTab& R, cons
   else gauss_jordan<MAXC>(m, lane);
 }
 
+// sum_j a[j] b[j] over a compile-time length, in four independent partial sums
+template <int N>
+__device__ __forceinline__ double core_dot(const double* __restrict__ a, const double* __restrict__ b) {
+  double s0 = 0., s1 = 0., s2 = 0., s3 = 0.;
+#pragma unroll
+  for (int j = 0; j + 3 < N; j += 4) {
+    s0 = fma(a[j], b[j], s0);
+    s1 = fma(a[j + 1], b[j + 1], s1);
+    s2 = fma(a[j + 2], b[j + 2], s2);
+    s3 = fma(a[j + 3], b[j + 3], s3);
+  }
+#pragma unroll
+  for (int j = N & ~3; j < N; ++j) s0 = fma(a[j], b[j], s0);
+  return (s0 + s1) + (s2 + s3);
+}
+
 // Solve M x = r in place (r holds the right-hand side on entry).
 __device__ void solve_newton(const Layout& L, WarpMem& m, double* r, int lane) {
   const int nc = L.nc;
@@ -568,7 +585,7 @@ __device__ void solve_newton(const Layout& L, WarpMem& m, double* r, int lane) {
     // factor_newton); vc already holds b[q_k] in slot k
     const double* row = m.Mc() + m.perm()[lane] * m.cs;
     const double* vc = m.vc();
-    for (int j = 0; j < nc; ++j) xc = fma(row[j], vc[j], xc);
+    xc = nc == 13 ? core_dot<13>(row, vc) : core_dot<MAXC>(row, vc);
   }
   __syncwarp();
   if (lane < nc) r[m.cmap()[lane]] = xc;
@@ -949,9 +966,14 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
           double* __restrict__ fw = fi;
           double* __restrict__ vw = m.v();
           for (int e = lane; e < n; e += WARP) {
-            double acc = 0.;
-            for (int j = 0; j < i; ++j) acc = fma(KV_A[i][j], Fr[j * n + e], acc);
-            const double be = y0[e] + h * acc;
+            double acc = 0., acc2 = 0.;
+            int j = 0;
+            for (; j + 1 < i; j += 2) {
+              acc = fma(KV_A[i][j], Fr[j * n + e], acc);
+              acc2 = fma(KV_A[i][j + 1], Fr[(j + 1) * n + e], acc2);
+            }
+            if (j < i) acc = fma(KV_A[i][j], Fr[j * n + e], acc);
+            const double be = y0[e] + h * (acc + acc2);
             const double fe = Fr[(i - 1) * n + e];              // predictor: the previous stage's f
             bw[e] = be;
             fw[e] = fe;
@@ -1012,15 +1034,17 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
         const double* __restrict__ y0 = m.y0();
         double* __restrict__ y1 = m.y1();
         for (int e = lane; e < n; e += WARP) {
-          double acc = 0., acce = 0.;
+          double acc = 0., acce = 0., accb = 0., acceb = 0.;
 #pragma unroll
-          for (int j = 0; j < 6; ++j) {
-            double fj = Fr[j * n + e];
-            acc = fma(KV_A[6][j], fj, acc);
-            acce = fma(KV_A[6][j] - KV_A[5][j], fj, acce);
+          for (int j = 0; j < 6; j += 2) {
+            const double fa = Fr[j * n + e], fb = Fr[(j + 1) * n + e];
+            acc = fma(KV_A[6][j], fa, acc);
+            acce = fma(KV_A[6][j] - KV_A[5][j], fa, acce);
+            accb = fma(KV_A[6][j + 1], fb, accb);
+            acceb = fma(KV_A[6][j + 1] - KV_A[5][j + 1], fb, acceb);
           }
-          acc = fma(KV_G, Fr[6 * n + e], acc);
-          acce += -KV_G * Fr[5 * n + e] + KV_G * Fr[6 * n + e];
+          acc = fma(KV_G, Fr[6 * n + e], acc + accb);
+          acce = (acce + acceb) + (-KV_G * Fr[5 * n + e] + KV_G * Fr[6 * n + e]);
           double y0e = y0[e];
           double y1e = y0e + h * acc;
           y1[e] = y1e;
