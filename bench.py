@@ -127,6 +127,14 @@ def cpu_sample(gw, stride: int, n_threads: int):
         rc, pt, ks = oracle.pert_forward(sub, st, n_threads)
         t_runs.append(time.perf_counter() - t0)
     t_ode = min(t_runs) * n_full / len(sel)
+    # the same sample on one thread (the reference's CI setting), on every
+    # 16th of the sampled items to bound the time
+    sel1 = sel[::16]
+    sub1 = packing.Batch(cosmo=b.cosmo, tables=b.tables, kbuf=b.kbuf, items=b.items[sel1].copy(),
+                         pt_size=b.pt_size, n_save=b.n_save, bgs=b.bgs, layouts=b.layouts)
+    t0 = time.perf_counter()
+    oracle.pert_forward(sub1, st, 1)
+    t_ode1 = (time.perf_counter() - t0) * n_full / len(sel1)
     one = packing.Batch(cosmo=b.cosmo[:1].copy(), tables=b.tables, kbuf=b.kbuf, items=b.items[:0], pt_size=b.pt_size,
                         n_save=b.n_save, bgs=b.bgs[:1], layouts=b.layouts[:1])
     ls = gw.base.los_settings()
@@ -138,7 +146,10 @@ def cpu_sample(gw, stride: int, n_threads: int):
             "sample": f"oracle (C, FP64, OpenMP) on 1 cosmology's 9 gradient variants: every {stride}th k mode of "
                       f"the ODE ({len(sel)}/{n_full} items, scaled) + 1 full line-of-sight run (x{nvar}); "
                       f"s per cosmology+grad: ode {t_ode:.2f} (faster of 2 runs; the other "
-                      f"{max(t_runs) * n_full / len(sel):.2f}) los {t_los:.2f}"}
+                      f"{max(t_runs) * n_full / len(sel):.2f}) los {t_los:.2f}",
+            "ode_one_thread": {"s_per_cosmology": t_ode1, "items": len(sel1),
+                               "sample": f"every 16th of the items above ({len(sel1)}) on 1 thread, scaled",
+                               "all_cores_speedup": t_ode1 / t_ode}}
 
 
 def plain_gpu_fwd_fd(gw, w, dev, stream, want_dns=True):
