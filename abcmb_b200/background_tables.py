@@ -308,30 +308,9 @@ def _tabulate_tau(p, has_ncdm):
     return tab
 
 
-# HyRex's output buffers (abcmb/hyrex/hyrex.py:183-206, helium.py, hydrogen.py):
-# x_e = Saha HeII/III on the points with z >= 3600, then post-Saha HeII
-# (4000), the HeII ODE (4096), post-Saha H (800), the two-photon EMLA phase,
-# the EMLA with T_m and the three-level-atom phase (8192 each); T_m = the
-# last two (8192 each).  array_with_padding.concat keeps every buffer's
-# length, so the arrays handed to Background are that long, inf-padded after
-# the last valid point; BG.xe / BG.Tm scale their interpolation index by the
-# padded length (background.py:593-603, 647-657).
-HYREX_XE_BUFFERS = 4000 + 4096 + 800 + 3 * 8192
-HYREX_TM_BUFFERS = 2 * 8192
-HYREX_Z_HE4_EQUIL = 3601.0
-
-
-def hyrex_padded_lengths(lna_full: np.ndarray) -> tuple:
-    """(x_e length, T_m length) of HyRex's padded output arrays."""
-    n_saha = int(np.count_nonzero(lna_full <= -math.log(HYREX_Z_HE4_EQUIL)))
-    return n_saha + HYREX_XE_BUFFERS, HYREX_TM_BUFFERS
-
-
-def make_recombination(params: dict, has_ncdm: bool, xe_pad: int | None = None,
-                       tm_pad: int | None = None) -> BackgroundTables:
+def make_recombination(params: dict, has_ncdm: bool, xe_pad: int = 37, tm_pad: int = 29) -> BackgroundTables:
     """The recombination and reionisation part of the synthetic background:
-    x_e (with reionisation) and T_m tables in HyRex's padded format (padded
-    to HyRex's buffer lengths unless xe_pad / tm_pad give the padding) and
+    x_e (with reionisation) and T_m tables in HyRex's padded format and
     z_reion.  The conformal-time table, the optical depth and the
     line-of-sight arrays are left to abcmb_bg_forward (tau_tab is None)."""
     p = params
@@ -345,17 +324,12 @@ def make_recombination(params: dict, has_ncdm: bool, xe_pad: int | None = None,
     else:
         z_re = p["z_reion"]
     xe_full = xe_rec + xe_reion(lna_full, z_re, p)
-    n_xe, n_tm = hyrex_padded_lengths(lna_full)
-    if xe_pad is None:
-        xe_pad = n_xe - len(xe_full)
     # inf padding of array_with_padding, replaced by the last valid value
     xe_arr = np.concatenate([xe_full, np.full(xe_pad, xe_full[-1])])
     lna_xe_arr = lna_full
     # T_m table starts at the late (z ~ 700) phase like HyRex's lna_Tm
     i_tm = int(np.searchsorted(lna_full, -math.log(1 + 700.0)))
     lna_tm = lna_full[i_tm:]
-    if tm_pad is None:
-        tm_pad = n_tm - len(lna_tm)
     tm_arr = np.concatenate([tm_rec[i_tm:], np.full(tm_pad, tm_rec[-1])])
 
     return BackgroundTables(
@@ -391,8 +365,7 @@ def complete_on_host(bg: BackgroundTables) -> BackgroundTables:
     return bg
 
 
-def make_background(params: dict, has_ncdm: bool, xe_pad: int | None = None,
-                    tm_pad: int | None = None) -> BackgroundTables:
+def make_background(params: dict, has_ncdm: bool, xe_pad: int = 37, tm_pad: int = 29) -> BackgroundTables:
     """Synthetic Background for one cosmology (derived params dict in), all
     of it on the host."""
     return complete_on_host(make_recombination(params, has_ncdm, xe_pad, tm_pad))
