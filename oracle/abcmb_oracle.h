@@ -56,6 +56,19 @@ int oracle_bg_forward(int n_cosmo, abcmb_cosmo* cosmo, double* tables, const abc
                       abcmb_bgstat* stat, int n_threads);
 int oracle_kappa_solve(const abcmb_cosmo* c, const double* tables, double rhs_scale, int max_steps,
                        int* nsteps, double* kappa_end);
+/* HyRex tables (abcmb/hyrex/tabs): Alpha_inf [100 x 40 x 4], R_inf [100],
+ * fit_swift [n_swift x 5]. */
+typedef struct oracle_hyrex_tables {
+  const double* alpha;
+  const double* R;
+  const double* swift;
+  int n_swift;
+} oracle_hyrex_tables;
+void oracle_kvaerno3_tableau(double* A16, double* c4, double* b4, double* be4);
+int oracle_hyrex_sizes(int n_grid, int* n_xe, int* n_tm);
+int oracle_hyrex(const oracle_hyrex_tables* tab, int n_grid, const double* TCMB, const double* nH,
+                 const double* H, double YHe, double omega_b, double omega_cdm, double Neff, double* xe_out,
+                 double* lna_out, int cap_xe, double* tm_out, double* lna_tm_out, int cap_tm, int* info);
 int oracle_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* kbuf, const double* pt, int n_save,
                   double k_pivot, int n_kout, const double* kout, int n_z, const double* z, double* pk);
 

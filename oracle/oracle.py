@@ -24,6 +24,10 @@ class COracleBessel(ctypes.Structure):
                 ("xmin", _dp * 3), ("xmax", _dp * 3), ("phi", _dp * 3)]
 
 
+class COracleHyrexTables(ctypes.Structure):
+    _fields_ = [("alpha", _dp), ("R", _dp), ("swift", _dp), ("n_swift", ctypes.c_int)]
+
+
 def build() -> str:
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return LIB_PATH
@@ -65,6 +69,13 @@ def lib():
                                          ctypes.POINTER(COracleBessel), _dp, _dp, ctypes.c_int]
         L.oracle_bg_forward.restype = ctypes.c_int
         L.oracle_bg_forward.argtypes = [ctypes.c_int, vp, _dp, vp, vp, ctypes.c_int]
+        L.oracle_kvaerno3_tableau.argtypes = [_dp, _dp, _dp, _dp]
+        L.oracle_hyrex_sizes.restype = ctypes.c_int
+        L.oracle_hyrex_sizes.argtypes = [ctypes.c_int, _ip, _ip]
+        L.oracle_hyrex.restype = ctypes.c_int
+        L.oracle_hyrex.argtypes = [ctypes.POINTER(COracleHyrexTables), ctypes.c_int, _dp, _dp, _dp,
+                                   ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                   _dp, _dp, ctypes.c_int, _dp, _dp, ctypes.c_int, _ip]
         L.oracle_kappa_solve.restype = ctypes.c_int
         L.oracle_kappa_solve.argtypes = [vp, _dp, ctypes.c_double, ctypes.c_int, _ip, _dp]
         L.oracle_pk_lin.restype = ctypes.c_int
@@ -187,3 +198,35 @@ def kappa_solve(batch, ci: int, rhs_scale: float = 1.0, max_steps: int = 100000)
     st = lib().oracle_kappa_solve(vptr(cos), dptr(batch.tables), float(rhs_scale), int(max_steps),
                                   ctypes.byref(n), dptr(k))
     return st, int(n.value), float(k[0])
+
+
+# HyRex's lna grid: arange(-log(1 + 8000), -log(1 + 0), 5e-4) (abcmb/hyrex/hyrex.py:131)
+def hyrex_grid() -> np.ndarray:
+    return np.arange(-np.log(1.0 + 8000.0), -np.log(1.0 + 0.0), 5.0e-4)
+
+
+def hyrex(params: dict, has_ncdm: bool):
+    """The oracle's HyRex history for a derived-parameter dict: (rc, out) with
+    out = dict(xe, lna_xe, Tm, lna_tm) -- the reference's inf-padded arrays
+    before reionisation -- and info (valid entries and steps per phase)."""
+    from abcmb_b200 import cosmology, constants as cnst, hyrex_tables
+    t = hyrex_tables.load()
+    grid = hyrex_grid()
+    a = np.exp(grid)
+    TCMB = np.ascontiguousarray(params["TCMB0"] / a)
+    nH = np.ascontiguousarray((1 - params["YHe"]) * 3.0 * params["omega_b"] * cnst.H0_over_h ** 2 / 8 / np.pi
+                              / cnst.G / cnst.mH / a ** 3)
+    H = np.ascontiguousarray(np.asarray(cosmology.H(grid, params, has_ncdm), dtype=np.float64))
+    n_xe = ctypes.c_int32(0)
+    n_tm = ctypes.c_int32(0)
+    lib().oracle_hyrex_sizes(len(grid), ctypes.byref(n_xe), ctypes.byref(n_tm))
+    xe = np.empty(n_xe.value)
+    lxe = np.empty(n_xe.value)
+    tm = np.empty(n_tm.value)
+    ltm = np.empty(n_tm.value)
+    info = np.zeros(16, dtype=np.int32)
+    tabs = COracleHyrexTables(dptr(t.alpha), dptr(t.R), dptr(t.swift), t.swift.shape[0])
+    rc = lib().oracle_hyrex(ctypes.byref(tabs), len(grid), dptr(TCMB), dptr(nH), dptr(H), float(params["YHe"]),
+                            float(params["omega_b"]), float(params["omega_cdm"]), float(params["Neff"]),
+                            dptr(xe), dptr(lxe), n_xe.value, dptr(tm), dptr(ltm), n_tm.value, iptr(info))
+    return rc, dict(xe=xe, lna_xe=lxe, Tm=tm, lna_tm=ltm, info=info)

@@ -1,0 +1,139 @@
+"""The oracle's restatement of HyRex (oracle/hyrex_oracle.c): the recombination
+history the reference computes with abcmb/hyrex/*.py, in its seven phases and
+its padded output layout.  The reference cannot run here (no jax), so the
+restatement is pinned by the Kvaerno3 order conditions, the analytic limits
+of the history and an independent recombination model (the host model's
+Peebles three-level atom with the RECFAST fudge factor, which is calibrated
+on multilevel-atom codes to ~1 %)."""
+import numpy as np
+import pytest
+
+from abcmb_b200 import background_tables as bt, configs, cosmology
+from abcmb_b200 import specs as sp
+
+
+def test_kvaerno3_order_conditions():
+    """Kvaerno's ESDIRK 3(2): the solution row is third order, the embedded
+    row (stage 3, stiffly accurate) second order, stage times are row sums."""
+    import ctypes
+    from oracle import oracle
+    A = np.zeros(16)
+    c = np.zeros(4)
+    b = np.zeros(4)
+    be = np.zeros(4)
+    dp = ctypes.POINTER(ctypes.c_double)
+    oracle.lib().oracle_kvaerno3_tableau(A.ctypes.data_as(dp), c.ctypes.data_as(dp), b.ctypes.data_as(dp),
+                                         be.ctypes.data_as(dp))
+    A = A.reshape(4, 4)
+    np.testing.assert_allclose(A.sum(axis=1), c, atol=1e-14)
+    np.testing.assert_allclose(b, A[3], atol=0)                 # stiffly accurate
+    np.testing.assert_allclose(be[:3], A[2, :3], atol=0)
+    for w, order in ((b, 3), (be, 2)):
+        assert abs(w.sum() - 1) < 1e-14
+        assert abs(w @ c - 1 / 2) < 1e-14
+        if order >= 3:
+            assert abs(w @ c ** 2 - 1 / 3) < 1e-14
+            assert abs(w @ (A @ c) - 1 / 6) < 1e-14
+    g = A[1, 1]
+    # L-stability root of the SDIRK3 polynomial 6g^3 - 18g^2 + 9g - 1 = 0
+    assert abs(6 * g ** 3 - 18 * g ** 2 + 9 * g - 1) < 1e-9
+
+
+@pytest.fixture(scope="module")
+def fiducial_history():
+    from oracle import oracle
+    w = configs.c1()
+    p = cosmology.add_derived_parameters(w.params_in[0], False, w.specs)
+    rc, out = oracle.hyrex(p, False)
+    assert rc == 0
+    return p, out
+
+
+def test_hyrex_layout_follows_the_reference_buffers(fiducial_history):
+    p, o = fiducial_history
+    info = o["info"]
+    grid = np.arange(-np.log(8001.0), 0.0, 5e-4)
+    n_saha = int(np.count_nonzero(grid <= -np.log(3601.0)))
+    assert len(o["xe"]) == n_saha + 4000 + 4096 + 800 + 3 * 8192 == info[12]
+    assert len(o["Tm"]) == 2 * 8192 == info[13]
+    assert (info[:7] > 0).all() and info[14] == 0
+    ok = np.isfinite(o["xe"])
+    n = int(ok.sum())
+    assert ok[:n].all() and not ok[n:].any()                 # finite prefix, inf padding
+    lna = o["lna_xe"][:n]
+    np.testing.assert_allclose(np.diff(lna), 5e-4, atol=1e-9)   # one uniform grid across the phases
+    assert lna[0] == pytest.approx(-np.log(8001.0)) and 0.0 <= lna[-1] < 0.1   # the last phase ends past lna = 0
+    okt = np.isfinite(o["Tm"])
+    assert okt[:int(okt.sum())].all()
+
+
+def test_hyrex_history_limits_and_independent_model(fiducial_history):
+    p, o = fiducial_history
+    ok = np.isfinite(o["xe"])
+    xe, lna = o["xe"][ok], o["lna_xe"][ok]
+    z = np.exp(-lna) - 1
+    fHe = p["YHe"] / (1 - p["YHe"]) / 3.97153
+    # fully ionised hydrogen and helium at z = 8000 (Saha HeIII), HeII gone by z = 1700
+    assert xe[0] == pytest.approx(1 + 2 * fHe, rel=5e-4)
+    assert xe[np.argmin(abs(z - 1700))] == pytest.approx(1.0, abs=0.01)
+    # the host model's Peebles atom (recombination part only) within 2 % through
+    # hydrogen recombination and freeze-out
+    bg = bt.make_background(p, False)
+    grid = np.arange(-np.log(8001.0), 0.0, 5e-4)
+    xh = bg.xe_arr[:len(grid)] - bt.xe_reion(grid, bg.z_reion, p)
+    xo = np.interp(grid, lna, xe)
+    zg = np.exp(-grid) - 1
+    m = (zg > 30) & (zg < 1600)
+    assert np.max(np.abs(xo[m] / xh[m] - 1)) < 0.02
+    # freeze-out and thermal decoupling
+    assert 1e-4 < xe[np.argmin(abs(z - 50))] < 5e-4
+    tm, ltm = o["Tm"][np.isfinite(o["Tm"])], o["lna_tm"][np.isfinite(o["lna_tm"])]
+    ratio = tm / (p["TCMB0"] / np.exp(ltm))
+    zt = np.exp(-ltm) - 1
+    assert ratio[np.argmin(abs(zt - 700))] > 0.99
+    assert 0.4 < ratio[np.argmin(abs(zt - 100))] < 0.8
+    assert (np.diff(ratio[zt < 500]) < 1e-12).all()          # T_m falls behind T_CMB monotonically
+
+
+def test_hyrex_massive_neutrinos_and_helium_fraction():
+    from oracle import oracle
+    w = configs.c2()
+    p = cosmology.add_derived_parameters(dict(w.params_in[0], YHe=0.26), True, w.specs)
+    rc, o = oracle.hyrex(p, True)
+    assert rc == 0 and (o["info"][:7] > 0).all()
+    fHe = 0.26 / 0.74 / 3.97153
+    assert o["xe"][0] == pytest.approx(1 + 2 * fHe, rel=5e-4)
+
+
+def test_hyrex_history_runs_through_the_oracle_path(fiducial_history):
+    """The HyRex-format tables (reionisation added, inf padding replaced by the
+    last value, background.py:534-550) through the oracle's background
+    producer and perturbations."""
+    from abcmb_b200 import packing
+    from oracle import oracle
+    p, o = fiducial_history
+    ok = np.isfinite(o["xe"])
+    n = int(ok.sum())
+    lna = o["lna_xe"][:n]
+    bg = bt.make_recombination(p, False)
+    xe = o["xe"][:n] + bt.xe_reion(lna, bg.z_reion, p)
+    okt = np.isfinite(o["Tm"])
+    nt = int(okt.sum())
+    bg.xe_arr = np.concatenate([xe, np.full(len(o["xe"]) - n, xe[-1])])
+    bg.lna_xe0, bg.lna_xe_dx, bg.lna_xe_last, bg.xe_last = float(lna[0]), float(lna[1] - lna[0]), float(lna[-1]), \
+        float(xe[-1])
+    tm = o["Tm"][:nt]
+    ltm = o["lna_tm"][:nt]
+    bg.tm_arr = np.concatenate([tm, np.full(len(o["Tm"]) - nt, tm[-1])])
+    bg.lna_tm0, bg.lna_tm_dx, bg.lna_tm_last, bg.tm_last = float(ltm[0]), float(ltm[1] - ltm[0]), \
+        float(ltm[-1]), float(tm[-1])
+    w = configs.c1(nk=6)
+    lay = sp.state_layout(w.specs, False)
+    b = packing.pack([bg], [lay], w.kgrids)
+    rc, cos, tab, st = oracle.bg_forward(b, packing.bg_settings())
+    assert rc == 0 and st[0]["status"] == 0
+    assert -7.1 < st[0]["lna_rec"] < -6.9                      # visibility peak near z = 1090
+    b.cosmo[:] = cos
+    b.tables = tab
+    rc, pt, ks = oracle.pert_forward(b, packing.pert_settings(w.specs, 500, b))
+    assert rc == 0 and (ks["status"] == 0).all()
