@@ -37,6 +37,10 @@ SIGNATURES = [
     ("abcmb_cl_spline", ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        _vp, _vp]),
     ("abcmb_pert_phase_clocks", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("abcmb_upload_hyrex_tables", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
+    ("abcmb_hyrex_sizes", ctypes.c_int, [ctypes.c_int, _vp, _vp]),
+    ("abcmb_hyrex_forward", ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                           _vp, _vp]),
     ("abcmb_bg_workspace_size", _i64, [ctypes.c_int, _vp]),
     ("abcmb_bg_forward", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _i64, _vp]),
     ("abcmb_lens_workspace_size", _i64, [ctypes.c_int, _vp]),

@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libabcmb_b200.so")
 LIB_PHASE = os.path.join(HERE, "libabcmb_b200_phase.so")
-SOURCES = ["capi.cu", "bg.cu", "pert.cu", "los.cu", "lens.cu", "probe.cu", "pert_noalloc.cu"]
+SOURCES = ["capi.cu", "bg.cu", "hyrex.cu", "pert.cu", "los.cu", "lens.cu", "probe.cu", "pert_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -30,6 +30,12 @@ cudaError_t launch_los_vjp(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcm
                            double* pt_bar, double* param_bar, void* ws, cudaStream_t stream);
 int64_t lens_workspace_bytes(int n_cosmo, const abcmb_lens_settings& s);
 int64_t bg_workspace_bytes(int n_cosmo, const abcmb_bg_settings& s);
+int hyrex_sizes(int n_grid, int* n_xe, int* n_tm);
+cudaError_t hyrex_upload_tables(const double* alpha, const double* R, const double* swift, int n_swift);
+bool hyrex_tables_ready();
+cudaError_t launch_hyrex(int n_cosmo, int n_grid, const double* T, const double* nH, const double* H,
+                         const abcmb_hyrex_params* params, double* xe, double* lna_xe, double* tm, double* lna_tm,
+                         int32_t* info, cudaStream_t stream);
 cudaError_t launch_bg(int n_cosmo, abcmb_cosmo* cosmo, double* tables, const abcmb_bg_settings& s,
                       abcmb_bgstat* stat, void* ws, cudaStream_t stream);
 cudaError_t launch_lens(int n_cosmo, const abcmb_cosmo* cosmo, const abcmb_lens_cosmo* lens, const double* tables,
@@ -125,6 +131,34 @@ int abcmb_upload_bessel(int n_l, int n_x, const int32_t* l_tab, const double* xm
   bc->mem = mem;
   bc->dev = abcmb::BesselDev{n_l, n_x, dl, dxmin, dxmax, dphi};
   bc->ready = true;
+  return ABCMB_OK;
+}
+
+int abcmb_upload_hyrex_tables(const double* alpha, const double* R, const double* swift, int n_swift) {
+  if (!alpha || !R || !swift || n_swift < 2) return fail(ABCMB_ERR_ARG, "abcmb_upload_hyrex_tables: bad argument");
+  cudaError_t e = abcmb::hyrex_upload_tables(alpha, R, swift, n_swift);
+  if (e != cudaSuccess) return cuda_fail(e, "abcmb_upload_hyrex_tables");
+  return ABCMB_OK;
+}
+
+int abcmb_hyrex_sizes(int n_grid, int* n_xe, int* n_tm) {
+  if (n_grid < 2 || !n_xe || !n_tm) return -1;
+  return abcmb::hyrex_sizes(n_grid, n_xe, n_tm);
+}
+
+int abcmb_hyrex_forward(int n_cosmo, int n_grid, const double* T_dev, const double* nH_dev, const double* H_dev,
+                        const abcmb_hyrex_params* params_dev, double* xe_dev, double* lna_xe_dev, double* tm_dev,
+                        double* lna_tm_dev, int32_t* info_dev, void* stream) {
+  if (n_cosmo <= 0 || !T_dev || !nH_dev || !H_dev || !params_dev || !xe_dev || !lna_xe_dev || !tm_dev ||
+      !lna_tm_dev || !info_dev)
+    return fail(ABCMB_ERR_ARG, "abcmb_hyrex_forward: null argument or n_cosmo <= 0");
+  int nx = 0, nt = 0;
+  if (n_grid < 2 || abcmb::hyrex_sizes(n_grid, &nx, &nt) < 2)
+    return fail(ABCMB_ERR_ARG, "abcmb_hyrex_forward: the grid must reach z = 3600 with two points");
+  if (!abcmb::hyrex_tables_ready()) return fail(ABCMB_ERR_TABLES, "abcmb_hyrex_forward: tables not uploaded");
+  cudaError_t e = abcmb::launch_hyrex(n_cosmo, n_grid, T_dev, nH_dev, H_dev, params_dev, xe_dev, lna_xe_dev, tm_dev,
+                                      lna_tm_dev, info_dev, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "abcmb_hyrex_forward");
   return ABCMB_OK;
 }
 

@@ -250,6 +250,47 @@ int abcmb_bg_forward(int n_cosmo, abcmb_cosmo* cosmo_dev, double* tables_dev,
                      void* workspace_dev, int64_t workspace_bytes, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Recombination: HyRex (abcmb/hyrex/hyrex.py recomb_model.get_history)      */
+/* ------------------------------------------------------------------------ */
+
+/* Parameters HyRex reads (params dict entries). */
+typedef struct abcmb_hyrex_params {
+  double YHe, omega_b, omega_cdm, Neff;
+} abcmb_hyrex_params;
+
+/*
+ * Upload HyRex's tables once per device (host arrays, as the reference's
+ * abcmb/hyrex/tabs files hold them): alpha [100 x 40 x 4] (Alpha_inf.dat,
+ * recomb_functions.py:11-24), R [100] (R_inf.dat), swift [n_swift x 5]
+ * (fit_swift.dat, hydrogen.py:53).
+ */
+int abcmb_upload_hyrex_tables(const double* alpha, const double* R, const double* swift, int n_swift);
+
+/* Lengths of HyRex's padded output arrays for a grid of n_grid points
+ * (the buffers the seven phases keep, joined by array_with_padding.concat);
+ * returns the number of grid points with z >= 3600, or -1. */
+int abcmb_hyrex_sizes(int n_grid, int* n_xe, int* n_tm);
+
+/*
+ * The recombination history of every cosmology (recomb_model.get_history,
+ * abcmb/hyrex/hyrex.py:146-206, with helium.py and hydrogen.py):
+ *   T_dev, nH_dev, H_dev [n_cosmo x n_grid]  RecombInputs: T_CMB (eV), n_H
+ *                    (cm^-3) and H (1/s) on lna_axis_full =
+ *                    arange(-log(8001), 0, 5e-4) (hyrex.py:16-90, 131)
+ *   params_dev [n_cosmo]
+ *   xe_dev, lna_xe_dev [n_cosmo x n_xe], tm_dev, lna_tm_dev [n_cosmo x n_tm]
+ *                    the reference's outputs (xe_full, lna_full, Tm, lna_Tm)
+ *                    before reionisation, +inf after the last valid entry
+ *   info_dev [n_cosmo x 16] int32: valid entries of the seven phases,
+ *                    steps of the four ODE phases, joined lengths, status,
+ *                    valid x_e entries
+ * Replaces: the CPU HyRex run of Model (main.py:220).
+ */
+int abcmb_hyrex_forward(int n_cosmo, int n_grid, const double* T_dev, const double* nH_dev, const double* H_dev,
+                        const abcmb_hyrex_params* params_dev, double* xe_dev, double* lna_xe_dev, double* tm_dev,
+                        double* lna_tm_dev, int32_t* info_dev, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Perturbations: PerturbationEvolver.full_evolution (perturbations.py:75)  */
 /* ------------------------------------------------------------------------ */
 

@@ -745,6 +745,7 @@ int oracle_hyrex(const oracle_hyrex_tables* tab, int n_grid, const double* TCMB,
     info[10] = nst;
     if (status != ABCMB_STATUS_OK) goto done;
   }
+  if (LT.valid < 1) { status = ABCMB_STATUS_NONFINITE; goto done; }   /* no T_m point to start from */
   /* 7 three-level atom to lna = 0 (hydrogen.py:704-780) */
   {
     double* s2 = sx;

@@ -208,15 +208,12 @@ def hyrex_grid() -> np.ndarray:
 def hyrex(params: dict, has_ncdm: bool):
     """The oracle's HyRex history for a derived-parameter dict: (rc, out) with
     out = dict(xe, lna_xe, Tm, lna_tm) -- the reference's inf-padded arrays
-    before reionisation -- and info (valid entries and steps per phase)."""
-    from abcmb_b200 import cosmology, constants as cnst, hyrex_tables
+    before reionisation -- and info (valid entries and steps per phase).  The
+    inputs are the same RecombInputs arrays the GPU path samples."""
+    from abcmb_b200 import hyrex_tables, recombination
     t = hyrex_tables.load()
     grid = hyrex_grid()
-    a = np.exp(grid)
-    TCMB = np.ascontiguousarray(params["TCMB0"] / a)
-    nH = np.ascontiguousarray((1 - params["YHe"]) * 3.0 * params["omega_b"] * cnst.H0_over_h ** 2 / 8 / np.pi
-                              / cnst.G / cnst.mH / a ** 3)
-    H = np.ascontiguousarray(np.asarray(cosmology.H(grid, params, has_ncdm), dtype=np.float64))
+    TCMB, nH, H = recombination.recomb_inputs(params, has_ncdm)
     n_xe = ctypes.c_int32(0)
     n_tm = ctypes.c_int32(0)
     lib().oracle_hyrex_sizes(len(grid), ctypes.byref(n_xe), ctypes.byref(n_tm))

@@ -137,3 +137,40 @@ def test_hyrex_history_runs_through_the_oracle_path(fiducial_history):
     b.tables = tab
     rc, pt, ks = oracle.pert_forward(b, packing.pert_settings(w.specs, 500, b))
     assert rc == 0 and (ks["status"] == 0).all()
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from abcmb_b200 import recombination
+    return recombination
+
+
+@pytest.mark.gpu
+def test_hyrex_gpu_matches_oracle(gpu):
+    """abcmb_hyrex_forward against the oracle on the same RecombInputs: every
+    phase ends, the layouts agree, and the histories agree on the common lna
+    grid (a phase boundary may move by a grid point between two rounding
+    patterns: the stop tests are thresholds)."""
+    from oracle import oracle
+    w1, w2, w4 = configs.c1(), configs.c2(), configs.c4(n_cosmo=1)
+    cases = [(cosmology.add_derived_parameters(w1.params_in[0], False, w1.specs), False),
+             (cosmology.add_derived_parameters(w2.params_in[0], True, w2.specs), True),
+             (cosmology.add_derived_parameters(w4.params_in[0], w4.has_ncdm[0], w4.specs), w4.has_ncdm[0])]
+    out = gpu.hyrex_forward([c[0] for c in cases], [c[1] for c in cases])
+    for i, (p, nc) in enumerate(cases):
+        rc, o = oracle.hyrex(p, nc)
+        assert rc == 0
+        info_g, info_o = out["info"][i], o["info"]
+        assert info_g[14] == 0 and info_g[12] == info_o[12] and info_g[13] == info_o[13]
+        assert (np.abs(info_g[:7] - info_o[:7]) <= 2).all(), (info_g, info_o)
+        for x, l in (("xe", "lna_xe"), ("Tm", "lna_tm")):
+            g, lg = out[x][i], out[l][i]
+            ok = np.isfinite(g)
+            n = int(ok.sum())
+            assert ok[:n].all() and not ok[n:].any()
+            oo = np.isfinite(o[x])
+            ref = np.interp(lg[:n], o[l][oo], o[x][oo])
+            assert np.max(np.abs(g[:n] / ref - 1)) < 1e-4, (x, i)
