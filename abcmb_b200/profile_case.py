@@ -4,6 +4,7 @@
     python -m abcmb_b200.profile_case c2        # the 600-k massive-neutrino cosmology
     python -m abcmb_b200.profile_case c1 --los  # C1 with the line of sight
     python -m abcmb_b200.profile_case c4 64 --bg-only   # the background producer alone
+    python -m abcmb_b200.profile_case c4 64 --hyrex     # the recombination histories alone
     ABCMB_B200_LIB=abcmb_b200/libabcmb_b200_phase.so \
         python -m abcmb_b200.profile_case c4 40 --phases  # cycles per phase of pert_kernel
 
@@ -36,10 +37,23 @@ def main():
     ap.add_argument("--los", action="store_true")
     ap.add_argument("--bg-only", action="store_true")
     ap.add_argument("--phases", action="store_true")
+    ap.add_argument("--hyrex", action="store_true")
     a = ap.parse_args()
     import torch
     from . import configs, engine
     w = {"c1": lambda: configs.c1(), "c2": lambda: configs.c2(), "c4": lambda: configs.c4(n_cosmo=a.n)}[a.case]()
+    if a.hyrex:
+        import time
+        from . import cosmology, recombination
+        ps = [cosmology.add_derived_parameters(p, nc, w.specs) for p, nc in zip(w.params_in, w.has_ncdm)]
+        recombination.hyrex_forward(ps, w.has_ncdm)            # warm-up (tables, allocation)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        out = recombination.hyrex_forward(ps, w.has_ncdm)
+        dt = time.perf_counter() - t
+        print(f"recombination histories of {len(ps)} cosmologies: {dt * 1000:.1f} ms wall (host inputs, H2D, kernel, "
+              f"D2H); ODE steps per cosmology max {int(out['info'][:, 8:12].sum(axis=1).max())}")
+        return
     if a.bg_only:
         from . import background_tables as bt, cosmology, packing
         from . import specs as sp
