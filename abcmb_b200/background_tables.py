@@ -293,6 +293,41 @@ def tau_reion_fn(z_reion, p, has_ncdm):
     return np.trapezoid(gam / cosmo.aH(lna, p, has_ncdm), lna)
 
 
+def find_z_reion(p: dict, has_ncdm: bool) -> float:
+    """z_reion from tau_reion (or given), as the reionisation model solves
+    for it (background.py:1014-1016)."""
+    if "tau_reion" in p:
+        return float(brentq(lambda z: tau_reion_fn(z, p, has_ncdm) - p["tau_reion"], 1.0, 40.0, xtol=1e-12))
+    return float(p["z_reion"])
+
+
+def from_hyrex(params: dict, has_ncdm: bool, xe, lna_xe, tm, lna_tm) -> BackgroundTables:
+    """BackgroundTables of a HyRex history (the inf-padded xe_full, lna_full,
+    Tm, lna_Tm of recomb_model, e.g. from recombination.hyrex_forward) the way
+    Background.__init__ takes it (background.py:527-550): the reionisation
+    x_e added, the +inf padding replaced by the last valid value, the padded
+    lengths kept.  Conformal time, optical depth and the line-of-sight arrays
+    are left to abcmb_bg_forward (tau_tab is None)."""
+    p = params
+    xe, lna_xe = np.asarray(xe, dtype=np.float64), np.asarray(lna_xe, dtype=np.float64)
+    tm, lna_tm = np.asarray(tm, dtype=np.float64), np.asarray(lna_tm, dtype=np.float64)
+    n = int(np.argmax(~np.isfinite(xe))) if not np.isfinite(xe).all() else len(xe)
+    nt = int(np.argmax(~np.isfinite(tm))) if not np.isfinite(tm).all() else len(tm)
+    if n < 2 or nt < 2:
+        raise ValueError("a HyRex history needs at least two valid x_e and T_m entries")
+    z_re = find_z_reion(p, has_ncdm)
+    xe_full = xe[:n] + xe_reion(lna_xe[:n], z_re, p)
+    xe_arr = np.concatenate([xe_full, np.full(len(xe) - n, xe_full[-1])])
+    tm_arr = np.concatenate([tm[:nt], np.full(len(tm) - nt, tm[nt - 1])])
+    return BackgroundTables(
+        params=p, has_ncdm=has_ncdm, tau_tab=None, tau0=float("nan"),
+        xe_arr=xe_arr, lna_xe0=float(lna_xe[0]), lna_xe_dx=float(lna_xe[1] - lna_xe[0]),
+        lna_xe_last=float(lna_xe[n - 1]), xe_last=float(xe_full[-1]),
+        tm_arr=tm_arr, lna_tm0=float(lna_tm[0]), lna_tm_dx=float(lna_tm[1] - lna_tm[0]),
+        lna_tm_last=float(lna_tm[nt - 1]), tm_last=float(tm[nt - 1]),
+        lna_transfer_start=float("nan"), lna_rec=float("nan"), z_reion=z_re)
+
+
 # ---------------------------------------------------------------------------
 def _tabulate_tau(p, has_ncdm):
     """Conformal time on LNA_TAU: radiation-era analytic value before -16.1,
@@ -319,10 +354,7 @@ def make_recombination(params: dict, has_ncdm: bool, xe_pad: int = 37, tm_pad: i
     lna_full = np.arange(-math.log(1 + 8000.0), -math.log(1 + 0.0), dx)
     xe_rec, tm_rec = _recombination(p, has_ncdm, lna_full)
 
-    if "tau_reion" in p:
-        z_re = brentq(lambda z: tau_reion_fn(z, p, has_ncdm) - p["tau_reion"], 1.0, 40.0, xtol=1e-12)
-    else:
-        z_re = p["z_reion"]
+    z_re = find_z_reion(p, has_ncdm)
     xe_full = xe_rec + xe_reion(lna_full, z_re, p)
     # inf padding of array_with_padding, replaced by the last valid value
     xe_arr = np.concatenate([xe_full, np.full(xe_pad, xe_full[-1])])

@@ -12,7 +12,10 @@
   depth, visibility and line-of-sight arrays are then produced on the GPU by
   abcmb_bg_forward with the reference's own Kvaerno5 solves
   (``background="device"``, the default), or by the host model
-  (``background="host"``).
+  (``background="host"``).  ``recombination="hyrex"`` takes the
+  recombination history from HyRex on the GPU instead (abcmb_hyrex_forward,
+  in the reference's padded layout); its end-to-end run through the spectra
+  is not yet covered by a GPU test.
 * ``write_class_cl`` / ``read_class_cl``: C_l files in CLASS's ``cl.dat``
   layout (dimensionless l(l+1)/2pi C_l, columns l, TT, EE, TE, BB, phiphi),
   the format the reference's example notebooks compare against
@@ -57,10 +60,17 @@ def _species_names(user_species) -> tuple:
 class B200Model:
     """Model(**specs)(params) on the CUDA path (abcmb/main.py:84-184)."""
 
-    def __init__(self, user_species=None, device=None, background: str = "device", **kwargs):
+    def __init__(self, user_species=None, device=None, background: str = "device", recombination: str = "peebles",
+                 **kwargs):
         if background not in ("device", "host"):
             raise ValueError("background must be 'device' or 'host'")
+        if recombination not in ("peebles", "hyrex"):
+            raise ValueError("recombination must be 'peebles' or 'hyrex'")
+        if recombination == "hyrex" and background != "device":
+            raise ValueError("recombination='hyrex' runs on the GPU: use background='device'")
         self.background = background
+        self.recombination = recombination
+        self.device = device
         specs = sp.load_specs(kwargs)
         self.specs = specs
         self.species = _species_names(user_species)
@@ -79,7 +89,12 @@ class B200Model:
 
     def __call__(self, params: dict) -> Output:
         p = self.add_derived_parameters(params)
-        BG = (bt.make_recombination if self.background == "device" else bt.make_background)(p, self.has_ncdm)
+        if self.recombination == "hyrex":
+            from . import recombination
+            h = recombination.hyrex_forward([p], [self.has_ncdm], self.device)
+            BG = bt.from_hyrex(p, self.has_ncdm, h["xe"][0], h["lna_xe"][0], h["Tm"][0], h["lna_tm"][0])
+        else:
+            BG = (bt.make_recombination if self.background == "device" else bt.make_background)(p, self.has_ncdm)
         PT = self.PE.full_evolution((BG, p))
         tt, te, ee = self.SS.get_Cl(PT, BG, p)
         Pk = self.SS.Pk_lin(self.k_axis_Pk_output, 0.0, PT, p)

@@ -213,3 +213,15 @@ def test_model_setup_mirrors_reference_defaults():
     assert len(m.PE.k_axis_perturbations) > 50 and m.k_axis_Pk_output[-1] <= m.specs["k_max"]
     m2 = B200Model(user_species=("MassiveNeutrino",), l_max=800)
     assert m2.has_ncdm and m2.PE.layout.has_ncdm
+
+
+def test_model_background_and_recombination_options():
+    from abcmb_b200.output import B200Model
+    assert B200Model(l_max=400).background == "device"
+    assert B200Model(l_max=400, recombination="hyrex").recombination == "hyrex"
+    with pytest.raises(ValueError):
+        B200Model(l_max=400, background="gpu")
+    with pytest.raises(ValueError):
+        B200Model(l_max=400, recombination="recfast")
+    with pytest.raises(ValueError):
+        B200Model(l_max=400, recombination="hyrex", background="host")

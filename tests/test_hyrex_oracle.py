@@ -112,21 +112,14 @@ def test_hyrex_history_runs_through_the_oracle_path(fiducial_history):
     from abcmb_b200 import packing
     from oracle import oracle
     p, o = fiducial_history
+    bg = bt.from_hyrex(p, False, o["xe"], o["lna_xe"], o["Tm"], o["lna_tm"])
     ok = np.isfinite(o["xe"])
     n = int(ok.sum())
-    lna = o["lna_xe"][:n]
-    bg = bt.make_recombination(p, False)
-    xe = o["xe"][:n] + bt.xe_reion(lna, bg.z_reion, p)
-    okt = np.isfinite(o["Tm"])
-    nt = int(okt.sum())
-    bg.xe_arr = np.concatenate([xe, np.full(len(o["xe"]) - n, xe[-1])])
-    bg.lna_xe0, bg.lna_xe_dx, bg.lna_xe_last, bg.xe_last = float(lna[0]), float(lna[1] - lna[0]), float(lna[-1]), \
-        float(xe[-1])
-    tm = o["Tm"][:nt]
-    ltm = o["lna_tm"][:nt]
-    bg.tm_arr = np.concatenate([tm, np.full(len(o["Tm"]) - nt, tm[-1])])
-    bg.lna_tm0, bg.lna_tm_dx, bg.lna_tm_last, bg.tm_last = float(ltm[0]), float(ltm[1] - ltm[0]), \
-        float(ltm[-1]), float(tm[-1])
+    assert len(bg.xe_arr) == len(o["xe"]) and len(bg.tm_arr) == len(o["Tm"])
+    assert np.isfinite(bg.xe_arr).all() and (bg.xe_arr[n:] == bg.xe_last).all()
+    assert bg.lna_xe_last == o["lna_xe"][n - 1] and bg.lna_xe_dx == pytest.approx(5e-4, rel=1e-9)
+    np.testing.assert_allclose(bg.xe_arr[:n] - o["xe"][:n], bt.xe_reion(o["lna_xe"][:n], bg.z_reion, p), atol=1e-15)
+    assert bg.on_device
     w = configs.c1(nk=6)
     lay = sp.state_layout(w.specs, False)
     b = packing.pack([bg], [lay], w.kgrids)
