@@ -69,6 +69,9 @@ int oracle_hyrex_sizes(int n_grid, int* n_xe, int* n_tm);
 int oracle_hyrex(const oracle_hyrex_tables* tab, int n_grid, const double* TCMB, const double* nH,
                  const double* H, double YHe, double omega_b, double omega_cdm, double Neff, double* xe_out,
                  double* lna_out, int cap_xe, double* tm_out, double* lna_tm_out, int cap_tm, int* info);
+int oracle_hyrex_rates(const oracle_hyrex_tables* tab, int n_grid, const double* TCMB, const double* nH,
+                       const double* H, double YHe, double omega_b, double omega_cdm, double Neff, double lna,
+                       double xe_he, double xe_h, double* out);
 int oracle_pk_lin(int n_cosmo, const abcmb_cosmo* cosmo, const double* kbuf, const double* pt, int n_save,
                   double k_pivot, int n_kout, const double* kout, int n_z, const double* z, double* pk);
 

@@ -329,6 +329,52 @@ static dl helium_dxHeIIdlna(const hx_t* h, dl xe, dl lna) {
   return ddiv(dmul(ydown, bracket), H);
 }
 
+/* The two rates whose jax.grad derivatives the post-Saha expansions take,
+ * with their forward-mode derivatives: out[0..1] = helium_dxHeIIdlna and its
+ * derivative in x_e (at xe_he, lna), out[2..3] = its derivative in lna and
+ * xHeII_post_Saha's, out[4..5] = dxe_dlna_twophoton(xe_h, T, Tm = T, H, n_H,
+ * Delta = 0) and its derivative in x_e (T, H, n_H from the inputs at lna),
+ * out[6] = xHeII_post_Saha.  For tests: the derivatives against finite
+ * differences. */
+int oracle_hyrex_rates(const oracle_hyrex_tables* tab, int n_grid, const double* TCMB, const double* nH,
+                       const double* H, double YHe, double omega_b, double omega_cdm, double Neff, double lna,
+                       double xe_he, double xe_h, double* out) {
+  hx_t* h = (hx_t*)calloc(1, sizeof(hx_t));
+  h->tab = tab;
+  for (int i = 0; i < HX_NTR * HX_NTM; ++i) {
+    h->logA[0][i] = log(tab->alpha[i * 4 + 0]);
+    h->logA[1][i] = log(tab->alpha[i * 4 + 1]);
+  }
+  for (int i = 0; i < HX_NTR; ++i) h->logR[i] = log(tab->R[i]);
+  h->swift_x = (double*)malloc(sizeof(double) * (tab->n_swift > 0 ? tab->n_swift : 1));
+  for (int i = 0; i < tab->n_swift; ++i) h->swift_x[i] = HX_KB * tab->swift[i * 5];
+  h->n = n_grid;
+  h->l0 = -log(1. + HX_Z0);
+  h->l1 = h->l0 + (double)(n_grid - 1) * HX_SPACING;
+  h->T = TCMB;
+  h->nH = nH;
+  h->H = H;
+  h->YHe = YHe;
+  h->omega_b = omega_b;
+  h->omega_cdm = omega_cdm;
+  h->Neff = Neff;
+  const dl a = helium_dxHeIIdlna(h, (dl){xe_he, 1.}, dc(lna));
+  const dl b = helium_dxHeIIdlna(h, dc(xe_he), (dl){lna, 1.});
+  const dl c = xHeII_post_saha(h, (dl){lna, 1.});
+  const double T = ri_T(h, dc(lna)).v, n = ri_nH(h, dc(lna)).v, Hv = ri_H(h, dc(lna)).v;
+  const dl d = dxe_dlna_twophoton(h, (dl){xe_h, 1.}, T, T, Hv, n, 0.0);
+  out[0] = a.v;
+  out[1] = a.d;
+  out[2] = b.d;
+  out[3] = c.d;
+  out[4] = d.v;
+  out[5] = d.d;
+  out[6] = c.v;
+  free(h->swift_x);
+  free(h);
+  return 0;
+}
+
 /* ---------------------------------------------------------------------- */
 /* Kvaerno3 (Kvaerno, BIT 44 (2004): ESDIRK 3(2), four stages, L-stable    */
 /* gamma, stiffly accurate, embedded solution = stage 3)                   */

@@ -76,6 +76,10 @@ def lib():
         L.oracle_hyrex.argtypes = [ctypes.POINTER(COracleHyrexTables), ctypes.c_int, _dp, _dp, _dp,
                                    ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                    _dp, _dp, ctypes.c_int, _dp, _dp, ctypes.c_int, _ip]
+        L.oracle_hyrex_rates.restype = ctypes.c_int
+        L.oracle_hyrex_rates.argtypes = [ctypes.POINTER(COracleHyrexTables), ctypes.c_int, _dp, _dp, _dp,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp]
         L.oracle_kappa_solve.restype = ctypes.c_int
         L.oracle_kappa_solve.argtypes = [vp, _dp, ctypes.c_double, ctypes.c_int, _ip, _dp]
         L.oracle_pk_lin.restype = ctypes.c_int
@@ -227,3 +231,18 @@ def hyrex(params: dict, has_ncdm: bool):
                             float(params["omega_b"]), float(params["omega_cdm"]), float(params["Neff"]),
                             dptr(xe), dptr(lxe), n_xe.value, dptr(tm), dptr(ltm), n_tm.value, iptr(info))
     return rc, dict(xe=xe, lna_xe=lxe, Tm=tm, lna_tm=ltm, info=info)
+
+
+def hyrex_rates(params: dict, has_ncdm: bool, lna: float, xe_he: float, xe_h: float) -> np.ndarray:
+    """oracle_hyrex_rates: [dxHeII/dlna, its d/dxe, its d/dlna, d xHeII_post_Saha/dlna,
+    dxe/dlna (EMLA, Tm = T, Delta = 0), its d/dxe, xHeII_post_Saha] at lna."""
+    from abcmb_b200 import hyrex_tables, recombination
+    t = hyrex_tables.load()
+    grid = hyrex_grid()
+    TCMB, nH, H = recombination.recomb_inputs(params, has_ncdm)
+    out = np.zeros(7)
+    tabs = COracleHyrexTables(dptr(t.alpha), dptr(t.R), dptr(t.swift), t.swift.shape[0])
+    lib().oracle_hyrex_rates(ctypes.byref(tabs), len(grid), dptr(TCMB), dptr(nH), dptr(H), float(params["YHe"]),
+                             float(params["omega_b"]), float(params["omega_cdm"]), float(params["Neff"]),
+                             float(lna), float(xe_he), float(xe_h), dptr(out))
+    return out

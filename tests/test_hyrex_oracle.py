@@ -167,3 +167,28 @@ def test_hyrex_gpu_matches_oracle(gpu):
             oo = np.isfinite(o[x])
             ref = np.interp(lg[:n], o[l][oo], o[x][oo])
             assert np.max(np.abs(g[:n] / ref - 1)) < 1e-4, (x, i)
+
+
+def test_post_saha_derivatives_match_finite_differences():
+    """The forward-mode derivatives the post-Saha expansions use (jax.grad in
+    the reference) against central differences of the same functions.  In
+    lna the lookups are piecewise linear, so the points sit inside one table
+    cell of the RecombInputs grid and the step stays inside it."""
+    from oracle import oracle
+    w = configs.c1()
+    p = cosmology.add_derived_parameters(w.params_in[0], False, w.specs)
+    grid = oracle.hyrex_grid()
+    for z, xe_he, xe_h in ((2500.0, 1.06, 0.999), (1900.0, 1.02, 0.99), (1650.0, 1.001, 0.97)):
+        i = int(np.searchsorted(grid, -np.log(1 + z)))
+        lna = 0.5 * (grid[i] + grid[i + 1])                      # mid-cell
+        r = oracle.hyrex_rates(p, False, lna, xe_he, xe_h)
+        hx = 1e-6
+        fp = oracle.hyrex_rates(p, False, lna, xe_he + hx, xe_h + hx)
+        fm = oracle.hyrex_rates(p, False, lna, xe_he - hx, xe_h - hx)
+        assert r[1] == pytest.approx((fp[0] - fm[0]) / (2 * hx), rel=1e-5)
+        assert r[5] == pytest.approx((fp[4] - fm[4]) / (2 * hx), rel=1e-5)
+        hl = 1e-5                                                # well inside the 5e-4 cell
+        lp = oracle.hyrex_rates(p, False, lna + hl, xe_he, xe_h)
+        lm = oracle.hyrex_rates(p, False, lna - hl, xe_he, xe_h)
+        assert r[2] == pytest.approx((lp[0] - lm[0]) / (2 * hl), rel=1e-4)
+        assert r[3] == pytest.approx((lp[6] - lm[6]) / (2 * hl), rel=1e-4)
