@@ -154,7 +154,7 @@ int abcmb_hyrex_forward(int n_cosmo, int n_grid, const double* T_dev, const doub
     return fail(ABCMB_ERR_ARG, "abcmb_hyrex_forward: null argument or n_cosmo <= 0");
   int nx = 0, nt = 0;
   if (n_grid < 2 || abcmb::hyrex_sizes(n_grid, &nx, &nt) < 2)
-    return fail(ABCMB_ERR_ARG, "abcmb_hyrex_forward: the grid must reach z = 3600 with two points");
+    return fail(ABCMB_ERR_ARG, "abcmb_hyrex_forward: the grid needs at least two points with z >= 3600");
   if (!abcmb::hyrex_tables_ready()) return fail(ABCMB_ERR_TABLES, "abcmb_hyrex_forward: tables not uploaded");
   cudaError_t e = abcmb::launch_hyrex(n_cosmo, n_grid, T_dev, nH_dev, H_dev, params_dev, xe_dev, lna_xe_dev, tm_dev,
                                       lna_tm_dev, info_dev, static_cast<cudaStream_t>(stream));

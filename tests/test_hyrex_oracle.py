@@ -192,3 +192,22 @@ def test_post_saha_derivatives_match_finite_differences():
         lm = oracle.hyrex_rates(p, False, lna - hl, xe_he, xe_h)
         assert r[2] == pytest.approx((lp[0] - lm[0]) / (2 * hl), rel=1e-4)
         assert r[3] == pytest.approx((lp[6] - lm[6]) / (2 * hl), rel=1e-4)
+
+
+def test_hyrex_c_abi_sizes_and_argument_errors_without_gpu():
+    import ctypes
+    from abcmb_b200 import _lib, recombination
+    lib = _lib.load()
+    n_xe, n_tm = ctypes.c_int32(0), ctypes.c_int32(0)
+    grid = recombination.hyrex_grid()
+    n1 = lib.abcmb_hyrex_sizes(len(grid), ctypes.byref(n_xe), ctypes.byref(n_tm))
+    assert n1 == int(np.count_nonzero(grid <= -np.log(3601.0)))
+    assert n_xe.value == n1 + 4000 + 4096 + 800 + 3 * 8192 and n_tm.value == 2 * 8192
+    assert lib.abcmb_hyrex_sizes(1, ctypes.byref(n_xe), ctypes.byref(n_tm)) == -1
+    p = ctypes.c_void_p(8)
+    assert lib.abcmb_hyrex_forward(0, len(grid), p, p, p, p, p, p, p, p, p, None) == -1
+    assert lib.abcmb_hyrex_forward(1, 1, p, p, p, p, p, p, p, p, p, None) == -1       # a one-point grid
+    assert b"grid" in lib.abcmb_last_error()
+    assert lib.abcmb_hyrex_forward(1, len(grid), p, p, p, p, p, p, p, p, p, None) == -4   # tables not uploaded
+    assert b"tables" in lib.abcmb_last_error()
+    assert lib.abcmb_upload_hyrex_tables(None, p, p, 265) == -1
