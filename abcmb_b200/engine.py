@@ -13,7 +13,7 @@ import torch
 
 from . import _lib
 from . import bessel as bessel_mod
-from .packing import Batch, NFIELDS, NTAU_TAB, CPertSettings, CLosSettings
+from .packing import Batch, NTAU_TAB, CPertSettings, CLosSettings
 
 _uploaded_devices: set = set()
 

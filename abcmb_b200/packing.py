@@ -10,8 +10,6 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .specs import StateLayout
-
 NFIELDS = 21
 NTAU_TAB = 10000        # ABCMB_NTAU_TAB
 FIELD_NAMES = (
