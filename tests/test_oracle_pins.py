@@ -214,3 +214,61 @@ def test_oracle_c1_runs(c1_oracle, c1_small):
     assert np.isfinite(v).all()
     # superhorizon adiabatic mode: eta stays close to its initial value ~1 at the first save point for small k
     assert abs(v[2, 0, 0] - 1.0) < 0.05
+
+
+def test_oracle_solver_converges_to_an_independent_integrator(c1_small):
+    """The restated Kvaerno5 / PID / very-chord / Hermite machinery, start time
+    and initial conditions, run at tight tolerances, against scipy's Radau
+    (rtol 1e-11) on the same right-hand side (oracle_rhs) and output fields:
+    the PerturbationTable of one k mode agrees to 1e-6 of each field's
+    maximum.  (At the reference's default tolerances the same comparison
+    gives 2e-4 to 2e-3 at k = 1e-4 .. 8e-3: the reference's own accuracy.)"""
+    import ctypes
+    from scipy.integrate import solve_ivp
+    from abcmb_b200 import packing
+    from oracle import oracle
+    b = c1_small.batch
+    ik = 0
+    sub = packing.Batch(cosmo=b.cosmo, tables=b.tables, kbuf=b.kbuf, items=np.array([[0, ik]], dtype=np.int32),
+                        pt_size=b.pt_size, n_save=b.n_save, bgs=b.bgs, layouts=b.layouts)
+    st = c1_small.pert_settings()
+    st.rtol_small = st.rtol_large = 1e-10
+    st.atol_small = st.atol_large = 1e-15
+    st.max_steps = 500000
+    rc, pt, ks = oracle.pert_forward(sub, st)
+    assert rc == 0
+    L = oracle.lib()
+    c = np.ascontiguousarray(b.cosmo[:1])
+    cp = ctypes.c_void_p(c.ctypes.data)
+    tab = oracle.dptr(b.tables)
+    ny = int(c[0]["ny"])
+    k = float(b.kbuf[ik])
+    l0 = float(ks["lna_start"][0])
+    y0 = np.zeros(ny)
+    L.oracle_initial_conditions(cp, tab, k, l0, oracle.dptr(y0))
+
+    def rhs(t, y):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        out = np.zeros(ny)
+        L.oracle_rhs(cp, tab, k, float(t), oracle.dptr(y), oracle.dptr(out))
+        return out
+
+    def jac(t, y):                                            # the system is linear: A(t) column by column
+        J = np.zeros((ny, ny))
+        for j in range(ny):
+            e = np.zeros(ny)
+            e[j] = 1.0
+            J[:, j] = rhs(t, e)
+        return J
+
+    save = np.linspace(float(c[0]["lna_transfer_start"]), 0.0, b.n_save)
+    sol = solve_ivp(rhs, (l0, 0.0), y0, method="Radau", jac=jac, rtol=1e-11, atol=1e-16, t_eval=save)
+    assert sol.status == 0
+    ref = np.zeros((packing.NFIELDS, b.n_save))
+    for i, ts in enumerate(save):
+        o = np.zeros(packing.NFIELDS)
+        L.oracle_output_fields(cp, tab, k, float(ts), oracle.dptr(np.ascontiguousarray(sol.y[:, i])), oracle.dptr(o))
+        ref[:, i] = o
+    got = b.pt_view(pt, 0)[:, :, ik]
+    err = (np.abs(got - ref).max(axis=1) / (np.abs(ref).max(axis=1) + 1e-300))[:18]
+    assert err.max() < 1e-6, err
