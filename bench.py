@@ -142,11 +142,19 @@ def cpu_sample(gw, stride: int, n_threads: int):
     oracle.los_forward(one, pt, gw.base.kt, ls, bessel.load(), n_threads)
     t_los = (time.perf_counter() - t0) * nvar
     total = t_ode + t_los
+    # the recombination history of one cosmology on one core (oracle HyRex)
+    from abcmb_b200 import cosmology
+    p0 = cosmology.add_derived_parameters(gw.base.params_in[0], gw.base.has_ncdm[0], gw.base.specs)
+    oracle.hyrex(p0, gw.base.has_ncdm[0])                  # first call: module and table loading
+    t0 = time.perf_counter()
+    oracle.hyrex(p0, gw.base.has_ncdm[0])
+    t_hyrex = time.perf_counter() - t0
     return {"value": 1.0 / total, "unit": UNIT, "cores": n_threads, "kind": "port",
             "sample": f"oracle (C, FP64, OpenMP) on 1 cosmology's 9 gradient variants: every {stride}th k mode of "
                       f"the ODE ({len(sel)}/{n_full} items, scaled) + 1 full line-of-sight run (x{nvar}); "
                       f"s per cosmology+grad: ode {t_ode:.2f} (faster of 2 runs; the other "
                       f"{max(t_runs) * n_full / len(sel):.2f}) los {t_los:.2f}",
+            "hyrex_oracle_ms_per_cosmology_one_core": t_hyrex * 1000.0,
             "ode_one_thread": {"s_per_cosmology": t_ode1, "items": len(sel1),
                                "sample": f"every 16th of the items above ({len(sel1)}) on 1 thread, scaled",
                                "all_cores_speedup": t_ode1 / t_ode}}
@@ -234,6 +242,24 @@ def bg_forward_timing(gw, db, dev, stream):
     return {"ms": ms, "cosmologies": n, "us_per_cosmology": 1000.0 * ms / n, "max_steps_kappa": s.max_steps_kappa,
             "ok": int((res["status"] == 0).sum()), "kappa_steps_max": int(res["n_steps_kappa"].max()),
             "tau_steps_max": int(res["n_steps_tau"].max()), "host_model_ms_per_cosmology": host_ms}
+
+
+def hyrex_timing(w, dev):
+    """The recombination histories (HyRex, abcmb_hyrex_forward) of the batch's
+    base cosmologies on the GPU, outside the timed step: wall time of the call
+    (host sampling of the inputs, transfers, kernel)."""
+    import torch
+    from abcmb_b200 import cosmology, recombination
+    ps = [cosmology.add_derived_parameters(p, nc, w.specs) for p, nc in zip(w.params_in, w.has_ncdm)]
+    recombination.hyrex_forward(ps, w.has_ncdm, dev)
+    torch.cuda.synchronize(dev)
+    t = time.perf_counter()
+    out = recombination.hyrex_forward(ps, w.has_ncdm, dev)
+    torch.cuda.synchronize(dev)
+    ms = (time.perf_counter() - t) * 1000.0
+    return {"ms_wall": ms, "cosmologies": len(ps), "ms_per_cosmology": ms / len(ps),
+            "ode_steps_max": int(out["info"][:, 8:12].sum(axis=1).max()),
+            "includes": "host sampling of the inputs, H2D, kernel, D2H"}
 
 
 def run_reference(args, rank, world):
@@ -429,6 +455,10 @@ def main():
             "ode_steps_mean": float(steps_k.mean()), "host_build_s": t_build}
     if rank == 0 and world == 1:
         line["bg_forward"] = bg_forward_timing(gw, db, dev, stream)
+        try:
+            line["hyrex_forward"] = hyrex_timing(w, dev)
+        except Exception as ex:                            # an extra measurement never costs the line
+            line["hyrex_forward"] = {"error": str(ex)[:200]}
         plain = plain_gpu_fwd_fd(gw, w, dev, stream)
         plain["batched_over_plain"] = value / plain["value"]
         line["plain_gpu_fwd_fd"] = plain
