@@ -262,7 +262,8 @@ typedef struct abcmb_hyrex_params {
  * Upload HyRex's tables once per device (host arrays, as the reference's
  * abcmb/hyrex/tabs files hold them): alpha [100 x 40 x 4] (Alpha_inf.dat,
  * recomb_functions.py:11-24), R [100] (R_inf.dat), swift [n_swift x 5]
- * (fit_swift.dat, hydrogen.py:53).
+ * (fit_swift.dat, hydrogen.py:53).  A second upload replaces the first:
+ * make it only while no abcmb_hyrex_forward launch is in flight.
  */
 int abcmb_upload_hyrex_tables(const double* alpha, const double* R, const double* swift, int n_swift);
 

@@ -98,6 +98,7 @@ typedef struct {
   double l0, l1;
   const double *T, *nH, *H;
   double YHe, omega_b, omega_cdm, Neff;
+  double twog_end;                   /* lna where the two-photon phase ends, -log(701) */
 } hx_t;
 
 /* RecombInputs.TCMB / nH / H: fast_interp(lna, grid[0], grid[-1], arr)
@@ -586,10 +587,9 @@ static void rhs_twophoton(const hx_t* h, double t, const double* y, double* f) {
   const double Delta = correction_delta(h, T);
   f[0] = dxe_dlna_twophoton(h, dc(y[0]), T, Tm, H, nH, Delta).v;
 }
-static double g_twog_end;
 static int ev_twophoton(const hx_t* h, double t, const double* y) {          /* hydrogen.py:365-367 */
-  (void)h; (void)y;
-  return t > g_twog_end;
+  (void)y;
+  return t > h->twog_end;
 }
 
 static void rhs_emla(const hx_t* h, double t, const double* y, double* f) {  /* hydrogen.py:385-419 */
@@ -759,7 +759,7 @@ int oracle_hyrex(const oracle_hyrex_tables* tab, int n_grid, const double* TCMB,
   {
     const double t0 = L.a[L.valid - 1];
     const double y0[1] = {X.a[X.valid - 1]};
-    g_twog_end = -log(HX_Z_TWOG);
+    h->twog_end = -log(HX_Z_TWOG);
     for (int i = 0; i < HX_N_LATE; ++i) sx[i] = sl[i] = INFINITY;
     status = kv3_solve(h, rhs_twophoton, ev_twophoton, 1, t0, y0, 1e-6, 1e-9, 4096, HX_N_LATE, sl, sx, &nsv, &nst);
     join_append(&X, sx, nsv, HX_N_LATE);
