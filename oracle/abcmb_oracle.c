@@ -1426,8 +1426,8 @@ static double rhs_dkappa(const abcmb_cosmo* c, const double* tables, double lna)
  * at the stage time; the step, error estimate, PID controller and end
  * clipping are those of solve_k.  Returns an ABCMB_STATUS_* code; *nsteps =
  * step attempts, d->n = accepted points (including the initial one). */
-static int quad_solve(bg_rhs_fn f, const abcmb_cosmo* c, const double* tables, double t0, double t1,
-                      double y0, double dt0, double rtol, double atol, double pcoeff, double icoeff,
+static int quad_solve(bg_rhs_fn f, double scale, const abcmb_cosmo* c, const double* tables, double t0,
+                      double t1, double y0, double dt0, double rtol, double atol, double pcoeff, double icoeff,
                       double dcoeff, int max_steps, dense_t* d, int* nsteps_out) {
   const double dir = t1 < t0 ? -1. : 1.;
   const double err_order = 5.0, safety = 0.9, factormin = 0.2, factormax = 10.0;
@@ -1440,7 +1440,7 @@ static int quad_solve(bg_rhs_fn f, const abcmb_cosmo* c, const double* tables, d
   if (s1 > s_end) s1 = s_end;
   double y = y0;
   double F[7];
-  F[0] = dir * f(c, tables, dir * s0);
+  F[0] = dir * scale * f(c, tables, dir * s0);
   double prev_inv = 1.0, prev_prev_inv = 1.0;
   int status = ABCMB_STATUS_OK, nsteps = 0;
   d->n = 1;
@@ -1449,7 +1449,7 @@ static int quad_solve(bg_rhs_fn f, const abcmb_cosmo* c, const double* tables, d
     if (nsteps >= max_steps) { status = ABCMB_STATUS_MAX_STEPS; break; }
     nsteps++;
     const double h = s1 - s0;
-    for (int i = 1; i < 7; ++i) F[i] = dir * f(c, tables, dir * (s0 + KV_C[i] * h));
+    for (int i = 1; i < 7; ++i) F[i] = dir * scale * f(c, tables, dir * (s0 + KV_C[i] * h));
     double acc = 0., acce = 0.;
     for (int j = 0; j < 6; ++j) {
       acc += KV_A[6][j] * F[j];
@@ -1552,9 +1552,9 @@ static int bg_one(abcmb_cosmo* c, double* tables, const abcmb_bg_settings* s, ab
   const double sq_or = sqrt(omega_r_of(c));
   /* conformal time: analytic before lna_cut, Kvaerno5 after */
   const double tau_cut = exp(lna_cut) / tscale / sq_or;
-  int st_tau = quad_solve(rhs_dtau, c, tables, lna_cut, 0.0, tau_cut, 1e-5, 1e-8, 1e-8, 0., 1., 0.,
+  int st_tau = quad_solve(rhs_dtau, 1.0, c, tables, lna_cut, 0.0, tau_cut, 1e-5, 1e-8, 1e-8, 0., 1., 0.,
                           s->max_steps_tau, dt, &st->n_steps_tau);
-  int st_kap = quad_solve(rhs_dkappa, c, tables, 0.0, -10.0, 0.0, -1e-3, 1e-10, 1e-10, 0.4, 0.3, 0.,
+  int st_kap = quad_solve(rhs_dkappa, 1.0, c, tables, 0.0, -10.0, 0.0, -1e-3, 1e-10, 1e-10, 0.4, 0.3, 0.,
                           s->max_steps_kappa, dk, &st->n_steps_kappa);
   st->n_accepted_kappa = dk->n - 1;
   st->status = st_tau != ABCMB_STATUS_OK ? st_tau : st_kap;
@@ -1617,10 +1617,6 @@ static int bg_one(abcmb_cosmo* c, double* tables, const abcmb_bg_settings* s, ab
  * rhs_scale: how far the reference's step sequence moves under a rounding-
  * level change of the integrand.  Returns the status; *nsteps = attempts,
  * *kappa_end = kappa(-10). */
-static double g_rhs_scale = 1.0;
-static double rhs_dkappa_scaled(const abcmb_cosmo* c, const double* tables, double lna) {
-  return g_rhs_scale * rhs_dkappa(c, tables, lna);
-}
 
 int oracle_kappa_solve(const abcmb_cosmo* c, const double* tables, double rhs_scale, int max_steps,
                        int* nsteps, double* kappa_end) {
@@ -1628,10 +1624,8 @@ int oracle_kappa_solve(const abcmb_cosmo* c, const double* tables, double rhs_sc
   d.s = (double*)malloc(sizeof(double) * 3 * (size_t)(max_steps + 1));
   d.y = d.s + max_steps + 1;
   d.f = d.y + max_steps + 1;
-  g_rhs_scale = rhs_scale;
-  int st = quad_solve(rhs_dkappa_scaled, c, tables, 0.0, -10.0, 0.0, -1e-3, 1e-10, 1e-10, 0.4, 0.3, 0.,
+  int st = quad_solve(rhs_dkappa, rhs_scale, c, tables, 0.0, -10.0, 0.0, -1e-3, 1e-10, 1e-10, 0.4, 0.3, 0.,
                       max_steps, &d, nsteps);
-  g_rhs_scale = 1.0;
   *kappa_end = d.y[d.n - 1];
   free(d.s);
   return st;
