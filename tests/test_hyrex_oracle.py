@@ -211,3 +211,23 @@ def test_hyrex_c_abi_sizes_and_argument_errors_without_gpu():
     assert lib.abcmb_hyrex_forward(1, len(grid), p, p, p, p, p, p, p, p, p, None) == -4   # tables not uploaded
     assert b"tables" in lib.abcmb_last_error()
     assert lib.abcmb_upload_hyrex_tables(None, p, p, 265) == -1
+
+
+def test_hyrex_agrees_with_the_host_model_across_a_batch():
+    """C4 draws (0/1/3 massive neutrinos, parameters within 5 % of the
+    fiducial): every history completes, and through hydrogen recombination and
+    freeze-out it stays within 2 % of the host model's Peebles atom."""
+    from oracle import oracle
+    w = configs.c4(n_cosmo=6)
+    grid = oracle.hyrex_grid()
+    zg = np.exp(-grid) - 1
+    m = (zg > 30) & (zg < 1600)
+    for p_in, nc in zip(w.params_in, w.has_ncdm):
+        p = cosmology.add_derived_parameters(p_in, nc, w.specs)
+        rc, o = oracle.hyrex(p, nc)
+        assert rc == 0 and (o["info"][:7] > 0).all()
+        ok = np.isfinite(o["xe"])
+        xo = np.interp(grid, o["lna_xe"][ok], o["xe"][ok])
+        bg = bt.make_recombination(p, nc)
+        xh = bg.xe_arr[:len(grid)] - bt.xe_reion(grid, bg.z_reion, p)
+        assert np.max(np.abs(xo[m] / xh[m] - 1)) < 0.02
