@@ -82,6 +82,11 @@ int g_last_grid = 0;
 namespace abcmb {
 // error message for abcmb_last_error from entry points in other files
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+// the launch configuration every perturbation entry point shares: warps per
+// block (abcmb_set_pert_warps_per_block) and the grid of the last launch
+// (abcmb_last_pert_grid)
+int pert_warps_per_block() { return g_warps_per_block; }
+void set_last_pert_grid(int grid) { g_last_grid = grid; }
 }  // namespace abcmb
 
 extern "C" {
@@ -350,7 +355,8 @@ int abcmb_set_pert_warps_per_block(int w) {
   return ABCMB_OK;
 }
 
-/* Grid size of the last perturbation launch (diagnostics). */
+/* Per-phase cycle counts of the perturbation kernel (a library built with
+ * ABCMB_PHASE_CLOCKS only). */
 int abcmb_pert_phase_clocks(uint64_t* cycles, int reset) {
   if (!cycles) return fail(ABCMB_ERR_ARG, "abcmb_pert_phase_clocks: null argument");
   const int rc = abcmb::pert_phase_clocks(reinterpret_cast<unsigned long long*>(cycles), reset);
@@ -359,6 +365,7 @@ int abcmb_pert_phase_clocks(uint64_t* cycles, int reset) {
   return ABCMB_OK;
 }
 
+/* Grid size of the last perturbation launch (diagnostics). */
 int abcmb_last_pert_grid(void) { return g_last_grid; }
 
 }  // extern "C"

@@ -33,6 +33,8 @@ cudaError_t launch_pert(int n_cosmo, const abcmb_cosmo* cosmo, const double* tab
                         int n_items, const int32_t* items, const abcmb_pert_settings& s, double* pt,
                         abcmb_kstat* kstat, void* ws, cudaStream_t stream, int warps_per_block, int* grid_out);
 void set_last_error(const std::string& msg);
+int pert_warps_per_block();
+void set_last_pert_grid(int grid);
 }  // namespace abcmb
 
 // queue counter (256 B) + lna1 (256 B for <= 32 cosmologies) + two start grids
@@ -91,8 +93,10 @@ extern "C" int abcmb_pert_forward_noalloc(int n_cosmo, const abcmb_cosmo* cosmo_
     }
     scratch = g_noalloc_addr[dev];
   }
+  int grid = 0;
   e = abcmb::launch_pert(n_cosmo, cosmo_dev, tables_dev, k_dev, n_items, items_dev, *settings, pt_dev, kstat_dev,
-                         scratch, static_cast<cudaStream_t>(stream), 4, nullptr);
+                         scratch, static_cast<cudaStream_t>(stream), abcmb::pert_warps_per_block(), &grid);
+  abcmb::set_last_pert_grid(grid);
   if (e != cudaSuccess) {
     abcmb::set_last_error(std::string("abcmb_pert_forward_noalloc: ") + cudaGetErrorString(e));
     return ABCMB_ERR_CUDA;

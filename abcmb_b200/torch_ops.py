@@ -110,16 +110,19 @@ class ClWithGrad(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, theta: Tensor, base) -> Tensor:
+        import dataclasses
         from . import configs, engine, gradients
         th = theta.detach().cpu().numpy()
-        for i, p in enumerate(base.params_in):
+        # a private copy: the caller's workload keeps its own parameters
+        w = dataclasses.replace(base, params_in=[dict(p) for p in base.params_in], batch=None)
+        for i, p in enumerate(w.params_in):
             for j, name in enumerate(configs.GRAD_PARAMS):
                 p[name] = float(th[i, j])
-        gw = gradients.expand(base)
+        gw = gradients.expand(w)
         db = engine.DeviceBatch.upload(gw.batch, theta.device if theta.is_cuda else None)
-        db.pert_forward(base.pert_settings())
+        db.pert_forward(w.pert_settings())
         db.check_status()
-        lr = engine.LosRunner(db, base.kt, base.los_settings(), want_dns=True)
+        lr = engine.LosRunner(db, w.kt, w.los_settings(), want_dns=True)
         lr.run()
         n_out = lr.n_out
         cl_all = lr.cl.cpu().numpy().reshape(-1, 3, n_out)

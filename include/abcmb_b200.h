@@ -330,7 +330,9 @@ int abcmb_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev,
  * abcmb_pert_forward for callers that cannot allocate device memory (no
  * cudaMalloc, no workspace of their own: e.g. code inside a framework that
  * owns every device byte).  No counterpart in the reference.  Same inputs,
- * outputs and results as abcmb_pert_forward, but the scratch lives in a
+ * outputs and results as abcmb_pert_forward (the same warps per block from
+ * abcmb_set_pert_warps_per_block; abcmb_last_pert_grid reports its launch
+ * too), but the scratch lives in a
  * library-owned static device array (about 1.2 MiB per device, held until
  * the process exits), so:
  *   - n_cosmo must not exceed ABCMB_PERT_NOALLOC_MAX_COSMO
