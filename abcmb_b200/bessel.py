@@ -35,7 +35,8 @@ class BesselTables:
 
 
 def reference_table_dir() -> str | None:
-    """Directory of the text tables: $ABCMB_BESSEL_DIR or the installed abcmb package."""
+    """Directory of the text tables: $ABCMB_BESSEL_DIR, the installed abcmb package, or
+    the reference installed under baseline/_ref."""
     d = os.environ.get("ABCMB_BESSEL_DIR")
     if d and os.path.isfile(os.path.join(d, "l.txt")):
         return d
@@ -49,6 +50,11 @@ def reference_table_dir() -> str | None:
                     return cand
     except (ImportError, ValueError):
         pass
+    # the reference installed beside the repository (pip install --target baseline/_ref)
+    cand = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "baseline", "_ref", "abcmb",
+                        "bessel_tab")
+    if os.path.isfile(os.path.join(cand, "l.txt")):
+        return cand
     return None
 
 

@@ -28,7 +28,8 @@ class HyrexTables:
 
 
 def reference_table_dir() -> str | None:
-    """Directory of the text tables: $ABCMB_HYREX_DIR or the installed abcmb package."""
+    """Directory of the text tables: $ABCMB_HYREX_DIR, the installed abcmb package, or
+    the reference installed under baseline/_ref."""
     d = os.environ.get("ABCMB_HYREX_DIR")
     if d and os.path.isfile(os.path.join(d, "Alpha_inf.dat")):
         return d
@@ -42,6 +43,11 @@ def reference_table_dir() -> str | None:
                     return cand
     except (ImportError, ValueError):
         pass
+    # the reference installed beside the repository (pip install --target baseline/_ref)
+    cand = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "baseline", "_ref", "abcmb",
+                        "hyrex", "tabs")
+    if os.path.isfile(os.path.join(cand, "Alpha_inf.dat")):
+        return cand
     return None
 
 
