@@ -343,11 +343,36 @@ def _tabulate_tau(p, has_ncdm):
     return tab
 
 
-def make_recombination(params: dict, has_ncdm: bool, xe_pad: int = 37, tm_pad: int = 29) -> BackgroundTables:
+# Lengths of HyRex's output arrays: recomb_model.get_history joins the seven
+# phases' fixed-size buffers with array_with_padding.concat
+# (abcmb/hyrex/hyrex.py:146-206, array_with_padding.py:41-83), so on the
+# 17 975-point lna_axis_full x_e always has 35 069 entries and T_m 16 384,
+# +inf after the last valid one (abcmb_hyrex_sizes gives the same numbers).
+HYREX_XE_LEN = 35069
+HYREX_TM_LEN = 16384
+# The two x_e / T_m layouts of the synthetic tables: "hyrex" pads the valid
+# entries to HyRex's lengths (what the reference's Background receives);
+# "compact" pads them by a few entries only.  The padded length enters every
+# lookup (BG.xe / BG.Tm scale the index by (n - 1) / n, n the padded length,
+# background.py:593-603, 647-657), so the two give slightly different
+# histories.
+XE_LAYOUTS = ("hyrex", "compact")
+
+
+def _pads(layout: str, n_xe_valid: int, n_tm_valid: int):
+    if layout == "hyrex":
+        return HYREX_XE_LEN - n_xe_valid, HYREX_TM_LEN - n_tm_valid
+    if layout == "compact":
+        return 37, 29
+    raise ValueError(f"x_e layout must be one of {XE_LAYOUTS}, not {layout!r}")
+
+
+def make_recombination(params: dict, has_ncdm: bool, layout: str = "compact") -> BackgroundTables:
     """The recombination and reionisation part of the synthetic background:
-    x_e (with reionisation) and T_m tables in HyRex's padded format and
-    z_reion.  The conformal-time table, the optical depth and the
-    line-of-sight arrays are left to abcmb_bg_forward (tau_tab is None)."""
+    x_e (with reionisation) and T_m tables in HyRex's padded format (padded
+    to HyRex's own lengths with layout="hyrex", by a few entries with
+    "compact") and z_reion.  The conformal-time table, the optical depth and
+    the line-of-sight arrays are left to abcmb_bg_forward (tau_tab is None)."""
     p = params
     # x_e grid: HyRex lna_axis_full = arange(-log(1+8000), 0, 5e-4)
     dx = 5.0e-4
@@ -356,12 +381,13 @@ def make_recombination(params: dict, has_ncdm: bool, xe_pad: int = 37, tm_pad: i
 
     z_re = find_z_reion(p, has_ncdm)
     xe_full = xe_rec + xe_reion(lna_full, z_re, p)
-    # inf padding of array_with_padding, replaced by the last valid value
-    xe_arr = np.concatenate([xe_full, np.full(xe_pad, xe_full[-1])])
-    lna_xe_arr = lna_full
     # T_m table starts at the late (z ~ 700) phase like HyRex's lna_Tm
     i_tm = int(np.searchsorted(lna_full, -math.log(1 + 700.0)))
     lna_tm = lna_full[i_tm:]
+    xe_pad, tm_pad = _pads(layout, len(xe_full), len(lna_tm))
+    # inf padding of array_with_padding, replaced by the last valid value
+    xe_arr = np.concatenate([xe_full, np.full(xe_pad, xe_full[-1])])
+    lna_xe_arr = lna_full
     tm_arr = np.concatenate([tm_rec[i_tm:], np.full(tm_pad, tm_rec[-1])])
 
     return BackgroundTables(
@@ -397,7 +423,7 @@ def complete_on_host(bg: BackgroundTables) -> BackgroundTables:
     return bg
 
 
-def make_background(params: dict, has_ncdm: bool, xe_pad: int = 37, tm_pad: int = 29) -> BackgroundTables:
+def make_background(params: dict, has_ncdm: bool, layout: str = "compact") -> BackgroundTables:
     """Synthetic Background for one cosmology (derived params dict in), all
-    of it on the host."""
-    return complete_on_host(make_recombination(params, has_ncdm, xe_pad, tm_pad))
+    of it on the host; layout as make_recombination."""
+    return complete_on_host(make_recombination(params, has_ncdm, layout))

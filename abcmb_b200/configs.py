@@ -15,7 +15,9 @@ configurations it is measured on, built from its own defaults:
       l_max_massless_nu=17, l_max_massive_nu=17); C_l to 2500.
 
 Background tables come from background_tables.make_background (synthetic
-recombination standing in for HyRex).  Seed: numpy default_rng(20261203).
+recombination standing in for HyRex), by default with x_e / T_m padded to
+HyRex's own output lengths (xe_layout="hyrex").  Seed: numpy
+default_rng(20261203).
 """
 from __future__ import annotations
 
@@ -50,13 +52,16 @@ class Workload:
     kt: np.ndarray = None
     idx_min: int = 0
     idx_max: int = 0
+    # x_e / T_m table layout (background_tables.XE_LAYOUTS): "hyrex" is the
+    # padded length the reference's Background receives from HyRex
+    xe_layout: str = "hyrex"
 
     def build(self, n_save: int = 500):
         self.bgs = []
         self.layouts = []
         for p_in, ncdm in zip(self.params_in, self.has_ncdm):
             p = cosmology.add_derived_parameters(p_in, ncdm, self.specs)
-            self.bgs.append(bt.make_background(p, ncdm))
+            self.bgs.append(bt.make_background(p, ncdm, self.xe_layout))
             self.layouts.append(sp.state_layout(self.specs, ncdm))
         self.batch = packing.pack(self.bgs, self.layouts, self.kgrids, n_save=n_save)
         ks = dict(self.specs)
@@ -66,6 +71,14 @@ class Workload:
         self.idx_min, self.idx_max, _ = sp.ell_index_range(B.l_tab, int(self.specs["l_min"]), self.l_max,
                                                            self.lensing)
         return self
+
+    def select(self, indices) -> "Workload":
+        """A workload of some of this one's cosmologies (same specs and
+        layout; not built)."""
+        idx = list(indices)
+        return Workload(self.name, dict(self.specs), [dict(self.params_in[i]) for i in idx],
+                        [self.has_ncdm[i] for i in idx], [self.kgrids[i] for i in idx], self.l_max, self.lensing,
+                        xe_layout=self.xe_layout)
 
     @property
     def l_los(self) -> int:
@@ -86,20 +99,22 @@ class Workload:
                                      int(self.batch.cosmo["nk"].max()))
 
 
-def c1(nk: int = 200, l_max: int = 1500, lensing: bool = False) -> Workload:
+def c1(nk: int = 200, l_max: int = 1500, lensing: bool = False, xe_layout: str = "hyrex") -> Workload:
     specs = sp.load_specs(dict(l_max=l_max, lensing=lensing, l_max_g=12, l_max_pol_g=12, l_max_massless_nu=12))
-    return Workload("C1", specs, [dict(FIDUCIAL)], [False], [np.geomspace(1e-4, 0.5, nk)], l_max, lensing)
+    return Workload("C1", specs, [dict(FIDUCIAL)], [False], [np.geomspace(1e-4, 0.5, nk)], l_max, lensing,
+                    xe_layout=xe_layout)
 
 
-def c2(nk: int = 600, l_max: int = 2500, lmax_h: int = 30) -> Workload:
+def c2(nk: int = 600, l_max: int = 2500, lmax_h: int = 30, xe_layout: str = "hyrex") -> Workload:
     specs = sp.load_specs(dict(l_max=l_max, lensing=False, l_max_g=lmax_h, l_max_pol_g=lmax_h,
                                l_max_massless_nu=lmax_h, l_max_massive_nu=lmax_h))
     p = dict(FIDUCIAL)
     p.update(N_nu_massive=1, m_nu_massive=0.06)
-    return Workload("C2", specs, [p], [True], [np.geomspace(1e-5, 1.0, nk)], l_max)
+    return Workload("C2", specs, [p], [True], [np.geomspace(1e-5, 1.0, nk)], l_max, xe_layout=xe_layout)
 
 
-def c4(n_cosmo: int = 64, l_max: int = 2500, nk_range=(400, 800), seed: int = SEED) -> Workload:
+def c4(n_cosmo: int = 64, l_max: int = 2500, nk_range=(400, 800), seed: int = SEED,
+       xe_layout: str = "hyrex") -> Workload:
     rng = np.random.default_rng(seed)
     specs = sp.load_specs(dict(l_max=l_max, lensing=False))
     params, ncdm, kgrids = [], [], []
@@ -114,7 +129,7 @@ def c4(n_cosmo: int = 64, l_max: int = 2500, nk_range=(400, 800), seed: int = SE
         params.append(p)
         ncdm.append(nnu > 0)
         kgrids.append(np.geomspace(1e-5, 1.0, nk))
-    return Workload("C4", specs, params, ncdm, kgrids, l_max)
+    return Workload("C4", specs, params, ncdm, kgrids, l_max, xe_layout=xe_layout)
 
 
 # three massive species already carry N_eff = 3 x 1.0132 (T_nu_massive =
@@ -125,7 +140,8 @@ NEFF_MIN_THREE_MASSIVE = 3.05
 C5_MAX_STEPS = 16384
 
 
-def c5(n_cosmo: int = 256, l_max: int = 3000, nk_range=(400, 800), seed: int = SEED, k_max: float = 5.0) -> Workload:
+def c5(n_cosmo: int = 256, l_max: int = 3000, nk_range=(400, 800), seed: int = SEED, k_max: float = 5.0,
+       xe_layout: str = "hyrex") -> Workload:
     """Lensed batch: C4's parameter draws plus N_eff uniform in 2.8..3.4
     (3.05..3.4 with three massive species), lensed TT/TE/EE to l_max with the
     line of sight to l_max + 500, k grids geomspace(1e-5, k_max, Nk') with Nk'
@@ -149,7 +165,7 @@ def c5(n_cosmo: int = 256, l_max: int = 3000, nk_range=(400, 800), seed: int = S
         params.append(p)
         ncdm.append(nnu > 0)
         kgrids.append(np.geomspace(1e-5, k_max, int(round(nk * dec))))
-    return Workload("C5", specs, params, ncdm, kgrids, l_max, lensing=True)
+    return Workload("C5", specs, params, ncdm, kgrids, l_max, lensing=True, xe_layout=xe_layout)
 
 
 # P(k) of the lensed batch: z in {0, 1, 2, 3}, k to 5 / Mpc

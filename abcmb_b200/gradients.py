@@ -43,9 +43,9 @@ def fd_variants(p_in: dict, rel_step: float = REL_STEP):
 
 
 def _bg_job(args):
-    p_in, ncdm, specs = args
+    p_in, ncdm, specs, layout = args
     p = cosmology.add_derived_parameters(p_in, ncdm, specs)
-    return bt.make_background(p, ncdm)
+    return bt.make_background(p, ncdm, layout)
 
 
 @dataclass
@@ -94,7 +94,7 @@ def expand(w: Workload, n_save: int = 500, processes: int = 0, rel_step: float =
         entries = [(v[0], v[1], v[2]) for v in var]
         base_index = len(jobs)
         for v in var:
-            jobs.append((v[3], ncdm, w.specs))
+            jobs.append((v[3], ncdm, w.specs, w.xe_layout))
             layouts.append(sp.state_layout(w.specs, ncdm))
             kgrids.append(kg)
             alias.append(None)

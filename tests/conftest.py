@@ -16,7 +16,7 @@ def pytest_configure(config):
 def c1_small():
     """C1 cosmology with 40 k modes: seconds on the oracle."""
     from abcmb_b200 import configs
-    return configs.c1(nk=40).build()
+    return configs.c1(nk=40, xe_layout="compact").build()
 
 
 @pytest.fixture(scope="session")

@@ -17,7 +17,7 @@ from abcmb_b200 import specs as sp
 
 def _recombination_batch(n_cosmo=3, nk=12):
     """C4 draws (both with and without massive neutrinos), x_e / T_m only."""
-    w = configs.c4(n_cosmo=n_cosmo, nk_range=(nk, nk))
+    w = configs.c4(n_cosmo=n_cosmo, nk_range=(nk, nk), xe_layout="compact")
     recs, lays, hosts = [], [], []
     for p_in, ncdm in zip(w.params_in, w.has_ncdm):
         p = cosmology.add_derived_parameters(p_in, ncdm, w.specs)
@@ -198,7 +198,7 @@ def test_device_background_pipeline_matches_oracle(gpu):
     within the optical depth's rounding-level spread."""
     from abcmb_b200 import bessel
     from oracle import oracle
-    w = configs.c1(nk=40, l_max=400)
+    w = configs.c1(nk=40, l_max=400, xe_layout="compact")
     p = cosmology.add_derived_parameters(w.params_in[0], False, w.specs)
     lay = sp.state_layout(w.specs, False)
     b = packing.pack([bt.make_recombination(p, False)], [lay], w.kgrids)

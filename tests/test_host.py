@@ -53,7 +53,7 @@ def test_derived_parameters():
 
 def test_pack_offsets_and_order():
     from abcmb_b200 import configs
-    w = configs.c4(n_cosmo=3, nk_range=(10, 14)).build()
+    w = configs.c4(n_cosmo=3, nk_range=(10, 14), xe_layout="compact").build()
     b = w.batch
     assert b.cosmo.dtype.itemsize == 304
     assert (b.cosmo["off_tau"] % 32 == 0).all() and (b.cosmo["off_pt"] % 32 == 0).all()
@@ -122,7 +122,7 @@ def test_gradient_variants_and_assembly():
     assert len(var) == 9 and var[0][0] is None
     assert {v[0] for v in var[1:]} == set(gradients.FD_PARAMS)
     # assembly on synthetic C_l linear in the parameters recovers the slopes exactly
-    w = configs.c4(n_cosmo=1)
+    w = configs.c4(n_cosmo=1, xe_layout="compact")
     gw = gradients.GradWorkload(base=w, variants=[[(v[0], v[1], v[2]) for v in var]], batch=None, n_var=9)
     slope = {"h": 2.0, "omega_b": -3.0, "omega_cdm": 0.5, "tau_reion": 7.0}
     cl = np.zeros((9, 3, 4))
@@ -141,7 +141,7 @@ def test_expanded_workload_los_settings():
     """The gradient-expanded workload (what bench.py runs) carries a valid
     line-of-sight range without a separate build()."""
     from abcmb_b200 import configs, gradients
-    w = configs.c4(n_cosmo=2, nk_range=(30, 40))
+    w = configs.c4(n_cosmo=2, nk_range=(30, 40), xe_layout="compact")
     gradients.expand(w, processes=1)
     ls = w.los_settings()
     assert ls.l_max == w.l_max == 2500 and ls.idx_max > ls.idx_min >= 0 and ls.nkt > 100
@@ -154,7 +154,7 @@ def test_lensed_expansion_shares_perturbations():
     cosmology's tables and PerturbationTable with no work items, and the
     assembly takes central differences for them."""
     from abcmb_b200 import configs, gradients
-    w = configs.c5(n_cosmo=2, l_max=300, nk_range=(30, 40))
+    w = configs.c5(n_cosmo=2, l_max=300, nk_range=(30, 40), xe_layout="compact")
     gw = gradients.expand(w, processes=1)
     b = gw.batch
     assert gw.n_var == 13 and b.n_cosmo == 26
@@ -225,3 +225,23 @@ def test_model_background_and_recombination_options():
         B200Model(l_max=400, recombination="recfast")
     with pytest.raises(ValueError):
         B200Model(l_max=400, recombination="hyrex", background="host")
+
+
+def test_hyrex_layout_lengths_match_hyrex_sizes():
+    """The synthetic tables' "hyrex" layout pads x_e / T_m to the lengths
+    HyRex's own buffers give (abcmb_hyrex_sizes, a host-side function of the
+    library), and packing carries the padded length into the lookup."""
+    import ctypes
+    from abcmb_b200 import _lib, background_tables as bt, configs, cosmology, recombination
+    lib = _lib.load()
+    n_xe, n_tm = ctypes.c_int(), ctypes.c_int()
+    assert lib.abcmb_hyrex_sizes(len(recombination.hyrex_grid()), ctypes.byref(n_xe), ctypes.byref(n_tm)) > 0
+    assert (n_xe.value, n_tm.value) == (bt.HYREX_XE_LEN, bt.HYREX_TM_LEN)
+    w = configs.c1(nk=4)
+    p = cosmology.add_derived_parameters(w.params_in[0], False, w.specs)
+    rec = bt.make_recombination(p, False, "hyrex")
+    assert rec.xe_arr.shape == (bt.HYREX_XE_LEN,) and rec.tm_arr.shape == (bt.HYREX_TM_LEN,)
+    assert rec.xe_arr[-1] == rec.xe_last and rec.tm_arr[-1] == rec.tm_last
+    b = w.build().batch
+    assert int(b.cosmo["n_xe"][0]) == bt.HYREX_XE_LEN
+    assert b.cosmo["lna_xe_max"][0] == pytest.approx(rec.lna_xe0 + bt.HYREX_XE_LEN * rec.lna_xe_dx, rel=1e-15)

@@ -42,7 +42,7 @@ def test_kvaerno3_order_conditions():
 @pytest.fixture(scope="module")
 def fiducial_history():
     from oracle import oracle
-    w = configs.c1()
+    w = configs.c1(xe_layout="compact")
     p = cosmology.add_derived_parameters(w.params_in[0], False, w.specs)
     rc, out = oracle.hyrex(p, False)
     assert rc == 0
@@ -97,7 +97,7 @@ def test_hyrex_history_limits_and_independent_model(fiducial_history):
 
 def test_hyrex_massive_neutrinos_and_helium_fraction():
     from oracle import oracle
-    w = configs.c2()
+    w = configs.c2(xe_layout="compact")
     p = cosmology.add_derived_parameters(dict(w.params_in[0], YHe=0.26), True, w.specs)
     rc, o = oracle.hyrex(p, True)
     assert rc == 0 and (o["info"][:7] > 0).all()
@@ -120,7 +120,7 @@ def test_hyrex_history_runs_through_the_oracle_path(fiducial_history):
     assert bg.lna_xe_last == o["lna_xe"][n - 1] and bg.lna_xe_dx == pytest.approx(5e-4, rel=1e-9)
     np.testing.assert_allclose(bg.xe_arr[:n] - o["xe"][:n], bt.xe_reion(o["lna_xe"][:n], bg.z_reion, p), atol=1e-15)
     assert bg.on_device
-    w = configs.c1(nk=6)
+    w = configs.c1(nk=6, xe_layout="compact")
     lay = sp.state_layout(w.specs, False)
     b = packing.pack([bg], [lay], w.kgrids)
     rc, cos, tab, st = oracle.bg_forward(b, packing.bg_settings())
@@ -148,7 +148,8 @@ def test_hyrex_gpu_matches_oracle(gpu):
     grid (a phase boundary may move by a grid point between two rounding
     patterns: the stop tests are thresholds)."""
     from oracle import oracle
-    w1, w2, w4 = configs.c1(), configs.c2(), configs.c4(n_cosmo=1)
+    w1, w2 = configs.c1(xe_layout="compact"), configs.c2(xe_layout="compact")
+    w4 = configs.c4(n_cosmo=1, xe_layout="compact")
     cases = [(cosmology.add_derived_parameters(w1.params_in[0], False, w1.specs), False),
              (cosmology.add_derived_parameters(w2.params_in[0], True, w2.specs), True),
              (cosmology.add_derived_parameters(w4.params_in[0], w4.has_ncdm[0], w4.specs), w4.has_ncdm[0])]
@@ -175,7 +176,7 @@ def test_post_saha_derivatives_match_finite_differences():
     lna the lookups are piecewise linear, so the points sit inside one table
     cell of the RecombInputs grid and the step stays inside it."""
     from oracle import oracle
-    w = configs.c1()
+    w = configs.c1(xe_layout="compact")
     p = cosmology.add_derived_parameters(w.params_in[0], False, w.specs)
     grid = oracle.hyrex_grid()
     for z, xe_he, xe_h in ((2500.0, 1.06, 0.999), (1900.0, 1.02, 0.99), (1650.0, 1.001, 0.97)):
@@ -218,7 +219,7 @@ def test_hyrex_agrees_with_the_host_model_across_a_batch():
     fiducial): every history completes, and through hydrogen recombination and
     freeze-out it stays within 2 % of the host model's Peebles atom."""
     from oracle import oracle
-    w = configs.c4(n_cosmo=6)
+    w = configs.c4(n_cosmo=6, xe_layout="compact")
     grid = oracle.hyrex_grid()
     zg = np.exp(-grid) - 1
     m = (zg > 30) & (zg < 1600)

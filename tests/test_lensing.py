@@ -88,7 +88,7 @@ def test_lens_argument_errors():
 @pytest.fixture(scope="module")
 def lensed_c1():
     """Oracle pipeline for C1 (40 k modes), lensed output to l = 400."""
-    w = configs.c1(nk=40, l_max=400, lensing=True).build()
+    w = configs.c1(nk=40, l_max=400, lensing=True, xe_layout="compact").build()
     rc, pt, _ = oracle.pert_forward(w.batch, w.pert_settings())
     assert rc == 0
     rc, _, cl = oracle.los_forward(w.batch, pt, w.kt, w.los_settings(), bessel.load())
@@ -168,7 +168,7 @@ def test_lensed_end_to_end_matches_oracle(lensed_c1):
 def test_lens_batch_equals_single():
     """Each cosmology of a batch lenses exactly as it does alone."""
     from abcmb_b200 import engine
-    w = configs.c4(n_cosmo=3, l_max=300, nk_range=(40, 60))
+    w = configs.c4(n_cosmo=3, l_max=300, nk_range=(40, 60), xe_layout="compact")
     w.lensing = True
     w.build()
     db = engine.DeviceBatch.upload(w.batch, "cuda:0")
@@ -221,7 +221,7 @@ def test_c5_lensed_batch_gradient_and_pk_match_oracle():
     gradient (13 variants, A_s / n_s sharing their base's perturbations) and
     P(k) at z = 0..3 against the oracle."""
     from abcmb_b200 import gradients, pipeline
-    w = configs.c5(n_cosmo=2, l_max=300, nk_range=(40, 60))
+    w = configs.c5(n_cosmo=2, l_max=300, nk_range=(40, 60), xe_layout="compact")
     gw = gradients.expand(w, processes=1)
     kout = configs.c5_pk_k(n=40)
     z = np.array(configs.C5_PK_Z)

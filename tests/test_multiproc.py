@@ -27,7 +27,7 @@ def _free_port():
 def _shard_cl(rank: int):
     from abcmb_b200 import configs, bessel
     from oracle import oracle
-    w = configs.c4(n_cosmo=1, nk_range=(12, 14), seed=configs.SEED + rank, l_max=300)
+    w = configs.c4(n_cosmo=1, nk_range=(12, 14), seed=configs.SEED + rank, l_max=300, xe_layout="compact")
     w.build()
     rc, pt, ks = oracle.pert_forward(w.batch, w.pert_settings(), 1)
     assert rc == 0
@@ -130,7 +130,7 @@ class _OracleCompute:
 
 def _one_cosmology():
     from abcmb_b200 import configs
-    return configs.c2(nk=24, l_max=300, lmax_h=8).build()
+    return configs.c2(nk=24, l_max=300, lmax_h=8, xe_layout="compact").build()
 
 
 def _split_worker(rank, world, port, out):
