@@ -4,9 +4,23 @@ A_s and n_s enter only the primordial factor of the k quadrature
 (spectrum.py:789-791), so dC_l/dA_s = C_l / A_s and dC_l/dn_s comes from the
 same line-of-sight launch as C_l (a ln(k/k_pivot)-weighted quadrature).
 h, omega_b, omega_cdm and tau_reion change the background and the
-perturbations; their derivatives are central differences with relative step
-1e-4 (the finite-difference check of the gradient configuration), all
-variants of all cosmologies integrated in one batched launch.
+perturbations.  Every cosmology gets, per such parameter, two more
+descriptors: the cosmology at theta +- eps (relative step 1e-4), with their
+own background tables.  Two ways to fill their PerturbationTables:
+
+  mode="tangent": abcmb_pert_forward_tangent integrates only the
+    base cosmology and carries the four directions' forward-mode
+    sensitivities along its steps (what jax.jacfwd through diffrax computes
+    in the reference, abcmb/main.py:111, docs/FAQ.rst:24-28); the variants'
+    tables are the first-order expansion around the base at their own save
+    times.  One integration per (cosmology, k) instead of nine, and no
+    step-sequence noise in the derivative.
+  mode="fd" (default): every variant is integrated on its own (central differences of
+    whole solves, the gradient configuration's finite-difference check).
+
+Either way the line of sight runs over all descriptors and dC_l/dtheta is
+(C_l(plus) - C_l(minus)) / (2 eps): exact in the PerturbationTable (C_l is
+quadratic in it), second-order accurate in the background.
 
 With lensing, A_s and n_s also set C_l^phiphi (lensing_power_spectrum goes
 through Pk_lin, spectrum.py:349-384), so the lensed spectra are not linear in
@@ -28,6 +42,8 @@ from .configs import GRAD_PARAMS, Workload
 
 FD_PARAMS = ("h", "omega_b", "omega_cdm", "tau_reion")
 REL_STEP = 1e-4
+MODES = ("tangent", "fd")
+MAX_TANGENTS = 4          # ABCMB_MAX_TANGENTS
 
 
 def fd_variants(p_in: dict, rel_step: float = REL_STEP):
@@ -55,6 +71,9 @@ class GradWorkload:
     variants: list          # per base cosmology: list of (param, sign, step) in batch order
     batch: packing.Batch
     n_var: int
+    mode: str = "fd"
+    dirs: np.ndarray = None  # tangent mode: int32 [n_descriptors, MAX_TANGENTS, 2] (plus, minus)
+    n_dir: int = 0
 
     def assemble(self, cl: np.ndarray, dcl_dns: np.ndarray):
         """cl, dcl_dns: (n_base * n_var, 3, n_l) -> C_l (n_base, 3, n_l), grad (n_base, 6, 3, n_l)."""
@@ -81,24 +100,31 @@ PRIMORDIAL_PARAMS = ("A_s", "n_s")
 
 
 def expand(w: Workload, n_save: int = 500, processes: int = 0, rel_step: float = REL_STEP,
-           primordial_fd: bool = None) -> GradWorkload:
+           primordial_fd: bool = None, mode: str = "fd") -> GradWorkload:
     """Background tables for every variant (host, optionally in a spawn pool).
 
     primordial_fd (default: the workload's lensing flag) adds the A_s and n_s
-    +- descriptors that share their base cosmology's perturbations."""
+    +- descriptors that share their base cosmology's perturbations.  mode:
+    "tangent" or "fd" (module docstring)."""
+    if mode not in MODES:
+        raise ValueError(f"mode must be one of {MODES}")
     if primordial_fd is None:
         primordial_fd = bool(w.lensing)
-    jobs, variants, layouts, kgrids, alias, overrides = [], [], [], [], [], []
+    jobs, variants, layouts, kgrids, alias, overrides, work, dir_rows = [], [], [], [], [], [], [], []
     for p_in, ncdm, kg in zip(w.params_in, w.has_ncdm, w.kgrids):
         var = fd_variants(p_in, rel_step)
         entries = [(v[0], v[1], v[2]) for v in var]
         base_index = len(jobs)
-        for v in var:
+        for j, v in enumerate(var):
             jobs.append((v[3], ncdm, w.specs, w.xe_layout))
             layouts.append(sp.state_layout(w.specs, ncdm))
             kgrids.append(kg)
             alias.append(None)
             overrides.append(None)
+            work.append(mode == "fd" or j == 0)
+        # (plus, minus) descriptors of each direction, in FD_PARAMS order
+        dir_rows.append((base_index, [(base_index + 1 + 2 * q, base_index + 2 + 2 * q)
+                                      for q in range(len(FD_PARAMS))]))
         if primordial_fd:
             for name in PRIMORDIAL_PARAMS:
                 hstep = rel_step * p_in[name]
@@ -109,6 +135,7 @@ def expand(w: Workload, n_save: int = 500, processes: int = 0, rel_step: float =
                     kgrids.append(kg)
                     alias.append(base_index)
                     overrides.append({name: p_in[name] + sgn * hstep})
+                    work.append(False)
         variants.append(entries)
     real = [j for j in jobs if j is not None]
     if processes and processes > 1:
@@ -123,7 +150,13 @@ def expand(w: Workload, n_save: int = 500, processes: int = 0, rel_step: float =
         if a is not None:
             bgs[i] = bgs[a]
     batch = packing.pack(bgs, layouts, kgrids, n_save=n_save, alias_of=alias if primordial_fd else None,
-                         overrides=overrides if primordial_fd else None)
+                         overrides=overrides if primordial_fd else None, work=work)
+    dirs = None
+    if mode == "tangent":
+        dirs = np.full((len(jobs), MAX_TANGENTS, 2), -1, dtype=np.int32)
+        for b, pairs in dir_rows:
+            for q, pm in enumerate(pairs):
+                dirs[b, q] = pm
     if w.kt is None:
         ks = dict(w.specs)
         sp.get_k_axis_perturbations(ks)
@@ -132,4 +165,5 @@ def expand(w: Workload, n_save: int = 500, processes: int = 0, rel_step: float =
         w.idx_min, w.idx_max, _ = sp.ell_index_range(bessel_mod.load().l_tab, int(w.specs["l_min"]), w.l_max,
                                                         w.lensing)
     w.batch = batch
-    return GradWorkload(base=w, variants=variants, batch=batch, n_var=len(variants[0]))
+    return GradWorkload(base=w, variants=variants, batch=batch, n_var=len(variants[0]), mode=mode, dirs=dirs,
+                        n_dir=len(FD_PARAMS) if mode == "tangent" else 0)

@@ -137,7 +137,7 @@ class Batch:
 
 
 def pack(bgs, layouts, kgrids, n_save: int = 500, order: str = "cost", alias_of=None,
-         overrides=None) -> Batch:
+         overrides=None, work=None) -> Batch:
     """Pack cosmologies (BackgroundTables, StateLayout, k grid) into a Batch.
 
     order="cost" hands the persistent queue the expensive items first:
@@ -149,6 +149,10 @@ def pack(bgs, layouts, kgrids, n_save: int = 500, order: str = "cost", alias_of=
     (a dict) then changes parameters that only the line of sight reads
     (A_s, n_s): the primordial finite-difference variants, which share their
     base cosmology's perturbations.
+
+    work[i] = False gives entry i its own tables and PerturbationTable slot
+    but no work items: the plus / minus variants of abcmb_pert_forward_tangent,
+    whose tables the base cosmology's items write.
     """
     n = len(bgs)
     rec = np.zeros(n, dtype=COSMO_DTYPE)
@@ -223,7 +227,7 @@ def pack(bgs, layouts, kgrids, n_save: int = 500, order: str = "cost", alias_of=
         r["ny"] = lay.ny
         r["nk"] = kg.shape[0]
     items = [(i, j) for i in range(n) for j in range(int(rec[i]["nk"]))
-             if alias_of is None or alias_of[i] is None]
+             if (alias_of is None or alias_of[i] is None) and (work is None or work[i])]
     if order == "cost":
         items.sort(key=lambda it: (-rec[it[0]]["ny"], -kgrids[it[0]][it[1]]))
     return Batch(cosmo=rec, tables=np.concatenate(chunks), kbuf=np.concatenate(kchunks),

@@ -327,6 +327,51 @@ int abcmb_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev,
                        void* stream);
 
 /*
+ * abcmb_pert_forward with forward-mode sensitivities: the PerturbationTable
+ * of a base cosmology and its first-order change along up to
+ * ABCMB_MAX_TANGENTS parameter directions, in one integration.  The
+ * reference differentiates through the same integration with jax.jacfwd /
+ * jax.grad (abcmb/main.py:111 adjoint=diffrax.ForwardMode,
+ * abcmb/perturbations.py:285-312, docs/FAQ.rst:24-28); here the tangents
+ * ride along the primal's accepted steps.
+ *
+ * Direction p of base cosmology ci is given by two more descriptors of the
+ * batch, the cosmology at theta + eps_p ("plus") and at theta - eps_p
+ * ("minus"), each with its own tables and PerturbationTable slot and no
+ * work items of its own: dir_dev[(ci * ABCMB_MAX_TANGENTS + p) * 2 + {0, 1}]
+ * = (plus, minus) descriptor indices (same state layout and k grid as ci).
+ * Because the right-hand side is linear in y and in the background basis,
+ * the change of A(lna) along p is the central difference of the background
+ * between plus and minus at the base's own times; the tangent u_p of the
+ * discrete Kvaerno5 step (step sizes frozen, each implicit stage's tangent
+ * solved to the primal's very-chord test with the primal's Newton matrix)
+ * starts from the central difference of the initial conditions at the two
+ * variants' start times.  Written outputs: the base's table (bit-identical
+ * to abcmb_pert_forward's), and each variant's table at its own save times
+ * as the fields of y(ts) +- (u_p(ts) + y'(ts) dts_p), dts_p the half
+ * difference of the variants' save times, with the variant's background.
+ * The line of sight over all descriptors then gives the C_l of every
+ * variant, and (C_l(plus) - C_l(minus)) / 2 eps_p the derivative.
+ *   items_dev   [n_items] (base cosmology, k) pairs
+ *   n_dir       1..ABCMB_MAX_TANGENTS
+ *   tstat_dev   [n_items x 2] int32 (optional): tangent chord iterations,
+ *               tangent stage solves left unconverged after the primal's
+ *               iteration limit (the last iterate is kept; the tangents
+ *               never change the primal's step sequence)
+ * Workspace: abcmb_pert_workspace_size(n_cosmo, n_items) (start-time grids
+ * of every descriptor).
+ */
+#define ABCMB_MAX_TANGENTS 4
+int abcmb_pert_forward_tangent(int n_cosmo, const abcmb_cosmo* cosmo_dev,
+                               const double* tables_dev, const double* k_dev,
+                               int n_items, const int32_t* items_dev,
+                               int n_dir, const int32_t* dir_dev,
+                               const abcmb_pert_settings* settings,
+                               double* pt_dev, abcmb_kstat* kstat_dev, int32_t* tstat_dev,
+                               void* workspace_dev, int64_t workspace_bytes,
+                               void* stream);
+
+/*
  * abcmb_pert_forward for callers that cannot allocate device memory (no
  * cudaMalloc, no workspace of their own: e.g. code inside a framework that
  * owns every device byte).  No counterpart in the reference.  Same inputs,

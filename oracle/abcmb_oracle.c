@@ -666,6 +666,82 @@ static void work_free(work_t* w) {
   free(w->Jm); free(w->piv); free(w->col); free(w->tmp); free(w->f2);
 }
 
+/* Forward-mode sensitivities (tangents) of one k mode with respect to up to
+ * ABCMB_MAX_TANGENTS parameter directions.  Direction p is given by two
+ * descriptors, the cosmology at theta + eps_p (plus) and at theta - eps_p
+ * (minus), with their own tables; the tangent u_p approximates
+ * eps_p dy/dtheta_p, the first-order part of (y(plus) - y(minus)) / 2.
+ *
+ * The right-hand side is linear in y and in the background "basis" (every
+ * coefficient of A(lna) is a constant times one background function), so
+ *   d/deps [A(lna; theta) y] = (f(plus, lna, y) - f(minus, lna, y)) / 2
+ * up to second order in eps: the central difference of the background
+ * alone, at the base trajectory's times.  The tangent is the forward-mode
+ * derivative of the discrete ESDIRK step with the base's step sizes frozen:
+ * each implicit stage's tangent solves (I - h gamma A_i) dF_i =
+ * A_i (du + h sum_{j<i} a_ij dF_j) + dA_i Y_i exactly, by chord iterations
+ * with the step's Newton matrix until the same very-chord test the primal
+ * stage uses is met (the iteration matrix is the primal's, so it converges
+ * as fast).  The start time moves with theta: u(t0) = dy0/deps - f(t0, y0)
+ * dt0/deps, with y0 = IC(theta, t0(theta)) differenced between the two
+ * descriptors.  Outputs are the two variants' PerturbationTables at their
+ * own save times ts(plus) and ts(minus): the fields of y(ts) +- (u(ts) +
+ * y'(ts) (ts(plus) - ts(minus)) / 2), with y' the derivative of the dense
+ * output, evaluated with each variant's own background. */
+typedef struct {
+  int nd;
+  const abcmb_cosmo* cp[ABCMB_MAX_TANGENTS];
+  const abcmb_cosmo* cm[ABCMB_MAX_TANGENTS];
+  const start_grid_t* sgp[ABCMB_MAX_TANGENTS];
+  const start_grid_t* sgm[ABCMB_MAX_TANGENTS];
+} tan_ctx_t;
+
+typedef struct {
+  double* u0;     /* nd x ny tangent at t0             */
+  double* u1;     /* nd x ny tangent at t1             */
+  double* dF;     /* nd x 7 x ny stage derivatives     */
+  double* Y;      /* ny primal stage value             */
+  double* z;      /* ny                                */
+  double* q;      /* ny                                */
+  double* r;      /* ny                                */
+  double* fp;     /* ny                                */
+  double* fm;     /* ny                                */
+  double* yp;     /* ny                                */
+  double* us;     /* ny                                */
+  double* yd;     /* ny                                */
+} tan_work_t;
+
+static void tan_work_alloc(tan_work_t* t, int ny) {
+  t->u0 = (double*)calloc((size_t)ABCMB_MAX_TANGENTS * ny, sizeof(double));
+  t->u1 = (double*)calloc((size_t)ABCMB_MAX_TANGENTS * ny, sizeof(double));
+  t->dF = (double*)calloc((size_t)ABCMB_MAX_TANGENTS * 7 * ny, sizeof(double));
+  t->Y = (double*)calloc(ny, sizeof(double));
+  t->z = (double*)calloc(ny, sizeof(double));
+  t->q = (double*)calloc(ny, sizeof(double));
+  t->r = (double*)calloc(ny, sizeof(double));
+  t->fp = (double*)calloc(ny, sizeof(double));
+  t->fm = (double*)calloc(ny, sizeof(double));
+  t->yp = (double*)calloc(ny, sizeof(double));
+  t->us = (double*)calloc(ny, sizeof(double));
+  t->yd = (double*)calloc(ny, sizeof(double));
+}
+
+static void tan_work_free(tan_work_t* t) {
+  free(t->u0); free(t->u1); free(t->dF); free(t->Y); free(t->z); free(t->q); free(t->r);
+  free(t->fp); free(t->fm); free(t->yp); free(t->us); free(t->yd);
+}
+
+/* dA y at lna for direction p: (f(plus, y) - f(minus, y)) / 2 into out. */
+static void tangent_dA(const tan_ctx_t* T, int p, const layout_t* L, const double* tables, double k, double lna,
+                       const double* y, tan_work_t* tw, double* out) {
+  bgs_t bp, bm;
+  bg_eval(T->cp[p], tables, lna, &bp);
+  bg_eval(T->cm[p], tables, lna, &bm);
+  rhs(T->cp[p], L, k, &bp, y, tw->fp);
+  rhs(T->cm[p], L, k, &bm, y, tw->fm);
+  for (int e = 0; e < L->ny; ++e) out[e] = 0.5 * (tw->fp[e] - tw->fm[e]);
+}
+
 /* Jacobian of the stage root function at lna_lin: M = I - h*gamma*A(lna_lin).
  * A is obtained column by column (the RHS is linear in y), the way JAX
  * materialises the Jacobian from JVPs of basis vectors. */
@@ -680,10 +756,91 @@ static void build_newton_matrix(const abcmb_cosmo* c, const layout_t* L, double 
   }
 }
 
+/* Tangents of one accepted step (the primal's stage derivatives F, its
+ * Newton matrix LU and y0 are those of the step).  ts[0] counts chord
+ * iterations, ts[1] stage solves that did not meet the test within
+ * root_max iterations (the last iterate is kept: the tangent never changes
+ * the primal's step sequence). */
+static void tangent_step(const abcmb_cosmo* c, const layout_t* L, const double* tables, double k, double h,
+                         double t0, double rtol, double atol, const tan_ctx_t* T, work_t* w, tan_work_t* tw,
+                         int32_t* ts) {
+  const int n = L->ny;
+  const double hg = h * KV_GAMMA;
+  const double kappa = 1e-2, small_res = 1e-13;
+  const int root_max = 10;
+  for (int i = 1; i < 7; ++i) {
+    const double ti = t0 + KV_C[i] * h;
+    bgs_t bi;
+    bg_eval(c, tables, ti, &bi);
+    /* the converged primal stage value, as the primal formed it */
+    for (int e = 0; e < n; ++e) {
+      double acc = 0.;
+      for (int j = 0; j < i; ++j) acc += KV_A[i][j] * w->F[j * n + e];
+      tw->Y[e] = (w->y0[e] + h * acc) + hg * w->F[i * n + e];
+    }
+    for (int p = 0; p < T->nd; ++p) {
+      double* dF = tw->dF + (size_t)p * 7 * n;
+      const double* u0 = tw->u0 + (size_t)p * n;
+      for (int e = 0; e < n; ++e) {
+        double acc = 0.;
+        for (int j = 0; j < i; ++j) acc += KV_A[i][j] * dF[j * n + e];
+        tw->z[e] = u0[e] + h * acc;
+      }
+      /* q = A_i z + dA_i Y_i: the part of the residual the iterations keep */
+      rhs(c, L, k, &bi, tw->z, tw->q);
+      tangent_dA(T, p, L, tables, k, ti, tw->Y, tw, tw->r);
+      for (int e = 0; e < n; ++e) tw->q[e] += tw->r[e];
+      double* fi = dF + i * n;
+      memcpy(fi, dF + (i - 1) * n, sizeof(double) * n);     /* the previous stage's, like the primal */
+      double diffsize = INFINITY, diffsize_prev = INFINITY;
+      int conv = 0;
+      for (int it = 1; it <= root_max; ++it) {
+        rhs(c, L, k, &bi, fi, tw->r);
+        /* residual h gamma A_i dF + q - dF, solved as the primal's (sign included) */
+        for (int e = 0; e < n; ++e) tw->r[e] = -((hg * tw->r[e] + tw->q[e]) - fi[e]);
+        lu_solve(w->Jm, n, w->piv, tw->r);
+        double ss = 0.;
+        for (int e = 0; e < n; ++e) {
+          double fnew = fi[e] - tw->r[e];
+          fi[e] = fnew;
+          double sc = atol + rtol * fabs(fnew);
+          double qq = tw->r[e] / sc;
+          ss += qq * qq;
+        }
+        diffsize_prev = diffsize;
+        diffsize = sqrt(ss / n);
+        ts[0]++;
+        if (it >= 2) {
+          double rate = diffsize / diffsize_prev;
+          double factor = diffsize * rate / (1. - rate);
+          int small = diffsize < small_res;
+          int diverged = !isfinite(rate) || rate > 2.;
+          int converged = factor > 0. && factor < kappa;
+          if (small || converged) { conv = 1; break; }
+          if (diverged) break;
+        }
+      }
+      if (!conv) ts[1]++;
+    }
+  }
+  for (int p = 0; p < T->nd; ++p) {
+    const double* dF = tw->dF + (size_t)p * 7 * n;
+    const double* u0 = tw->u0 + (size_t)p * n;
+    double* u1 = tw->u1 + (size_t)p * n;
+    for (int e = 0; e < n; ++e) {
+      double acc = 0.;
+      for (int j = 0; j < 6; ++j) acc += KV_A[6][j] * dF[j * n + e];
+      acc += KV_GAMMA * dF[6 * n + e];
+      u1[e] = u0[e] + h * acc;
+    }
+  }
+}
+
 /* One k mode from its start time to lna = 0 (perturbations.py:250-316). */
 static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kbuf,
                     const abcmb_pert_settings* s, const start_grid_t* sg, int ik,
-                    double* pt, abcmb_kstat* st, work_t* w) {
+                    double* pt, abcmb_kstat* st, work_t* w, const tan_ctx_t* T, tan_work_t* tw,
+                    int32_t* tst) {
   layout_t L;
   make_layout(c, &L);
   const int n = L.ny;
@@ -723,6 +880,22 @@ static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kb
   bgs_t b;
   bg_eval(c, tables, t0, &b);
   rhs(c, &L, k, &b, w->y0, w->F);
+  if (T) {
+    /* tangents at the start: u = dy0/deps - f(t0, y0) dt0/deps, dF_0 = A u + dA y0 */
+    for (int p = 0; p < T->nd; ++p) {
+      const double tp = start_time_from_grid(T->sgp[p], k, s->R_large, w->f2);
+      const double tm = start_time_from_grid(T->sgm[p], k, s->R_large, w->f2);
+      initial_conditions(T->cp[p], &L, tables, k, tp, tw->yp);
+      initial_conditions(T->cm[p], &L, tables, k, tm, tw->us);
+      const double dt0 = 0.5 * (tp - tm);
+      double* u = tw->u0 + (size_t)p * n;
+      for (int e = 0; e < n; ++e) u[e] = 0.5 * (tw->yp[e] - tw->us[e]) - w->F[e] * dt0;
+      double* dF0 = tw->dF + (size_t)p * 7 * n;
+      rhs(c, &L, k, &b, u, dF0);
+      tangent_dA(T, p, &L, tables, k, t0, w->y0, tw, tw->q);
+      for (int e = 0; e < n; ++e) dF0[e] += tw->q[e];
+    }
+  }
 
   int nsteps = 0;
   while (t0 < t_end) {
@@ -811,6 +984,7 @@ static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kb
     if (inv == 0. || isinf(inv)) inv = 1.;
     if (keep) {
       st->n_accepted++;
+      if (T) tangent_step(c, &L, tables, k, h, t0, rtol, atol, T, w, tw, tst);
       /* dense output: cubic Hermite on [t0, t1] (ThirdOrderHermitePolynomialInterpolation) */
       const double* fa = w->F;            /* f(t0, y0) */
       const double* fb = w->F + 6 * n;    /* f(t1, y1) */
@@ -828,12 +1002,49 @@ static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kb
         output_fields(c, &L, tables, k, ts, ysave, outv);
         for (int f = 0; f < ABCMB_NFIELDS; ++f)
           ptc[((size_t)f * nsave + isave) * nk + ik] = outv[f];
+        if (T) {
+          /* d/dt of the dense output at ts */
+          for (int e = 0; e < n; ++e) {
+            double y0e = w->y0[e], y1e = w->y1[e];
+            double k0 = h * fa[e], k1 = h * fb[e];
+            double a2 = 3. * (y1e - y0e) - 2. * k0 - k1, a3 = 2. * (y0e - y1e) + k0 + k1;
+            tw->yd[e] = (k0 + th * (2. * a2 + 3. * th * a3)) / h;
+          }
+          for (int p = 0; p < T->nd; ++p) {
+            const double* u0 = tw->u0 + (size_t)p * n;
+            const double* u1 = tw->u1 + (size_t)p * n;
+            const double* dF = tw->dF + (size_t)p * 7 * n;
+            const double tsp = linspace_at(T->cp[p]->lna_transfer_start, 0.0, nsave, isave);
+            const double tsm = linspace_at(T->cm[p]->lna_transfer_start, 0.0, nsave, isave);
+            const double dts = 0.5 * (tsp - tsm);
+            for (int e = 0; e < n; ++e) {
+              double k0 = h * dF[e], k1 = h * dF[6 * n + e];
+              double us = u0[e] + th * (k0 + th * ((3. * (u1[e] - u0[e]) - 2. * k0 - k1) +
+                                                   th * (2. * (u0[e] - u1[e]) + k0 + k1)));
+              tw->us[e] = us + tw->yd[e] * dts;
+            }
+            for (int sgn = 0; sgn < 2; ++sgn) {
+              const abcmb_cosmo* cv = sgn == 0 ? T->cp[p] : T->cm[p];
+              for (int e = 0; e < n; ++e) tw->yp[e] = sgn == 0 ? ysave[e] + tw->us[e] : ysave[e] - tw->us[e];
+              output_fields(cv, &L, tables, k, sgn == 0 ? tsp : tsm, tw->yp, outv);
+              double* ptv = pt + cv->off_pt;
+              for (int f = 0; f < ABCMB_NFIELDS; ++f)
+                ptv[((size_t)f * nsave + isave) * cv->nk + ik] = outv[f];
+            }
+          }
+        }
         isave++;
       }
       prev_prev_inv = prev_inv;
       prev_inv = inv;
       memcpy(w->y0, w->y1, sizeof(double) * n);
       memcpy(w->F, w->F + 6 * n, sizeof(double) * n);   /* FSAL */
+      if (T) {
+        for (int p = 0; p < T->nd; ++p) {
+          memcpy(tw->u0 + (size_t)p * n, tw->u1 + (size_t)p * n, sizeof(double) * n);
+          memcpy(tw->dF + (size_t)p * 7 * n, tw->dF + ((size_t)p * 7 + 6) * n, sizeof(double) * n);
+        }
+      }
       t0 = t1;
     } else {
       st->n_rejected++;
@@ -867,8 +1078,68 @@ int oracle_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo, const double* tab
 #pragma omp for schedule(dynamic, 1)
     for (int it = 0; it < n_items; ++it) {
       int ci = items[2 * it], ik = items[2 * it + 1];
-      solve_k(&cosmo[ci], tables, kbuf, s, &sg[ci], ik, pt, &kstat[it], &w);
+      solve_k(&cosmo[ci], tables, kbuf, s, &sg[ci], ik, pt, &kstat[it], &w, NULL, NULL, NULL);
     }
+    work_free(&w);
+  }
+  for (int c = 0; c < n_cosmo; ++c) start_grid_free(&sg[c]);
+  free(sg);
+  int bad = 0;
+  for (int it = 0; it < n_items; ++it) if (kstat[it].status != ABCMB_STATUS_OK) bad = 1;
+  return bad ? ABCMB_ERR_SOLVER : ABCMB_OK;
+}
+
+/* oracle_pert_forward with forward-mode sensitivities (see tan_ctx_t):
+ * items name base cosmologies; dirs[ci][p] = (plus, minus) descriptor
+ * indices of direction p of base ci (ABCMB_MAX_TANGENTS x 2 int32 per
+ * descriptor, -1 where unused).  Writes the base's and every variant's
+ * PerturbationTable; tstat[2 it] = tangent chord iterations,
+ * tstat[2 it + 1] = tangent stage solves left unconverged. */
+int oracle_pert_forward_tangent(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
+                                int n_items, const int32_t* items, int n_dir, const int32_t* dirs,
+                                const abcmb_pert_settings* s, double* pt, abcmb_kstat* kstat, int32_t* tstat,
+                                int n_threads) {
+  if (n_dir < 1 || n_dir > ABCMB_MAX_TANGENTS) return ABCMB_ERR_ARG;
+  for (int it = 0; it < n_items; ++it) {
+    const int ci = items[2 * it];
+    for (int p = 0; p < n_dir; ++p) {
+      const int a = dirs[(ci * ABCMB_MAX_TANGENTS + p) * 2], b = dirs[(ci * ABCMB_MAX_TANGENTS + p) * 2 + 1];
+      if (a < 0 || b < 0 || a >= n_cosmo || b >= n_cosmo || cosmo[a].ny != cosmo[ci].ny ||
+          cosmo[b].ny != cosmo[ci].ny || cosmo[a].nk != cosmo[ci].nk || cosmo[b].nk != cosmo[ci].nk)
+        return ABCMB_ERR_ARG;
+    }
+  }
+  start_grid_t* sg = (start_grid_t*)calloc(n_cosmo, sizeof(start_grid_t));
+  int maxny = 0;
+  for (int c = 0; c < n_cosmo; ++c) {
+    start_grid_init(&cosmo[c], tables, s->R_tc, &sg[c]);
+    if (cosmo[c].ny > maxny) maxny = cosmo[c].ny;
+  }
+#ifdef _OPENMP
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+#endif
+#pragma omp parallel
+  {
+    work_t w;
+    work_alloc(&w, maxny);
+    tan_work_t tw;
+    tan_work_alloc(&tw, maxny);
+#pragma omp for schedule(dynamic, 1)
+    for (int it = 0; it < n_items; ++it) {
+      int ci = items[2 * it], ik = items[2 * it + 1];
+      tan_ctx_t T;
+      T.nd = n_dir;
+      for (int p = 0; p < n_dir; ++p) {
+        const int a = dirs[(ci * ABCMB_MAX_TANGENTS + p) * 2], b = dirs[(ci * ABCMB_MAX_TANGENTS + p) * 2 + 1];
+        T.cp[p] = &cosmo[a];
+        T.cm[p] = &cosmo[b];
+        T.sgp[p] = &sg[a];
+        T.sgm[p] = &sg[b];
+      }
+      tstat[2 * it] = tstat[2 * it + 1] = 0;
+      solve_k(&cosmo[ci], tables, kbuf, s, &sg[ci], ik, pt, &kstat[it], &w, &T, &tw, tstat + 2 * it);
+    }
+    tan_work_free(&tw);
     work_free(&w);
   }
   for (int c = 0; c < n_cosmo; ++c) start_grid_free(&sg[c]);

@@ -38,6 +38,10 @@ void oracle_output_fields(const abcmb_cosmo* c, const double* tables, double k, 
 int oracle_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
                         int n_items, const int32_t* items, const abcmb_pert_settings* s,
                         double* pt, abcmb_kstat* kstat, int n_threads);
+int oracle_pert_forward_tangent(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
+                                int n_items, const int32_t* items, int n_dir, const int32_t* dirs,
+                                const abcmb_pert_settings* s, double* pt, abcmb_kstat* kstat, int32_t* tstat,
+                                int n_threads);
 void oracle_spline_slopes(const double* x, const double* y, int n, double* s);
 double oracle_spline_eval(const double* x, const double* y, const double* s, int n, double xq);
 double oracle_phi(int which, const oracle_bessel* B, int idx, double x);

@@ -58,6 +58,9 @@ def lib():
         L.oracle_output_fields.argtypes = [vp, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp]
         L.oracle_pert_forward.restype = ctypes.c_int
         L.oracle_pert_forward.argtypes = [ctypes.c_int, vp, _dp, _dp, ctypes.c_int, _ip, vp, _dp, vp, ctypes.c_int]
+        L.oracle_pert_forward_tangent.restype = ctypes.c_int
+        L.oracle_pert_forward_tangent.argtypes = [ctypes.c_int, vp, _dp, _dp, ctypes.c_int, _ip, ctypes.c_int, _ip,
+                                                  vp, _dp, vp, _ip, ctypes.c_int]
         L.oracle_spline_slopes.argtypes = [_dp, _dp, ctypes.c_int, _dp]
         L.oracle_spline_eval.restype = ctypes.c_double
         L.oracle_spline_eval.argtypes = [_dp, _dp, _dp, ctypes.c_int, ctypes.c_double]
@@ -132,6 +135,22 @@ def pert_forward(batch, settings, n_threads: int = 0):
                                    batch.n_items, iptr(items), ctypes.byref(settings), dptr(pt), vptr(kstat),
                                    n_threads)
     return rc, pt, kstat
+
+
+def pert_forward_tangent(batch, settings, dirs, n_dir: int, n_threads: int = 0):
+    """Oracle perturbations with forward-mode sensitivities: the batch's
+    items name base cosmologies, dirs (int32, n_cosmo x 4 x 2) their
+    (plus, minus) variant descriptors.  Returns (rc, pt, kstat, tstat)."""
+    from abcmb_b200.packing import KSTAT_DTYPE
+    pt = np.zeros(batch.pt_size)
+    kstat = np.zeros(batch.n_items, dtype=KSTAT_DTYPE)
+    tstat = np.zeros(2 * batch.n_items, dtype=np.int32)
+    items = np.ascontiguousarray(batch.items, dtype=np.int32)
+    d = np.ascontiguousarray(dirs, dtype=np.int32).reshape(-1)
+    rc = lib().oracle_pert_forward_tangent(batch.n_cosmo, vptr(batch.cosmo), dptr(batch.tables), dptr(batch.kbuf),
+                                           batch.n_items, iptr(items), n_dir, iptr(d), ctypes.byref(settings),
+                                           dptr(pt), vptr(kstat), iptr(tstat), n_threads)
+    return rc, pt, kstat, tstat.reshape(-1, 2)
 
 
 def los_forward(batch, pt, kt, ls, bt, n_threads: int = 0):

@@ -272,3 +272,37 @@ def test_oracle_solver_converges_to_an_independent_integrator(c1_small):
     got = b.pt_view(pt, 0)[:, :, ik]
     err = (np.abs(got - ref).max(axis=1) / (np.abs(ref).max(axis=1) + 1e-300))[:18]
     assert err.max() < 1e-6, err
+
+
+def test_oracle_tangents_match_central_differences_of_tight_solves():
+    """The forward-mode sensitivities (oracle_pert_forward_tangent: tangents
+    of the discrete steps, background change as the central difference of
+    the variants' backgrounds, start-time and save-time shifts) against
+    central differences of whole solves, both at rtol 1e-10 so the
+    differences' own solver noise (~1e-10 / 1e-4 of a field) stays small:
+    every PerturbationTable field of every direction within 5e-7 of the
+    field's maximum, and within 2e-3 of the largest change along that
+    direction.  The base table is the forward solve's, bit for bit."""
+    from abcmb_b200 import configs, gradients
+    from oracle import oracle
+    w = configs.c1(nk=2, l_max=400, xe_layout="compact")
+    w.kgrids = [np.array([2e-3, 0.08])]
+    w.specs.update(rtol_small_k_PE=1e-10, rtol_large_k_PE=1e-10, atol_small_k_PE=1e-14, atol_large_k_PE=1e-14,
+                   max_steps_PE=100000)
+    gt = gradients.expand(w, processes=1, mode="tangent")
+    gf = gradients.expand(w, processes=1, mode="fd")
+    st = w.pert_settings()
+    rc, pt_t, _, ts = oracle.pert_forward_tangent(gt.batch, st, gt.dirs, gt.n_dir)
+    assert rc == 0 and ts[:, 1].sum() == 0
+    rc, pt_f, _ = oracle.pert_forward(gf.batch, st)
+    assert rc == 0
+    base = gt.batch.pt_view(pt_t, 0)
+    np.testing.assert_array_equal(base, gf.batch.pt_view(pt_f, 0))
+    scale = np.abs(base).max(axis=(1, 2))[:18]
+    for q, name in enumerate(gradients.FD_PARAMS):
+        dt = (gt.batch.pt_view(pt_t, 1 + 2 * q) - gt.batch.pt_view(pt_t, 2 + 2 * q))[:18] / 2
+        df = (gf.batch.pt_view(pt_f, 1 + 2 * q) - gf.batch.pt_view(pt_f, 2 + 2 * q))[:18] / 2
+        err = np.abs(dt - df).max(axis=(1, 2)) / scale
+        sens = np.abs(df).max(axis=(1, 2)) / scale
+        assert err.max() < 5e-7, (name, err.max())
+        assert err.max() < 2e-3 * sens.max(), (name, err.max(), sens.max())
