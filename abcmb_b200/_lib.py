@@ -49,6 +49,8 @@ SIGNATURES = [
     ("abcmb_set_pert_warps_per_block", ctypes.c_int, [ctypes.c_int]),
     ("abcmb_last_pert_grid", ctypes.c_int, []),
     ("abcmb_probe_fp64_tflops", ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.c_int, _vp]),
+    ("abcmb_pert_forward_tangent", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp,
+                                                  _vp, _vp, _vp, _vp, _vp, _i64, _vp]),
     ("abcmb_pert_forward_noalloc", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp,
                                                   _vp]),
 ]

@@ -218,20 +218,13 @@ __device__ __forceinline__ void bg_load(const double* s, BG& b) {
   b.iaH = s[17];
 }
 
-// Background basis of one stage time; with sv != null the same lane instead
-// stores the full background of a save time (lanes 0-4 stage times, lane 5
-// the next save point: one instruction stream, no divergence).
-// ik2 = 1/k^2 of the item; ncdm_w the block table's massive-neutrino bin
-// weights w_b (1 + e^-q_b) / q_b^2 and / q_b (constants, not recomputed here)
-__device__ __noinline__ void stage_basis(const abcmb_cosmo& c, const BGK& K, const double* __restrict__ tables,
-                                         double k, double ik2, const double* __restrict__ ncdm_w, double lna, double* B,
-                                         double* sv) {
-  BG b;
-  bg_eval(c, K, tables, lna, b);
-  if (sv) {
-    bg_store(b, sv);
-    return;
-  }
+// The basis values of one background state b into B[0..NB) (B may be a
+// register array: every index is a compile-time constant).  ik2 = 1/k^2 of
+// the item; ncdm_w the block table's massive-neutrino bin weights
+// w_b (1 + e^-q_b) / q_b^2 and / q_b (constants, not recomputed here).
+template <typename Arr>
+__device__ __forceinline__ void basis_values(const BG& b, double k, double ik2, const double* __restrict__ ncdm_w,
+                                             Arr& B) {
   const double iaH = b.iaH;
   const double kap = iaH * b.itau_c;                         // 1/(aH tau_c)
   B[B_ONE] = 1.;
@@ -241,6 +234,7 @@ __device__ __noinline__ void stage_basis(const abcmb_cosmo& c, const BGK& K, con
   B[B_KAP] = kap;
   B[B_RKAP] = b.R * kap;
   B[B_CS2K2IAH] = b.cs2 * k * k * iaH;
+#pragma unroll
   for (int bb = 0; bb < 3; ++bb) {
     double s = Q3[bb] * rsqrt(b.eps[bb] * b.eps[bb]) * iaH;  // q/(eps aH)
     B[B_NCDM + 3 * bb] = s;
@@ -260,11 +254,43 @@ __device__ __noinline__ void stage_basis(const abcmb_cosmo& c, const BGK& K, con
   B[B_WE + 0] = wef * b.rho_b;
   B[B_WE + 1] = wef * ((4. / 3.) * b.rho_g);
   B[B_WE + 2] = wef * ((4. / 3.) * b.rho_nu);
+#pragma unroll
   for (int bb = 0; bb < 3; ++bb) {
     B[B_WH + 5 + bb] = whf * b.ncdm_fac * (ncdm_w[3 * bb] * b.eps[bb]);
     B[B_WE + 3 + bb] = wef * b.ncdm_fac * ncdm_w[3 * bb + 1];
   }
   B[31] = 0.;
+}
+
+// Background basis of one stage time; with sv != null the same lane instead
+// stores the full background of a save time (lanes 0-4 stage times, lane 5
+// the next save point: one instruction stream, no divergence).
+__device__ __noinline__ void stage_basis(const abcmb_cosmo& c, const BGK& K, const double* __restrict__ tables,
+                                         double k, double ik2, const double* __restrict__ ncdm_w, double lna, double* B,
+                                         double* sv) {
+  BG b;
+  bg_eval(c, K, tables, lna, b);
+  if (sv) {
+    bg_store(b, sv);
+    return;
+  }
+  basis_values(b, k, ik2, ncdm_w, B);
+}
+
+// Change of the basis along one parameter direction at lna: half the
+// difference of the plus and minus descriptors' bases (the central
+// difference of the background alone, at the base trajectory's time).
+__device__ __noinline__ void stage_basis_diff(const abcmb_cosmo& cp, const abcmb_cosmo& cm,
+                                              const double* __restrict__ tables, double k, double ik2,
+                                              const double* __restrict__ ncdm_w, double lna, double* Bd) {
+  BG b;
+  double Bp[NB], Bm[NB];
+  bg_eval(cp, bg_constants(cp), tables, lna, b);
+  basis_values(b, k, ik2, ncdm_w, Bp);
+  bg_eval(cm, bg_constants(cm), tables, lna, b);
+  basis_values(b, k, ik2, ncdm_w, Bm);
+#pragma unroll
+  for (int j = 0; j < NB; ++j) Bd[j] = 0.5 * (Bp[j] - Bm[j]);
 }
 
 // Sparse description of one core row of A: up to five terms
@@ -735,6 +761,433 @@ __global__ void start_lna1_kernel(int n_cosmo, const double* __restrict__ f1g, d
   lna1[ci] = np_interp_lna(R_tc, f1g + (int64_t)ci * NSTART, nullptr, 0.);
 }
 
+// Adiabatic initial conditions (perturbations.py:161-199 + species y_ini)
+// of descriptor c at lna: the nonzero entries of y, written by one lane
+// (y zeroed beforehand).
+__device__ __noinline__ void write_ic(const abcmb_cosmo& c, const Layout& L, const double* __restrict__ tables,
+                                      double k, double lna, double* y) {
+  const double tau_ini = tau_of(c, tables, lna);
+  const double om = c.om, Rn = c.R_nu, Rb = c.R_b;
+  const double kt = k * tau_ini;
+  y[0] = (1. - k * k * tau_ini * tau_ini / 12. / (15. + 4. * Rn) *
+                   (5. + 4. * Rn - (16. * Rn * Rn + 280. * Rn + 325) / 10. / (2. * Rn + 15.) * tau_ini * om));
+  y[1] = -(kt * kt) / 4. * (1. - om * tau_ini / 5.);
+  y[2] = -(kt * kt) / 4. * (1. - om * tau_ini / 5.);
+  const double thb = -k * k * k * k * tau_ini * tau_ini * tau_ini / 36. *
+                     (1. - 3. * (1. + 5. * Rb - Rn) / 20. / (1. - Rn) * om * tau_ini);
+  y[3] = thb;
+  y[L.i_g] = -(kt * kt) / 3. * (1. - om * tau_ini / 5.);
+  y[L.i_g + 1] = thb;
+  const double nd = -(kt * kt) / 3. * (1. - om * tau_ini / 5.);
+  const double nth = -k * (kt * kt * kt) / 36. / (4. * Rn + 15.) *
+                     (4. * Rn + 11. + 12. - 3. * (8. * Rn * Rn + 50. * Rn + 275.) / 20. / (2. * Rn + 15.) * tau_ini * om);
+  const double ns = (kt * kt) / (45. + 12. * Rn) * 2. * (1. + (4. * Rn - 5.) / 4. / (2. * Rn + 15.) * tau_ini * om);
+  y[L.i_nu] = nd;
+  y[L.i_nu + 1] = nth;
+  y[L.i_nu + 2] = ns;
+  if (c.has_ncdm) {
+    for (int i = 0; i < 3; ++i) {
+      double q = Q3[i];
+      double fac = q / (1. + exp(-q));
+      double* Pb = y + L.i_ncdm + i * L.nM;
+      Pb[0] = nd / 4. * fac;
+      Pb[1] = nth / 3. * fac;
+      Pb[2] = ns / 2. * fac;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Forward-mode sensitivities (abcmb_pert_forward_tangent)
+// ---------------------------------------------------------------------------
+// The tangent u_q of the discrete Kvaerno5 step along parameter direction q
+// (at most ND_MAX of them, all carried by the warp that integrates the base
+// item): after a step is accepted, each implicit stage i's tangent
+// derivative solves (I - h gamma A_i) dF_i = A_i z + dA_i Y_i with
+// z = u0 + h sum_{j<i} a_ij dF_j and Y_i the converged primal stage value,
+// by chord iterations with the step's own factorisation (the primal's
+// iteration matrix, so the same very-chord test applies).  dA_i is A with
+// the basis replaced by its change along q (A is linear in the basis), the
+// half difference of the plus and minus descriptors' bases at t_i.  All
+// directions run through the same sweeps together: the tail sweeps take one
+// lane per (chain, direction), the core mat-vec one lane per row with one
+// accumulator per direction, so the extra work fills lanes the single
+// primal solve leaves idle.
+constexpr int ND_MAX = ABCMB_MAX_TANGENTS;
+
+// Per-warp tangent scratch, after the primal's WarpMem.  Per direction q:
+// u0 (tangent at t0), dF (7 stage derivatives, stride ny), q (the constant
+// part of a stage's residual; u1 once the stages are done), r (residual,
+// solve vector and temporaries).  Shared: yd (dy/dt of the dense output),
+// yv (a variant's state at a save point), the basis changes at the five
+// stage times, the variants' backgrounds at their save times, the gathered
+// core vectors of the solve, and the variants' descriptor indices.
+struct TanMem {
+  double* p;
+  int my, nd, ncm;
+  __device__ __forceinline__ double* u0(int q) const { return p + q * my; }
+  __device__ __forceinline__ double* dF(int q) const { return p + nd * my + q * 7 * my; }
+  __device__ __forceinline__ double* qv(int q) const { return p + 8 * nd * my + q * my; }
+  __device__ __forceinline__ double* rv(int q) const { return p + 9 * nd * my + q * my; }
+  __device__ __forceinline__ double* yd() const { return p + 10 * nd * my; }
+  __device__ __forceinline__ double* yv() const { return yd() + my; }
+  __device__ __forceinline__ double* bd(int slot, int q) const { return yv() + my + ((slot - 1) * nd + q) * NB; }
+  __device__ __forceinline__ double* sv(int j) const { return yv() + my + 5 * nd * NB + j * NSV; }
+  __device__ __forceinline__ double* vc(int q) const { return sv(2 * nd) + q * ncm; }
+  __device__ __forceinline__ int* vix() const { return reinterpret_cast<int*>(vc(nd)); }   // 2 nd ints
+};
+
+__host__ __device__ inline size_t tan_mem_doubles(int max_ny, int ncm, int nd) {
+  if (nd <= 0) return 0;
+  return (size_t)nd * (10 * (size_t)max_ny + 5 * NB + 2 * NSV + (size_t)ncm) + 2 * (size_t)max_ny + ND_MAX;
+}
+
+// Q_q = A(B) z_q + A(dB_q) Y for every direction (z_q read from rv(q)): the
+// part of a stage's tangent residual the chord iterations keep.
+__device__ __noinline__ void tan_const(const Layout& L, const WarpMem& m, const TanMem& t, const RowTab& R,
+                                       const CoreRow& cr, const double* __restrict__ B, int slot,
+                                       const double* __restrict__ Y, bool ncdm, int lane) {
+  const int nd = t.nd;
+  double hp[ND_MAX], ep[ND_MAX], hpd[ND_MAX], epd[ND_MAX];
+#pragma unroll
+  for (int q = 0; q < ND_MAX; ++q) {
+    hp[q] = ep[q] = hpd[q] = epd[q] = 0.;
+    if (q < nd) {
+      metric(L, B, t.rv(q), ncdm, hp[q], ep[q]);
+      metric(L, t.bd(slot, q), Y, ncdm, hpd[q], epd[q]);
+    }
+  }
+  if (lane < L.nc) {
+    const int r = lane;
+    const int nt = R.n[r];
+    const int tch = R.tch[r];
+#pragma unroll
+    for (int q = 0; q < ND_MAX; ++q) {
+      if (q < nd) {
+        const double* __restrict__ z = t.rv(q);
+        const double* __restrict__ Bd = t.bd(slot, q);
+        double acc = cr.uh * hp[q] + cr.ue * ep[q];
+        double accd = cr.uh * hpd[q] + cr.ue * epd[q];
+#pragma unroll
+        for (int u = 0; u < 5; ++u) {
+          acc = fma(cr.c[u], z[cr.s[u]], acc);
+          const double cd = u < nt ? R.cst[r * 5 + u] * Bd[R.bid[r * 5 + u]] : 0.;
+          accd = fma(cd, Y[cr.s[u]], accd);
+        }
+        acc = fma(cr.tc, z[cr.ts], acc);
+        const double tcd = tch >= 0 ? R.tco[r] * Bd[chain_speed_bid(tch)] : 0.;
+        accd = fma(tcd, Y[cr.ts], accd);
+        t.qv(q)[cr.out] = acc + accd;
+      }
+    }
+  }
+  const double trunc = B[B_TRUNC];
+  for (int u = lane; u < L.ntail; u += WARP) {
+    const int info = m.tinfo()[u];
+    const int e = info & 0xFFF, chn = (info >> 12) & 7;
+    const bool last = (info >> 15) & 1;
+    const int li = info >> 16;
+    const int sb = chain_speed_bid(chn);
+    const double sp = B[sb];
+    const double d = chn < 2 ? B[B_KAP] : 0.;
+    const double lc1 = (double)(m.chL()[chn] + 1);
+    const double ta = R.ta[li], tg = R.tg[li];
+#pragma unroll
+    for (int q = 0; q < ND_MAX; ++q) {
+      if (q < nd) {
+        const double* __restrict__ z = t.rv(q);
+        const double* __restrict__ Bd = t.bd(slot, q);
+        const double sd = Bd[sb], dd = chn < 2 ? Bd[B_KAP] : 0., trd = Bd[B_TRUNC];
+        double fv, fvd;
+        if (last) {
+          fv = sp * z[e - 1] - (d + lc1 * trunc) * z[e];
+          fvd = sd * Y[e - 1] - (dd + lc1 * trd) * Y[e];
+        } else {
+          fv = sp * (ta * z[e - 1] - tg * z[e + 1]) - d * z[e];
+          fvd = sd * (ta * Y[e - 1] - tg * Y[e + 1]) - dd * Y[e];
+        }
+        t.qv(q)[e] = fv + fvd;
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// r_q = h gamma A(B) F_q + Q_q - F_q for the directions in mask, F_q the
+// stage's tangent derivative (dF(q) + stage ny).
+__device__ __noinline__ void tan_resid(const Layout& L, const WarpMem& m, const TanMem& t, const RowTab& R,
+                                       const CoreRow& cr, const double* __restrict__ B, int stage, double hg,
+                                       unsigned mask, bool ncdm, int lane) {
+  const int n = L.ny;
+  double hp[ND_MAX], ep[ND_MAX];
+#pragma unroll
+  for (int q = 0; q < ND_MAX; ++q) {
+    hp[q] = ep[q] = 0.;
+    if ((mask >> q) & 1u) metric(L, B, t.dF(q) + stage * n, ncdm, hp[q], ep[q]);
+  }
+  if (lane < L.nc) {
+    const int o = cr.out;
+#pragma unroll
+    for (int q = 0; q < ND_MAX; ++q) {
+      if ((mask >> q) & 1u) {
+        const double* __restrict__ F = t.dF(q) + stage * n;
+        double acc = cr.uh * hp[q] + cr.ue * ep[q];
+#pragma unroll
+        for (int u = 0; u < 5; ++u) acc = fma(cr.c[u], F[cr.s[u]], acc);
+        acc = fma(cr.tc, F[cr.ts], acc);
+        t.rv(q)[o] = fma(hg, acc, t.qv(q)[o]) - F[o];
+      }
+    }
+  }
+  const double trunc = B[B_TRUNC];
+  for (int u = lane; u < L.ntail; u += WARP) {
+    const int info = m.tinfo()[u];
+    const int e = info & 0xFFF, chn = (info >> 12) & 7;
+    const bool last = (info >> 15) & 1;
+    const int li = info >> 16;
+    const double sp = B[chain_speed_bid(chn)];
+    const double d = chn < 2 ? B[B_KAP] : 0.;
+    const double dl = last ? d + (double)(m.chL()[chn] + 1) * trunc : d;
+    const double ta = last ? 1. : R.ta[li], tg = last ? 0. : R.tg[li];
+#pragma unroll
+    for (int q = 0; q < ND_MAX; ++q) {
+      if ((mask >> q) & 1u) {
+        const double* __restrict__ F = t.dF(q) + stage * n;
+        const double fn = last ? 0. : F[e + 1];
+        const double fv = sp * (ta * F[e - 1] - tg * fn) - dl * F[e];
+        t.rv(q)[e] = fma(hg, fv, t.qv(q)[e]) - F[e];
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// sum_j a[j] v_q[j] for every direction in mask, the row loaded once
+template <int N>
+__device__ __forceinline__ void core_dot_multi(const double* __restrict__ a, const TanMem& t, unsigned mask,
+                                               double* out) {
+  double s0[ND_MAX], s1[ND_MAX];
+#pragma unroll
+  for (int q = 0; q < ND_MAX; ++q) s0[q] = s1[q] = 0.;
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    const double aj = a[j];
+#pragma unroll
+    for (int q = 0; q < ND_MAX; ++q) {
+      if ((mask >> q) & 1u) {
+        if (j & 1) s1[q] = fma(aj, t.vc(q)[j], s1[q]);
+        else s0[q] = fma(aj, t.vc(q)[j], s0[q]);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < ND_MAX; ++q) out[q] = s0[q] + s1[q];
+}
+
+// Solve M x = r_q in place (rv(q)) for the directions in mask with the
+// step's factorisation: solve_newton for several right-hand sides.
+__device__ __noinline__ void solve_multi(const Layout& L, const WarpMem& m, const TanMem& t, unsigned mask,
+                                         int lane) {
+  const int nc = L.nc;
+  const int chn = lane % NCHAIN, qd = lane / NCHAIN;
+  const bool mine = qd < ND_MAX && chn < L.nchain && ((mask >> qd) & 1u);
+  if (mine) {
+    double* r = t.rv(qd);
+    const double* mult = m.mult();
+    const int e3 = m.chs()[chn];
+    int e = e3 + (m.chL()[chn] - 3);
+    double nxt = r[e];
+    --e;
+    for (; e - 1 >= e3; e -= 2) {
+      const double ra = r[e], ma = mult[e], rb = r[e - 1], mb = mult[e - 1];
+      const double va = ra - ma * nxt;
+      const double vb = rb - mb * va;
+      r[e] = va;
+      r[e - 1] = vb;
+      nxt = vb;
+    }
+    if (e >= e3) {
+      nxt = r[e] - mult[e] * nxt;
+      r[e] = nxt;
+    }
+    const int cc = chain_core_l2(chn);
+    t.vc(qd)[m.iperm()[cc]] = r[m.cmap()[cc]] - m.m3()[chn] * nxt;
+  }
+  if (lane < nc && !(lane >= 4 && (lane - 4) % 3 == 2)) {
+    const int slot = m.iperm()[lane], src = m.cmap()[lane];
+#pragma unroll
+    for (int q = 0; q < ND_MAX; ++q)
+      if ((mask >> q) & 1u) t.vc(q)[slot] = t.rv(q)[src];
+  }
+  __syncwarp();
+  double xc[ND_MAX];
+  if (lane < nc) {
+    const double* row = m.Mc() + m.perm()[lane] * m.cs;
+    if (nc == 13) core_dot_multi<13>(row, t, mask, xc);
+    else core_dot_multi<MAXC>(row, t, mask, xc);
+  }
+  __syncwarp();
+  if (lane < nc) {
+    const int dst = m.cmap()[lane];
+#pragma unroll
+    for (int q = 0; q < ND_MAX; ++q)
+      if ((mask >> q) & 1u) t.rv(q)[dst] = xc[q];
+  }
+  __syncwarp();
+  if (mine) {
+    double* r = t.rv(qd);
+    const double* sub = m.sub();
+    const double* invd = m.invd();
+    const int e3 = m.chs()[chn];
+    const int eL = e3 + (m.chL()[chn] - 3);
+    double prev = r[e3 - 1];
+    int e = e3;
+    for (; e + 1 <= eL; e += 2) {
+      const double ra = r[e], sa = sub[e], ia = invd[e], rb = r[e + 1], sb = sub[e + 1], ib = invd[e + 1];
+      const double xa = (ra - sa * prev) * ia;
+      const double xb = (rb - sb * xa) * ib;
+      r[e] = xa;
+      r[e + 1] = xb;
+      prev = xb;
+    }
+    if (e <= eL) r[e] = (r[e] - sub[e] * prev) * invd[e];
+  }
+  __syncwarp();
+}
+
+// The tangents of one accepted step: stages 1..6 (the basis changes of the
+// step's stage times in bd, the factorisation, F, y0 and the basis slots
+// are the step's), then u1 into qv(q).  titer counts chord iterations,
+// tunconv stage solves that did not meet the test within root_max
+// iterations (their last iterate is kept: the tangents never change the
+// primal's step sequence).
+__device__ __noinline__ void tangent_step(const Layout& L, const WarpMem& m, const TanMem& t, const RowTab& R,
+                                          double h, double rtol, double atol, double inv_n, bool ncdm, int lane,
+                                          int& titer, int& tunconv) {
+  const int n = L.ny;
+  const int nd = t.nd;
+  const double hg = h * KV_G;
+  const double kappa = 1e-2, small_res = 1e-13;
+  const int root_max = 10;
+  CoreRow cr;
+  for (int i = 1; i < 7; ++i) {
+    const int slot = (i == 6) ? 5 : i;
+    const double* B = m.SB() + slot * NB;
+    core_row_at(L, R, m, B, lane, cr);
+    {
+      // the converged primal stage value Y_i, formed as the primal formed it
+      const double* __restrict__ Fr = m.F();
+      const double* __restrict__ y0 = m.y0();
+      double* __restrict__ vw = m.v();
+      for (int e = lane; e < n; e += WARP) {
+        double acc = 0., acc2 = 0.;
+        int j = 0;
+        for (; j + 1 < i; j += 2) {
+          acc = fma(KV_A[i][j], Fr[j * n + e], acc);
+          acc2 = fma(KV_A[i][j + 1], Fr[(j + 1) * n + e], acc2);
+        }
+        if (j < i) acc = fma(KV_A[i][j], Fr[j * n + e], acc);
+        const double be = y0[e] + h * (acc + acc2);
+        vw[e] = be + hg * Fr[i * n + e];
+      }
+      // z_q into rv(q); the predictor dF_i = dF_{i-1}
+#pragma unroll
+      for (int q = 0; q < ND_MAX; ++q) {
+        if (q < nd) {
+          const double* __restrict__ dF = t.dF(q);
+          double* __restrict__ dFi = t.dF(q) + i * n;
+          const double* __restrict__ u0 = t.u0(q);
+          double* __restrict__ z = t.rv(q);
+          for (int e = lane; e < n; e += WARP) {
+            double acc = 0., acc2 = 0.;
+            int j = 0;
+            for (; j + 1 < i; j += 2) {
+              acc = fma(KV_A[i][j], dF[j * n + e], acc);
+              acc2 = fma(KV_A[i][j + 1], dF[(j + 1) * n + e], acc2);
+            }
+            if (j < i) acc = fma(KV_A[i][j], dF[j * n + e], acc);
+            z[e] = u0[e] + h * (acc + acc2);
+            dFi[e] = dF[(i - 1) * n + e];
+          }
+        }
+      }
+    }
+    __syncwarp();
+    tan_const(L, m, t, R, cr, B, slot, m.v(), ncdm, lane);
+    unsigned active = (1u << nd) - 1u;
+    double dsz[ND_MAX];
+#pragma unroll
+    for (int q = 0; q < ND_MAX; ++q) dsz[q] = INFINITY;
+    for (int it = 1; it <= root_max && active; ++it) {
+      tan_resid(L, m, t, R, cr, B, i, hg, active, ncdm, lane);
+      solve_multi(L, m, t, active, lane);
+      double ss[ND_MAX];
+#pragma unroll
+      for (int q = 0; q < ND_MAX; ++q) {
+        ss[q] = 0.;
+        if ((active >> q) & 1u) {
+          const double* __restrict__ rr = t.rv(q);
+          double* __restrict__ ff = t.dF(q) + i * n;
+          for (int e = lane; e < n; e += WARP) {
+            const double x = rr[e];
+            const double fnew = ff[e] + x;
+            ff[e] = fnew;
+            const double qq = x * pos_rcp(atol + rtol * fabs(fnew));
+            ss[q] += qq * qq;
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < ND_MAX; ++q)
+        if ((active >> q) & 1u) ss[q] = warp_sum(ss[q]);
+      __syncwarp();
+      unsigned next = active;
+#pragma unroll
+      for (int q = 0; q < ND_MAX; ++q) {
+        if ((active >> q) & 1u) {
+          const double dp = dsz[q];
+          const double d = sqrt(ss[q] * inv_n);
+          dsz[q] = d;
+          ++titer;
+          if (it >= 2) {
+            // the primal's very-chord test (division-free form)
+            const bool small = d < small_res;
+            const bool converged = d > 0. && d < dp && d * d < kappa * (dp - d);
+            const bool diverged = !(d <= 2. * dp);
+            if (small || converged) next &= ~(1u << q);
+            else if (diverged) {
+              next &= ~(1u << q);
+              ++tunconv;
+            }
+          }
+        }
+      }
+      active = next;
+    }
+    tunconv += __popc(active);
+  }
+  // u1 = u0 + h (sum_j a_7j dF_j + gamma dF_7) into qv(q)
+#pragma unroll
+  for (int q = 0; q < ND_MAX; ++q) {
+    if (q < nd) {
+      const double* __restrict__ Fr = t.dF(q);
+      const double* __restrict__ u0 = t.u0(q);
+      double* __restrict__ u1 = t.qv(q);
+      for (int e = lane; e < n; e += WARP) {
+        double acc = 0., accb = 0.;
+#pragma unroll
+        for (int j = 0; j < 6; j += 2) {
+          acc = fma(KV_A[6][j], Fr[j * n + e], acc);
+          accb = fma(KV_A[6][j + 1], Fr[(j + 1) * n + e], accb);
+        }
+        acc = fma(KV_G, Fr[6 * n + e], acc + accb);
+        u1[e] = u0[e] + h * acc;
+      }
+    }
+  }
+  __syncwarp();
+}
+
 struct PertArgs {
   int n_cosmo, n_items, max_ny, ncm;
   const abcmb_cosmo* cosmo;
@@ -747,7 +1200,70 @@ struct PertArgs {
   const double* lna1;
   int* queue;
   abcmb_pert_settings s;
+  // forward-mode sensitivities (nd = 0: none)
+  int nd;
+  const int32_t* dirs;     // [n_cosmo][ND_MAX][2] (plus, minus) descriptors
+  int32_t* tstat;          // [n_items][2] or null
 };
+
+// The variants' PerturbationTables at save point isave (after the base's):
+// each variant's fields at its own save time ts_v, from the base's dense
+// state y(ts) (m.v()) moved by +-(u_q(ts) + y'(ts) (ts_plus - ts_minus) / 2),
+// with the variant's own background.  th = (ts - t0) / h of the base's
+// save time in the accepted step.
+__device__ __noinline__ void tangent_save(const Layout& L, const WarpMem& m, const TanMem& t, const PertArgs& P,
+                                          double k, double h, double th, int isave, int nsave, int ik, int lane,
+                                          const double* ncdm_w) {
+  const int n = L.ny, nd = t.nd;
+  if (lane < 2 * nd) {
+    const abcmb_cosmo& cv = P.cosmo[t.vix()[lane]];
+    const double tsv = linspace_at(cv.lna_transfer_start, 0.0, nsave, isave);
+    BG b;
+    bg_eval(cv, bg_constants(cv), P.tables, tsv, b);
+    bg_store(b, t.sv(lane));
+    t.sv(lane)[16] = tsv;
+  }
+  {
+    // dy/dt of the base's dense output at ts
+    const double* __restrict__ y0 = m.y0();
+    const double* __restrict__ y1 = m.y1();
+    const double* __restrict__ Fr = m.F();
+    double* __restrict__ yd = t.yd();
+    for (int e = lane; e < n; e += WARP) {
+      const double y0e = y0[e], y1e = y1[e];
+      const double k0 = h * Fr[e], k1 = h * Fr[6 * n + e];
+      const double a2 = 3. * (y1e - y0e) - 2. * k0 - k1, a3 = 2. * (y0e - y1e) + k0 + k1;
+      yd[e] = (k0 + th * (2. * a2 + 3. * th * a3)) / h;
+    }
+  }
+  __syncwarp();
+  for (int q = 0; q < nd; ++q) {
+    const double dts = 0.5 * (t.sv(2 * q)[16] - t.sv(2 * q + 1)[16]);
+    const double* __restrict__ dF = t.dF(q);
+    const double* __restrict__ u0 = t.u0(q);
+    const double* __restrict__ u1 = t.qv(q);
+    const double* __restrict__ yd = t.yd();
+    double* __restrict__ ut = t.rv(q);
+    for (int e = lane; e < n; e += WARP) {
+      const double u0e = u0[e], u1e = u1[e];
+      const double k0 = h * dF[e], k1 = h * dF[6 * n + e];
+      const double us = u0e + th * (k0 + th * ((3. * (u1e - u0e) - 2. * k0 - k1) + th * (2. * (u0e - u1e) + k0 + k1)));
+      ut[e] = us + yd[e] * dts;
+    }
+  }
+  __syncwarp();
+  for (int j = 0; j < 2 * nd; ++j) {
+    const double* __restrict__ ys = m.v();
+    const double* __restrict__ ut = t.rv(j >> 1);
+    double* __restrict__ yv = t.yv();
+    const bool minus = j & 1;
+    for (int e = lane; e < n; e += WARP) yv[e] = minus ? ys[e] - ut[e] : ys[e] + ut[e];
+    __syncwarp();
+    const abcmb_cosmo& cv = P.cosmo[t.vix()[j]];
+    write_fields(cv, L, P.tables, k, t.sv(j)[16], t.yv(), P.pt, nsave, isave, ik, lane, t.sv(j), ncdm_w);
+    __syncwarp();
+  }
+}
 
 // Two instantiations of the same kernel, differing only in the register cap:
 // 2 blocks of 4 warps per SM (250 registers, no spills: the shortest time per
@@ -784,6 +1300,7 @@ __device__ unsigned long long g_pert_phase[PHASE_SLOTS * PHASE_N];
   } while (0)
 #endif
 
+template <bool TAN>
 __device__ __forceinline__ void pert_body(const PertArgs& P) {
   extern __shared__ double smem[];
   __shared__ RowTab R;
@@ -817,7 +1334,13 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
   }
   __syncthreads();
   WarpMem m;
-  carve(smem + (size_t)wib * warp_mem_doubles(P.max_ny, P.ncm), P.max_ny, P.ncm, m);
+  const size_t wdoubles = warp_mem_doubles(P.max_ny, P.ncm);
+  carve(smem + (size_t)wib * (wdoubles + tan_mem_doubles(P.max_ny, P.ncm, TAN ? P.nd : 0)), P.max_ny, P.ncm, m);
+  TanMem tm;
+  tm.p = m.p + wdoubles;
+  tm.my = P.max_ny;
+  tm.nd = TAN ? P.nd : 0;
+  tm.ncm = P.ncm;
 #ifdef ABCMB_PHASE_CLOCKS
   const int ph_index = blockIdx.x * (blockDim.x >> 5) + wib;
   unsigned long long* ph_slot = ph_index < PHASE_SLOTS ? g_pert_phase + (size_t)ph_index * PHASE_N : nullptr;
@@ -847,10 +1370,24 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
     {
       const int lmx = max(max(L.lg, L.lp), max(L.lnu, ncdm ? L.lm : 4));
       const int lmn = min(min(L.lg, L.lp), min(L.lnu, ncdm ? L.lm : 4));
-      if (n > P.max_ny || L.nc > P.ncm || lmx > LMAXT || lmn < 4 || n != c.ny) {
+      bool bad = n > P.max_ny || L.nc > P.ncm || lmx > LMAXT || lmn < 4 || n != c.ny;
+      if constexpr (TAN) {
+        // every variant shares the base's state layout and k grid
+        for (int j = 0; j < 2 * tm.nd; ++j) {
+          const int v = P.dirs[(ci * ND_MAX + (j >> 1)) * 2 + (j & 1)];
+          bad = bad || v < 0 || v >= P.n_cosmo;
+          if (!bad) {
+            const abcmb_cosmo& cv = P.cosmo[v];
+            bad = cv.ny != c.ny || cv.nk != c.nk || cv.has_ncdm != c.has_ncdm || cv.lmax_g != c.lmax_g ||
+                  cv.lmax_pol_g != c.lmax_pol_g || cv.lmax_nu != c.lmax_nu || cv.lmax_ncdm != c.lmax_ncdm;
+          }
+        }
+      }
+      if (bad) {
         if (lane == 0) {
           abcmb_kstat st{ABCMB_STATUS_BAD_LAYOUT, 0, 0, 0, 0.};
           P.kstat[item] = st;
+          if (TAN && P.tstat) P.tstat[2 * item] = P.tstat[2 * item + 1] = 0;
         }
         continue;
       }
@@ -891,35 +1428,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
     for (int e = lane; e < n; e += WARP) m.y0()[e] = 0.;
     __syncwarp();
     if (lane == 0) {
-      const double tau_ini = tau_of(c, P.tables, lna_start);
-      const double om = c.om, Rn = c.R_nu, Rb = c.R_b;
-      const double kt = k * tau_ini;
-      m.y0()[0] = (1. - k * k * tau_ini * tau_ini / 12. / (15. + 4. * Rn) *
-                          (5. + 4. * Rn - (16. * Rn * Rn + 280. * Rn + 325) / 10. / (2. * Rn + 15.) * tau_ini * om));
-      m.y0()[1] = -(kt * kt) / 4. * (1. - om * tau_ini / 5.);
-      m.y0()[2] = -(kt * kt) / 4. * (1. - om * tau_ini / 5.);
-      const double thb = -k * k * k * k * tau_ini * tau_ini * tau_ini / 36. *
-                         (1. - 3. * (1. + 5. * Rb - Rn) / 20. / (1. - Rn) * om * tau_ini);
-      m.y0()[3] = thb;
-      m.y0()[L.i_g] = -(kt * kt) / 3. * (1. - om * tau_ini / 5.);
-      m.y0()[L.i_g + 1] = thb;
-      const double nd = -(kt * kt) / 3. * (1. - om * tau_ini / 5.);
-      const double nth = -k * (kt * kt * kt) / 36. / (4. * Rn + 15.) *
-                         (4. * Rn + 11. + 12. - 3. * (8. * Rn * Rn + 50. * Rn + 275.) / 20. / (2. * Rn + 15.) * tau_ini * om);
-      const double ns = (kt * kt) / (45. + 12. * Rn) * 2. * (1. + (4. * Rn - 5.) / 4. / (2. * Rn + 15.) * tau_ini * om);
-      m.y0()[L.i_nu] = nd;
-      m.y0()[L.i_nu + 1] = nth;
-      m.y0()[L.i_nu + 2] = ns;
-      if (ncdm) {
-        for (int i = 0; i < 3; ++i) {
-          double q = Q3[i];
-          double fac = q / (1. + exp(-q));
-          double* Pb = m.y0() + L.i_ncdm + i * L.nM;
-          Pb[0] = nd / 4. * fac;
-          Pb[1] = nth / 3. * fac;
-          Pb[2] = ns / 2. * fac;
-        }
-      }
+      write_ic(c, L, P.tables, k, lna_start, m.y0());
       stage_basis(c, K, P.tables, k, ik2, R.ncdm_w, lna_start, m.SB(), nullptr);
       m.SV()[16] = -1.;                                      // no save background computed yet
     }
@@ -932,6 +1441,41 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
     CoreRow cr;
     core_row_at(L, R, m, m.SB(), lane, cr);
     apply_A(L, m, R, cr, m.SB(), m.y0(), m.F(), nullptr, ncdm, lane);   // FSAL stage 1
+    int titer = 0, tunconv = 0;
+    if constexpr (TAN) {
+      const int nd = tm.nd;
+      if (lane < 2 * nd) tm.vix()[lane] = P.dirs[(ci * ND_MAX + (lane >> 1)) * 2 + (lane & 1)];
+      for (int q = 0; q < nd; ++q)
+        for (int e = lane; e < n; e += WARP) tm.qv(q)[e] = tm.rv(q)[e] = 0.;
+      __syncwarp();
+      // the variants' start times and initial conditions (plus into qv, minus into rv)
+      if (lane < 2 * nd) {
+        const int v = tm.vix()[lane];
+        const double l2 = np_interp_lna(S.R_large, nullptr, P.aHg + (int64_t)v * NSTART, k);
+        const double tv = fmin(fmin(P.lna1[v], l2), -10.);
+        write_ic(P.cosmo[v], L, P.tables, k, tv, (lane & 1) ? tm.rv(lane >> 1) : tm.qv(lane >> 1));
+        tm.sv(0)[lane] = tv;
+      }
+      __syncwarp();
+      // u(t0) = dy0/deps - f(t0, y0) dt0/deps (also into rv: the z of tan_const)
+      for (int q = 0; q < nd; ++q) {
+        const double dt0 = 0.5 * (tm.sv(0)[2 * q] - tm.sv(0)[2 * q + 1]);
+        for (int e = lane; e < n; e += WARP) {
+          const double u = 0.5 * (tm.qv(q)[e] - tm.rv(q)[e]) - m.F()[e] * dt0;
+          tm.u0(q)[e] = u;
+          tm.rv(q)[e] = u;
+        }
+      }
+      if (lane < nd)
+        stage_basis_diff(P.cosmo[tm.vix()[2 * lane]], P.cosmo[tm.vix()[2 * lane + 1]], P.tables, k, ik2, R.ncdm_w,
+                         lna_start, tm.bd(1, lane));
+      __syncwarp();
+      // dF_0 = A(t0) u + dA(t0) y0
+      tan_const(L, m, tm, R, cr, m.SB(), 1, m.y0(), ncdm, lane);
+      for (int q = 0; q < nd; ++q)
+        for (int e = lane; e < n; e += WARP) tm.dF(q)[e] = tm.qv(q)[e];
+      __syncwarp();
+    }
 
     while (t0 < 0.0) {
       PERT_PHASE(7);
@@ -949,6 +1493,15 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
           stage_basis(c, K, P.tables, k, ik2, R.ncdm_w, want_sv ? tsn : t0 + KV_C[lane + 1] * h, m.SB() + (lane + 1) * NB,
                       want_sv ? m.SV() : nullptr);
         if (want_sv) m.SV()[16] = (double)isave;
+        if constexpr (TAN) {
+          // lanes 6.. : the basis change of each (stage time, direction)
+          const int task = lane - NSLOT;
+          if (task >= 0 && task < 5 * tm.nd) {
+            const int slot = task / tm.nd + 1, q = task % tm.nd;
+            stage_basis_diff(P.cosmo[tm.vix()[2 * q]], P.cosmo[tm.vix()[2 * q + 1]], P.tables, k, ik2, R.ncdm_w,
+                             t0 + KV_C[slot] * h, tm.bd(slot, q));
+          }
+        }
       }
       __syncwarp();
       PERT_PHASE(0);
@@ -1068,6 +1621,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
       PERT_PHASE(6);
       if (keep) {
         ++nacc;
+        if constexpr (TAN) tangent_step(L, m, tm, R, h, rtol, atol, inv_n, ncdm, lane, titer, tunconv);
         // cubic Hermite dense output on [t0, t1] at every save point it covers
         while (isave < nsave) {
           double ts = linspace_at(lts, 0.0, nsave, isave);
@@ -1088,6 +1642,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
           write_fields(c, L, P.tables, k, ts, m.v(), P.pt, nsave, isave, ik, lane,
                        m.SV()[16] == (double)isave ? m.SV() : nullptr, R.ncdm_w);
           __syncwarp();
+          if constexpr (TAN) tangent_save(L, m, tm, P, k, h, th, isave, nsave, ik, lane, R.ncdm_w);
           ++isave;
         }
         prev_prev_inv = prev_inv;
@@ -1095,6 +1650,13 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
         for (int e = lane; e < n; e += WARP) {
           m.y0()[e] = m.y1()[e];
           m.F()[e] = m.F()[6 * n + e];
+        }
+        if constexpr (TAN) {
+          for (int q = 0; q < tm.nd; ++q)
+            for (int e = lane; e < n; e += WARP) {
+              tm.u0(q)[e] = tm.qv(q)[e];
+              tm.dF(q)[e] = tm.dF(q)[6 * n + e];
+            }
         }
         m.SB()[lane] = m.SB()[5 * NB + lane];                  // basis at the new t0
         __syncwarp();
@@ -1117,6 +1679,10 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
       st.n_newton = nnewton;
       st.lna_start = lna_start;
       P.kstat[item] = st;
+      if (TAN && P.tstat) {
+        P.tstat[2 * item] = titer;
+        P.tstat[2 * item + 1] = tunconv;
+      }
     }
     __syncwarp();
   }
@@ -1131,7 +1697,13 @@ namespace abcmb {
 
 template <int MIN_BLOCKS>
 __global__ void __launch_bounds__(PERT_THREADS_MAX, MIN_BLOCKS) pert_kernel(PertArgs P) {
-  pert_body(P);
+  pert_body<false>(P);
+}
+
+// The same integration with the tangents; shared memory (not registers)
+// limits its occupancy, so the register cap stays off.
+__global__ void __launch_bounds__(PERT_THREADS_MAX, 1) pert_kernel_tangent(PertArgs P) {
+  pert_body<true>(P);
 }
 
 int pert_phase_clocks(unsigned long long* out, int reset) {
@@ -1196,6 +1768,9 @@ cudaError_t launch_pert(int n_cosmo, const abcmb_cosmo* cosmo, const double* tab
   A.lna1 = lna1;
   A.queue = queue;
   A.s = s;
+  A.nd = 0;
+  A.dirs = nullptr;
+  A.tstat = nullptr;
   if (warps_per_block < 1 || 32 * warps_per_block > PERT_THREADS_MAX) return cudaErrorInvalidConfiguration;
   const int threads = 32 * warps_per_block;
   const size_t smem = (size_t)warps_per_block * pert_smem_per_warp(s.max_ny, A.ncm);
@@ -1221,6 +1796,86 @@ cudaError_t launch_pert(int n_cosmo, const abcmb_cosmo* cosmo, const double* tab
   if (grid_out) *grid_out = grid;
   if (throughput) pert_kernel<PERT_BLOCKS_THROUGHPUT><<<grid, threads, smem, stream>>>(A);
   else pert_kernel<PERT_BLOCKS_LATENCY><<<grid, threads, smem, stream>>>(A);
+  return cudaGetLastError();
+}
+
+size_t pert_tangent_smem_per_warp(int max_ny, int ncm, int nd) {
+  return (warp_mem_doubles(max_ny, ncm) + tan_mem_doubles(max_ny, ncm, nd)) * sizeof(double);
+}
+
+// abcmb_pert_forward_tangent: the items are base cosmologies; warps per
+// block is chosen (1..4) for the most resident warps per SM, since the
+// per-warp shared memory (the tangents' stage derivatives) sets occupancy.
+cudaError_t launch_pert_tangent(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
+                                int n_items, const int32_t* items, int nd, const int32_t* dirs,
+                                const abcmb_pert_settings& s, double* pt, abcmb_kstat* kstat, int32_t* tstat,
+                                void* ws, cudaStream_t stream, int* grid_out, int* warps_out) {
+  if (nd < 1 || nd > ND_MAX) return cudaErrorInvalidValue;
+  char* w = static_cast<char*>(ws);
+  int* queue = reinterpret_cast<int*>(w);
+  w += 256;
+  double* lna1 = reinterpret_cast<double*>(w);
+  w += ((int64_t)n_cosmo * 8 + 255) / 256 * 256;
+  double* aHg = reinterpret_cast<double*>(w);
+  w += ((int64_t)n_cosmo * NSTART * 8 + 255) / 256 * 256;
+  double* f1g = reinterpret_cast<double*>(w);
+  cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int), stream);
+  if (e != cudaSuccess) return e;
+  dim3 g1((NSTART + 255) / 256, n_cosmo);
+  start_grid_kernel<<<g1, 256, 0, stream>>>(n_cosmo, cosmo, tables, aHg, f1g);
+  start_lna1_kernel<<<(n_cosmo + 127) / 128, 128, 0, stream>>>(n_cosmo, f1g, s.R_tc, lna1);
+  PertArgs A;
+  A.n_cosmo = n_cosmo;
+  A.n_items = n_items;
+  A.max_ny = s.max_ny;
+  A.ncm = s.any_ncdm ? 22 : 13;
+  A.cosmo = cosmo;
+  A.tables = tables;
+  A.kbuf = kbuf;
+  A.items = items;
+  A.pt = pt;
+  A.kstat = kstat;
+  A.aHg = aHg;
+  A.lna1 = lna1;
+  A.queue = queue;
+  A.s = s;
+  A.nd = nd;
+  A.dirs = dirs;
+  A.tstat = tstat;
+  const size_t per_warp = pert_tangent_smem_per_warp(s.max_ny, A.ncm, nd);
+  const void* fn = (const void*)pert_kernel_tangent;
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  int best_w = 0, best_blocks = 0, best_total = 0;
+  for (int wpb = PERT_THREADS_MAX / 32; wpb >= 1; --wpb) {
+    const size_t smem = (size_t)wpb * per_warp;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, smem) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (per_sm * wpb > best_total) {
+      best_total = per_sm * wpb;
+      best_w = wpb;
+      best_blocks = per_sm;
+    }
+  }
+  if (best_total < 1) return cudaErrorInvalidConfiguration;
+  const size_t smem = (size_t)best_w * per_warp;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int grid = nsm * best_blocks;
+  const int need = (n_items + best_w - 1) / best_w;
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
+  if (grid_out) *grid_out = grid;
+  if (warps_out) *warps_out = best_w;
+  pert_kernel_tangent<<<grid, 32 * best_w, smem, stream>>>(A);
   return cudaGetLastError();
 }
 

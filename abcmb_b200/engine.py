@@ -94,6 +94,33 @@ class DeviceBatch:
                                     ctypes.c_void_p(st.cuda_stream))
         _lib.check(rc, "abcmb_pert_forward")
 
+    def pert_forward_tangent(self, settings: CPertSettings, dirs: np.ndarray, n_dir: int, stream=None):
+        """abcmb_pert_forward_tangent: the batch's items are base cosmologies,
+        dirs (int32 [n_cosmo, 4, 2]) their (plus, minus) variant
+        descriptors; fills the base's and every variant's PerturbationTable.
+        The tangent statistics go to self.tstat ([n_items, 2] int32)."""
+        lib = _lib.load()
+        st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        key = (dirs.ctypes.data, dirs.nbytes)
+        if getattr(self, "_dirs_key", None) != key:
+            self.dirs = torch.from_numpy(np.ascontiguousarray(dirs, dtype=np.int32).reshape(-1)).to(self.device)
+            self.tstat = torch.zeros(2 * max(self.batch.n_items, 1), dtype=torch.int32, device=self.device)
+            self._dirs_key = key
+        rc = lib.abcmb_pert_forward_tangent(self.batch.n_cosmo, _ptr(self.cosmo), _ptr(self.tables),
+                                            _ptr(self.kbuf), self.batch.n_items, _ptr(self.items), int(n_dir),
+                                            _ptr(self.dirs), ctypes.byref(settings), _ptr(self.pt), _ptr(self.kstat),
+                                            _ptr(self.tstat), _ptr(self.ws_pert), self.ws_pert.numel(),
+                                            ctypes.c_void_p(st.cuda_stream))
+        _lib.check(rc, "abcmb_pert_forward_tangent")
+
+    def pert_forward_grad(self, gw, settings: CPertSettings, stream=None):
+        """The perturbations of a gradient-expanded batch (gradients.expand):
+        one tangent launch, or every finite-difference variant integrated."""
+        if gw.mode == "tangent":
+            self.pert_forward_tangent(settings, gw.dirs, gw.n_dir, stream)
+        else:
+            self.pert_forward(settings, stream)
+
     def bg_forward(self, settings=None, stream=None, fetch_tables: bool = False) -> np.ndarray:
         """abcmb_bg_forward on the whole batch: the conformal-time tables,
         tau0, lna_transfer_start and line-of-sight arrays of every cosmology,

@@ -19,7 +19,7 @@ def run_cl_grad(gw, device=None, pk_k=None, pk_z=None, return_variants: bool = F
     and, with return_variants, the C_l of every variant [n * n_var, 3, l_max-1] last."""
     w = gw.base
     db = engine.DeviceBatch.upload(gw.batch, device)
-    db.pert_forward(w.pert_settings())
+    db.pert_forward_grad(gw, w.pert_settings())
     db.check_status()
     lr = engine.LosRunner(db, w.kt, w.los_settings(), want_dns=not w.lensing)
     lr.run()

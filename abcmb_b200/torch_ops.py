@@ -120,7 +120,7 @@ class ClWithGrad(torch.autograd.Function):
                 p[name] = float(th[i, j])
         gw = gradients.expand(w)
         db = engine.DeviceBatch.upload(gw.batch, theta.device if theta.is_cuda else None)
-        db.pert_forward(w.pert_settings())
+        db.pert_forward_grad(gw, w.pert_settings())
         db.check_status()
         lr = engine.LosRunner(db, w.kt, w.los_settings(), want_dns=True)
         lr.run()
