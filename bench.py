@@ -4,16 +4,19 @@
 Workload (per GPU, weak scaling): the batched uneven configuration -- 64
 cosmologies with parameters uniform within +-5% of the LCDM fiducial,
 massive-neutrino count drawn from {0, 1, 3}, per-cosmology k grids of
-400..800 modes on [1e-5, 1] / Mpc, unlensed TT/TE/EE to l = 2500 -- with the
-C_l gradient with respect to (h, omega_b, omega_cdm, A_s, n_s, tau_reio):
-central differences (relative step 1e-4) for the four background
-parameters, exact A_s / n_s derivatives from the same line-of-sight launch.
-One step = perturbations of all 9 variants of all 64 cosmologies (one
-persistent launch) + line of sight + gradient assembly.  Inputs are seeded
+400..800 modes on [1e-5, 1] / Mpc, x_e / T_m tables in HyRex's padded
+layout, unlensed TT/TE/EE to l = 2500 -- with the C_l gradient with respect
+to (h, omega_b, omega_cdm, A_s, n_s, tau_reio).  One step = the
+perturbations of the 64 cosmologies with the forward-mode sensitivities of
+h, omega_b, omega_cdm and tau_reio (one persistent tangent launch; the
+plus / minus variants' tables written around each base) + the line of sight
+over all 576 descriptors + gradient assembly (exact A_s / n_s derivatives
+from the same line-of-sight launch).  --grad fd integrates every variant on
+its own instead (central differences of whole solves).  Inputs are seeded
 synthetic (numpy default_rng(20261203 + rank)); background tables are
 produced on the host before timing (they are inputs of this path).
 
-  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--grad tangent|fd]
 """
 from __future__ import annotations
 
@@ -45,15 +48,27 @@ def parse():
     ap.add_argument("--n-cosmo", type=int, default=64)
     ap.add_argument("--l-max", type=int, default=2500)
     ap.add_argument("--e2e-steps", type=int, default=1)
-    ap.add_argument("--cpu-sample-stride", type=int, default=24)
+    ap.add_argument("--grad", default="tangent", choices=["tangent", "fd"])
+    ap.add_argument("--plain-sample", type=int, default=8,
+                    help="cosmologies of the batch timed on the plain (unbatched forward + FD) path")
+    # internal: the CPU baseline in a process of its own (no torch, no CUDA)
+    ap.add_argument("--cpu-worker", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--seed", type=int, default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--one-thread", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--out", default=None, help=argparse.SUPPRESS)
     return ap.parse_args()
+
+
+GRAD_DESC = {"tangent": "forward-mode tangents of (h,ob,oc,tau) in one integration per (cosmology,k), variants' "
+                        "tables at rel step 1e-4 from them; exact A_s,n_s",
+             "fd": "central FD rel 1e-4 (h,ob,oc,tau): every variant integrated; exact A_s,n_s"}
 
 
 def workload_config(args, world):
     return {"workload": f"batched uneven LCDM(+0/1/3 massive nu): {args.n_cosmo} cosmologies x 9 "
-                        f"gradient variants per GPU, Nk 400-800 on [1e-5,1]/Mpc, unlensed TT/TE/EE to "
-                        f"l={args.l_max}, grad wrt (h,omega_b,omega_cdm,A_s,n_s,tau_reio)",
-            "n_cosmo_per_gpu": args.n_cosmo, "grad": "central FD rel 1e-4 (h,ob,oc,tau) + exact A_s,n_s",
+                        f"gradient descriptors per GPU, Nk 400-800 on [1e-5,1]/Mpc, x_e/T_m in HyRex's padded "
+                        f"layout, unlensed TT/TE/EE to l={args.l_max}, grad wrt (h,omega_b,omega_cdm,A_s,n_s,tau_reio)",
+            "n_cosmo_per_gpu": args.n_cosmo, "grad": GRAD_DESC[args.grad],
             "hierarchies": "l_max_g=12 l_max_pol_g=10 l_max_nu=17 l_max_ncdm=17 (reference defaults)",
             "precision": "FP64 ODE, FP64 LOS", "l2": "inputs > L2 (126 MB) per step",
             "parallelism": f"dp{world} (independent cosmologies per GPU, no collective)"}
@@ -107,105 +122,145 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-def cpu_sample(gw, stride: int, n_threads: int, extras: bool = True):
-    """Oracle time for one cosmology's C_l + gradient (9 ODE variants + LOS),
-    measured on every `stride`-th k mode of its 9 variants plus one full
-    line-of-sight run, scaled to the whole unit."""
+def cpu_cosmology(seed: int, l_max: int, n_threads: int, one_thread: bool = False, out: str = None) -> dict:
+    """The oracle (the CPU restatement of the reference's path, C + OpenMP)
+    on the first cosmology of the batch a rank draws: its C_l and gradient
+    the way the reference computes them -- forward-mode sensitivities through
+    the whole perturbation integration (the analogue of jax.jacfwd through
+    diffrax) over every k mode, then the line of sight of all 13 gradient
+    descriptors (A_s and n_s by central differences of the line of sight).
+    Runs in a process without torch or CUDA.  With `out`, the C_l and
+    gradient go to that .npz for the GPU's error report."""
+    from abcmb_b200 import bessel, configs, gradients
     from oracle import oracle
-    from abcmb_b200 import packing
-    b = gw.batch
-    nvar = gw.n_var
-    sel = [i for i in range(b.n_items) if b.items[i, 0] < nvar and b.items[i, 1] % stride == 0]
-    n_full = sum(1 for i in range(b.n_items) if b.items[i, 0] < nvar)
-    sub = packing.Batch(cosmo=b.cosmo, tables=b.tables, kbuf=b.kbuf, items=b.items[sel].copy(), pt_size=b.pt_size,
-                        n_save=b.n_save, bgs=b.bgs, layouts=b.layouts)
-    st = gw.base.pert_settings()
-    # the host is shared: the faster of two identical runs
-    t_runs = []
-    for _ in range(2):
-        t0 = time.perf_counter()
-        rc, pt, ks = oracle.pert_forward(sub, st, n_threads)
-        t_runs.append(time.perf_counter() - t0)
-    t_ode = min(t_runs) * n_full / len(sel)
-    t_los = _los_sample(gw, pt, n_threads)
-    total = t_ode + t_los
-    sample = (f"oracle (C, FP64, OpenMP) on 1 cosmology's 9 gradient variants: every {stride}th k mode of "
-              f"the ODE ({len(sel)}/{n_full} items, scaled) + 1 full line-of-sight run (x{nvar}); "
-              f"s per cosmology+grad: ode {t_ode:.2f} (faster of 2 runs; the other "
-              f"{max(t_runs) * n_full / len(sel):.2f}) los {t_los:.2f}")
-    base = {"value": 1.0 / total, "unit": UNIT, "cores": n_threads, "kind": "port", "sample": sample}
-    if not extras:
-        return base
-    # the same sample on one thread (the reference's CI setting), on every
-    # 16th of the sampled items to bound the time
-    sel1 = sel[::16]
-    sub1 = packing.Batch(cosmo=b.cosmo, tables=b.tables, kbuf=b.kbuf, items=b.items[sel1].copy(),
-                         pt_size=b.pt_size, n_save=b.n_save, bgs=b.bgs, layouts=b.layouts)
-    t0 = time.perf_counter()
-    oracle.pert_forward(sub1, st, 1)
-    t_ode1 = (time.perf_counter() - t0) * n_full / len(sel1)
-    # the recombination history of one cosmology on one core (oracle HyRex)
-    from abcmb_b200 import cosmology
-    p0 = cosmology.add_derived_parameters(gw.base.params_in[0], gw.base.has_ncdm[0], gw.base.specs)
-    oracle.hyrex(p0, gw.base.has_ncdm[0])                  # first call: module and table loading
-    t0 = time.perf_counter()
-    oracle.hyrex(p0, gw.base.has_ncdm[0])
-    t_hyrex = time.perf_counter() - t0
-    base.update({"hyrex_oracle_ms_per_cosmology_one_core": t_hyrex * 1000.0,
-                 "ode_one_thread": {"s_per_cosmology": t_ode1, "items": len(sel1),
-                                    "sample": f"every 16th of the items above ({len(sel1)}) on 1 thread, scaled",
-                                    "all_cores_speedup": t_ode1 / t_ode}})
-    return base
-
-
-def _los_sample(gw, pt, n_threads: int) -> float:
-    """Oracle line of sight of the first cosmology, times the variant count."""
-    from oracle import oracle
-    from abcmb_b200 import bessel, packing
-    b = gw.batch
-    one = packing.Batch(cosmo=b.cosmo[:1].copy(), tables=b.tables, kbuf=b.kbuf, items=b.items[:0], pt_size=b.pt_size,
-                        n_save=b.n_save, bgs=b.bgs[:1], layouts=b.layouts[:1])
-    t0 = time.perf_counter()
-    oracle.los_forward(one, pt, gw.base.kt, gw.base.los_settings(), bessel.load(), n_threads)
-    return (time.perf_counter() - t0) * gw.n_var
-
-
-def plain_gpu_fwd_fd(gw, w, dev, stream, want_dns=True):
-    """The metric's comparison path, on this library's kernels (the
-    reference's JAX GPU path is not installable here): one cosmology's C_l and
-    gradient with every finite-difference variant run on its own -- its own
-    perturbation launch over its k modes, its own line of sight, C_l copied
-    back -- one after another, as a caller without batching would."""
-    import torch
-    from abcmb_b200 import engine, packing
-    b = gw.batch
-    runs = []
-    for v in range(gw.n_var):
-        sub = packing.pack([b.bgs[v]], [b.layouts[v]], [w.kgrids[0]], n_save=b.n_save)
-        db = engine.DeviceBatch.upload(sub, dev)
-        lr = engine.LosRunner(db, w.kt, w.los_settings(), want_dns=want_dns)
-        runs.append((db, lr))
+    w = configs.c4(n_cosmo=1, l_max=l_max, seed=seed)
+    gw = gradients.expand(w, processes=min(13, os.cpu_count() or 1), mode="tangent", primordial_fd=True)
     st = w.pert_settings()
+    ls = w.los_settings()
+    bt = bessel.load()
+    t0 = time.perf_counter()
+    rc, pt, ks, ts = oracle.pert_forward_tangent(gw.batch, st, gw.dirs, gw.n_dir, n_threads)
+    t1 = time.perf_counter()
+    _, _, cl = oracle.los_forward(gw.batch, pt, w.kt, ls, bt, n_threads)
+    t2 = time.perf_counter()
+    if rc != 0:
+        raise RuntimeError(f"oracle perturbations failed ({rc})")
+    cl_b, grad = gw.assemble(cl, np.zeros_like(cl))
+    res = {"s_ode": t1 - t0, "s_los": t2 - t1, "s_total": t2 - t0, "nk": int(gw.batch.cosmo["nk"][0]),
+           "descriptors": int(gw.batch.n_cosmo), "cores": n_threads}
+    if out:
+        np.savez(out, cl=cl_b[0], grad=grad[0])
+    if one_thread:
+        # the same tangent integration on one thread (the reference's CI
+        # setting), on every 8th k mode, scaled to all of them
+        from abcmb_b200 import packing
+        b = gw.batch
+        sel = np.arange(0, b.n_items, 8)
+        sub = packing.Batch(cosmo=b.cosmo, tables=b.tables, kbuf=b.kbuf, items=b.items[sel].copy(),
+                            pt_size=b.pt_size, n_save=b.n_save, bgs=b.bgs, layouts=b.layouts)
+        t0 = time.perf_counter()
+        oracle.pert_forward_tangent(sub, st, gw.dirs, gw.n_dir, 1)
+        res["ode_one_thread"] = {"s_per_cosmology": (time.perf_counter() - t0) * b.n_items / len(sel),
+                                 "items": int(len(sel)), "of": int(b.n_items),
+                                 "sample": "every 8th k mode of the tangent integration on 1 thread, scaled"}
+        p0 = gw.batch.bgs[0].params
+        oracle.hyrex(p0, w.has_ncdm[0])                  # first call: module and table loading
+        t0 = time.perf_counter()
+        oracle.hyrex(p0, w.has_ncdm[0])
+        res["hyrex_oracle_ms_per_cosmology_one_core"] = (time.perf_counter() - t0) * 1000.0
+    return res
 
-    def once():
-        for db, lr in runs:
-            db.pert_forward(st, stream)
-            lr.run(stream)
-            lr.cl.cpu()                      # the caller reads each variant's C_l
 
-    once()
-    torch.cuda.synchronize(dev)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    once()
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    ms = e0.elapsed_time(e1)
-    return {"value": 1000.0 / ms, "unit": UNIT, "ms_per_cosmology": ms,
-            "sample": f"first cosmology of the batch, its {gw.n_var} variants each run alone (own perturbation "
-                      f"launch over its {int(b.cosmo['nk'][0])} k modes + own line of sight + C_l read back), "
-                      f"this library's kernels"}
+def cpu_baseline_subprocess(seed: int, l_max: int, one_thread: bool, out: str = None) -> dict:
+    """cpu_cosmology in a fresh interpreter (no torch, no CUDA context, all
+    host threads), so the timing is the same as the reference arm's."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", "--seed", str(seed), "--l-max", str(l_max)]
+    if one_thread:
+        cmd.append("--one-thread")
+    if out:
+        cmd += ["--out", out]
+    env = dict(os.environ)
+    env.pop("CUDA_VISIBLE_DEVICES", None)
+    r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
+    if r.returncode != 0:
+        raise RuntimeError(f"cpu worker failed: {r.stderr[-500:]}")
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def cpu_baseline_line(res: dict) -> dict:
+    v = 1.0 / res["s_total"]
+    cb = {"value": v, "unit": UNIT, "cores": res["cores"], "kind": "port",
+          "sample": f"oracle (C, FP64, OpenMP, its own process) on the batch's first cosmology ({res['nk']} k "
+                    f"modes): forward-mode tangent integration of (h,ob,oc,tau) over every k mode "
+                    f"{res['s_ode']:.2f} s + line of sight of {res['descriptors']} descriptors {res['s_los']:.2f} s"}
+    for key in ("ode_one_thread", "hyrex_oracle_ms_per_cosmology_one_core"):
+        if key in res:
+            cb[key] = res[key]
+    return cb
+
+
+def plain_gpu_fwd_fd(gw, w, dev, stream, n_sample: int):
+    """The metric's comparison path, on this library's kernels (the
+    reference's JAX GPU path is not installable here): a cosmology's C_l and
+    gradient the plain way -- one forward evaluation per finite-difference
+    point, 13 of them (the base and +-1e-4 relative in each of the six
+    parameters), each its own perturbation launch over the cosmology's k
+    modes and its own line of sight, C_l copied back -- one after another, as
+    a caller without batching would.  Timed on n_sample cosmologies spread
+    over the batch and averaged."""
+    import dataclasses as dc
+    import torch
+    from abcmb_b200 import configs, engine, packing
+    b = gw.batch
+    nb = len(w.params_in)
+    picks = sorted({int(round(i * nb / n_sample)) for i in range(n_sample)} - {nb})
+    st = w.pert_settings()
+    per = []
+    nks = []
+    for ci in picks:
+        base_idx = ci * gw.n_var
+        var = gw.variants[ci]
+        runs = []
+        bgs = [b.bgs[base_idx]]
+        for name in configs.GRAD_PARAMS:
+            for sgn in (+1, -1):
+                j = next((jj for jj, v in enumerate(var) if v[0] == name and v[1] == sgn), None)
+                if j is not None:
+                    bgs.append(b.bgs[base_idx + j])
+                else:               # A_s, n_s: the base background with the parameter moved
+                    bg0 = b.bgs[base_idx]
+                    p = dict(bg0.params)
+                    p[name] = p[name] * (1.0 + sgn * 1e-4)
+                    bgs.append(dc.replace(bg0, params=p))
+        for bg in bgs:
+            sub = packing.pack([bg], [b.layouts[base_idx]], [w.kgrids[ci]], n_save=b.n_save)
+            db = engine.DeviceBatch.upload(sub, dev)
+            lr = engine.LosRunner(db, w.kt, w.los_settings())
+            runs.append((db, lr))
+
+        def once():
+            for db, lr in runs:
+                db.pert_forward(st, stream)
+                lr.run(stream)
+                lr.cl.cpu()                      # the caller reads each evaluation's C_l
+
+        once()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        once()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        per.append(e0.elapsed_time(e1))
+        nks.append(int(w.kgrids[ci].shape[0]))
+        del runs
+    ms = float(np.mean(per))
+    return {"value": 1000.0 / ms, "unit": UNIT, "ms_per_cosmology": ms, "evaluations_per_cosmology": 13,
+            "cosmologies": picks, "nk": nks,
+            "sample": f"{len(picks)} cosmologies of the batch (Nk {min(nks)}-{max(nks)}), each as 13 forward "
+                      f"evaluations run alone (own perturbation launch + own line of sight + C_l read back), "
+                      f"this library's kernels; mean time per cosmology"}
 
 
 def bg_forward_timing(gw, db, dev, stream):
@@ -303,24 +358,28 @@ def hyrex_timing(w, dev):
 
 
 def run_reference(args, rank, world):
-    """Reference arm: the CPU restatement of the path on the host cores."""
+    """Reference arm: the CPU restatement of the path (the oracle) on the
+    host cores.  Each step is one whole cosmology's C_l + gradient (every k
+    mode, every line of sight), so ms_per_step is the time a step takes."""
     if rank != 0:
         return
-    from abcmb_b200 import configs, gradients
-    w = configs.c4(n_cosmo=1, l_max=args.l_max)
-    gw = gradients.expand(w, processes=min(9, os.cpu_count() or 1))
+    from abcmb_b200 import configs
     nthr = os.cpu_count() or 1
-    vals = []
-    for _ in range(max(args.warmup, 0)):
-        cpu_sample(gw, args.cpu_sample_stride * 2, nthr, extras=False)
-    n_steps = max(args.steps, 1)
-    for i in range(n_steps):
-        vals.append(cpu_sample(gw, args.cpu_sample_stride, nthr, extras=(i == n_steps - 1)))
-    v = statistics.median([x["value"] for x in vals])
-    cb = dict(vals[-1])
+    steps = []
+    # the oracle has nothing to warm beyond its first call (table loading):
+    # one untimed step, so the whole run stays within a few minutes
+    warm = min(max(args.warmup, 0), 1)
+    for i in range(warm + max(args.steps, 1)):
+        res = cpu_cosmology(configs.SEED, args.l_max, nthr, one_thread=(i == warm))
+        if i >= warm:
+            steps.append(res)
+    ms = statistics.median([r["s_total"] for r in steps]) * 1000.0
+    v = 1000.0 / ms
+    cb = cpu_baseline_line(steps[0])
     cb["value"] = v
-    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+    cb["sample"] += f"; median of {len(steps)} steps"
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": len(steps), "warmup": warm,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic", "impl": "reference", "config": workload_config(args, world),
             "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -332,6 +391,11 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.cpu_worker:
+        res = cpu_cosmology(args.seed if args.seed is not None else 20261203, args.l_max, os.cpu_count() or 1,
+                            one_thread=args.one_thread, out=args.out)
+        print(json.dumps(res), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
@@ -340,7 +404,7 @@ def main():
     from abcmb_b200 import configs, gradients
     t_build = time.perf_counter()
     w = configs.c4(n_cosmo=args.n_cosmo, l_max=args.l_max, seed=configs.SEED + rank)
-    gw = gradients.expand(w, processes=os.cpu_count() or 1)
+    gw = gradients.expand(w, processes=os.cpu_count() or 1, mode=args.grad)
     t_build = time.perf_counter() - t_build
 
     import torch
@@ -394,7 +458,7 @@ def main():
     def step(record=False):
         if record:
             ev_p0.record(stream)
-        db.pert_forward(st, stream)
+        db.pert_forward_grad(gw, st, stream)
         if record:
             ev_p1.record(stream)
         lr.run(stream)
@@ -459,30 +523,46 @@ def main():
     e2e = {"value": world * nb / (ms_e2e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e}
 
-    # roofline of the dominant kernel (the perturbation launch): FP64 work
+    # roofline of the dominant kernel (the perturbation launch): FP64 work,
+    # the survey's convention per solve of the primal (every attempted step:
+    # 7 stages x (RHS 8 Ny + 200, structured solve 20 Ny)) plus, with the
+    # tangents, one RHS + solve per tangent chord iteration and two RHS per
+    # (accepted step, direction, implicit stage) for the stage's constant part
     steps_k = (ks["n_accepted"] + ks["n_rejected"]).astype(np.float64)
     ny_k = b.cosmo["ny"][b.items[:, 0]].astype(np.float64)
     flops = float(np.sum(steps_k * 7.0 * ((8.0 * ny_k + 200.0) + 20.0 * ny_k)))
+    flops_def = "sum_k steps_k * 7 * (8 Ny + 200 + 20 Ny)"
+    tangent_stats = None
+    if gw.mode == "tangent":
+        ts = db.tstat.cpu().numpy().reshape(-1, 2)[:b.n_items].astype(np.float64)
+        flops += float(np.sum(ts[:, 0] * (28.0 * ny_k + 200.0)
+                              + ks["n_accepted"] * gw.n_dir * 6 * 2 * (8.0 * ny_k + 200.0)))
+        flops_def += (" + sum_k [tangent chord iterations_k * (28 Ny + 200) + accepted_k * n_dir * 6 * 2 "
+                      "* (8 Ny + 200)]")
+        tangent_stats = {"directions": gw.n_dir, "chord_iterations_per_item": float(ts[:, 0].mean()),
+                         "unconverged_stage_solves": int(ts[:, 1].sum())}
     pert_avg = float(np.mean(pert_ms))
     peak = __import__("ctypes").c_double(0.0)
     rc = lib.abcmb_probe_fp64_tflops(__import__("ctypes").byref(peak), 20000,
                                      __import__("ctypes").c_void_p(stream.cuda_stream))
     achieved = flops / (pert_avg / 1000.0) / 1e12
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "pert_kernel_traffic.json")
+    tfile = os.path.join(ROOT, "profiles", ("pert_kernel_tangent" if gw.mode == "tangent" else "pert_kernel")
+                         + "_traffic.json")
     if os.path.isfile(tfile):
         try:
             tj = json.load(open(tfile))
             traffic = tj["bytes_per_item"] * b.n_items
         except (ValueError, KeyError):
             traffic = None
-    roofline = {"bound": "fp64", "kernel": "pert_kernel", "achieved": achieved,
+    roofline = {"bound": "fp64", "kernel": "pert_kernel_tangent" if gw.mode == "tangent" else "pert_kernel",
+                "achieved": achieved,
                 "peak": peak.value if rc == 0 else None, "unit": "TFLOP/s",
                 "frac": (achieved / peak.value) if rc == 0 and peak.value > 0 else None,
                 "traffic": traffic,
                 "peak_source": "measured in this run: FP64 FMA probe (abcmb_probe_fp64_tflops); "
                                "MEASURED_PEAKS.json has no FP64 figure",
-                "flops_def": "sum_k steps_k * 7 * (8 Ny + 200 + 20 Ny)", "launch_ms": pert_avg,
+                "flops_def": flops_def, "launch_ms": pert_avg,
                 "hbm_gbs_peak": _peak_hbm()[0], "hbm_gbs_peak_source": _peak_hbm()[1]}
     # our kernel launches per step: pert (2 start kernels + the persistent
     # kernel) + 5 per line-of-sight chunk of engine.LOS_CHUNK cosmologies
@@ -494,20 +574,46 @@ def main():
             "config": workload_config(args, world), "e2e": e2e, "roofline": roofline, "gpu_launches": launches,
             "clocks": clk.summary(), "items_per_step": int(b.n_items),
             "ode_steps_mean": float(steps_k.mean()), "host_build_s": t_build}
+    if tangent_stats:
+        line["tangents"] = tangent_stats
     if rank == 0 and world == 1:
         line["bg_forward"] = bg_forward_timing(gw, db, dev, stream)
         try:
             line["hyrex_forward"] = hyrex_timing(w, dev)
         except Exception as ex:                            # an extra measurement never costs the line
             line["hyrex_forward"] = {"error": str(ex)[:200]}
-        plain = plain_gpu_fwd_fd(gw, w, dev, stream)
+        plain = plain_gpu_fwd_fd(gw, w, dev, stream, args.plain_sample)
         plain["batched_over_plain"] = value / plain["value"]
         line["plain_gpu_fwd_fd"] = plain
-        line["cpu_baseline"] = cpu_sample(gw, args.cpu_sample_stride, os.cpu_count() or 1)
+        import tempfile
+        with tempfile.TemporaryDirectory() as tmp:
+            ref_file = os.path.join(tmp, "oracle_cl.npz")
+            res = cpu_baseline_subprocess(configs.SEED + rank, args.l_max, one_thread=True, out=ref_file)
+            line["cpu_baseline"] = cpu_baseline_line(res)
+            o = np.load(ref_file)
+            line["err_vs_oracle"] = err_vs_oracle(res_cl.numpy()[0], res_grad.numpy()[0], o["cl"], o["grad"])
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def err_vs_oracle(cl, grad, cl_o, grad_o) -> dict:
+    """C_l and gradient of the batch's first cosmology against the oracle's
+    (the CPU baseline's own run of that cosmology): max relative error of
+    TT and EE, TE relative to |TT| + |TE|, each gradient series relative to
+    its own maximum over l."""
+    tt = float(np.max(np.abs(cl[0] - cl_o[0]) / np.abs(cl_o[0])))
+    ee = float(np.max(np.abs(cl[2] - cl_o[2]) / np.abs(cl_o[2])))
+    te = float(np.max(np.abs(cl[1] - cl_o[1]) / (np.abs(cl_o[0]) + np.abs(cl_o[1]))))
+    g = np.abs(grad - grad_o).max(axis=-1) / (np.abs(grad_o).max(axis=-1) + 1e-300)
+    from abcmb_b200.configs import GRAD_PARAMS
+    return {"cosmology": 0, "cl_max_rel": {"TT": tt, "TE": te, "EE": ee},
+            "grad_max_rel": {name: {"TT": float(g[i, 0]), "TE": float(g[i, 1]), "EE": float(g[i, 2])}
+                             for i, name in enumerate(GRAD_PARAMS)},
+            "grad_max_rel_all": float(g.max()),
+            "oracle": "oracle C restatement, FP64, same tangent algorithm and inputs (A_s, n_s rows: central "
+                      "differences of its line of sight)"}
 
 
 HBM_GBS_FALLBACK = 6650.0     # copy bandwidth measured earlier on this pool's B200s

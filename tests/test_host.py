@@ -245,3 +245,29 @@ def test_hyrex_layout_lengths_match_hyrex_sizes():
     b = w.build().batch
     assert int(b.cosmo["n_xe"][0]) == bt.HYREX_XE_LEN
     assert b.cosmo["lna_xe_max"][0] == pytest.approx(rec.lna_xe0 + bt.HYREX_XE_LEN * rec.lna_xe_dx, rel=1e-15)
+
+
+def test_tangent_expansion_layout():
+    """Tangent mode: every cosmology keeps its 8 plus / minus descriptors
+    (own tables and PerturbationTable slots) but only the base has work
+    items, and dirs names each direction's (plus, minus) pair in FD_PARAMS
+    order; the assembly is the same central difference of the variants."""
+    from abcmb_b200 import configs, gradients
+    w = configs.c4(n_cosmo=2, nk_range=(30, 40), xe_layout="compact")
+    gt = gradients.expand(w, processes=1, mode="tangent")
+    b = gt.batch
+    assert gt.mode == "tangent" and gt.n_dir == 4 and gt.n_var == 9 and b.n_cosmo == 18
+    assert set(int(x) for x in b.items[:, 0]) == {0, 9}
+    assert b.n_items == int(b.cosmo["nk"][0] + b.cosmo["nk"][9])
+    assert gt.dirs.shape == (18, gradients.MAX_TANGENTS, 2) and gt.dirs.dtype == np.int32
+    for base in (0, 9):
+        var = gt.variants[base // 9]
+        for q, name in enumerate(gradients.FD_PARAMS):
+            p, m = gt.dirs[base, q]
+            assert var[p - base][:2] == (name, 1) and var[m - base][:2] == (name, -1)
+            assert b.cosmo["nk"][p] == b.cosmo["nk"][base] and b.cosmo["ny"][m] == b.cosmo["ny"][base]
+            assert b.cosmo["off_pt"][p] != b.cosmo["off_pt"][base] != b.cosmo["off_pt"][m]
+    assert (gt.dirs[[i for i in range(18) if i not in (0, 9)]] == -1).all()
+    gf = gradients.expand(w, processes=1, mode="fd")
+    assert gf.batch.n_items == 9 * b.n_items and gf.dirs is None
+    np.testing.assert_array_equal(gf.batch.cosmo, b.cosmo)
