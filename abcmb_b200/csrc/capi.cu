@@ -14,7 +14,7 @@ cudaError_t launch_pert(int n_cosmo, const abcmb_cosmo* cosmo, const double* tab
                         int n_items, const int32_t* items, const abcmb_pert_settings& s, double* pt,
                         abcmb_kstat* kstat, void* ws, cudaStream_t stream, int warps_per_block, int* grid_out);
 cudaError_t launch_pert_tangent(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
-                                int n_items, const int32_t* items, int nd, const int32_t* dirs,
+                                int n_items, const int32_t* items, int nd, const int32_t* dirs, double tscale,
                                 const abcmb_pert_settings& s, double* pt, abcmb_kstat* kstat, int32_t* tstat,
                                 void* ws, cudaStream_t stream, int* grid_out, int* warps_out);
 int64_t los_workspace_bytes(int n_cosmo, int max_nk, int nkt, int n_ell_tab, int n_save, int precision);
@@ -223,7 +223,8 @@ int abcmb_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* 
 
 int abcmb_pert_forward_tangent(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* tables_dev,
                                const double* k_dev, int n_items, const int32_t* items_dev, int n_dir,
-                               const int32_t* dir_dev, const abcmb_pert_settings* settings, double* pt_dev,
+                               const int32_t* dir_dev, double tangent_scale, const abcmb_pert_settings* settings,
+                               double* pt_dev,
                                abcmb_kstat* kstat_dev, int32_t* tstat_dev, void* workspace_dev,
                                int64_t workspace_bytes, void* stream) {
   if (n_cosmo <= 0 || n_items < 0 || !cosmo_dev || !tables_dev || !k_dev || !settings || !pt_dev || !kstat_dev ||
@@ -231,6 +232,8 @@ int abcmb_pert_forward_tangent(int n_cosmo, const abcmb_cosmo* cosmo_dev, const 
     return fail(ABCMB_ERR_ARG, "abcmb_pert_forward_tangent: null argument");
   if (n_dir < 1 || n_dir > ABCMB_MAX_TANGENTS)
     return fail(ABCMB_ERR_ARG, "abcmb_pert_forward_tangent: n_dir must be 1..ABCMB_MAX_TANGENTS");
+  if (!(tangent_scale > 0. && tangent_scale <= 1.))
+    return fail(ABCMB_ERR_ARG, "abcmb_pert_forward_tangent: tangent_scale must be in (0, 1]");
   if (settings->max_ny <= 0 || settings->n_save < 2 || settings->max_steps <= 0)
     return fail(ABCMB_ERR_ARG, "abcmb_pert_forward_tangent: settings.max_ny / n_save / max_steps");
   if (workspace_bytes < abcmb::pert_workspace_bytes(n_cosmo) || !workspace_dev)
@@ -238,7 +241,8 @@ int abcmb_pert_forward_tangent(int n_cosmo, const abcmb_cosmo* cosmo_dev, const 
   if (n_items == 0) return ABCMB_OK;
   int warps = 0;
   cudaError_t e = abcmb::launch_pert_tangent(n_cosmo, cosmo_dev, tables_dev, k_dev, n_items, items_dev, n_dir,
-                                             dir_dev, *settings, pt_dev, kstat_dev, tstat_dev, workspace_dev,
+                                             dir_dev, tangent_scale, *settings, pt_dev, kstat_dev, tstat_dev,
+                                             workspace_dev,
                                              static_cast<cudaStream_t>(stream), &g_last_grid, &warps);
   if (e != cudaSuccess) return cuda_fail(e, "abcmb_pert_forward_tangent");
   return ABCMB_OK;

@@ -814,6 +814,7 @@ __device__ __noinline__ void write_ic(const abcmb_cosmo& c, const Layout& L, con
 // accumulator per direction, so the extra work fills lanes the single
 // primal solve leaves idle.
 constexpr int ND_MAX = ABCMB_MAX_TANGENTS;
+constexpr int TANGENT_ROOT_MAX = 16;
 
 // Per-warp tangent scratch, after the primal's WarpMem.  Per direction q:
 // u0 (tangent at t0), dF (7 stage derivatives, stride ny), q (the constant
@@ -1057,7 +1058,15 @@ __device__ __noinline__ void solve_multi(const Layout& L, const WarpMem& m, cons
 
 // The tangents of one accepted step: stages 1..6 (the basis changes of the
 // step's stage times in bd, the factorisation, F, y0 and the basis slots
-// are the step's), then u1 into qv(q).  titer counts chord iterations,
+// are the step's), then u1 into qv(q).  atol is the primal's scaled by the
+// tangents' relative size (PertArgs.tscale).  The tangent iteration is
+// linear with the primal's iteration matrix I - M_lin^-1 M_i: its spectral
+// radius is small whenever the primal stage converged, but it is far from
+// normal in the tight-coupling era, so an error with a stiff component (the
+// initial tangent's start-time term puts one there) can grow ~25x over the
+// first iteration before it contracts.  A growing step therefore does not
+// stop the tangent iterations (only a non-finite one does), and they get
+// TANGENT_ROOT_MAX iterations.  titer counts chord iterations,
 // tunconv stage solves that did not meet the test within root_max
 // iterations (their last iterate is kept: the tangents never change the
 // primal's step sequence).
@@ -1068,7 +1077,7 @@ __device__ __noinline__ void tangent_step(const Layout& L, const WarpMem& m, con
   const int nd = t.nd;
   const double hg = h * KV_G;
   const double kappa = 1e-2, small_res = 1e-13;
-  const int root_max = 10;
+  const int root_max = TANGENT_ROOT_MAX;
   CoreRow cr;
   for (int i = 1; i < 7; ++i) {
     const int slot = (i == 6) ? 5 : i;
@@ -1150,12 +1159,12 @@ __device__ __noinline__ void tangent_step(const Layout& L, const WarpMem& m, con
           dsz[q] = d;
           ++titer;
           if (it >= 2) {
-            // the primal's very-chord test (division-free form)
+            // the primal's very-chord termination test (division-free form);
+            // no divergence stop but a non-finite size
             const bool small = d < small_res;
             const bool converged = d > 0. && d < dp && d * d < kappa * (dp - d);
-            const bool diverged = !(d <= 2. * dp);
             if (small || converged) next &= ~(1u << q);
-            else if (diverged) {
+            else if (!isfinite(d)) {
               next &= ~(1u << q);
               ++tunconv;
             }
@@ -1202,6 +1211,7 @@ struct PertArgs {
   abcmb_pert_settings s;
   // forward-mode sensitivities (nd = 0: none)
   int nd;
+  double tscale;           // tangent size relative to the state's (atol of the tangent solves x tscale)
   const int32_t* dirs;     // [n_cosmo][ND_MAX][2] (plus, minus) descriptors
   int32_t* tstat;          // [n_items][2] or null
 };
@@ -1621,7 +1631,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
       PERT_PHASE(6);
       if (keep) {
         ++nacc;
-        if constexpr (TAN) tangent_step(L, m, tm, R, h, rtol, atol, inv_n, ncdm, lane, titer, tunconv);
+        if constexpr (TAN) tangent_step(L, m, tm, R, h, rtol, atol * P.tscale, inv_n, ncdm, lane, titer, tunconv);
         // cubic Hermite dense output on [t0, t1] at every save point it covers
         while (isave < nsave) {
           double ts = linspace_at(lts, 0.0, nsave, isave);
@@ -1769,6 +1779,7 @@ cudaError_t launch_pert(int n_cosmo, const abcmb_cosmo* cosmo, const double* tab
   A.queue = queue;
   A.s = s;
   A.nd = 0;
+  A.tscale = 1.;
   A.dirs = nullptr;
   A.tstat = nullptr;
   if (warps_per_block < 1 || 32 * warps_per_block > PERT_THREADS_MAX) return cudaErrorInvalidConfiguration;
@@ -1807,7 +1818,7 @@ size_t pert_tangent_smem_per_warp(int max_ny, int ncm, int nd) {
 // block is chosen (1..4) for the most resident warps per SM, since the
 // per-warp shared memory (the tangents' stage derivatives) sets occupancy.
 cudaError_t launch_pert_tangent(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
-                                int n_items, const int32_t* items, int nd, const int32_t* dirs,
+                                int n_items, const int32_t* items, int nd, const int32_t* dirs, double tscale,
                                 const abcmb_pert_settings& s, double* pt, abcmb_kstat* kstat, int32_t* tstat,
                                 void* ws, cudaStream_t stream, int* grid_out, int* warps_out) {
   if (nd < 1 || nd > ND_MAX) return cudaErrorInvalidValue;
@@ -1840,6 +1851,7 @@ cudaError_t launch_pert_tangent(int n_cosmo, const abcmb_cosmo* cosmo, const dou
   A.queue = queue;
   A.s = s;
   A.nd = nd;
+  A.tscale = tscale;
   A.dirs = dirs;
   A.tstat = tstat;
   const size_t per_warp = pert_tangent_smem_per_warp(s.max_ny, A.ncm, nd);

@@ -94,10 +94,12 @@ class DeviceBatch:
                                     ctypes.c_void_p(st.cuda_stream))
         _lib.check(rc, "abcmb_pert_forward")
 
-    def pert_forward_tangent(self, settings: CPertSettings, dirs: np.ndarray, n_dir: int, stream=None):
+    def pert_forward_tangent(self, settings: CPertSettings, dirs: np.ndarray, n_dir: int, tscale: float,
+                             stream=None):
         """abcmb_pert_forward_tangent: the batch's items are base cosmologies,
         dirs (int32 [n_cosmo, 4, 2]) their (plus, minus) variant
-        descriptors; fills the base's and every variant's PerturbationTable.
+        descriptors, tscale the parameter step as a fraction of the
+        parameter; fills the base's and every variant's PerturbationTable.
         The tangent statistics go to self.tstat ([n_items, 2] int32)."""
         lib = _lib.load()
         st = stream if stream is not None else torch.cuda.current_stream(self.device)
@@ -108,7 +110,7 @@ class DeviceBatch:
             self._dirs_key = key
         rc = lib.abcmb_pert_forward_tangent(self.batch.n_cosmo, _ptr(self.cosmo), _ptr(self.tables),
                                             _ptr(self.kbuf), self.batch.n_items, _ptr(self.items), int(n_dir),
-                                            _ptr(self.dirs), ctypes.byref(settings), _ptr(self.pt), _ptr(self.kstat),
+                                            _ptr(self.dirs), float(tscale), ctypes.byref(settings), _ptr(self.pt), _ptr(self.kstat),
                                             _ptr(self.tstat), _ptr(self.ws_pert), self.ws_pert.numel(),
                                             ctypes.c_void_p(st.cuda_stream))
         _lib.check(rc, "abcmb_pert_forward_tangent")
@@ -117,7 +119,7 @@ class DeviceBatch:
         """The perturbations of a gradient-expanded batch (gradients.expand):
         one tangent launch, or every finite-difference variant integrated."""
         if gw.mode == "tangent":
-            self.pert_forward_tangent(settings, gw.dirs, gw.n_dir, stream)
+            self.pert_forward_tangent(settings, gw.dirs, gw.n_dir, gw.rel_step, stream)
         else:
             self.pert_forward(settings, stream)
 

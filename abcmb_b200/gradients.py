@@ -74,6 +74,7 @@ class GradWorkload:
     mode: str = "fd"
     dirs: np.ndarray = None  # tangent mode: int32 [n_descriptors, MAX_TANGENTS, 2] (plus, minus)
     n_dir: int = 0
+    rel_step: float = REL_STEP
 
     def assemble(self, cl: np.ndarray, dcl_dns: np.ndarray):
         """cl, dcl_dns: (n_base * n_var, 3, n_l) -> C_l (n_base, 3, n_l), grad (n_base, 6, 3, n_l)."""
@@ -166,4 +167,4 @@ def expand(w: Workload, n_save: int = 500, processes: int = 0, rel_step: float =
                                                         w.lensing)
     w.batch = batch
     return GradWorkload(base=w, variants=variants, batch=batch, n_var=len(variants[0]), mode=mode, dirs=dirs,
-                        n_dir=len(FD_PARAMS) if mode == "tangent" else 0)
+                        n_dir=len(FD_PARAMS) if mode == "tangent" else 0, rel_step=rel_step)

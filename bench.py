@@ -139,7 +139,7 @@ def cpu_cosmology(seed: int, l_max: int, n_threads: int, one_thread: bool = Fals
     ls = w.los_settings()
     bt = bessel.load()
     t0 = time.perf_counter()
-    rc, pt, ks, ts = oracle.pert_forward_tangent(gw.batch, st, gw.dirs, gw.n_dir, n_threads)
+    rc, pt, ks, ts = oracle.pert_forward_tangent(gw.batch, st, gw.dirs, gw.n_dir, gw.rel_step, n_threads)
     t1 = time.perf_counter()
     _, _, cl = oracle.los_forward(gw.batch, pt, w.kt, ls, bt, n_threads)
     t2 = time.perf_counter()
@@ -159,7 +159,7 @@ def cpu_cosmology(seed: int, l_max: int, n_threads: int, one_thread: bool = Fals
         sub = packing.Batch(cosmo=b.cosmo, tables=b.tables, kbuf=b.kbuf, items=b.items[sel].copy(),
                             pt_size=b.pt_size, n_save=b.n_save, bgs=b.bgs, layouts=b.layouts)
         t0 = time.perf_counter()
-        oracle.pert_forward_tangent(sub, st, gw.dirs, gw.n_dir, 1)
+        oracle.pert_forward_tangent(sub, st, gw.dirs, gw.n_dir, gw.rel_step, 1)
         res["ode_one_thread"] = {"s_per_cosmology": (time.perf_counter() - t0) * b.n_items / len(sel),
                                  "items": int(len(sel)), "of": int(b.n_items),
                                  "sample": "every 8th k mode of the tangent integration on 1 thread, scaled"}

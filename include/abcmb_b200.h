@@ -354,6 +354,12 @@ int abcmb_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev,
  * variant, and (C_l(plus) - C_l(minus)) / 2 eps_p the derivative.
  *   items_dev   [n_items] (base cosmology, k) pairs
  *   n_dir       1..ABCMB_MAX_TANGENTS
+ *   tangent_scale  the tangents' size relative to the state's: the
+ *               parameter step as a fraction of the parameter (eps_p /
+ *               theta_p, e.g. 1e-4).  The tangent stage solves use the
+ *               primal's very-chord test with atol scaled by it, so they
+ *               stop at the same relative accuracy as the primal instead of
+ *               iterating at rounding level.
  *   tstat_dev   [n_items x 2] int32 (optional): tangent chord iterations,
  *               tangent stage solves left unconverged after the primal's
  *               iteration limit (the last iterate is kept; the tangents
@@ -365,7 +371,7 @@ int abcmb_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev,
 int abcmb_pert_forward_tangent(int n_cosmo, const abcmb_cosmo* cosmo_dev,
                                const double* tables_dev, const double* k_dev,
                                int n_items, const int32_t* items_dev,
-                               int n_dir, const int32_t* dir_dev,
+                               int n_dir, const int32_t* dir_dev, double tangent_scale,
                                const abcmb_pert_settings* settings,
                                double* pt_dev, abcmb_kstat* kstat_dev, int32_t* tstat_dev,
                                void* workspace_dev, int64_t workspace_bytes,

@@ -39,7 +39,7 @@ int oracle_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo, const double* tab
                         int n_items, const int32_t* items, const abcmb_pert_settings* s,
                         double* pt, abcmb_kstat* kstat, int n_threads);
 int oracle_pert_forward_tangent(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
-                                int n_items, const int32_t* items, int n_dir, const int32_t* dirs,
+                                int n_items, const int32_t* items, int n_dir, const int32_t* dirs, double tscale,
                                 const abcmb_pert_settings* s, double* pt, abcmb_kstat* kstat, int32_t* tstat,
                                 int n_threads);
 void oracle_spline_slopes(const double* x, const double* y, int n, double* s);

@@ -60,7 +60,7 @@ def lib():
         L.oracle_pert_forward.argtypes = [ctypes.c_int, vp, _dp, _dp, ctypes.c_int, _ip, vp, _dp, vp, ctypes.c_int]
         L.oracle_pert_forward_tangent.restype = ctypes.c_int
         L.oracle_pert_forward_tangent.argtypes = [ctypes.c_int, vp, _dp, _dp, ctypes.c_int, _ip, ctypes.c_int, _ip,
-                                                  vp, _dp, vp, _ip, ctypes.c_int]
+                                                  ctypes.c_double, vp, _dp, vp, _ip, ctypes.c_int]
         L.oracle_spline_slopes.argtypes = [_dp, _dp, ctypes.c_int, _dp]
         L.oracle_spline_eval.restype = ctypes.c_double
         L.oracle_spline_eval.argtypes = [_dp, _dp, _dp, ctypes.c_int, ctypes.c_double]
@@ -137,10 +137,11 @@ def pert_forward(batch, settings, n_threads: int = 0):
     return rc, pt, kstat
 
 
-def pert_forward_tangent(batch, settings, dirs, n_dir: int, n_threads: int = 0):
+def pert_forward_tangent(batch, settings, dirs, n_dir: int, tscale: float, n_threads: int = 0):
     """Oracle perturbations with forward-mode sensitivities: the batch's
     items name base cosmologies, dirs (int32, n_cosmo x 4 x 2) their
-    (plus, minus) variant descriptors.  Returns (rc, pt, kstat, tstat)."""
+    (plus, minus) variant descriptors, tscale the parameter step as a
+    fraction of the parameter.  Returns (rc, pt, kstat, tstat)."""
     from abcmb_b200.packing import KSTAT_DTYPE
     pt = np.zeros(batch.pt_size)
     kstat = np.zeros(batch.n_items, dtype=KSTAT_DTYPE)
@@ -148,7 +149,8 @@ def pert_forward_tangent(batch, settings, dirs, n_dir: int, n_threads: int = 0):
     items = np.ascontiguousarray(batch.items, dtype=np.int32)
     d = np.ascontiguousarray(dirs, dtype=np.int32).reshape(-1)
     rc = lib().oracle_pert_forward_tangent(batch.n_cosmo, vptr(batch.cosmo), dptr(batch.tables), dptr(batch.kbuf),
-                                           batch.n_items, iptr(items), n_dir, iptr(d), ctypes.byref(settings),
+                                           batch.n_items, iptr(items), n_dir, iptr(d), float(tscale),
+                                           ctypes.byref(settings),
                                            dptr(pt), vptr(kstat), iptr(tstat), n_threads)
     return rc, pt, kstat, tstat.reshape(-1, 2)
 

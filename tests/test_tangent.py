@@ -38,11 +38,11 @@ def _both(engine, gw, st):
     from oracle import oracle
     db = engine.DeviceBatch.upload(gw.batch)
     db.pt.zero_()
-    db.pert_forward_tangent(st, gw.dirs, gw.n_dir)
+    db.pert_forward_tangent(st, gw.dirs, gw.n_dir, gw.rel_step)
     ks = db.check_status()
     pt = db.pt.cpu().numpy()
     ts = db.tstat.cpu().numpy().reshape(-1, 2)
-    rc, pt_o, ks_o, ts_o = oracle.pert_forward_tangent(gw.batch, st, gw.dirs, gw.n_dir)
+    rc, pt_o, ks_o, ts_o = oracle.pert_forward_tangent(gw.batch, st, gw.dirs, gw.n_dir, gw.rel_step)
     assert rc == 0
     return db, pt, ks, ts, pt_o, ks_o, ts_o
 
@@ -74,7 +74,7 @@ def test_tangent_base_table_is_the_forward_table(gpu, c1_small):
     gw = gradients.expand(w, processes=1, mode="tangent")
     st = w.pert_settings()
     db = gpu.DeviceBatch.upload(gw.batch)
-    db.pert_forward_tangent(st, gw.dirs, gw.n_dir)
+    db.pert_forward_tangent(st, gw.dirs, gw.n_dir, gw.rel_step)
     db.check_status()
     ref = gpu.DeviceBatch.upload(c1_small.batch)
     ref.pert_forward(c1_small.pert_settings())
@@ -123,7 +123,7 @@ def _grad_both(engine, w, gw):
     n_out = ls.l_max - 1
     dns = lr.dcl_dns.cpu().numpy().reshape(-1, 3, n_out)
     cl_b, grad = gw.assemble(lr.cl_host(), dns)
-    rc, pt_o, _, _ = oracle.pert_forward_tangent(gw.batch, st, gw.dirs, gw.n_dir)
+    rc, pt_o, _, _ = oracle.pert_forward_tangent(gw.batch, st, gw.dirs, gw.n_dir, gw.rel_step)
     assert rc == 0
     _, _, cl_o = oracle.los_forward(gw.batch, pt_o, w.kt, ls, bessel.load())
     cl_bo, grad_o = gw.assemble(cl_o, dns)           # the n_s row is the GPU's own in both
