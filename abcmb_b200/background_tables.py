@@ -90,6 +90,13 @@ class BackgroundTables:
         line-of-sight arrays are still to be produced by abcmb_bg_forward."""
         return self.tau_tab is None
 
+    @property
+    def needs_los(self) -> bool:
+        """True for a background that has its conformal-time table (e.g. the
+        reference's, from_reference) but neither line-of-sight arrays nor a
+        host optical depth: abcmb_bg_forward supplies the six arrays."""
+        return self.tau_tab is not None and self.los is None and self.kappa_lna is None
+
     def set_device_result(self, tau_tab, los, stat):
         """Take the tables and scalars abcmb_bg_forward produced for this
         cosmology (stat: one BGSTAT_DTYPE record)."""
@@ -326,6 +333,57 @@ def from_hyrex(params: dict, has_ncdm: bool, xe, lna_xe, tm, lna_tm) -> Backgrou
         tm_arr=tm_arr, lna_tm0=float(lna_tm[0]), lna_tm_dx=float(lna_tm[1] - lna_tm[0]),
         lna_tm_last=float(lna_tm[nt - 1]), tm_last=float(tm[nt - 1]),
         lna_transfer_start=float("nan"), lna_rec=float("nan"), z_reion=z_re)
+
+
+def _padded(x):
+    """(finite array, lastval) of an array_with_padding (arr, lastnum, lastval;
+    abcmb/hyrex/array_with_padding.py:18-40) or of a plain inf-padded array.
+    The +inf padding is replaced by the last valid value, as
+    Background.__init__ does (background.py:536-550); an object whose arr was
+    already made finite keeps the lastval it carries."""
+    arr = np.asarray(getattr(x, "arr", x), dtype=np.float64).copy()
+    if hasattr(x, "lastval"):
+        lastval = float(np.asarray(x.lastval))
+    else:
+        bad = ~np.isfinite(arr)
+        last = int(np.argmax(bad)) - 1 if bad.any() else arr.size - 1
+        if last < 0:
+            raise ValueError("a padded table needs at least one valid entry")
+        lastval = float(arr[last])
+    arr[np.isinf(arr)] = lastval
+    return arr, lastval
+
+
+def from_reference(BG, params: dict, has_ncdm: bool = None) -> BackgroundTables:
+    """BackgroundTables of the reference's own Background
+    (abcmb/background.py:420-564), read by attribute name, so any object with
+    the same fields works (no jax needed): tau_tab (10000 values on
+    linspace(-33, 0, 10000)), tau0, lna_transfer_start, lna_rec, z_reion,
+    and the HyRex tables xe_tab, lna_xe_tab, Tm_tab, lna_Tm_tab as
+    array_with_padding (arr, lastnum, lastval).  The x_e / T_m lookups use
+    the reference's conventions: fast_interp over lna_tab.arr[0] +
+    [0, len(arr)] * (arr[1] - arr[0]) with the padded length, the first
+    value before the table, lastval from lna_tab.lastval on
+    (background.py:593-603, 647-657).  The optical depth (kappa_func, a
+    diffrax solution object) is not read: the six line-of-sight arrays come
+    from abcmb_bg_forward's restatement of the same solve (needs_los)."""
+    p = dict(params)
+    if has_ncdm is None:
+        names = [getattr(s, "name", type(s).__name__) for s in getattr(BG, "species_list", ())]
+        has_ncdm = "MassiveNeutrino" in names or float(p.get("N_nu_massive", 0.0)) > 0.0
+    xe_arr, xe_last = _padded(BG.xe_tab)
+    lxe, lxe_last = _padded(BG.lna_xe_tab)
+    tm_arr, tm_last = _padded(BG.Tm_tab)
+    ltm, ltm_last = _padded(BG.lna_Tm_tab)
+    tau_tab = np.asarray(BG.tau_tab, dtype=np.float64).reshape(-1).copy()
+    if tau_tab.shape != (NTAU,) or xe_arr.shape != lxe.shape or tm_arr.shape != ltm.shape:
+        raise ValueError("Background tables have unexpected shapes")
+    return BackgroundTables(
+        params=p, has_ncdm=bool(has_ncdm), tau_tab=tau_tab, tau0=float(np.asarray(BG.tau0)),
+        xe_arr=xe_arr, lna_xe0=float(lxe[0]), lna_xe_dx=float(lxe[1] - lxe[0]), lna_xe_last=lxe_last,
+        xe_last=xe_last, tm_arr=tm_arr, lna_tm0=float(ltm[0]), lna_tm_dx=float(ltm[1] - ltm[0]),
+        lna_tm_last=ltm_last, tm_last=tm_last, lna_transfer_start=float(np.asarray(BG.lna_transfer_start)),
+        lna_rec=float(np.asarray(BG.lna_rec)), z_reion=float(np.asarray(getattr(BG, "z_reion", np.nan))))
 
 
 # ---------------------------------------------------------------------------

@@ -195,7 +195,8 @@ def pack(bgs, layouts, kgrids, n_save: int = 500, order: str = "cost", alias_of=
         r["lna_tm_max"] = bg.lna_tm0 + ntm * bg.lna_tm_dx
         r["lna_tm_last"] = bg.lna_tm_last
         r["tm_last"] = bg.tm_last
-        los = np.zeros((6, nl)) if pending else bg.los_arrays(n_save)
+        needs_los = getattr(bg, "needs_los", False)
+        los = np.zeros((6, nl)) if (pending or needs_los) else bg.los_arrays(n_save)
         tau_tab = np.zeros(NTAU_TAB) if pending else bg.tau_tab
         r["off_tau"] = off
         chunks.append(tau_tab); off += tau_tab.shape[0]

@@ -10,7 +10,11 @@ metric_alpha_prime and species_perturbations -- computed by the CUDA kernels
 BackgroundPreRecomb / HyRex / Background produce); one that carries only the
 x_e / T_m history (``background_tables.make_recombination``) is completed on
 the GPU first (abcmb_bg_forward: conformal time, optical depth, visibility,
-line-of-sight arrays).  Only the six shipped
+line-of-sight arrays).  The reference's own Background object (or anything
+with its field names: tau_tab, tau0, lna_transfer_start, lna_rec and the
+HyRex tables as array_with_padding) is taken as it is
+(``background_tables.from_reference``), its line-of-sight arrays computed by
+abcmb_bg_forward.  Only the six shipped
 species are supported; any other species tuple raises, as the CUDA path
 cannot compile arbitrary Python right-hand sides.
 """
@@ -95,8 +99,13 @@ class B200PerturbationEvolver:
         self.bg_max_steps = dict(max_steps_tau=packing.BG_MAX_STEPS_TAU, max_steps_kappa=packing.BG_MAX_STEPS_KAPPA)
 
     def full_evolution(self, args, n_save: int = 500) -> PerturbationTable:
-        """args = (BG, params): BG a BackgroundTables; params unused beyond BG.params."""
-        BG, _params = args
+        """args = (BG, params): BG a BackgroundTables, or the reference's
+        Background (converted by background_tables.from_reference with the
+        derived params dict)."""
+        from . import background_tables as bt
+        BG, params = args
+        if not isinstance(BG, bt.BackgroundTables):
+            BG = bt.from_reference(BG, params, self.has_ncdm)
         batch = packing.pack([BG], [self.layout], [self.k_axis_perturbations], n_save=n_save)
         st = packing.pert_settings(self.specs, n_save, batch)
         db = engine.DeviceBatch.upload(batch, self.device)
@@ -104,6 +113,8 @@ class B200PerturbationEvolver:
             # x_e / T_m only: conformal time, optical depth and the
             # line-of-sight arrays come from abcmb_bg_forward
             db.bg_forward(packing.bg_settings(n_save, **self.bg_max_steps), fetch_tables=True)
+        elif getattr(BG, "needs_los", False):
+            complete_los(db, 0, BG, n_save, self.bg_max_steps)
         db.pert_forward(st)
         ks = db.check_status()
         fields = batch.pt_view(db.pt.cpu().numpy(), 0)
@@ -111,4 +122,25 @@ class B200PerturbationEvolver:
         return table_from_fields(fields, self.k_axis_perturbations, lna, self.species, dbatch=db, kstat=ks)
 
 
-__all__ = ["B200PerturbationEvolver", "PerturbationTable", "table_from_fields", "_lib"]
+def complete_los(db, ci: int, BG, n_save: int, bg_max_steps: dict):
+    """The line-of-sight arrays of a background that brings its own
+    conformal-time table (background_tables.from_reference): abcmb_bg_forward
+    runs the optical-depth solve and writes the six arrays; the caller's
+    conformal-time table, tau0 and lna_transfer_start are then put back, so
+    the perturbations see exactly the reference's background."""
+    import torch
+    keep = (BG.tau_tab.copy(), BG.tau0, BG.lna_transfer_start, BG.lna_rec)
+    b = db.batch
+    c = b.cosmo[ci]
+    db.bg_forward(packing.bg_settings(n_save, **bg_max_steps), fetch_tables=True)
+    los = BG.los
+    BG.tau_tab, BG.tau0, BG.lna_transfer_start, BG.lna_rec = keep
+    BG.los = los
+    o = int(c["off_tau"])
+    db.tables[o:o + packing.NTAU_TAB].copy_(torch.from_numpy(BG.tau_tab))
+    b.cosmo["tau0"][ci] = BG.tau0
+    b.cosmo["lna_transfer_start"][ci] = BG.lna_transfer_start
+    db.cosmo.copy_(torch.from_numpy(b.cosmo.view(np.uint8)).to(db.cosmo.device))
+
+
+__all__ = ["B200PerturbationEvolver", "PerturbationTable", "table_from_fields", "complete_los", "_lib"]

@@ -428,3 +428,33 @@ def test_model_output_matches_oracle(gpu):
     assert np.max(np.abs(out.ClTT - cl_o[0, 0]) / cl_o[0, 0]) < 1e-5
     pk_o = oracle.pk_lin(batch, pt, m.specs["k_pivot"], out.k, np.array([0.0]))[0, 0]
     np.testing.assert_allclose(out.Pk, pk_o, rtol=1e-5)
+
+
+def test_reference_background_object_gives_the_same_table(gpu):
+    """full_evolution((BG, params)) with an object carrying the reference
+    Background's fields (array_with_padding HyRex tables, its own
+    conformal-time table) gives the PerturbationTable of the equivalent
+    BackgroundTables bit for bit; its line-of-sight arrays come from
+    abcmb_bg_forward and agree with the host model's within the optical-depth
+    solve's spread."""
+    from abcmb_b200 import background_tables as bt, cosmology
+    from abcmb_b200.perturbations import B200PerturbationEvolver
+    from test_host import reference_background_stand_in
+    from abcmb_b200 import configs
+    w = configs.c1(nk=30, l_max=400)
+    p = cosmology.add_derived_parameters(w.params_in[0], False, w.specs)
+    bg = bt.make_background(p, False, "hyrex")
+    PE = B200PerturbationEvolver(k_axis_perturbations=w.kgrids[0], specs=w.specs)
+    pt_ref = PE.full_evolution((bg, p))
+    pt_obj = PE.full_evolution((reference_background_stand_in(bg), p))
+    np.testing.assert_array_equal(pt_obj.lna, pt_ref.lna)
+    for f in ("delta_m", "theta_b_prime", "metric_eta", "metric_h_prime", "metric_alpha_prime"):
+        np.testing.assert_array_equal(getattr(pt_obj, f), getattr(pt_ref, f))
+    np.testing.assert_array_equal(pt_obj.species_perturbations["Photon"]["G2"],
+                                  pt_ref.species_perturbations["Photon"]["G2"])
+    db = pt_obj.device_batch
+    c = db.batch.cosmo[0]
+    los = db.tables[int(c["off_los"]):int(c["off_los"]) + 6 * 499].cpu().numpy().reshape(6, 499)
+    host = bg.los_arrays(500)
+    for i, tol in ((0, 1e-10), (1, 1e-5), (3, 1e-12), (4, 1e-5)):       # tau, g, aH, exp(-kappa)
+        assert np.max(np.abs(los[i] - host[i])) <= tol * np.abs(host[i]).max(), i

@@ -271,3 +271,57 @@ def test_tangent_expansion_layout():
     gf = gradients.expand(w, processes=1, mode="fd")
     assert gf.batch.n_items == 9 * b.n_items and gf.dirs is None
     np.testing.assert_array_equal(gf.batch.cosmo, b.cosmo)
+
+
+class _Padded:
+    """Stand-in for abcmb.hyrex.array_with_padding: arr (finite, as
+    Background leaves it), lastnum, lastval."""
+
+    def __init__(self, arr_inf):
+        bad = ~np.isfinite(arr_inf)
+        self.lastnum = int(np.argmax(bad)) - 1
+        self.lastval = float(arr_inf[self.lastnum])
+        self.arr = np.where(np.isinf(arr_inf), self.lastval, arr_inf)
+
+
+def reference_background_stand_in(bg):
+    """An object with the reference Background's field names
+    (abcmb/background.py:420-564) built from a BackgroundTables: the HyRex
+    tables back in their +inf-padded array_with_padding form."""
+    from types import SimpleNamespace
+    n_xe_valid = int(round((bg.lna_xe_last - bg.lna_xe0) / bg.lna_xe_dx)) + 1
+    n_tm_valid = int(round((bg.lna_tm_last - bg.lna_tm0) / bg.lna_tm_dx)) + 1
+
+    def pad(a, nvalid):
+        out = np.array(a, dtype=np.float64)
+        out[nvalid:] = np.inf
+        return out
+    lxe = bg.lna_xe0 + bg.lna_xe_dx * np.arange(bg.xe_arr.size)
+    ltm = bg.lna_tm0 + bg.lna_tm_dx * np.arange(bg.tm_arr.size)
+    return SimpleNamespace(tau_tab=bg.tau_tab.copy(), tau0=bg.tau0, lna_transfer_start=bg.lna_transfer_start,
+                           lna_rec=bg.lna_rec, z_reion=bg.z_reion,
+                           xe_tab=_Padded(pad(bg.xe_arr, n_xe_valid)), lna_xe_tab=_Padded(pad(lxe, n_xe_valid)),
+                           Tm_tab=_Padded(pad(bg.tm_arr, n_tm_valid)), lna_Tm_tab=_Padded(pad(ltm, n_tm_valid)),
+                           species_list=())
+
+
+def test_from_reference_packs_like_background_tables():
+    """background_tables.from_reference reads the reference's Background
+    fields (array_with_padding tables in HyRex's padded layout) into the
+    same descriptor and tables the BackgroundTables of the same history
+    give; only the line-of-sight arrays are left to abcmb_bg_forward."""
+    from abcmb_b200 import background_tables as bt, configs, cosmology, packing, specs as sp
+    w = configs.c4(n_cosmo=1, nk_range=(20, 20))
+    p = cosmology.add_derived_parameters(w.params_in[0], w.has_ncdm[0], w.specs)
+    bg = bt.make_background(p, w.has_ncdm[0], "hyrex")
+    ref = bt.from_reference(reference_background_stand_in(bg), p)
+    assert ref.has_ncdm == w.has_ncdm[0] and ref.needs_los and not ref.on_device and not bg.needs_los
+    lay = sp.state_layout(w.specs, w.has_ncdm[0])
+    a = packing.pack([bg], [lay], w.kgrids)
+    b = packing.pack([ref], [lay], w.kgrids)
+    for f in packing.COSMO_DTYPE.names:
+        assert a.cosmo[f][0] == b.cosmo[f][0], f
+    o = int(a.cosmo["off_los"][0])
+    np.testing.assert_array_equal(a.tables[:o], b.tables[:o])
+    assert not b.tables[o:o + 6 * 499].any()
+    assert int(b.cosmo["n_xe"][0]) == bt.HYREX_XE_LEN
