@@ -574,8 +574,9 @@ __device__ __forceinline__ double core_dot(const double* __restrict__ a, const d
   return (s0 + s1) + (s2 + s3);
 }
 
-// Solve M x = r in place (r holds the right-hand side on entry).
-__device__ void solve_newton(const Layout& L, WarpMem& m, double* r, int lane) {
+// Solve M x = r in place (r holds the right-hand side on entry); vcb is the
+// warp buffer of the gathered core vector (ncm doubles).
+__device__ void solve_newton(const Layout& L, WarpMem& m, double* r, int lane, double* vcb) {
   const int nc = L.nc;
   // upward sweeps of the tails (l = L-1 .. 3); the l = 2 right-hand side
   // picks up the tail.  Two elements per trip so the loads run ahead.
@@ -599,18 +600,18 @@ __device__ void solve_newton(const Layout& L, WarpMem& m, double* r, int lane) {
       r[e] = nxt;
     }
     const int cc = chain_core_l2(chn);
-    m.vc()[m.iperm()[cc]] = r[m.cmap()[cc]] - m.m3()[chn] * nxt;
+    vcb[m.iperm()[cc]] = r[m.cmap()[cc]] - m.m3()[chn] * nxt;
   }
   // every other core row gathers its right-hand side directly
   // (vc is stored permuted: the entry for core row j goes to slot iperm[j])
-  if (lane < nc && !(lane >= 4 && (lane - 4) % 3 == 2)) m.vc()[m.iperm()[lane]] = r[m.cmap()[lane]];
+  if (lane < nc && !(lane >= 4 && (lane - 4) % 3 == 2)) vcb[m.iperm()[lane]] = r[m.cmap()[lane]];
   __syncwarp();
   double xc = 0.;
   if (lane < nc) {
     // x_i = sum_k Mc[q_i][k] b[q_k] (pivot rows left in place, see
     // factor_newton); vc already holds b[q_k] in slot k
     const double* row = m.Mc() + m.perm()[lane] * m.cs;
-    const double* vc = m.vc();
+    const double* vc = vcb;
     xc = nc == 13 ? core_dot<13>(row, vc) : core_dot<MAXC>(row, vc);
   }
   __syncwarp();
@@ -801,398 +802,138 @@ __device__ __noinline__ void write_ic(const abcmb_cosmo& c, const Layout& L, con
 // Forward-mode sensitivities (abcmb_pert_forward_tangent)
 // ---------------------------------------------------------------------------
 // The tangent u_q of the discrete Kvaerno5 step along parameter direction q
-// (at most ND_MAX of them, all carried by the warp that integrates the base
-// item): after a step is accepted, each implicit stage i's tangent
+// is integrated by the warp that integrates the base item, one direction
+// after another once a step is accepted.  Each implicit stage i's tangent
 // derivative solves (I - h gamma A_i) dF_i = A_i z + dA_i Y_i with
 // z = u0 + h sum_{j<i} a_ij dF_j and Y_i the converged primal stage value,
 // by chord iterations with the step's own factorisation (the primal's
-// iteration matrix, so the same very-chord test applies).  dA_i is A with
-// the basis replaced by its change along q (A is linear in the basis), the
-// half difference of the plus and minus descriptors' bases at t_i.  All
-// directions run through the same sweeps together: the tail sweeps take one
-// lane per (chain, direction), the core mat-vec one lane per row with one
-// accumulator per direction, so the extra work fills lanes the single
-// primal solve leaves idle.
+// iteration matrix); dA_i is A with the basis replaced by its change along
+// q (A is linear in the basis): half the difference of the plus and minus
+// descriptors' bases at t_i.  The stage-1 derivative is re-evaluated as
+// A(t0) u0 + dA(t0) y0 at every step.  Only u0 and the basis change at t0
+// persist per direction; the seven stage derivatives and the work vectors
+// are reused by the next direction, which keeps the shared memory per warp
+// (and so the resident warps per SM) close to the forward kernel's.
+//
+// The tangent iteration is linear with the primal's iteration matrix
+// I - M_lin^-1 M_i: its spectral radius is small whenever the primal stage
+// converged, but it is far from normal in the tight-coupling era, so an
+// error with a stiff component (the initial tangent's start-time term puts
+// one there) can grow ~25x over the first iteration before it contracts.  A
+// growing step therefore does not stop the tangent iterations (only a
+// non-finite one does); they get TANGENT_ROOT_MAX iterations and the last
+// iterate is kept (the tangents never change the primal's step sequence).
 constexpr int ND_MAX = ABCMB_MAX_TANGENTS;
 constexpr int TANGENT_ROOT_MAX = 16;
 
-// Per-warp tangent scratch, after the primal's WarpMem.  Per direction q:
-// u0 (tangent at t0), dF (7 stage derivatives, stride ny), q (the constant
-// part of a stage's residual; u1 once the stages are done), r (residual,
-// solve vector and temporaries).  Shared: yd (dy/dt of the dense output),
-// yv (a variant's state at a save point), the basis changes at the five
-// stage times, the variants' backgrounds at their save times, the gathered
-// core vectors of the solve, and the variants' descriptor indices.
+// Per-warp tangent scratch, after the primal's WarpMem: per direction u0
+// and the basis change at t0; shared by the directions: the seven stage
+// derivatives dF, q (the constant part of a stage's residual; u1 once the
+// stages are done), r (residual and solve vector; a variant's state at a
+// save point), yd (dy/dt of the dense output), yv (a variant's state), the
+// basis changes at the five stage times, the variants' backgrounds at a save
+// point, the solve's gathered core vector and the variants' descriptor
+// indices.
 struct TanMem {
   double* p;
   int my, nd, ncm;
   __device__ __forceinline__ double* u0(int q) const { return p + q * my; }
-  __device__ __forceinline__ double* dF(int q) const { return p + nd * my + q * 7 * my; }
-  __device__ __forceinline__ double* qv(int q) const { return p + 8 * nd * my + q * my; }
-  __device__ __forceinline__ double* rv(int q) const { return p + 9 * nd * my + q * my; }
-  __device__ __forceinline__ double* yd() const { return p + 10 * nd * my; }
+  __device__ __forceinline__ double* bdt0(int q) const { return p + nd * my + q * NB; }
+  __device__ __forceinline__ double* dF() const { return p + nd * (my + NB); }
+  __device__ __forceinline__ double* qv() const { return dF() + 7 * my; }
+  __device__ __forceinline__ double* rv() const { return qv() + my; }
+  __device__ __forceinline__ double* yd() const { return rv() + my; }
   __device__ __forceinline__ double* yv() const { return yd() + my; }
-  __device__ __forceinline__ double* bd(int slot, int q) const { return yv() + my + ((slot - 1) * nd + q) * NB; }
-  __device__ __forceinline__ double* sv(int j) const { return yv() + my + 5 * nd * NB + j * NSV; }
-  __device__ __forceinline__ double* vc(int q) const { return sv(2 * nd) + q * ncm; }
-  __device__ __forceinline__ int* vix() const { return reinterpret_cast<int*>(vc(nd)); }   // 2 nd ints
+  __device__ __forceinline__ double* bd(int slot) const { return yv() + my + (slot - 1) * NB; }
+  __device__ __forceinline__ double* sv(int j) const { return yv() + my + 5 * NB + j * NSV; }
+  __device__ __forceinline__ double* vc() const { return sv(2); }
+  __device__ __forceinline__ int* vix() const { return reinterpret_cast<int*>(vc() + ncm); }   // 2 ND_MAX ints
+  // the item's tangent chord iterations and unconverged stage solves
+  __device__ __forceinline__ int* cnt() const { return vix() + 2 * ND_MAX; }
 };
 
 __host__ __device__ inline size_t tan_mem_doubles(int max_ny, int ncm, int nd) {
   if (nd <= 0) return 0;
-  return (size_t)nd * (10 * (size_t)max_ny + 5 * NB + 2 * NSV + (size_t)ncm) + 2 * (size_t)max_ny + ND_MAX;
+  return (size_t)nd * ((size_t)max_ny + NB) + 11 * (size_t)max_ny + 5 * NB + 2 * NSV + (size_t)ncm + ND_MAX + 1;
 }
 
-// Q_q = A(B) z_q + A(dB_q) Y for every direction (z_q read from rv(q)): the
-// part of a stage's tangent residual the chord iterations keep.
-__device__ __noinline__ void tan_const(const Layout& L, const WarpMem& m, const TanMem& t, const RowTab& R,
-                                       const CoreRow& cr, const double* __restrict__ B, int slot,
-                                       const double* __restrict__ Y, bool ncdm, int lane) {
-  const int nd = t.nd;
-  double hp[ND_MAX], ep[ND_MAX], hpd[ND_MAX], epd[ND_MAX];
-#pragma unroll
-  for (int q = 0; q < ND_MAX; ++q) {
-    hp[q] = ep[q] = hpd[q] = epd[q] = 0.;
-    if (q < nd) {
-      metric(L, B, t.rv(q), ncdm, hp[q], ep[q]);
-      metric(L, t.bd(slot, q), Y, ncdm, hpd[q], epd[q]);
-    }
-  }
+// out = A(B) z + A(Bd) Y for one direction: the part of a stage's tangent
+// residual the chord iterations keep (Bd the basis change).
+__device__ __forceinline__ void tan_const(const Layout& L, const WarpMem& m, const RowTab& R, const CoreRow& cr,
+                                          const double* __restrict__ B, const double* __restrict__ Bd,
+                                          const double* __restrict__ z, const double* __restrict__ Y,
+                                          double* __restrict__ out, bool ncdm, int lane) {
+  double hp, ep, hpd, epd;
+  metric(L, B, z, ncdm, hp, ep);
+  metric(L, Bd, Y, ncdm, hpd, epd);
   if (lane < L.nc) {
     const int r = lane;
     const int nt = R.n[r];
     const int tch = R.tch[r];
+    double acc = cr.uh * hp + cr.ue * ep;
+    double accd = cr.uh * hpd + cr.ue * epd;
 #pragma unroll
-    for (int q = 0; q < ND_MAX; ++q) {
-      if (q < nd) {
-        const double* __restrict__ z = t.rv(q);
-        const double* __restrict__ Bd = t.bd(slot, q);
-        double acc = cr.uh * hp[q] + cr.ue * ep[q];
-        double accd = cr.uh * hpd[q] + cr.ue * epd[q];
-#pragma unroll
-        for (int u = 0; u < 5; ++u) {
-          acc = fma(cr.c[u], z[cr.s[u]], acc);
-          const double cd = u < nt ? R.cst[r * 5 + u] * Bd[R.bid[r * 5 + u]] : 0.;
-          accd = fma(cd, Y[cr.s[u]], accd);
-        }
-        acc = fma(cr.tc, z[cr.ts], acc);
-        const double tcd = tch >= 0 ? R.tco[r] * Bd[chain_speed_bid(tch)] : 0.;
-        accd = fma(tcd, Y[cr.ts], accd);
-        t.qv(q)[cr.out] = acc + accd;
-      }
+    for (int u = 0; u < 5; ++u) {
+      acc = fma(cr.c[u], z[cr.s[u]], acc);
+      const double cd = u < nt ? R.cst[r * 5 + u] * Bd[R.bid[r * 5 + u]] : 0.;
+      accd = fma(cd, Y[cr.s[u]], accd);
     }
+    acc = fma(cr.tc, z[cr.ts], acc);
+    const double tcd = tch >= 0 ? R.tco[r] * Bd[chain_speed_bid(tch)] : 0.;
+    accd = fma(tcd, Y[cr.ts], accd);
+    out[cr.out] = acc + accd;
   }
-  const double trunc = B[B_TRUNC];
+  const double trunc = B[B_TRUNC], trd = Bd[B_TRUNC];
   for (int u = lane; u < L.ntail; u += WARP) {
     const int info = m.tinfo()[u];
     const int e = info & 0xFFF, chn = (info >> 12) & 7;
-    const bool last = (info >> 15) & 1;
-    const int li = info >> 16;
     const int sb = chain_speed_bid(chn);
-    const double sp = B[sb];
-    const double d = chn < 2 ? B[B_KAP] : 0.;
-    const double lc1 = (double)(m.chL()[chn] + 1);
-    const double ta = R.ta[li], tg = R.tg[li];
-#pragma unroll
-    for (int q = 0; q < ND_MAX; ++q) {
-      if (q < nd) {
-        const double* __restrict__ z = t.rv(q);
-        const double* __restrict__ Bd = t.bd(slot, q);
-        const double sd = Bd[sb], dd = chn < 2 ? Bd[B_KAP] : 0., trd = Bd[B_TRUNC];
-        double fv, fvd;
-        if (last) {
-          fv = sp * z[e - 1] - (d + lc1 * trunc) * z[e];
-          fvd = sd * Y[e - 1] - (dd + lc1 * trd) * Y[e];
-        } else {
-          fv = sp * (ta * z[e - 1] - tg * z[e + 1]) - d * z[e];
-          fvd = sd * (ta * Y[e - 1] - tg * Y[e + 1]) - dd * Y[e];
-        }
-        t.qv(q)[e] = fv + fvd;
-      }
+    const double sp = B[sb], sd = Bd[sb];
+    const double d = chn < 2 ? B[B_KAP] : 0., dd = chn < 2 ? Bd[B_KAP] : 0.;
+    double fv, fvd;
+    if ((info >> 15) & 1) {
+      const double lc1 = (double)(m.chL()[chn] + 1);
+      fv = sp * z[e - 1] - (d + lc1 * trunc) * z[e];
+      fvd = sd * Y[e - 1] - (dd + lc1 * trd) * Y[e];
+    } else {
+      const int li = info >> 16;
+      const double ta = R.ta[li], tg = R.tg[li];
+      fv = sp * (ta * z[e - 1] - tg * z[e + 1]) - d * z[e];
+      fvd = sd * (ta * Y[e - 1] - tg * Y[e + 1]) - dd * Y[e];
     }
+    out[e] = fv + fvd;
   }
   __syncwarp();
 }
 
-// r_q = h gamma A(B) F_q + Q_q - F_q for the directions in mask, F_q the
-// stage's tangent derivative (dF(q) + stage ny).
-__device__ __noinline__ void tan_resid(const Layout& L, const WarpMem& m, const TanMem& t, const RowTab& R,
-                                       const CoreRow& cr, const double* __restrict__ B, int stage, double hg,
-                                       unsigned mask, bool ncdm, int lane) {
-  const int n = L.ny;
-  double hp[ND_MAX], ep[ND_MAX];
-#pragma unroll
-  for (int q = 0; q < ND_MAX; ++q) {
-    hp[q] = ep[q] = 0.;
-    if ((mask >> q) & 1u) metric(L, B, t.dF(q) + stage * n, ncdm, hp[q], ep[q]);
-  }
+// r = h gamma A(B) F + q - F: the residual of a stage's tangent derivative F.
+__device__ __forceinline__ void tan_resid(const Layout& L, const WarpMem& m, const RowTab& R, const CoreRow& cr,
+                                          const double* __restrict__ B, const double* __restrict__ F,
+                                          const double* __restrict__ q, double* __restrict__ r, double hg,
+                                          bool ncdm, int lane) {
+  double hp, ep;
+  metric(L, B, F, ncdm, hp, ep);
   if (lane < L.nc) {
+    double acc = cr.uh * hp + cr.ue * ep;
+#pragma unroll
+    for (int u = 0; u < 5; ++u) acc = fma(cr.c[u], F[cr.s[u]], acc);
+    acc = fma(cr.tc, F[cr.ts], acc);
     const int o = cr.out;
-#pragma unroll
-    for (int q = 0; q < ND_MAX; ++q) {
-      if ((mask >> q) & 1u) {
-        const double* __restrict__ F = t.dF(q) + stage * n;
-        double acc = cr.uh * hp[q] + cr.ue * ep[q];
-#pragma unroll
-        for (int u = 0; u < 5; ++u) acc = fma(cr.c[u], F[cr.s[u]], acc);
-        acc = fma(cr.tc, F[cr.ts], acc);
-        t.rv(q)[o] = fma(hg, acc, t.qv(q)[o]) - F[o];
-      }
-    }
+    r[o] = fma(hg, acc, q[o]) - F[o];
   }
   const double trunc = B[B_TRUNC];
   for (int u = lane; u < L.ntail; u += WARP) {
     const int info = m.tinfo()[u];
     const int e = info & 0xFFF, chn = (info >> 12) & 7;
-    const bool last = (info >> 15) & 1;
-    const int li = info >> 16;
     const double sp = B[chain_speed_bid(chn)];
     const double d = chn < 2 ? B[B_KAP] : 0.;
-    const double dl = last ? d + (double)(m.chL()[chn] + 1) * trunc : d;
-    const double ta = last ? 1. : R.ta[li], tg = last ? 0. : R.tg[li];
-#pragma unroll
-    for (int q = 0; q < ND_MAX; ++q) {
-      if ((mask >> q) & 1u) {
-        const double* __restrict__ F = t.dF(q) + stage * n;
-        const double fn = last ? 0. : F[e + 1];
-        const double fv = sp * (ta * F[e - 1] - tg * fn) - dl * F[e];
-        t.rv(q)[e] = fma(hg, fv, t.qv(q)[e]) - F[e];
-      }
+    double fv;
+    if ((info >> 15) & 1) fv = sp * F[e - 1] - (d + (double)(m.chL()[chn] + 1) * trunc) * F[e];
+    else {
+      const int li = info >> 16;
+      fv = sp * (R.ta[li] * F[e - 1] - R.tg[li] * F[e + 1]) - d * F[e];
     }
-  }
-  __syncwarp();
-}
-
-// sum_j a[j] v_q[j] for every direction in mask, the row loaded once
-template <int N>
-__device__ __forceinline__ void core_dot_multi(const double* __restrict__ a, const TanMem& t, unsigned mask,
-                                               double* out) {
-  double s0[ND_MAX], s1[ND_MAX];
-#pragma unroll
-  for (int q = 0; q < ND_MAX; ++q) s0[q] = s1[q] = 0.;
-#pragma unroll
-  for (int j = 0; j < N; ++j) {
-    const double aj = a[j];
-#pragma unroll
-    for (int q = 0; q < ND_MAX; ++q) {
-      if ((mask >> q) & 1u) {
-        if (j & 1) s1[q] = fma(aj, t.vc(q)[j], s1[q]);
-        else s0[q] = fma(aj, t.vc(q)[j], s0[q]);
-      }
-    }
-  }
-#pragma unroll
-  for (int q = 0; q < ND_MAX; ++q) out[q] = s0[q] + s1[q];
-}
-
-// Solve M x = r_q in place (rv(q)) for the directions in mask with the
-// step's factorisation: solve_newton for several right-hand sides.
-__device__ __noinline__ void solve_multi(const Layout& L, const WarpMem& m, const TanMem& t, unsigned mask,
-                                         int lane) {
-  const int nc = L.nc;
-  const int chn = lane % NCHAIN, qd = lane / NCHAIN;
-  const bool mine = qd < ND_MAX && chn < L.nchain && ((mask >> qd) & 1u);
-  if (mine) {
-    double* r = t.rv(qd);
-    const double* mult = m.mult();
-    const int e3 = m.chs()[chn];
-    int e = e3 + (m.chL()[chn] - 3);
-    double nxt = r[e];
-    --e;
-    for (; e - 1 >= e3; e -= 2) {
-      const double ra = r[e], ma = mult[e], rb = r[e - 1], mb = mult[e - 1];
-      const double va = ra - ma * nxt;
-      const double vb = rb - mb * va;
-      r[e] = va;
-      r[e - 1] = vb;
-      nxt = vb;
-    }
-    if (e >= e3) {
-      nxt = r[e] - mult[e] * nxt;
-      r[e] = nxt;
-    }
-    const int cc = chain_core_l2(chn);
-    t.vc(qd)[m.iperm()[cc]] = r[m.cmap()[cc]] - m.m3()[chn] * nxt;
-  }
-  if (lane < nc && !(lane >= 4 && (lane - 4) % 3 == 2)) {
-    const int slot = m.iperm()[lane], src = m.cmap()[lane];
-#pragma unroll
-    for (int q = 0; q < ND_MAX; ++q)
-      if ((mask >> q) & 1u) t.vc(q)[slot] = t.rv(q)[src];
-  }
-  __syncwarp();
-  double xc[ND_MAX];
-  if (lane < nc) {
-    const double* row = m.Mc() + m.perm()[lane] * m.cs;
-    if (nc == 13) core_dot_multi<13>(row, t, mask, xc);
-    else core_dot_multi<MAXC>(row, t, mask, xc);
-  }
-  __syncwarp();
-  if (lane < nc) {
-    const int dst = m.cmap()[lane];
-#pragma unroll
-    for (int q = 0; q < ND_MAX; ++q)
-      if ((mask >> q) & 1u) t.rv(q)[dst] = xc[q];
-  }
-  __syncwarp();
-  if (mine) {
-    double* r = t.rv(qd);
-    const double* sub = m.sub();
-    const double* invd = m.invd();
-    const int e3 = m.chs()[chn];
-    const int eL = e3 + (m.chL()[chn] - 3);
-    double prev = r[e3 - 1];
-    int e = e3;
-    for (; e + 1 <= eL; e += 2) {
-      const double ra = r[e], sa = sub[e], ia = invd[e], rb = r[e + 1], sb = sub[e + 1], ib = invd[e + 1];
-      const double xa = (ra - sa * prev) * ia;
-      const double xb = (rb - sb * xa) * ib;
-      r[e] = xa;
-      r[e + 1] = xb;
-      prev = xb;
-    }
-    if (e <= eL) r[e] = (r[e] - sub[e] * prev) * invd[e];
-  }
-  __syncwarp();
-}
-
-// The tangents of one accepted step: stages 1..6 (the basis changes of the
-// step's stage times in bd, the factorisation, F, y0 and the basis slots
-// are the step's), then u1 into qv(q).  atol is the primal's scaled by the
-// tangents' relative size (PertArgs.tscale).  The tangent iteration is
-// linear with the primal's iteration matrix I - M_lin^-1 M_i: its spectral
-// radius is small whenever the primal stage converged, but it is far from
-// normal in the tight-coupling era, so an error with a stiff component (the
-// initial tangent's start-time term puts one there) can grow ~25x over the
-// first iteration before it contracts.  A growing step therefore does not
-// stop the tangent iterations (only a non-finite one does), and they get
-// TANGENT_ROOT_MAX iterations.  titer counts chord iterations,
-// tunconv stage solves that did not meet the test within root_max
-// iterations (their last iterate is kept: the tangents never change the
-// primal's step sequence).
-__device__ __noinline__ void tangent_step(const Layout& L, const WarpMem& m, const TanMem& t, const RowTab& R,
-                                          double h, double rtol, double atol, double inv_n, bool ncdm, int lane,
-                                          int& titer, int& tunconv) {
-  const int n = L.ny;
-  const int nd = t.nd;
-  const double hg = h * KV_G;
-  const double kappa = 1e-2, small_res = 1e-13;
-  const int root_max = TANGENT_ROOT_MAX;
-  CoreRow cr;
-  for (int i = 1; i < 7; ++i) {
-    const int slot = (i == 6) ? 5 : i;
-    const double* B = m.SB() + slot * NB;
-    core_row_at(L, R, m, B, lane, cr);
-    {
-      // the converged primal stage value Y_i, formed as the primal formed it
-      const double* __restrict__ Fr = m.F();
-      const double* __restrict__ y0 = m.y0();
-      double* __restrict__ vw = m.v();
-      for (int e = lane; e < n; e += WARP) {
-        double acc = 0., acc2 = 0.;
-        int j = 0;
-        for (; j + 1 < i; j += 2) {
-          acc = fma(KV_A[i][j], Fr[j * n + e], acc);
-          acc2 = fma(KV_A[i][j + 1], Fr[(j + 1) * n + e], acc2);
-        }
-        if (j < i) acc = fma(KV_A[i][j], Fr[j * n + e], acc);
-        const double be = y0[e] + h * (acc + acc2);
-        vw[e] = be + hg * Fr[i * n + e];
-      }
-      // z_q into rv(q); the predictor dF_i = dF_{i-1}
-#pragma unroll
-      for (int q = 0; q < ND_MAX; ++q) {
-        if (q < nd) {
-          const double* __restrict__ dF = t.dF(q);
-          double* __restrict__ dFi = t.dF(q) + i * n;
-          const double* __restrict__ u0 = t.u0(q);
-          double* __restrict__ z = t.rv(q);
-          for (int e = lane; e < n; e += WARP) {
-            double acc = 0., acc2 = 0.;
-            int j = 0;
-            for (; j + 1 < i; j += 2) {
-              acc = fma(KV_A[i][j], dF[j * n + e], acc);
-              acc2 = fma(KV_A[i][j + 1], dF[(j + 1) * n + e], acc2);
-            }
-            if (j < i) acc = fma(KV_A[i][j], dF[j * n + e], acc);
-            z[e] = u0[e] + h * (acc + acc2);
-            dFi[e] = dF[(i - 1) * n + e];
-          }
-        }
-      }
-    }
-    __syncwarp();
-    tan_const(L, m, t, R, cr, B, slot, m.v(), ncdm, lane);
-    unsigned active = (1u << nd) - 1u;
-    double dsz[ND_MAX];
-#pragma unroll
-    for (int q = 0; q < ND_MAX; ++q) dsz[q] = INFINITY;
-    for (int it = 1; it <= root_max && active; ++it) {
-      tan_resid(L, m, t, R, cr, B, i, hg, active, ncdm, lane);
-      solve_multi(L, m, t, active, lane);
-      double ss[ND_MAX];
-#pragma unroll
-      for (int q = 0; q < ND_MAX; ++q) {
-        ss[q] = 0.;
-        if ((active >> q) & 1u) {
-          const double* __restrict__ rr = t.rv(q);
-          double* __restrict__ ff = t.dF(q) + i * n;
-          for (int e = lane; e < n; e += WARP) {
-            const double x = rr[e];
-            const double fnew = ff[e] + x;
-            ff[e] = fnew;
-            const double qq = x * pos_rcp(atol + rtol * fabs(fnew));
-            ss[q] += qq * qq;
-          }
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < ND_MAX; ++q)
-        if ((active >> q) & 1u) ss[q] = warp_sum(ss[q]);
-      __syncwarp();
-      unsigned next = active;
-#pragma unroll
-      for (int q = 0; q < ND_MAX; ++q) {
-        if ((active >> q) & 1u) {
-          const double dp = dsz[q];
-          const double d = sqrt(ss[q] * inv_n);
-          dsz[q] = d;
-          ++titer;
-          if (it >= 2) {
-            // the primal's very-chord termination test (division-free form);
-            // no divergence stop but a non-finite size
-            const bool small = d < small_res;
-            const bool converged = d > 0. && d < dp && d * d < kappa * (dp - d);
-            if (small || converged) next &= ~(1u << q);
-            else if (!isfinite(d)) {
-              next &= ~(1u << q);
-              ++tunconv;
-            }
-          }
-        }
-      }
-      active = next;
-    }
-    tunconv += __popc(active);
-  }
-  // u1 = u0 + h (sum_j a_7j dF_j + gamma dF_7) into qv(q)
-#pragma unroll
-  for (int q = 0; q < ND_MAX; ++q) {
-    if (q < nd) {
-      const double* __restrict__ Fr = t.dF(q);
-      const double* __restrict__ u0 = t.u0(q);
-      double* __restrict__ u1 = t.qv(q);
-      for (int e = lane; e < n; e += WARP) {
-        double acc = 0., accb = 0.;
-#pragma unroll
-        for (int j = 0; j < 6; j += 2) {
-          acc = fma(KV_A[6][j], Fr[j * n + e], acc);
-          accb = fma(KV_A[6][j + 1], Fr[(j + 1) * n + e], accb);
-        }
-        acc = fma(KV_G, Fr[6 * n + e], acc + accb);
-        u1[e] = u0[e] + h * acc;
-      }
-    }
+    r[e] = fma(hg, fv, q[e]) - F[e];
   }
   __syncwarp();
 }
@@ -1216,61 +957,211 @@ struct PertArgs {
   int32_t* tstat;          // [n_items][2] or null
 };
 
-// The variants' PerturbationTables at save point isave (after the base's):
-// each variant's fields at its own save time ts_v, from the base's dense
-// state y(ts) (m.v()) moved by +-(u_q(ts) + y'(ts) (ts_plus - ts_minus) / 2),
-// with the variant's own background.  th = (ts - t0) / h of the base's
-// save time in the accepted step.
-__device__ __noinline__ void tangent_save(const Layout& L, const WarpMem& m, const TanMem& t, const PertArgs& P,
-                                          double k, double h, double th, int isave, int nsave, int ik, int lane,
-                                          const double* ncdm_w) {
-  const int n = L.ny, nd = t.nd;
-  if (lane < 2 * nd) {
-    const abcmb_cosmo& cv = P.cosmo[t.vix()[lane]];
-    const double tsv = linspace_at(cv.lna_transfer_start, 0.0, nsave, isave);
-    BG b;
-    bg_eval(cv, bg_constants(cv), P.tables, tsv, b);
-    bg_store(b, t.sv(lane));
-    t.sv(lane)[16] = tsv;
+__device__ __forceinline__ TanMem tan_mem(const WarpMem& m, const PertArgs& P) {
+  TanMem t;
+  t.p = m.p + warp_mem_doubles(P.max_ny, P.ncm);
+  t.my = P.max_ny;
+  t.nd = P.nd;
+  t.ncm = P.ncm;
+  return t;
+}
+
+// Direction q of one accepted step [t0, t0 + h] (the primal's stage
+// derivatives F, y0, y1, factorisation and basis slots are the step's):
+// the basis changes at the five stage times (lanes 0-4), the stage-1
+// derivative, stages 1..6 by chord iterations, u1, then the variants'
+// PerturbationTables at every save point of the step, each at its own save
+// time: the fields of y(ts) +- (u_q(ts) + y'(ts) (ts_plus - ts_minus) / 2)
+// with the variant's own background; finally u0 <- u1.  isave0 is the first
+// save index the step covers (the primal writes its own fields afterwards).
+// atol_t is the primal's atol scaled by the tangents' relative size.
+__device__ __noinline__ void tangent_pass(const Layout& L, WarpMem& m, const RowTab& R, const PertArgs& P, int q,
+                                          double k, double ik2, double t0, double h, double rtol, double atol_t,
+                                          double inv_n, double lts, int isave0, int ik, int lane) {
+  const TanMem t = tan_mem(m, P);
+  int titer = 0, tunconv = 0;
+  const int n = L.ny;
+  const bool ncdm = L.nM > 0;
+  const double hg = h * KV_G;
+  const double kappa = 1e-2, small_res = 1e-13;
+  const abcmb_cosmo& cp = P.cosmo[t.vix()[2 * q]];
+  const abcmb_cosmo& cm = P.cosmo[t.vix()[2 * q + 1]];
+  double* __restrict__ dF = t.dF();
+  if (lane < 5) stage_basis_diff(cp, cm, P.tables, k, ik2, R.ncdm_w, t0 + KV_C[lane + 1] * h, t.bd(lane + 1));
+  CoreRow cr;
+  core_row_at(L, R, m, m.SB(), lane, cr);
+  __syncwarp();
+  // stage-1 derivative dF_0 = A(t0) u0 + dA(t0) y0
+  tan_const(L, m, R, cr, m.SB(), t.bdt0(q), t.u0(q), m.y0(), dF, ncdm, lane);
+  for (int i = 1; i < 7; ++i) {
+    const int slot = (i == 6) ? 5 : i;
+    const double* B = m.SB() + slot * NB;
+    core_row_at(L, R, m, B, lane, cr);
+    {
+      // the converged primal stage value Y_i (into v), formed as the primal
+      // formed it; z (into r); the predictor dF_i = dF_{i-1}
+      const double* __restrict__ Fr = m.F();
+      const double* __restrict__ y0 = m.y0();
+      const double* __restrict__ u0 = t.u0(q);
+      double* __restrict__ vw = m.v();
+      double* __restrict__ z = t.rv();
+      for (int e = lane; e < n; e += WARP) {
+        double acc = 0., acc2 = 0., tc = 0., tc2 = 0.;
+        int j = 0;
+        for (; j + 1 < i; j += 2) {
+          acc = fma(KV_A[i][j], Fr[j * n + e], acc);
+          acc2 = fma(KV_A[i][j + 1], Fr[(j + 1) * n + e], acc2);
+          tc = fma(KV_A[i][j], dF[j * n + e], tc);
+          tc2 = fma(KV_A[i][j + 1], dF[(j + 1) * n + e], tc2);
+        }
+        if (j < i) {
+          acc = fma(KV_A[i][j], Fr[j * n + e], acc);
+          tc = fma(KV_A[i][j], dF[j * n + e], tc);
+        }
+        const double be = y0[e] + h * (acc + acc2);
+        vw[e] = be + hg * Fr[i * n + e];
+        z[e] = u0[e] + h * (tc + tc2);
+        dF[i * n + e] = dF[(i - 1) * n + e];
+      }
+    }
+    __syncwarp();
+    tan_const(L, m, R, cr, B, t.bd(slot), t.rv(), m.v(), t.qv(), ncdm, lane);
+    double* __restrict__ fi = dF + i * n;
+    double dsz = INFINITY;
+    bool conv = false;
+    for (int it = 1; it <= TANGENT_ROOT_MAX; ++it) {
+      tan_resid(L, m, R, cr, B, fi, t.qv(), t.rv(), hg, ncdm, lane);
+      solve_newton(L, m, t.rv(), lane, t.vc());
+      double ss = 0.;
+      {
+        const double* __restrict__ rr = t.rv();
+        for (int e = lane; e < n; e += WARP) {
+          const double x = rr[e];
+          const double fnew = fi[e] + x;
+          fi[e] = fnew;
+          const double qq = x * pos_rcp(atol_t + rtol * fabs(fnew));
+          ss += qq * qq;
+        }
+      }
+      ss = warp_sum(ss);
+      __syncwarp();
+      const double dp = dsz;
+      const double d = sqrt(ss * inv_n);
+      dsz = d;
+      ++titer;
+      if (it >= 2) {
+        // the primal's very-chord termination test (division-free form); no
+        // divergence stop but a non-finite size
+        const bool small = d < small_res;
+        const bool converged = d > 0. && d < dp && d * d < kappa * (dp - d);
+        if (small || converged) {
+          conv = true;
+          break;
+        }
+        if (!isfinite(d)) break;
+      }
+    }
+    if (!conv) ++tunconv;
   }
   {
-    // dy/dt of the base's dense output at ts
-    const double* __restrict__ y0 = m.y0();
-    const double* __restrict__ y1 = m.y1();
-    const double* __restrict__ Fr = m.F();
-    double* __restrict__ yd = t.yd();
+    // u1 = u0 + h (sum_j a_7j dF_j + gamma dF_7) into q
+    const double* __restrict__ u0 = t.u0(q);
+    double* __restrict__ u1 = t.qv();
     for (int e = lane; e < n; e += WARP) {
-      const double y0e = y0[e], y1e = y1[e];
-      const double k0 = h * Fr[e], k1 = h * Fr[6 * n + e];
-      const double a2 = 3. * (y1e - y0e) - 2. * k0 - k1, a3 = 2. * (y0e - y1e) + k0 + k1;
-      yd[e] = (k0 + th * (2. * a2 + 3. * th * a3)) / h;
+      double acc = 0., accb = 0.;
+#pragma unroll
+      for (int j = 0; j < 6; j += 2) {
+        acc = fma(KV_A[6][j], dF[j * n + e], acc);
+        accb = fma(KV_A[6][j + 1], dF[(j + 1) * n + e], accb);
+      }
+      acc = fma(KV_G, dF[6 * n + e], acc + accb);
+      u1[e] = u0[e] + h * acc;
     }
   }
+  __syncwarp();
+  // the variants' tables at the save points of this step
+  const int nsave = P.s.n_save;
+  const double t1 = t0 + h;
+  for (int is = isave0; is < nsave; ++is) {
+    const double ts = linspace_at(lts, 0.0, nsave, is);
+    if (!(ts <= t1)) break;
+    const double th = (ts - t0) / h;
+    const double tsp = linspace_at(cp.lna_transfer_start, 0.0, nsave, is);
+    const double tsm = linspace_at(cm.lna_transfer_start, 0.0, nsave, is);
+    const double dts = 0.5 * (tsp - tsm);
+    if (lane < 2) {
+      const abcmb_cosmo& cv = lane ? cm : cp;
+      BG b;
+      bg_eval(cv, bg_constants(cv), P.tables, lane ? tsm : tsp, b);
+      bg_store(b, t.sv(lane));
+    }
+    {
+      const double* __restrict__ y0 = m.y0();
+      const double* __restrict__ y1 = m.y1();
+      const double* __restrict__ Fr = m.F();
+      const double* __restrict__ u0 = t.u0(q);
+      const double* __restrict__ u1 = t.qv();
+      double* __restrict__ yp = t.yv();
+      double* __restrict__ ym = t.rv();
+      for (int e = lane; e < n; e += WARP) {
+        const double y0e = y0[e], y1e = y1[e];
+        const double k0 = h * Fr[e], k1 = h * Fr[6 * n + e];
+        const double a2 = 3. * (y1e - y0e) - 2. * k0 - k1, a3 = 2. * (y0e - y1e) + k0 + k1;
+        const double ys = y0e + th * (k0 + th * (a2 + th * a3));
+        const double yd = (k0 + th * (2. * a2 + 3. * th * a3)) / h;
+        const double u0e = u0[e], u1e = u1[e];
+        const double g0 = h * dF[e], g1 = h * dF[6 * n + e];
+        const double us = u0e + th * (g0 + th * ((3. * (u1e - u0e) - 2. * g0 - g1) + th * (2. * (u0e - u1e) + g0 + g1)));
+        const double ut = us + yd * dts;
+        yp[e] = ys + ut;
+        ym[e] = ys - ut;
+      }
+    }
+    __syncwarp();
+    write_fields(cp, L, P.tables, k, tsp, t.yv(), P.pt, nsave, is, ik, lane, t.sv(0), R.ncdm_w);
+    write_fields(cm, L, P.tables, k, tsm, t.rv(), P.pt, nsave, is, ik, lane, t.sv(1), R.ncdm_w);
+    __syncwarp();
+  }
+  {
+    const double* __restrict__ u1 = t.qv();
+    double* __restrict__ u0 = t.u0(q);
+    for (int e = lane; e < n; e += WARP) u0[e] = u1[e];
+    double* __restrict__ b0 = t.bdt0(q);
+    if (lane < NB) b0[lane] = t.bd(5)[lane];          // the basis change at the next t0
+    if (lane == 0) {
+      t.cnt()[0] += titer;
+      t.cnt()[1] += tunconv;
+    }
+  }
+  __syncwarp();
+}
+
+// The tangents at an item's start: u = dy0/deps - f(t0, y0) dt0/deps from
+// the variants' initial conditions at their own start times (plus into q,
+// minus into r), the basis change at t0, the counters cleared.
+__device__ __noinline__ void tangent_init(const Layout& L, const WarpMem& m, const RowTab& R, const PertArgs& P,
+                                          int ci, double k, double ik2, double lna_start, int lane) {
+  const TanMem tm = tan_mem(m, P);
+  const int n = L.ny, nd = tm.nd;
+  if (lane < 2 * nd) tm.vix()[lane] = P.dirs[(ci * ND_MAX + (lane >> 1)) * 2 + (lane & 1)];
+  if (lane < 2) tm.cnt()[lane] = 0;
   __syncwarp();
   for (int q = 0; q < nd; ++q) {
-    const double dts = 0.5 * (t.sv(2 * q)[16] - t.sv(2 * q + 1)[16]);
-    const double* __restrict__ dF = t.dF(q);
-    const double* __restrict__ u0 = t.u0(q);
-    const double* __restrict__ u1 = t.qv(q);
-    const double* __restrict__ yd = t.yd();
-    double* __restrict__ ut = t.rv(q);
-    for (int e = lane; e < n; e += WARP) {
-      const double u0e = u0[e], u1e = u1[e];
-      const double k0 = h * dF[e], k1 = h * dF[6 * n + e];
-      const double us = u0e + th * (k0 + th * ((3. * (u1e - u0e) - 2. * k0 - k1) + th * (2. * (u0e - u1e) + k0 + k1)));
-      ut[e] = us + yd[e] * dts;
-    }
-  }
-  __syncwarp();
-  for (int j = 0; j < 2 * nd; ++j) {
-    const double* __restrict__ ys = m.v();
-    const double* __restrict__ ut = t.rv(j >> 1);
-    double* __restrict__ yv = t.yv();
-    const bool minus = j & 1;
-    for (int e = lane; e < n; e += WARP) yv[e] = minus ? ys[e] - ut[e] : ys[e] + ut[e];
+    for (int e = lane; e < n; e += WARP) tm.qv()[e] = tm.rv()[e] = 0.;
     __syncwarp();
-    const abcmb_cosmo& cv = P.cosmo[t.vix()[j]];
-    write_fields(cv, L, P.tables, k, t.sv(j)[16], t.yv(), P.pt, nsave, isave, ik, lane, t.sv(j), ncdm_w);
+    if (lane < 2) {
+      const int v = tm.vix()[2 * q + lane];
+      const double l2 = np_interp_lna(P.s.R_large, nullptr, P.aHg + (int64_t)v * NSTART, k);
+      const double tv = fmin(fmin(P.lna1[v], l2), -10.);
+      write_ic(P.cosmo[v], L, P.tables, k, tv, lane ? tm.rv() : tm.qv());
+      tm.sv(0)[lane] = tv;
+    }
+    if (lane == 2)
+      stage_basis_diff(P.cosmo[tm.vix()[2 * q]], P.cosmo[tm.vix()[2 * q + 1]], P.tables, k, ik2, R.ncdm_w,
+                       lna_start, tm.bdt0(q));
+    __syncwarp();
+    const double dt0 = 0.5 * (tm.sv(0)[0] - tm.sv(0)[1]);
+    for (int e = lane; e < n; e += WARP) tm.u0(q)[e] = 0.5 * (tm.qv()[e] - tm.rv()[e]) - m.F()[e] * dt0;
     __syncwarp();
   }
 }
@@ -1344,13 +1235,8 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
   }
   __syncthreads();
   WarpMem m;
-  const size_t wdoubles = warp_mem_doubles(P.max_ny, P.ncm);
-  carve(smem + (size_t)wib * (wdoubles + tan_mem_doubles(P.max_ny, P.ncm, TAN ? P.nd : 0)), P.max_ny, P.ncm, m);
-  TanMem tm;
-  tm.p = m.p + wdoubles;
-  tm.my = P.max_ny;
-  tm.nd = TAN ? P.nd : 0;
-  tm.ncm = P.ncm;
+  carve(smem + (size_t)wib * (warp_mem_doubles(P.max_ny, P.ncm) + tan_mem_doubles(P.max_ny, P.ncm, TAN ? P.nd : 0)),
+        P.max_ny, P.ncm, m);
 #ifdef ABCMB_PHASE_CLOCKS
   const int ph_index = blockIdx.x * (blockDim.x >> 5) + wib;
   unsigned long long* ph_slot = ph_index < PHASE_SLOTS ? g_pert_phase + (size_t)ph_index * PHASE_N : nullptr;
@@ -1383,7 +1269,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
       bool bad = n > P.max_ny || L.nc > P.ncm || lmx > LMAXT || lmn < 4 || n != c.ny;
       if constexpr (TAN) {
         // every variant shares the base's state layout and k grid
-        for (int j = 0; j < 2 * tm.nd; ++j) {
+        for (int j = 0; j < 2 * P.nd; ++j) {
           const int v = P.dirs[(ci * ND_MAX + (j >> 1)) * 2 + (j & 1)];
           bad = bad || v < 0 || v >= P.n_cosmo;
           if (!bad) {
@@ -1451,41 +1337,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
     CoreRow cr;
     core_row_at(L, R, m, m.SB(), lane, cr);
     apply_A(L, m, R, cr, m.SB(), m.y0(), m.F(), nullptr, ncdm, lane);   // FSAL stage 1
-    int titer = 0, tunconv = 0;
-    if constexpr (TAN) {
-      const int nd = tm.nd;
-      if (lane < 2 * nd) tm.vix()[lane] = P.dirs[(ci * ND_MAX + (lane >> 1)) * 2 + (lane & 1)];
-      for (int q = 0; q < nd; ++q)
-        for (int e = lane; e < n; e += WARP) tm.qv(q)[e] = tm.rv(q)[e] = 0.;
-      __syncwarp();
-      // the variants' start times and initial conditions (plus into qv, minus into rv)
-      if (lane < 2 * nd) {
-        const int v = tm.vix()[lane];
-        const double l2 = np_interp_lna(S.R_large, nullptr, P.aHg + (int64_t)v * NSTART, k);
-        const double tv = fmin(fmin(P.lna1[v], l2), -10.);
-        write_ic(P.cosmo[v], L, P.tables, k, tv, (lane & 1) ? tm.rv(lane >> 1) : tm.qv(lane >> 1));
-        tm.sv(0)[lane] = tv;
-      }
-      __syncwarp();
-      // u(t0) = dy0/deps - f(t0, y0) dt0/deps (also into rv: the z of tan_const)
-      for (int q = 0; q < nd; ++q) {
-        const double dt0 = 0.5 * (tm.sv(0)[2 * q] - tm.sv(0)[2 * q + 1]);
-        for (int e = lane; e < n; e += WARP) {
-          const double u = 0.5 * (tm.qv(q)[e] - tm.rv(q)[e]) - m.F()[e] * dt0;
-          tm.u0(q)[e] = u;
-          tm.rv(q)[e] = u;
-        }
-      }
-      if (lane < nd)
-        stage_basis_diff(P.cosmo[tm.vix()[2 * lane]], P.cosmo[tm.vix()[2 * lane + 1]], P.tables, k, ik2, R.ncdm_w,
-                         lna_start, tm.bd(1, lane));
-      __syncwarp();
-      // dF_0 = A(t0) u + dA(t0) y0
-      tan_const(L, m, tm, R, cr, m.SB(), 1, m.y0(), ncdm, lane);
-      for (int q = 0; q < nd; ++q)
-        for (int e = lane; e < n; e += WARP) tm.dF(q)[e] = tm.qv(q)[e];
-      __syncwarp();
-    }
+    if constexpr (TAN) tangent_init(L, m, R, P, ci, k, ik2, lna_start, lane);
 
     while (t0 < 0.0) {
       PERT_PHASE(7);
@@ -1503,15 +1355,6 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
           stage_basis(c, K, P.tables, k, ik2, R.ncdm_w, want_sv ? tsn : t0 + KV_C[lane + 1] * h, m.SB() + (lane + 1) * NB,
                       want_sv ? m.SV() : nullptr);
         if (want_sv) m.SV()[16] = (double)isave;
-        if constexpr (TAN) {
-          // lanes 6.. : the basis change of each (stage time, direction)
-          const int task = lane - NSLOT;
-          if (task >= 0 && task < 5 * tm.nd) {
-            const int slot = task / tm.nd + 1, q = task % tm.nd;
-            stage_basis_diff(P.cosmo[tm.vix()[2 * q]], P.cosmo[tm.vix()[2 * q + 1]], P.tables, k, ik2, R.ncdm_w,
-                             t0 + KV_C[slot] * h, tm.bd(slot, q));
-          }
-        }
       }
       __syncwarp();
       PERT_PHASE(0);
@@ -1551,7 +1394,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
         for (int it = 1; it <= root_max; ++it) {
           apply_A(L, m, R, cr, B, m.v(), m.r(), fi, ncdm, lane);    // residual A v - f
           PERT_PHASE(3);
-          solve_newton(L, m, m.r(), lane);
+          solve_newton(L, m, m.r(), lane, m.vc());
           PERT_PHASE(4);
           double ss = 0.;
           {
@@ -1631,7 +1474,10 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
       PERT_PHASE(6);
       if (keep) {
         ++nacc;
-        if constexpr (TAN) tangent_step(L, m, tm, R, h, rtol, atol * P.tscale, inv_n, ncdm, lane, titer, tunconv);
+        if constexpr (TAN) {
+          for (int q = 0; q < P.nd; ++q)
+            tangent_pass(L, m, R, P, q, k, ik2, t0, h, rtol, atol * P.tscale, inv_n, lts, isave, ik, lane);
+        }
         // cubic Hermite dense output on [t0, t1] at every save point it covers
         while (isave < nsave) {
           double ts = linspace_at(lts, 0.0, nsave, isave);
@@ -1652,7 +1498,6 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
           write_fields(c, L, P.tables, k, ts, m.v(), P.pt, nsave, isave, ik, lane,
                        m.SV()[16] == (double)isave ? m.SV() : nullptr, R.ncdm_w);
           __syncwarp();
-          if constexpr (TAN) tangent_save(L, m, tm, P, k, h, th, isave, nsave, ik, lane, R.ncdm_w);
           ++isave;
         }
         prev_prev_inv = prev_inv;
@@ -1660,13 +1505,6 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
         for (int e = lane; e < n; e += WARP) {
           m.y0()[e] = m.y1()[e];
           m.F()[e] = m.F()[6 * n + e];
-        }
-        if constexpr (TAN) {
-          for (int q = 0; q < tm.nd; ++q)
-            for (int e = lane; e < n; e += WARP) {
-              tm.u0(q)[e] = tm.qv(q)[e];
-              tm.dF(q)[e] = tm.dF(q)[6 * n + e];
-            }
         }
         m.SB()[lane] = m.SB()[5 * NB + lane];                  // basis at the new t0
         __syncwarp();
@@ -1690,8 +1528,9 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
       st.lna_start = lna_start;
       P.kstat[item] = st;
       if (TAN && P.tstat) {
-        P.tstat[2 * item] = titer;
-        P.tstat[2 * item + 1] = tunconv;
+        const int* cnt = tan_mem(m, P).cnt();
+        P.tstat[2 * item] = cnt[0];
+        P.tstat[2 * item + 1] = cnt[1];
       }
     }
     __syncwarp();
