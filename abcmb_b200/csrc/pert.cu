@@ -809,11 +809,13 @@ __device__ __noinline__ void write_ic(const abcmb_cosmo& c, const Layout& L, con
 // by chord iterations with the step's own factorisation (the primal's
 // iteration matrix); dA_i is A with the basis replaced by its change along
 // q (A is linear in the basis): half the difference of the plus and minus
-// descriptors' bases at t_i.  The stage-1 derivative is re-evaluated as
-// A(t0) u0 + dA(t0) y0 at every step.  Only u0 and the basis change at t0
-// persist per direction; the seven stage derivatives and the work vectors
-// are reused by the next direction, which keeps the shared memory per warp
-// (and so the resident warps per SM) close to the forward kernel's.
+// descriptors' bases at t_i.  Only u0 and the stage-1 derivative (the last
+// stage's of the previous step, first-same-as-last like the primal's: a
+// re-evaluation A(t0) u0 + dA(t0) y0 would multiply the stiff components'
+// tolerance-level residue by |A|) persist per direction; the other stage
+// derivatives and the work vectors are reused by the next direction, which
+// keeps the shared memory per warp (and so the resident warps per SM) close
+// to the forward kernel's.
 //
 // The tangent iteration is linear with the primal's iteration matrix
 // I - M_lin^-1 M_i: its spectral radius is small whenever the primal stage
@@ -827,7 +829,7 @@ constexpr int ND_MAX = ABCMB_MAX_TANGENTS;
 constexpr int TANGENT_ROOT_MAX = 16;
 
 // Per-warp tangent scratch, after the primal's WarpMem: per direction u0
-// and the basis change at t0; shared by the directions: the seven stage
+// and the stage-1 derivative f0; shared by the directions: the seven stage
 // derivatives dF, q (the constant part of a stage's residual; u1 once the
 // stages are done), r (residual and solve vector; a variant's state at a
 // save point), yd (dy/dt of the dense output), yv (a variant's state), the
@@ -838,8 +840,8 @@ struct TanMem {
   double* p;
   int my, nd, ncm;
   __device__ __forceinline__ double* u0(int q) const { return p + q * my; }
-  __device__ __forceinline__ double* bdt0(int q) const { return p + nd * my + q * NB; }
-  __device__ __forceinline__ double* dF() const { return p + nd * (my + NB); }
+  __device__ __forceinline__ double* f0(int q) const { return p + nd * my + q * my; }
+  __device__ __forceinline__ double* dF() const { return p + 2 * nd * my; }
   __device__ __forceinline__ double* qv() const { return dF() + 7 * my; }
   __device__ __forceinline__ double* rv() const { return qv() + my; }
   __device__ __forceinline__ double* yd() const { return rv() + my; }
@@ -854,7 +856,7 @@ struct TanMem {
 
 __host__ __device__ inline size_t tan_mem_doubles(int max_ny, int ncm, int nd) {
   if (nd <= 0) return 0;
-  return (size_t)nd * ((size_t)max_ny + NB) + 11 * (size_t)max_ny + 5 * NB + 2 * NSV + (size_t)ncm + ND_MAX + 1;
+  return (size_t)nd * 2 * (size_t)max_ny + 11 * (size_t)max_ny + 5 * NB + 2 * NSV + (size_t)ncm + ND_MAX + 1;
 }
 
 // out = A(B) z + A(Bd) Y for one direction: the part of a stage's tangent
@@ -989,10 +991,8 @@ __device__ __noinline__ void tangent_pass(const Layout& L, WarpMem& m, const Row
   double* __restrict__ dF = t.dF();
   if (lane < 5) stage_basis_diff(cp, cm, P.tables, k, ik2, R.ncdm_w, t0 + KV_C[lane + 1] * h, t.bd(lane + 1));
   CoreRow cr;
-  core_row_at(L, R, m, m.SB(), lane, cr);
+  for (int e = lane; e < n; e += WARP) dF[e] = t.f0(q)[e];     // the stage-1 derivative (FSAL)
   __syncwarp();
-  // stage-1 derivative dF_0 = A(t0) u0 + dA(t0) y0
-  tan_const(L, m, R, cr, m.SB(), t.bdt0(q), t.u0(q), m.y0(), dF, ncdm, lane);
   for (int i = 1; i < 7; ++i) {
     const int slot = (i == 6) ? 5 : i;
     const double* B = m.SB() + slot * NB;
@@ -1126,8 +1126,8 @@ __device__ __noinline__ void tangent_pass(const Layout& L, WarpMem& m, const Row
     const double* __restrict__ u1 = t.qv();
     double* __restrict__ u0 = t.u0(q);
     for (int e = lane; e < n; e += WARP) u0[e] = u1[e];
-    double* __restrict__ b0 = t.bdt0(q);
-    if (lane < NB) b0[lane] = t.bd(5)[lane];          // the basis change at the next t0
+    double* __restrict__ f0 = t.f0(q);
+    for (int e = lane; e < n; e += WARP) f0[e] = dF[6 * n + e];   // first same as last
     if (lane == 0) {
       t.cnt()[0] += titer;
       t.cnt()[1] += tunconv;
@@ -1138,7 +1138,8 @@ __device__ __noinline__ void tangent_pass(const Layout& L, WarpMem& m, const Row
 
 // The tangents at an item's start: u = dy0/deps - f(t0, y0) dt0/deps from
 // the variants' initial conditions at their own start times (plus into q,
-// minus into r), the basis change at t0, the counters cleared.
+// minus into r), the stage-1 derivative A(t0) u + dA(t0) y0 (the basis
+// change at t0 into bd(1)), the counters cleared.
 __device__ __noinline__ void tangent_init(const Layout& L, const WarpMem& m, const RowTab& R, const PertArgs& P,
                                           int ci, double k, double ik2, double lna_start, int lane) {
   const TanMem tm = tan_mem(m, P);
@@ -1158,11 +1159,14 @@ __device__ __noinline__ void tangent_init(const Layout& L, const WarpMem& m, con
     }
     if (lane == 2)
       stage_basis_diff(P.cosmo[tm.vix()[2 * q]], P.cosmo[tm.vix()[2 * q + 1]], P.tables, k, ik2, R.ncdm_w,
-                       lna_start, tm.bdt0(q));
+                       lna_start, tm.bd(1));
     __syncwarp();
     const double dt0 = 0.5 * (tm.sv(0)[0] - tm.sv(0)[1]);
     for (int e = lane; e < n; e += WARP) tm.u0(q)[e] = 0.5 * (tm.qv()[e] - tm.rv()[e]) - m.F()[e] * dt0;
     __syncwarp();
+    CoreRow cr;
+    core_row_at(L, R, const_cast<WarpMem&>(m), m.SB(), lane, cr);
+    tan_const(L, m, R, cr, m.SB(), tm.bd(1), tm.u0(q), m.y0(), tm.f0(q), L.nM > 0, lane);
   }
 }
 

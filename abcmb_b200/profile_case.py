@@ -7,6 +7,8 @@
     python -m abcmb_b200.profile_case c4 64 --hyrex     # the recombination histories alone
     ABCMB_B200_LIB=abcmb_b200/libabcmb_b200_phase.so \
         python -m abcmb_b200.profile_case c4 40 --phases  # cycles per phase of pert_kernel
+    python -m abcmb_b200.profile_case c4 16 --grad tangent   # the gradient batch: one tangent
+    python -m abcmb_b200.profile_case c4 16 --grad fd        # launch, or every variant integrated
 
 Runs the perturbation launch twice (warm-up + measured) and, with --los, the
 line of sight twice, then checks the per-k status.  With --bg-only the batch
@@ -30,6 +32,11 @@ def _phase_clocks(reset: bool):
     return [int(c) for c in cyc]
 
 
+def _grid():
+    from . import _lib
+    return _lib.load().abcmb_last_pert_grid()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["c1", "c2", "c4"])
@@ -38,6 +45,7 @@ def main():
     ap.add_argument("--bg-only", action="store_true")
     ap.add_argument("--phases", action="store_true")
     ap.add_argument("--hyrex", action="store_true")
+    ap.add_argument("--grad", choices=["tangent", "fd"], default=None)
     a = ap.parse_args()
     import torch
     from . import configs, engine
@@ -65,7 +73,12 @@ def main():
             st = db.bg_forward()
         print("ok cosmologies", len(st), "optical-depth steps max", int(st["n_steps_kappa"].max()))
         return
-    w.build()
+    gw = None
+    if a.grad:
+        from . import gradients
+        gw = gradients.expand(w, processes=4, mode=a.grad)
+    else:
+        w.build()
     st = w.pert_settings()
     db = engine.DeviceBatch.upload(w.batch)
     e0 = torch.cuda.Event(enable_timing=True)
@@ -75,10 +88,17 @@ def main():
             _phase_clocks(reset=True)
         if i == 1:
             e0.record()
-        db.pert_forward(st)
+        if gw is not None:
+            db.pert_forward_grad(gw, st)
+        else:
+            db.pert_forward(st)
     e1.record()
     torch.cuda.synchronize()
-    print(f"perturbation launch {e0.elapsed_time(e1):.1f} ms")
+    print(f"perturbation launch {e0.elapsed_time(e1):.1f} ms" + (f" ({a.grad}, {w.batch.n_items} items, grid "
+          f"{_grid()})" if gw is not None else ""))
+    if gw is not None and gw.mode == "tangent":
+        ts = db.tstat.cpu().numpy().reshape(-1, 2)
+        print(f"tangent chord iterations per item {ts[:, 0].mean():.0f}; unconverged stage solves {int(ts[:, 1].sum())}")
     if a.phases:
         torch.cuda.synchronize()
         cyc = _phase_clocks(reset=False)

@@ -684,8 +684,9 @@ static void work_free(work_t* w) {
  * stage uses is met (the iteration matrix is the primal's, so it converges
  * as fast).  The start time moves with theta: u(t0) = dy0/deps - f(t0, y0)
  * dt0/deps, with y0 = IC(theta, t0(theta)) differenced between the two
- * descriptors.  The stage-1 derivative dF_0 = A(t0) u0 + dA(t0) y0 is
- * evaluated afresh at every step.  Outputs are the two variants' PerturbationTables at their
+ * descriptors; afterwards the stage-1 derivative is the previous step's last
+ * stage's (first same as last, like the primal's).  Outputs are the two
+ * variants' PerturbationTables at their
  * own save times ts(plus) and ts(minus): the fields of y(ts) +- (u(ts) +
  * y'(ts) (ts(plus) - ts(minus)) / 2), with y' the derivative of the dense
  * output, evaluated with each variant's own background. */
@@ -777,18 +778,6 @@ static void tangent_step(const abcmb_cosmo* c, const layout_t* L, const double* 
   const double hg = h * KV_GAMMA;
   const double kappa = 1e-2, small_res = 1e-13;
   const int root_max = TANGENT_ROOT_MAX;
-  /* the stage-1 derivatives dF_0 = A(t0) u0 + dA(t0) y0, evaluated afresh at
-   * every step (not carried over from the previous step's last stage) */
-  {
-    bgs_t b0;
-    bg_eval(c, tables, t0, &b0);
-    for (int p = 0; p < T->nd; ++p) {
-      double* dF0 = tw->dF + (size_t)p * 7 * n;
-      rhs(c, L, k, &b0, tw->u0 + (size_t)p * n, dF0);
-      tangent_dA(T, p, L, tables, k, t0, w->y0, tw, tw->q);
-      for (int e = 0; e < n; ++e) dF0[e] += tw->q[e];
-    }
-  }
   for (int i = 1; i < 7; ++i) {
     const double ti = t0 + KV_C[i] * h;
     bgs_t bi;
@@ -901,7 +890,7 @@ static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kb
   bg_eval(c, tables, t0, &b);
   rhs(c, &L, k, &b, w->y0, w->F);
   if (T) {
-    /* tangents at the start: u = dy0/deps - f(t0, y0) dt0/deps */
+    /* tangents at the start: u = dy0/deps - f(t0, y0) dt0/deps, dF_0 = A u + dA y0 */
     for (int p = 0; p < T->nd; ++p) {
       const double tp = start_time_from_grid(T->sgp[p], k, s->R_large, w->f2);
       const double tm = start_time_from_grid(T->sgm[p], k, s->R_large, w->f2);
@@ -910,6 +899,10 @@ static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kb
       const double dt0 = 0.5 * (tp - tm);
       double* u = tw->u0 + (size_t)p * n;
       for (int e = 0; e < n; ++e) u[e] = 0.5 * (tw->yp[e] - tw->us[e]) - w->F[e] * dt0;
+      double* dF0 = tw->dF + (size_t)p * 7 * n;
+      rhs(c, &L, k, &b, u, dF0);
+      tangent_dA(T, p, &L, tables, k, t0, w->y0, tw, tw->q);
+      for (int e = 0; e < n; ++e) dF0[e] += tw->q[e];
     }
   }
 
@@ -1056,8 +1049,12 @@ static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kb
       memcpy(w->y0, w->y1, sizeof(double) * n);
       memcpy(w->F, w->F + 6 * n, sizeof(double) * n);   /* FSAL */
       if (T) {
-        for (int p = 0; p < T->nd; ++p)
+        for (int p = 0; p < T->nd; ++p) {
           memcpy(tw->u0 + (size_t)p * n, tw->u1 + (size_t)p * n, sizeof(double) * n);
+          /* first same as last: a re-evaluation A(t0) u0 + dA(t0) y0 would
+           * multiply the stiff components' tolerance-level residue by |A| */
+          memcpy(tw->dF + (size_t)p * 7 * n, tw->dF + ((size_t)p * 7 + 6) * n, sizeof(double) * n);
+        }
       }
       t0 = t1;
     } else {
