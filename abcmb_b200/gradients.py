@@ -168,3 +168,29 @@ def expand(w: Workload, n_save: int = 500, processes: int = 0, rel_step: float =
     w.batch = batch
     return GradWorkload(base=w, variants=variants, batch=batch, n_var=len(variants[0]), mode=mode, dirs=dirs,
                         n_dir=len(FD_PARAMS) if mode == "tangent" else 0, rel_step=rel_step)
+
+
+def as_tangent(gw: GradWorkload) -> GradWorkload:
+    """The tangent-mode view of a finite-difference expansion: the same
+    descriptors, tables and PerturbationTable slots, work items only for the
+    base cosmologies, and the (plus, minus) direction table.  No background
+    is recomputed."""
+    if gw.mode == "tangent":
+        return gw
+    import dataclasses
+    b = gw.batch
+    n = b.n_cosmo
+    nvar = gw.n_var
+    base = np.zeros(n, dtype=bool)
+    dirs = np.full((n, MAX_TANGENTS, 2), -1, dtype=np.int32)
+    for i, var in enumerate(gw.variants):
+        b0 = i * nvar
+        base[b0] = True
+        for q, name in enumerate(FD_PARAMS):
+            jp = next(j for j, v in enumerate(var) if v[0] == name and v[1] > 0)
+            jm = next(j for j, v in enumerate(var) if v[0] == name and v[1] < 0)
+            dirs[b0, q] = (b0 + jp, b0 + jm)
+    items = b.items[base[b.items[:, 0]]].copy()
+    tb = dataclasses.replace(b, items=items)
+    return dataclasses.replace(gw, batch=tb, mode="tangent", dirs=dirs, n_dir=len(FD_PARAMS))
+

@@ -7,12 +7,14 @@ massive-neutrino count drawn from {0, 1, 3}, per-cosmology k grids of
 400..800 modes on [1e-5, 1] / Mpc, x_e / T_m tables in HyRex's padded
 layout, unlensed TT/TE/EE to l = 2500 -- with the C_l gradient with respect
 to (h, omega_b, omega_cdm, A_s, n_s, tau_reio).  One step = the
-perturbations of the 64 cosmologies with the forward-mode sensitivities of
-h, omega_b, omega_cdm and tau_reio (one persistent tangent launch; the
-plus / minus variants' tables written around each base) + the line of sight
-over all 576 descriptors + gradient assembly (exact A_s / n_s derivatives
-from the same line-of-sight launch).  --grad fd integrates every variant on
-its own instead (central differences of whole solves).  Inputs are seeded
+perturbations of all 9 gradient descriptors of the 64 cosmologies (the base
+and +-1e-4 relative in h, omega_b, omega_cdm, tau_reio: one persistent
+launch) + the line of sight over all 576 descriptors + gradient assembly
+(central differences; exact A_s / n_s derivatives from the same
+line-of-sight launch).  --grad tangent integrates only the base cosmologies
+and carries the four directions' forward-mode sensitivities instead (one
+tangent launch); the line also reports that mode's own measurement.  Inputs
+are seeded
 synthetic (numpy default_rng(20261203 + rank)); background tables are
 produced on the host before timing (they are inputs of this path).
 
@@ -48,7 +50,7 @@ def parse():
     ap.add_argument("--n-cosmo", type=int, default=64)
     ap.add_argument("--l-max", type=int, default=2500)
     ap.add_argument("--e2e-steps", type=int, default=1)
-    ap.add_argument("--grad", default="tangent", choices=["tangent", "fd"])
+    ap.add_argument("--grad", default="fd", choices=["tangent", "fd"])
     ap.add_argument("--plain-sample", type=int, default=8,
                     help="cosmologies of the batch timed on the plain (unbatched forward + FD) path")
     # internal: the CPU baseline in a process of its own (no torch, no CUDA)
@@ -582,6 +584,11 @@ def main():
             line["hyrex_forward"] = hyrex_timing(w, dev)
         except Exception as ex:                            # an extra measurement never costs the line
             line["hyrex_forward"] = {"error": str(ex)[:200]}
+        if gw.mode == "fd":
+            tan = tangent_extra(gw, w, db, lr, st, dev, stream, assemble, out_cl, out_grad)
+            tan_cl0, tan_grad0 = tan.pop("cl0"), tan.pop("grad0")
+            tan["vs_fd_step"] = ms / tan["ms_per_step"]
+            line["grad_tangent"] = tan
         plain = plain_gpu_fwd_fd(gw, w, dev, stream, args.plain_sample)
         plain["batched_over_plain"] = value / plain["value"]
         line["plain_gpu_fwd_fd"] = plain
@@ -592,17 +599,64 @@ def main():
             line["cpu_baseline"] = cpu_baseline_line(res)
             o = np.load(ref_file)
             line["err_vs_oracle"] = err_vs_oracle(res_cl.numpy()[0], res_grad.numpy()[0], o["cl"], o["grad"])
+            line["err_vs_oracle"]["gpu_grad"] = GRAD_DESC[gw.mode]
+            if "grad_tangent" in line:
+                line["grad_tangent"]["err_vs_oracle"] = err_vs_oracle(tan_cl0, tan_grad0, o["cl"], o["grad"])
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
 
+def tangent_extra(gw, w, db, lr, st, dev, stream, assemble, out_cl, out_grad, steps: int = 2) -> dict:
+    """The same step with the tangent kernel (abcmb_pert_forward_tangent over
+    the base cosmologies, the variants' tables from the tangents), on the
+    same descriptors and buffers: CUDA-event time of `steps` steps after one
+    warm-up, the tangent statistics, and C_l / gradient of cosmology 0."""
+    import dataclasses as dc
+    import torch
+    from abcmb_b200 import gradients
+    gt = gradients.as_tangent(gw)
+    tdb = dc.replace(db, batch=gt.batch,
+                     items=torch.from_numpy(gt.batch.items.reshape(-1).copy()).to(dev),
+                     kstat=torch.zeros(gt.batch.n_items * 24, dtype=torch.uint8, device=dev))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    pert = []
+
+    def one(rec):
+        if rec:
+            ev[2].record(stream)
+        tdb.pert_forward_tangent(st, gt.dirs, gt.n_dir, gt.rel_step, stream)
+        if rec:
+            ev[3].record(stream)
+        lr.run(stream)
+        assemble()
+
+    one(False)
+    torch.cuda.synchronize(dev)
+    tdb.check_status()
+    ev[0].record(stream)
+    for _ in range(steps):
+        one(True)
+        ev[3].synchronize()
+        pert.append(ev[2].elapsed_time(ev[3]))
+    ev[1].record(stream)
+    torch.cuda.synchronize(dev)
+    ms = ev[0].elapsed_time(ev[1]) / steps
+    ts = tdb.tstat.cpu().numpy().reshape(-1, 2)[:gt.batch.n_items]
+    nb = len(w.params_in)
+    return {"value": nb / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms, "steps": steps,
+            "pert_launch_ms": float(np.mean(pert)), "items": int(gt.batch.n_items),
+            "chord_iterations_per_item": float(ts[:, 0].mean()), "unconverged_stage_solves": int(ts[:, 1].sum()),
+            "cl0": out_cl[0].cpu().numpy(), "grad0": out_grad[0].cpu().numpy()}
+
+
 def err_vs_oracle(cl, grad, cl_o, grad_o) -> dict:
     """C_l and gradient of the batch's first cosmology against the oracle's
-    (the CPU baseline's own run of that cosmology): max relative error of
-    TT and EE, TE relative to |TT| + |TE|, each gradient series relative to
-    its own maximum over l."""
+    (the CPU baseline's own run of that cosmology: forward-mode tangents, the
+    derivative without step-sequence noise): max relative error of TT and EE,
+    TE relative to |TT| + |TE|, each gradient series relative to its own
+    maximum over l."""
     tt = float(np.max(np.abs(cl[0] - cl_o[0]) / np.abs(cl_o[0])))
     ee = float(np.max(np.abs(cl[2] - cl_o[2]) / np.abs(cl_o[2])))
     te = float(np.max(np.abs(cl[1] - cl_o[1]) / (np.abs(cl_o[0]) + np.abs(cl_o[1]))))
@@ -612,7 +666,7 @@ def err_vs_oracle(cl, grad, cl_o, grad_o) -> dict:
             "grad_max_rel": {name: {"TT": float(g[i, 0]), "TE": float(g[i, 1]), "EE": float(g[i, 2])}
                              for i, name in enumerate(GRAD_PARAMS)},
             "grad_max_rel_all": float(g.max()),
-            "oracle": "oracle C restatement, FP64, same tangent algorithm and inputs (A_s, n_s rows: central "
+            "oracle": "oracle C restatement, FP64, forward-mode tangents, same inputs (A_s, n_s rows: central "
                       "differences of its line of sight)"}
 
 

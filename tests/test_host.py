@@ -325,3 +325,17 @@ def test_from_reference_packs_like_background_tables():
     np.testing.assert_array_equal(a.tables[:o], b.tables[:o])
     assert not b.tables[o:o + 6 * 499].any()
     assert int(b.cosmo["n_xe"][0]) == bt.HYREX_XE_LEN
+
+
+def test_as_tangent_matches_tangent_expansion():
+    """The tangent view of a finite-difference expansion has the tangent
+    expansion's descriptors, items and direction table."""
+    from abcmb_b200 import configs, gradients
+    w = configs.c4(n_cosmo=2, nk_range=(20, 24), xe_layout="compact")
+    gf = gradients.expand(w, processes=1, mode="fd")
+    gt = gradients.expand(w, processes=1, mode="tangent")
+    gv = gradients.as_tangent(gf)
+    np.testing.assert_array_equal(gv.batch.cosmo, gt.batch.cosmo)
+    np.testing.assert_array_equal(gv.batch.items, gt.batch.items)
+    np.testing.assert_array_equal(gv.dirs, gt.dirs)
+    assert gv.mode == "tangent" and gv.n_dir == 4 and gf.mode == "fd" and gf.batch.n_items == 9 * gv.batch.n_items
