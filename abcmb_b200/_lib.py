@@ -48,6 +48,8 @@ SIGNATURES = [
                                           _i64, _vp]),
     ("abcmb_set_pert_warps_per_block", ctypes.c_int, [ctypes.c_int]),
     ("abcmb_last_pert_grid", ctypes.c_int, []),
+    ("abcmb_set_pert_variant", ctypes.c_int, [ctypes.c_int]),
+    ("abcmb_set_pert_tangent_warps_per_block", ctypes.c_int, [ctypes.c_int]),
     ("abcmb_probe_fp64_tflops", ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.c_int, _vp]),
     ("abcmb_pert_forward_tangent", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp,
                                                   _d, _vp, _vp, _vp, _vp, _vp, _i64, _vp]),

@@ -80,6 +80,8 @@ BesselCache* bessel_for_current_device() {
 
 int g_warps_per_block = 4;
 int g_last_grid = 0;
+int g_pert_variant = 0;        // 0 automatic, 1 two blocks/SM, 2 three blocks/SM
+int g_pert_tangent_warps = 0;  // 0 automatic (most resident warps), else warps per block
 
 }  // namespace
 
@@ -90,6 +92,8 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 // block (abcmb_set_pert_warps_per_block) and the grid of the last launch
 // (abcmb_last_pert_grid)
 int pert_warps_per_block() { return g_warps_per_block; }
+int pert_variant() { return g_pert_variant; }
+int pert_tangent_warps() { return g_pert_tangent_warps; }
 void set_last_pert_grid(int grid) { g_last_grid = grid; }
 }  // namespace abcmb
 
@@ -383,6 +387,22 @@ int abcmb_lens_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_le
 int abcmb_set_pert_warps_per_block(int w) {
   if (w < 1 || w > 4) return fail(ABCMB_ERR_ARG, "warps per block must be 1..4");
   g_warps_per_block = w;
+  return ABCMB_OK;
+}
+
+/* Tuning knob: which instantiation of the perturbation kernel runs (0 =
+ * by queue length, 1 = two blocks per SM, 2 = three blocks per SM). */
+int abcmb_set_pert_variant(int v) {
+  if (v < 0 || v > 2) return fail(ABCMB_ERR_ARG, "perturbation kernel variant must be 0, 1 or 2");
+  g_pert_variant = v;
+  return ABCMB_OK;
+}
+
+/* Tuning knob: warps per block of the tangent kernel (0 = the count with the
+ * most resident warps, else 1..4). */
+int abcmb_set_pert_tangent_warps_per_block(int w) {
+  if (w < 0 || w > 4) return fail(ABCMB_ERR_ARG, "tangent warps per block must be 0..4");
+  g_pert_tangent_warps = w;
   return ABCMB_OK;
 }
 

@@ -1580,6 +1580,10 @@ int pert_phase_clocks(unsigned long long* out, int reset) {
 #endif
 }
 
+// launch choices set through the C ABI (capi.cu): 0 = automatic
+int pert_variant();
+int pert_tangent_warps();
+
 int64_t pert_workspace_bytes(int n_cosmo) {
   int64_t b = 256;                                        // queue counter
   b += ((int64_t)n_cosmo * 8 + 255) / 256 * 256;          // lna1
@@ -1633,8 +1637,11 @@ cudaError_t launch_pert(int n_cosmo, const abcmb_cosmo* cosmo, const double* tab
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   // a long queue (many items per warp) favours more resident warps; a short
   // one is bounded by its slowest items and favours the uncapped registers
+  const int variant = pert_variant();
   const bool throughput =
-      (int64_t)n_items >= (int64_t)PERT_THROUGHPUT_ITEMS_PER_WARP * nsm * PERT_BLOCKS_LATENCY * warps_per_block;
+      variant == 2 ||
+      (variant == 0 &&
+       (int64_t)n_items >= (int64_t)PERT_THROUGHPUT_ITEMS_PER_WARP * nsm * PERT_BLOCKS_LATENCY * warps_per_block);
   const void* fn = throughput ? (const void*)pert_kernel<PERT_BLOCKS_THROUGHPUT>
                               : (const void*)pert_kernel<PERT_BLOCKS_LATENCY>;
   e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1703,7 +1710,9 @@ cudaError_t launch_pert_tangent(int n_cosmo, const abcmb_cosmo* cosmo, const dou
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   int best_w = 0, best_blocks = 0, best_total = 0;
+  const int fixed_w = pert_tangent_warps();
   for (int wpb = PERT_THREADS_MAX / 32; wpb >= 1; --wpb) {
+    if (fixed_w > 0 && wpb != fixed_w) continue;
     const size_t smem = (size_t)wpb * per_warp;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
       cudaGetLastError();

@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--l-max", type=int, default=2500)
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--grad", default="fd", choices=["tangent", "fd"])
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch choices instead of the tuned ones")
     ap.add_argument("--plain-sample", type=int, default=8,
                     help="cosmologies of the batch timed on the plain (unbatched forward + FD) path")
     # internal: the CPU baseline in a process of its own (no torch, no CUDA)
@@ -455,6 +457,18 @@ def main():
         out_grad[:, 4] = dns[:, 0]
         out_grad[:, 5] = fd[:, 3]
 
+    # launch choices of the perturbation kernel: measured once per (shape,
+    # GPU) on a sample of the queue and cached on disk (abcmb_b200.autotune);
+    # every choice gives the same results bit for bit
+    launch = {"tuned": False}
+    if not args.no_autotune:
+        from abcmb_b200 import autotune
+        t_tune = time.perf_counter()
+        kind, key, choice = autotune.tune_batch(db, gw, st)
+        launch = {"tuned": True, "key": key, "choice": list(choice) if isinstance(choice, tuple) else choice,
+                  "what": "[warps per block, variant 1 = 2 blocks/SM, 2 = 3 blocks/SM]" if kind == "fd"
+                  else "warps per block (0 = by occupancy)", "tune_s": time.perf_counter() - t_tune}
+
     pert_ms = []
 
     def step(record=False):
@@ -578,6 +592,7 @@ def main():
             "ode_steps_mean": float(steps_k.mean()), "host_build_s": t_build}
     if tangent_stats:
         line["tangents"] = tangent_stats
+    line["launch"] = launch
     if rank == 0 and world == 1:
         line["bg_forward"] = bg_forward_timing(gw, db, dev, stream)
         try:

@@ -538,6 +538,17 @@ int abcmb_lens_forward(int n_cosmo, const abcmb_cosmo* cosmo_dev,
 /* Warps per block of the perturbation kernel (1..4; default 4). */
 int abcmb_set_pert_warps_per_block(int warps);
 
+/* Instantiation of the perturbation kernel: 0 = chosen by queue length
+ * (default), 1 = two blocks per SM (no register cap: shortest time per
+ * item), 2 = three blocks per SM (168 registers: most resident warps).
+ * Either gives the same results bit for bit (every item is one warp's
+ * independent computation). */
+int abcmb_set_pert_variant(int variant);
+
+/* Warps per block of the tangent kernel: 0 = the count with the most
+ * resident warps per SM (default), else 1..4. */
+int abcmb_set_pert_tangent_warps_per_block(int warps);
+
 /* Cycles the perturbation kernel's warps spent per phase since the last
  * reset, summed over warps: cycles[8] = stage-time background, Newton-matrix
  * factorisation, stage set-up, residual, structured solve, chord update and
