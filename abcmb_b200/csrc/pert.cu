@@ -968,6 +968,47 @@ __device__ __forceinline__ TanMem tan_mem(const WarpMem& m, const PertArgs& P) {
   return t;
 }
 
+// Optional per-phase cycle accounting, compiled in only with
+// -DABCMB_PHASE_CLOCKS (python -m abcmb_b200.build --phase-clocks): every
+// warp adds the clock64() cycles it spends in each phase of its steps to its
+// own slot of g_pert_phase with reductions whose result nobody waits for;
+// abcmb_pert_phase_clocks sums the slots.  Phases: 0 stage-time background,
+// 1 Newton-matrix factorisation, 2 stage set-up, 3 residual (apply_A),
+// 4 structured solve, 5 chord update and convergence test, 6 error estimate
+// and step-size control, 7 the rest (dense output and PerturbationTable
+// writes, item start and end, queue); the tangent kernel adds 8 the basis
+// changes, 9 the stages' constant parts (primal stage values, z, A z +
+// dA Y), 10 the tangent chord iterations, 11 the variants' tables.
+#ifdef ABCMB_PHASE_CLOCKS
+constexpr int PHASE_N = 12;
+constexpr int PHASE_SLOTS = 8192;
+__device__ unsigned long long g_pert_phase[PHASE_SLOTS * PHASE_N];
+#define PERT_PHASE(k)                                                                      \
+  do {                                                                                    \
+    const long long ph_now = clock64();                                                   \
+    if (lane == 0 && ph_slot) atomicAdd(ph_slot + (k), (unsigned long long)(ph_now - ph_t)); \
+    ph_t = ph_now;                                                                        \
+  } while (0)
+#else
+#define PERT_PHASE(k) \
+  do {                \
+  } while (0)
+#endif
+#ifdef ABCMB_PHASE_CLOCKS
+#define PERT_PHASE_BEGIN()                                                                                    \
+  const int ph_index = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);                                 \
+  unsigned long long* ph_slot = ph_index < PHASE_SLOTS ? g_pert_phase + (size_t)ph_index * PHASE_N : nullptr; \
+  long long ph_t = clock64()
+#define PERT_PHASE_RESET() ph_t = clock64()
+#else
+#define PERT_PHASE_BEGIN() \
+  do {                     \
+  } while (0)
+#define PERT_PHASE_RESET() \
+  do {                     \
+  } while (0)
+#endif
+
 // Direction q of one accepted step [t0, t0 + h] (the primal's stage
 // derivatives F, y0, y1, factorisation and basis slots are the step's):
 // the basis changes at the five stage times (lanes 0-4), the stage-1
@@ -981,6 +1022,7 @@ __device__ __noinline__ void tangent_pass(const Layout& L, WarpMem& m, const Row
                                           double k, double ik2, double t0, double h, double rtol, double atol_t,
                                           double inv_n, double lts, int isave0, int ik, int lane) {
   const TanMem t = tan_mem(m, P);
+  PERT_PHASE_BEGIN();
   int titer = 0, tunconv = 0;
   const int n = L.ny;
   const bool ncdm = L.nM > 0;
@@ -993,6 +1035,7 @@ __device__ __noinline__ void tangent_pass(const Layout& L, WarpMem& m, const Row
   CoreRow cr;
   for (int e = lane; e < n; e += WARP) dF[e] = t.f0(q)[e];     // the stage-1 derivative (FSAL)
   __syncwarp();
+  PERT_PHASE(8);
   for (int i = 1; i < 7; ++i) {
     const int slot = (i == 6) ? 5 : i;
     const double* B = m.SB() + slot * NB;
@@ -1026,6 +1069,7 @@ __device__ __noinline__ void tangent_pass(const Layout& L, WarpMem& m, const Row
     }
     __syncwarp();
     tan_const(L, m, R, cr, B, t.bd(slot), t.rv(), m.v(), t.qv(), ncdm, lane);
+    PERT_PHASE(9);
     double* __restrict__ fi = dF + i * n;
     double dsz = INFINITY;
     bool conv = false;
@@ -1062,6 +1106,7 @@ __device__ __noinline__ void tangent_pass(const Layout& L, WarpMem& m, const Row
       }
     }
     if (!conv) ++tunconv;
+    PERT_PHASE(10);
   }
   {
     // u1 = u0 + h (sum_j a_7j dF_j + gamma dF_7) into q
@@ -1134,6 +1179,7 @@ __device__ __noinline__ void tangent_pass(const Layout& L, WarpMem& m, const Row
     }
   }
   __syncwarp();
+  PERT_PHASE(11);
 }
 
 // The tangents at an item's start: u = dy0/deps - f(t0, y0) dt0/deps from
@@ -1180,30 +1226,7 @@ constexpr int PERT_THREADS_MAX = 128;
 // queue length per warp (at 2 blocks/SM) from which the throughput variant wins
 constexpr int PERT_THROUGHPUT_ITEMS_PER_WARP = 16;
 
-// Optional per-phase cycle accounting, compiled in only with
-// -DABCMB_PHASE_CLOCKS (python -m abcmb_b200.build --phase-clocks): every
-// warp adds the clock64() cycles it spends in each phase of its steps to its
-// own slot of g_pert_phase with reductions whose result nobody waits for;
-// abcmb_pert_phase_clocks sums the slots.  Phases: 0 stage-time background,
-// 1 Newton-matrix factorisation, 2 stage set-up, 3 residual (apply_A),
-// 4 structured solve, 5 chord update and convergence test, 6 error estimate
-// and step-size control, 7 the rest (dense output and PerturbationTable
-// writes, item start and end, queue).
-#ifdef ABCMB_PHASE_CLOCKS
-constexpr int PHASE_N = 8;
-constexpr int PHASE_SLOTS = 8192;
-__device__ unsigned long long g_pert_phase[PHASE_SLOTS * PHASE_N];
-#define PERT_PHASE(k)                                                                      \
-  do {                                                                                    \
-    const long long ph_now = clock64();                                                   \
-    if (lane == 0 && ph_slot) atomicAdd(ph_slot + (k), (unsigned long long)(ph_now - ph_t)); \
-    ph_t = ph_now;                                                                        \
-  } while (0)
-#else
-#define PERT_PHASE(k) \
-  do {                \
-  } while (0)
-#endif
+
 
 template <bool TAN>
 __device__ __forceinline__ void pert_body(const PertArgs& P) {
@@ -1481,6 +1504,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
         if constexpr (TAN) {
           for (int q = 0; q < P.nd; ++q)
             tangent_pass(L, m, R, P, q, k, ik2, t0, h, rtol, atol * P.tscale, inv_n, lts, isave, ik, lane);
+          PERT_PHASE_RESET();
         }
         // cubic Hermite dense output on [t0, t1] at every save point it covers
         while (isave < nsave) {

@@ -21,13 +21,15 @@ import argparse
 
 PHASES = ("stage-time background (stage_basis)", "Newton-matrix factorisation", "stage set-up",
           "residual (apply_A)", "structured solve (solve_newton)", "chord update + convergence test",
-          "error estimate + step-size control", "rest (dense output, table writes, item start/end)")
+          "error estimate + step-size control", "rest (dense output, table writes, item start/end)",
+          "tangent: basis changes", "tangent: stage constant parts", "tangent: chord iterations",
+          "tangent: variants' tables")
 
 
 def _phase_clocks(reset: bool):
     import ctypes
     from . import _lib
-    cyc = (ctypes.c_uint64 * 8)()
+    cyc = (ctypes.c_uint64 * len(PHASES))()
     _lib.check(_lib.load().abcmb_pert_phase_clocks(cyc, 1 if reset else 0), "abcmb_pert_phase_clocks")
     return [int(c) for c in cyc]
 

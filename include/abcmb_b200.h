@@ -549,10 +549,12 @@ int abcmb_set_pert_variant(int variant);
  * resident warps per SM (default), else 1..4. */
 int abcmb_set_pert_tangent_warps_per_block(int warps);
 
-/* Cycles the perturbation kernel's warps spent per phase since the last
- * reset, summed over warps: cycles[8] = stage-time background, Newton-matrix
+/* Cycles the perturbation kernels' warps spent per phase since the last
+ * reset, summed over warps: cycles[12] = stage-time background, Newton-matrix
  * factorisation, stage set-up, residual, structured solve, chord update and
- * convergence test, error estimate and step-size control, the rest.  Only a
+ * convergence test, error estimate and step-size control, the rest; and in
+ * the tangent kernel the basis changes, the tangent stages' constant parts,
+ * the tangent chord iterations, the variants' tables.  Only a
  * library built with ABCMB_PHASE_CLOCKS counts (python -m abcmb_b200.build
  * --phase-clocks); others return ABCMB_ERR_ARG.  reset != 0 zeroes the
  * counters after reading. */
