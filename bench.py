@@ -7,14 +7,15 @@ massive-neutrino count drawn from {0, 1, 3}, per-cosmology k grids of
 400..800 modes on [1e-5, 1] / Mpc, x_e / T_m tables in HyRex's padded
 layout, unlensed TT/TE/EE to l = 2500 -- with the C_l gradient with respect
 to (h, omega_b, omega_cdm, A_s, n_s, tau_reio).  One step = the
-perturbations of all 9 gradient descriptors of the 64 cosmologies (the base
-and +-1e-4 relative in h, omega_b, omega_cdm, tau_reio: one persistent
-launch) + the line of sight over all 576 descriptors + gradient assembly
-(central differences; exact A_s / n_s derivatives from the same
-line-of-sight launch).  --grad tangent integrates only the base cosmologies
-and carries the four directions' forward-mode sensitivities instead (one
-tangent launch); the line also reports that mode's own measurement.  Inputs
-are seeded
+perturbations of the 64 base cosmologies with the forward-mode
+sensitivities of h, omega_b, omega_cdm and tau_reio (one persistent tangent
+launch that also writes the tables of the +-1e-4 relative variants) + the
+line of sight over all 576 descriptors + gradient assembly (exact A_s / n_s
+derivatives from the same line-of-sight launch).  --grad fd integrates every
+variant on its own instead (central differences of whole solves: faster on
+the GPU, but the variants' different step sequences put up to tens of per
+cent of noise into the low-l derivatives); the line reports the other
+mode's measurement too.  Inputs are seeded
 synthetic (numpy default_rng(20261203 + rank)); background tables are
 produced on the host before timing (they are inputs of this path).
 
@@ -50,7 +51,7 @@ def parse():
     ap.add_argument("--n-cosmo", type=int, default=64)
     ap.add_argument("--l-max", type=int, default=2500)
     ap.add_argument("--e2e-steps", type=int, default=1)
-    ap.add_argument("--grad", default="fd", choices=["tangent", "fd"])
+    ap.add_argument("--grad", default="tangent", choices=["tangent", "fd"])
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch choices instead of the tuned ones")
     ap.add_argument("--plain-sample", type=int, default=8,
@@ -408,7 +409,11 @@ def main():
     from abcmb_b200 import configs, gradients
     t_build = time.perf_counter()
     w = configs.c4(n_cosmo=args.n_cosmo, l_max=args.l_max, seed=configs.SEED + rank)
-    gw = gradients.expand(w, processes=os.cpu_count() or 1, mode=args.grad)
+    # the nine descriptors of every cosmology; the tangent view shares them
+    # (items for the base cosmologies only)
+    gw_fd = gradients.expand(w, processes=os.cpu_count() or 1, mode="fd")
+    gw_t = gradients.as_tangent(gw_fd)
+    gw, gw_other = (gw_t, gw_fd) if args.grad == "tangent" else (gw_fd, gw_t)
     t_build = time.perf_counter() - t_build
 
     import torch
@@ -599,11 +604,10 @@ def main():
             line["hyrex_forward"] = hyrex_timing(w, dev)
         except Exception as ex:                            # an extra measurement never costs the line
             line["hyrex_forward"] = {"error": str(ex)[:200]}
-        if gw.mode == "fd":
-            tan = tangent_extra(gw, w, db, lr, st, dev, stream, assemble, out_cl, out_grad)
-            tan_cl0, tan_grad0 = tan.pop("cl0"), tan.pop("grad0")
-            tan["vs_fd_step"] = ms / tan["ms_per_step"]
-            line["grad_tangent"] = tan
+        other = mode_extra(gw_other, w, db, lr, st, dev, stream, assemble, out_cl, out_grad)
+        oth_cl0, oth_grad0 = other.pop("cl0"), other.pop("grad0")
+        other["step_time_vs_headline"] = other["ms_per_step"] / ms
+        line["grad_" + gw_other.mode] = other
         plain = plain_gpu_fwd_fd(gw, w, dev, stream, args.plain_sample)
         plain["batched_over_plain"] = value / plain["value"]
         line["plain_gpu_fwd_fd"] = plain
@@ -615,33 +619,30 @@ def main():
             o = np.load(ref_file)
             line["err_vs_oracle"] = err_vs_oracle(res_cl.numpy()[0], res_grad.numpy()[0], o["cl"], o["grad"])
             line["err_vs_oracle"]["gpu_grad"] = GRAD_DESC[gw.mode]
-            if "grad_tangent" in line:
-                line["grad_tangent"]["err_vs_oracle"] = err_vs_oracle(tan_cl0, tan_grad0, o["cl"], o["grad"])
+            line["grad_" + gw_other.mode]["err_vs_oracle"] = err_vs_oracle(oth_cl0, oth_grad0, o["cl"], o["grad"])
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
 
-def tangent_extra(gw, w, db, lr, st, dev, stream, assemble, out_cl, out_grad, steps: int = 2) -> dict:
-    """The same step with the tangent kernel (abcmb_pert_forward_tangent over
-    the base cosmologies, the variants' tables from the tangents), on the
-    same descriptors and buffers: CUDA-event time of `steps` steps after one
-    warm-up, the tangent statistics, and C_l / gradient of cosmology 0."""
+def mode_extra(go, w, db, lr, st, dev, stream, assemble, out_cl, out_grad, steps: int = 2) -> dict:
+    """The same step in the other gradient mode (go: the tangent or the
+    finite-difference view of the same descriptors), on the same buffers:
+    CUDA-event time of `steps` steps after one warm-up, the tangent
+    statistics, and C_l / gradient of cosmology 0."""
     import dataclasses as dc
     import torch
-    from abcmb_b200 import gradients
-    gt = gradients.as_tangent(gw)
-    tdb = dc.replace(db, batch=gt.batch,
-                     items=torch.from_numpy(gt.batch.items.reshape(-1).copy()).to(dev),
-                     kstat=torch.zeros(gt.batch.n_items * 24, dtype=torch.uint8, device=dev))
+    tdb = dc.replace(db, batch=go.batch,
+                     items=torch.from_numpy(go.batch.items.reshape(-1).copy()).to(dev),
+                     kstat=torch.zeros(go.batch.n_items * 24, dtype=torch.uint8, device=dev))
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     pert = []
 
     def one(rec):
         if rec:
             ev[2].record(stream)
-        tdb.pert_forward_tangent(st, gt.dirs, gt.n_dir, gt.rel_step, stream)
+        tdb.pert_forward_grad(go, st, stream)
         if rec:
             ev[3].record(stream)
         lr.run(stream)
@@ -658,12 +659,14 @@ def tangent_extra(gw, w, db, lr, st, dev, stream, assemble, out_cl, out_grad, st
     ev[1].record(stream)
     torch.cuda.synchronize(dev)
     ms = ev[0].elapsed_time(ev[1]) / steps
-    ts = tdb.tstat.cpu().numpy().reshape(-1, 2)[:gt.batch.n_items]
     nb = len(w.params_in)
-    return {"value": nb / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms, "steps": steps,
-            "pert_launch_ms": float(np.mean(pert)), "items": int(gt.batch.n_items),
-            "chord_iterations_per_item": float(ts[:, 0].mean()), "unconverged_stage_solves": int(ts[:, 1].sum()),
-            "cl0": out_cl[0].cpu().numpy(), "grad0": out_grad[0].cpu().numpy()}
+    res = {"grad": GRAD_DESC[go.mode], "value": nb / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms,
+           "steps": steps, "pert_launch_ms": float(np.mean(pert)), "items": int(go.batch.n_items),
+           "cl0": out_cl[0].cpu().numpy(), "grad0": out_grad[0].cpu().numpy()}
+    if go.mode == "tangent":
+        ts = tdb.tstat.cpu().numpy().reshape(-1, 2)[:go.batch.n_items]
+        res.update(chord_iterations_per_item=float(ts[:, 0].mean()), unconverged_stage_solves=int(ts[:, 1].sum()))
+    return res
 
 
 def err_vs_oracle(cl, grad, cl_o, grad_o) -> dict:
