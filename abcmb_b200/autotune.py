@@ -7,7 +7,9 @@ The perturbation launch has choices that change only its speed:
     instantiation (two blocks per SM without a register cap, or three
     blocks per SM at 168 registers; abcmb_set_pert_variant);
   * the tangent kernel (abcmb_pert_forward_tangent): warps per block (0 =
-    the count with the most resident warps per SM, or 1..4).
+    the count with the most resident warps per SM, or 1..4);
+  * the record and replay launches of abcmb_pert_forward_ind: the forward
+    kernel's two knobs, tuned on the ind workload (its own key).
 
 Every choice gives bit-identical results -- each (cosmology, k) item is one
 warp's independent computation -- so the tuner only measures.  A choice is
@@ -27,7 +29,7 @@ import os
 
 FD_CANDIDATES = [(w, v) for v in (1, 2) for w in (4, 3, 2, 1)]      # (warps per block, variant)
 TANGENT_CANDIDATES = [0, 4, 3, 2, 1]                                  # warps per block, 0 = by occupancy
-DEFAULT = {"fd": (4, 0), "tangent": 0}
+DEFAULT = {"fd": (4, 0), "ind": (4, 0), "tangent": 0}
 SAMPLE_ITEMS = 40000       # items timed per candidate at most
 
 
@@ -47,7 +49,7 @@ def apply(kind: str, choice) -> None:
     """Set the C ABI's knobs to a choice (DEFAULT restores the defaults)."""
     from . import _lib
     lib = _lib.load()
-    if kind == "fd":
+    if kind in ("fd", "ind"):
         w, v = choice
         _lib.check(lib.abcmb_set_pert_warps_per_block(int(w)), "abcmb_set_pert_warps_per_block")
         _lib.check(lib.abcmb_set_pert_variant(int(v)), "abcmb_set_pert_variant")
@@ -97,7 +99,7 @@ class Autotuner:
         if got is not None:
             apply(kind, got)
             return got
-        cands = FD_CANDIDATES if kind == "fd" else TANGENT_CANDIDATES
+        cands = TANGENT_CANDIDATES if kind == "tangent" else FD_CANDIDATES
         times = {}
         for c in cands:
             times[c] = self._time(kind, c, run, repeats)
@@ -130,6 +132,7 @@ def tune_batch(db, gw, settings, tuner: Autotuner = None, sample_items: int = SA
     remember and apply the fastest.  Returns (kind, key, choice)."""
     import dataclasses
 
+    import numpy as np
     import torch
 
     from .packing import KSTAT_DTYPE
@@ -142,12 +145,19 @@ def tune_batch(db, gw, settings, tuner: Autotuner = None, sample_items: int = SA
     if tuner.lookup(key) is not None:
         return kind, key, tuner.tune(kind, key)
     stride = max(1, b.n_items // sample_items)
-    items = b.items[::stride].copy()
-    sb = dataclasses.replace(b, items=items)
-    sdb = dataclasses.replace(db, batch=sb, items=torch.from_numpy(items.reshape(-1)).to(db.device),
+    if kind == "ind":
+        # whole groups: a strided sample of the base items and their variants
+        from .gradients import ind_subset
+        sgw = ind_subset(gw, np.arange(0, gw.n_base_items, stride))
+        sb = sgw.batch
+        items = sb.items
+    else:
+        items = b.items[::stride].copy()
+        sb = dataclasses.replace(b, items=items)
+        sgw = dataclasses.replace(gw, batch=sb)
+    sdb = dataclasses.replace(db, batch=sb, items=torch.from_numpy(items.reshape(-1).copy()).to(db.device),
                               kstat=torch.zeros(len(items) * KSTAT_DTYPE.itemsize, dtype=torch.uint8,
                                                 device=db.device))
-    sgw = dataclasses.replace(gw, batch=sb)
 
     def run():
         sdb.pert_forward_grad(sgw, settings)

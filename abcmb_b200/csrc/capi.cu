@@ -17,6 +17,11 @@ cudaError_t launch_pert_tangent(int n_cosmo, const abcmb_cosmo* cosmo, const dou
                                 int n_items, const int32_t* items, int nd, const int32_t* dirs, double tscale,
                                 const abcmb_pert_settings& s, double* pt, abcmb_kstat* kstat, int32_t* tstat,
                                 void* ws, cudaStream_t stream, int* grid_out, int* warps_out);
+int64_t pert_ind_workspace_bytes(int n_cosmo, int n_base, int max_steps);
+cudaError_t launch_pert_ind(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
+                            int n_base, int n_var, const int32_t* items, const int32_t* var_base,
+                            const abcmb_pert_settings& s, double* pt, abcmb_kstat* kstat, void* ws,
+                            cudaStream_t stream, int warps_per_block, int* grid_out);
 int64_t los_workspace_bytes(int n_cosmo, int max_nk, int nkt, int n_ell_tab, int n_save, int precision);
 cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_cosmo* cosmo_host,
                        const double* tables, const double* kbuf, const double* pt, const double* kt,
@@ -249,6 +254,34 @@ int abcmb_pert_forward_tangent(int n_cosmo, const abcmb_cosmo* cosmo_dev, const 
                                              workspace_dev,
                                              static_cast<cudaStream_t>(stream), &g_last_grid, &warps);
   if (e != cudaSuccess) return cuda_fail(e, "abcmb_pert_forward_tangent");
+  return ABCMB_OK;
+}
+
+int64_t abcmb_pert_ind_workspace_size(int n_cosmo, int n_base_items, int max_steps) {
+  if (n_cosmo <= 0 || n_base_items < 0 || max_steps <= 0)
+    return fail(ABCMB_ERR_ARG, "abcmb_pert_ind_workspace_size: bad argument");
+  return abcmb::pert_ind_workspace_bytes(n_cosmo, n_base_items, max_steps);
+}
+
+int abcmb_pert_forward_ind(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* tables_dev, const double* k_dev,
+                           int n_base_items, int n_var_items, const int32_t* items_dev, const int32_t* var_base_dev,
+                           const abcmb_pert_settings* settings, double* pt_dev, abcmb_kstat* kstat_dev,
+                           void* workspace_dev, int64_t workspace_bytes, void* stream) {
+  if (n_cosmo <= 0 || n_base_items < 0 || n_var_items < 0 || !cosmo_dev || !tables_dev || !k_dev || !settings ||
+      !pt_dev || !kstat_dev || (n_base_items + n_var_items > 0 && !items_dev) || (n_var_items > 0 && !var_base_dev))
+    return fail(ABCMB_ERR_ARG, "abcmb_pert_forward_ind: null argument");
+  if (settings->max_ny <= 0 || settings->n_save < 2 || settings->max_steps <= 0)
+    return fail(ABCMB_ERR_ARG, "abcmb_pert_forward_ind: settings.max_ny / n_save / max_steps");
+  if (n_var_items > 0 && n_base_items == 0)
+    return fail(ABCMB_ERR_ARG, "abcmb_pert_forward_ind: variant items without base items");
+  if (!workspace_dev ||
+      workspace_bytes < abcmb::pert_ind_workspace_bytes(n_cosmo, n_base_items, settings->max_steps))
+    return fail(ABCMB_ERR_WORKSPACE, "abcmb_pert_forward_ind: workspace too small");
+  if (n_base_items + n_var_items == 0) return ABCMB_OK;
+  cudaError_t e = abcmb::launch_pert_ind(n_cosmo, cosmo_dev, tables_dev, k_dev, n_base_items, n_var_items, items_dev,
+                                         var_base_dev, *settings, pt_dev, kstat_dev, workspace_dev,
+                                         static_cast<cudaStream_t>(stream), g_warps_per_block, &g_last_grid);
+  if (e != cudaSuccess) return cuda_fail(e, "abcmb_pert_forward_ind");
   return ABCMB_OK;
 }
 

@@ -957,6 +957,16 @@ struct PertArgs {
   double tscale;           // tangent size relative to the state's (atol of the tangent solves x tscale)
   const int32_t* dirs;     // [n_cosmo][ND_MAX][2] (plus, minus) descriptors
   int32_t* tstat;          // [n_items][2] or null
+  // internal numerical differentiation: the base items' accepted steps (end
+  // time, chord iterations of the six implicit stages, 4 bits each),
+  // recorded by one launch and replayed by the variants' launch
+  double* rec_t1;          // [n_base][rec_cap]
+  int32_t* rec_it;         // [n_base][rec_cap]
+  int32_t* rec_n;          // [n_base] accepted steps, -1 if the base item failed
+  int rec_cap;
+  int n_base;              // replay: the record launch's items
+  const int32_t* base_items;
+  const int32_t* var_base; // replay: [n_items] index of each variant item's base item
 };
 
 __device__ __forceinline__ TanMem tan_mem(const WarpMem& m, const PertArgs& P) {
@@ -1228,7 +1238,15 @@ constexpr int PERT_THROUGHPUT_ITEMS_PER_WARP = 16;
 
 
 
-template <bool TAN>
+// IND: 0 = the adaptive integration; 1 = the same, recording every accepted
+// step (end time and the chord-iteration count of each implicit stage) of
+// the item into the record buffers; 2 = replay: the item (a variant of a base
+// cosmology) takes its base item's recorded step ends and per-stage chord
+// iteration counts instead of the step-size controller and the termination
+// test, so every variant follows one fixed discrete map and the central
+// difference of two variants is a smooth function of the parameter step
+// (internal numerical differentiation, Bock 1981: no step-sequence noise).
+template <bool TAN, int IND = 0>
 __device__ __forceinline__ void pert_body(const PertArgs& P) {
   extern __shared__ double smem[];
   __shared__ RowTab R;
@@ -1306,11 +1324,27 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
           }
         }
       }
+      if constexpr (IND == 2) {
+        // a variant replays a base item of the same k and state layout
+        const int rb = P.var_base[item];
+        bad = bad || rb < 0 || rb >= P.n_base;
+        if (!bad) {
+          const int cb = P.base_items[2 * rb];
+          bad = cb < 0 || cb >= P.n_cosmo || P.base_items[2 * rb + 1] != ik;
+          if (!bad) {
+            const abcmb_cosmo& cv = P.cosmo[cb];
+            bad = cv.ny != c.ny || cv.nk != c.nk || cv.has_ncdm != c.has_ncdm || cv.lmax_g != c.lmax_g ||
+                  cv.lmax_pol_g != c.lmax_pol_g || cv.lmax_nu != c.lmax_nu || cv.lmax_ncdm != c.lmax_ncdm ||
+                  ik < 0 || ik >= c.nk || P.kbuf[cv.off_k + ik] != P.kbuf[c.off_k + ik];
+          }
+        }
+      }
       if (bad) {
         if (lane == 0) {
           abcmb_kstat st{ABCMB_STATUS_BAD_LAYOUT, 0, 0, 0, 0.};
           P.kstat[item] = st;
           if (TAN && P.tstat) P.tstat[2 * item] = P.tstat[2 * item + 1] = 0;
+          if (IND == 1) P.rec_n[item] = -1;
         }
         continue;
       }
@@ -1361,14 +1395,29 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
     double t1 = fmin(t0 + S.dt0, 0.0);
     double prev_inv = 1.0, prev_prev_inv = 1.0;
     int isave = 0, nsteps = 0, nacc = 0, nrej = 0, nnewton = 0, status = ABCMB_STATUS_OK;
+    unsigned itbits = 0u;            // chord iterations of the step's stages (record / replay)
+    int rbase = 0, rn = 0;           // replay: the base item and its recorded steps
+    if constexpr (IND == 2) {
+      rbase = P.var_base[item];
+      rn = P.rec_n[rbase];
+      if (rn <= 0) status = ABCMB_STATUS_NONFINITE;      // the base item failed: nothing to replay
+    }
     CoreRow cr;
     core_row_at(L, R, m, m.SB(), lane, cr);
     apply_A(L, m, R, cr, m.SB(), m.y0(), m.F(), nullptr, ncdm, lane);   // FSAL stage 1
     if constexpr (TAN) tangent_init(L, m, R, P, ci, k, ik2, lna_start, lane);
 
-    while (t0 < 0.0) {
+    while (t0 < 0.0 && status == ABCMB_STATUS_OK) {
       PERT_PHASE(7);
-      if (nsteps >= S.max_steps) { status = ABCMB_STATUS_MAX_STEPS; break; }
+      if constexpr (IND == 2) {
+        if (nsteps >= rn) { status = ABCMB_STATUS_NONFINITE; break; }
+        t1 = P.rec_t1[(int64_t)rbase * P.rec_cap + nsteps];
+        itbits = (unsigned)P.rec_it[(int64_t)rbase * P.rec_cap + nsteps];
+        if (!(t1 > t0)) { status = ABCMB_STATUS_DT_UNDERFLOW; break; }
+      } else {
+        if (nsteps >= S.max_steps) { status = ABCMB_STATUS_MAX_STEPS; break; }
+        itbits = 0u;
+      }
       ++nsteps;
       const double h = t1 - t0;
       const double hg = h * KV_G;
@@ -1418,6 +1467,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
         PERT_PHASE(2);
         double diffsize = INFINITY, diffsize_prev;
         bool conv = false;
+        const int it_replay = (int)((itbits >> (4 * (i - 1))) & 15u);
         for (int it = 1; it <= root_max; ++it) {
           apply_A(L, m, R, cr, B, m.v(), m.r(), fi, ncdm, lane);    // residual A v - f
           PERT_PHASE(3);
@@ -1445,7 +1495,12 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
           diffsize = sqrt(ss * inv_n);
           ++nnewton;
           PERT_PHASE(5);
-          if (it >= 2) {
+          if constexpr (IND == 2) {
+            if (it >= it_replay) {
+              conv = true;
+              break;
+            }
+          } else if (it >= 2) {
             // optimistix very-chord termination, without divisions:
             // rate = d/dp; converged <=> 0 < rate < 1 and d rate / (1 - rate) < kappa
             //                        <=> 0 < d < dp and d^2 < kappa (dp - d);
@@ -1454,7 +1509,11 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
             const bool small = d < small_res;
             const bool converged = d > 0. && d < dp && d * d < kappa * (dp - d);
             const bool diverged = !(d <= 2. * dp);
-            if (small || converged) { conv = true; break; }
+            if (small || converged) {
+              if constexpr (IND == 1) itbits |= (unsigned)it << (4 * (i - 1));
+              conv = true;
+              break;
+            }
             if (diverged) break;
           }
         }
@@ -1490,7 +1549,13 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
         if (!isfinite(scaled)) scaled = INFINITY;
       }
       __syncwarp();
-      const bool keep = scaled < 1.0;
+      bool keep = scaled < 1.0;
+      if constexpr (IND == 2) {
+        // the base accepted this step: the variant takes it whatever its own
+        // error estimate says (a non-finite one still stops it)
+        keep = isfinite(scaled);
+        if (!keep) status = ABCMB_STATUS_NONFINITE;
+      }
       double inv = 1.0 / scaled;
       double f1v = (coeff1 == 0.) ? 1. : pow(inv, coeff1);
       double f2v = (coeff2 == 0.) ? 1. : pow(prev_inv, coeff2);
@@ -1500,6 +1565,12 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
       if (inv == 0. || isinf(inv)) inv = 1.;
       PERT_PHASE(6);
       if (keep) {
+        if constexpr (IND == 1) {
+          if (lane == 0) {
+            P.rec_t1[(int64_t)item * P.rec_cap + nacc] = t1;
+            P.rec_it[(int64_t)item * P.rec_cap + nacc] = (int32_t)itbits;
+          }
+        }
         ++nacc;
         if constexpr (TAN) {
           for (int q = 0; q < P.nd; ++q)
@@ -1540,7 +1611,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
       } else {
         ++nrej;
       }
-      if (t0 >= 0.0) break;
+      if (t0 >= 0.0 || IND == 2) continue;
       double tn = t0 + dt_new;
       if (tn > 0.0 - 1e-10) tn = keep ? 0.0 : t0 + 0.5 * (0.0 - t0);
       t1 = tn;
@@ -1555,6 +1626,7 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
       st.n_newton = nnewton;
       st.lna_start = lna_start;
       P.kstat[item] = st;
+      if (IND == 1) P.rec_n[item] = status == ABCMB_STATUS_OK ? nacc : -1;
       if (TAN && P.tstat) {
         const int* cnt = tan_mem(m, P).cnt();
         P.tstat[2 * item] = cnt[0];
@@ -1575,6 +1647,12 @@ namespace abcmb {
 template <int MIN_BLOCKS>
 __global__ void __launch_bounds__(PERT_THREADS_MAX, MIN_BLOCKS) pert_kernel(PertArgs P) {
   pert_body<false>(P);
+}
+
+// The record (IND = 1) and replay (IND = 2) integrations of abcmb_pert_forward_ind.
+template <int MIN_BLOCKS, int IND>
+__global__ void __launch_bounds__(PERT_THREADS_MAX, MIN_BLOCKS) pert_kernel_ind(PertArgs P) {
+  pert_body<false, IND>(P);
 }
 
 // The same integration with the tangents; shared memory (not registers)
@@ -1634,7 +1712,7 @@ cudaError_t launch_pert(int n_cosmo, const abcmb_cosmo* cosmo, const double* tab
   dim3 g1((NSTART + 255) / 256, n_cosmo);
   start_grid_kernel<<<g1, 256, 0, stream>>>(n_cosmo, cosmo, tables, aHg, f1g);
   start_lna1_kernel<<<(n_cosmo + 127) / 128, 128, 0, stream>>>(n_cosmo, f1g, s.R_tc, lna1);
-  PertArgs A;
+  PertArgs A{};
   A.n_cosmo = n_cosmo;
   A.n_items = n_items;
   A.max_ny = s.max_ny;
@@ -1684,6 +1762,106 @@ cudaError_t launch_pert(int n_cosmo, const abcmb_cosmo* cosmo, const double* tab
   return cudaGetLastError();
 }
 
+int64_t pert_ind_workspace_bytes(int n_cosmo, int n_base, int max_steps) {
+  int64_t b = pert_workspace_bytes(n_cosmo) + 256;                   // + the replay's queue counter
+  b += ((int64_t)n_base * max_steps * 8 + 255) / 256 * 256;          // recorded step ends
+  b += ((int64_t)n_base * max_steps * 4 + 255) / 256 * 256;          // recorded chord iterations
+  b += ((int64_t)n_base * 4 + 255) / 256 * 256;                      // recorded step counts
+  return b;
+}
+
+// abcmb_pert_forward_ind: the base items (the first n_base of items) are
+// integrated recording their accepted steps, then the variant items replay
+// their base item's steps; both launches in stream order on one queue each.
+cudaError_t launch_pert_ind(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
+                            int n_base, int n_var, const int32_t* items, const int32_t* var_base,
+                            const abcmb_pert_settings& s, double* pt, abcmb_kstat* kstat, void* ws,
+                            cudaStream_t stream, int warps_per_block, int* grid_out) {
+  if (warps_per_block < 1 || 32 * warps_per_block > PERT_THREADS_MAX) return cudaErrorInvalidConfiguration;
+  char* w = static_cast<char*>(ws);
+  int* queue = reinterpret_cast<int*>(w);
+  w += 256;
+  double* lna1 = reinterpret_cast<double*>(w);
+  w += ((int64_t)n_cosmo * 8 + 255) / 256 * 256;
+  double* aHg = reinterpret_cast<double*>(w);
+  w += ((int64_t)n_cosmo * NSTART * 8 + 255) / 256 * 256;
+  double* f1g = reinterpret_cast<double*>(w);
+  w += ((int64_t)n_cosmo * NSTART * 8 + 255) / 256 * 256;
+  int* queue2 = reinterpret_cast<int*>(w);
+  w += 256;
+  double* rec_t1 = reinterpret_cast<double*>(w);
+  w += ((int64_t)n_base * s.max_steps * 8 + 255) / 256 * 256;
+  int32_t* rec_it = reinterpret_cast<int32_t*>(w);
+  w += ((int64_t)n_base * s.max_steps * 4 + 255) / 256 * 256;
+  int32_t* rec_n = reinterpret_cast<int32_t*>(w);
+  cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int), stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(queue2, 0, sizeof(int), stream);
+  if (e != cudaSuccess) return e;
+  dim3 g1((NSTART + 255) / 256, n_cosmo);
+  start_grid_kernel<<<g1, 256, 0, stream>>>(n_cosmo, cosmo, tables, aHg, f1g);
+  start_lna1_kernel<<<(n_cosmo + 127) / 128, 128, 0, stream>>>(n_cosmo, f1g, s.R_tc, lna1);
+  PertArgs A{};
+  A.n_cosmo = n_cosmo;
+  A.max_ny = s.max_ny;
+  A.ncm = s.any_ncdm ? 22 : 13;
+  A.cosmo = cosmo;
+  A.tables = tables;
+  A.kbuf = kbuf;
+  A.pt = pt;
+  A.aHg = aHg;
+  A.lna1 = lna1;
+  A.s = s;
+  A.nd = 0;
+  A.tscale = 1.;
+  A.rec_t1 = rec_t1;
+  A.rec_it = rec_it;
+  A.rec_n = rec_n;
+  A.rec_cap = s.max_steps;
+  A.n_base = n_base;
+  A.base_items = items;
+  A.var_base = var_base;
+  const int threads = 32 * warps_per_block;
+  const size_t smem = (size_t)warps_per_block * pert_smem_per_warp(s.max_ny, A.ncm);
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int variant = pert_variant();
+  for (int pass = 0; pass < 2; ++pass) {
+    const int n_items = pass == 0 ? n_base : n_var;
+    if (n_items == 0) continue;
+    A.n_items = n_items;
+    A.items = pass == 0 ? items : items + 2 * (int64_t)n_base;
+    A.kstat = pass == 0 ? kstat : kstat + n_base;
+    A.queue = pass == 0 ? queue : queue2;
+    const bool throughput =
+        variant == 2 ||
+        (variant == 0 &&
+         (int64_t)n_items >= (int64_t)PERT_THROUGHPUT_ITEMS_PER_WARP * nsm * PERT_BLOCKS_LATENCY * warps_per_block);
+    const void* fn;
+    if (pass == 0)
+      fn = throughput ? (const void*)pert_kernel_ind<PERT_BLOCKS_THROUGHPUT, 1>
+                      : (const void*)pert_kernel_ind<PERT_BLOCKS_LATENCY, 1>;
+    else
+      fn = throughput ? (const void*)pert_kernel_ind<PERT_BLOCKS_THROUGHPUT, 2>
+                      : (const void*)pert_kernel_ind<PERT_BLOCKS_LATENCY, 2>;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    int grid = nsm * per_sm;
+    const int need = (n_items + warps_per_block - 1) / warps_per_block;
+    if (grid > need) grid = need;
+    if (grid < 1) grid = 1;
+    if (grid_out) *grid_out = grid;
+    void* args[] = {&A};
+    e = cudaLaunchKernel(fn, dim3(grid), dim3(threads), args, smem, stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaGetLastError();
+}
+
 size_t pert_tangent_smem_per_warp(int max_ny, int ncm, int nd) {
   return (warp_mem_doubles(max_ny, ncm) + tan_mem_doubles(max_ny, ncm, nd)) * sizeof(double);
 }
@@ -1709,7 +1887,7 @@ cudaError_t launch_pert_tangent(int n_cosmo, const abcmb_cosmo* cosmo, const dou
   dim3 g1((NSTART + 255) / 256, n_cosmo);
   start_grid_kernel<<<g1, 256, 0, stream>>>(n_cosmo, cosmo, tables, aHg, f1g);
   start_lna1_kernel<<<(n_cosmo + 127) / 128, 128, 0, stream>>>(n_cosmo, f1g, s.R_tc, lna1);
-  PertArgs A;
+  PertArgs A{};
   A.n_cosmo = n_cosmo;
   A.n_items = n_items;
   A.max_ny = s.max_ny;

@@ -115,11 +115,36 @@ class DeviceBatch:
                                             ctypes.c_void_p(st.cuda_stream))
         _lib.check(rc, "abcmb_pert_forward_tangent")
 
+    def pert_forward_ind(self, settings: CPertSettings, n_base: int, var_base: np.ndarray, stream=None):
+        """abcmb_pert_forward_ind: the batch's first n_base items are base
+        items (integrated, their steps recorded), the rest variant items
+        replaying the base item var_base (int32 [n_items - n_base]) names."""
+        lib = _lib.load()
+        st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        key = (var_base.ctypes.data, var_base.nbytes, int(n_base), int(settings.max_steps))
+        if getattr(self, "_ind_key", None) != key:
+            self.var_base = torch.from_numpy(np.ascontiguousarray(var_base, dtype=np.int32)).to(self.device)
+            nws = int(lib.abcmb_pert_ind_workspace_size(self.batch.n_cosmo, int(n_base), int(settings.max_steps)))
+            if nws < 0:
+                _lib.check(int(nws), "abcmb_pert_ind_workspace_size")
+            self.ws_ind = torch.empty(nws, dtype=torch.uint8, device=self.device)
+            self._ind_key = key
+        n_var = self.batch.n_items - int(n_base)
+        rc = lib.abcmb_pert_forward_ind(self.batch.n_cosmo, _ptr(self.cosmo), _ptr(self.tables), _ptr(self.kbuf),
+                                        int(n_base), n_var, _ptr(self.items), _ptr(self.var_base),
+                                        ctypes.byref(settings), _ptr(self.pt), _ptr(self.kstat), _ptr(self.ws_ind),
+                                        self.ws_ind.numel(), ctypes.c_void_p(st.cuda_stream))
+        _lib.check(rc, "abcmb_pert_forward_ind")
+
     def pert_forward_grad(self, gw, settings: CPertSettings, stream=None):
         """The perturbations of a gradient-expanded batch (gradients.expand):
-        one tangent launch, or every finite-difference variant integrated."""
+        one tangent launch, the record + replay launches of internal
+        numerical differentiation, or every finite-difference variant
+        integrated."""
         if gw.mode == "tangent":
             self.pert_forward_tangent(settings, gw.dirs, gw.n_dir, gw.rel_step, stream)
+        elif gw.mode == "ind":
+            self.pert_forward_ind(settings, gw.n_base_items, gw.var_base, stream)
         else:
             self.pert_forward(settings, stream)
 

@@ -15,6 +15,14 @@ own background tables.  Two ways to fill their PerturbationTables:
     tables are the first-order expansion around the base at their own save
     times.  One integration per (cosmology, k) instead of nine, and no
     step-sequence noise in the derivative.
+  mode="ind": internal numerical differentiation (abcmb_pert_forward_ind):
+    the base cosmology is integrated adaptively with its accepted steps
+    recorded, then every variant replays that discretisation (the same step
+    ends, the same chord iterations per stage).  The central difference is
+    then the derivative of one smooth discrete map -- the base's
+    integration, which is what the tangent mode differentiates too -- with
+    no step-sequence noise, at the cost of nine forward integrations of
+    which eight need no error control.
   mode="fd" (default): every variant is integrated on its own (central differences of
     whole solves, the gradient configuration's finite-difference check).
 
@@ -42,7 +50,7 @@ from .configs import GRAD_PARAMS, Workload
 
 FD_PARAMS = ("h", "omega_b", "omega_cdm", "tau_reion")
 REL_STEP = 1e-4
-MODES = ("tangent", "fd")
+MODES = ("tangent", "ind", "fd")
 MAX_TANGENTS = 4          # ABCMB_MAX_TANGENTS
 
 
@@ -75,6 +83,8 @@ class GradWorkload:
     dirs: np.ndarray = None  # tangent mode: int32 [n_descriptors, MAX_TANGENTS, 2] (plus, minus)
     n_dir: int = 0
     rel_step: float = REL_STEP
+    n_base_items: int = 0    # ind mode: the batch's first n_base_items items are the base items
+    var_base: np.ndarray = None  # ind mode: int32 [n_items - n_base_items] base item of each variant item
 
     def assemble(self, cl: np.ndarray, dcl_dns: np.ndarray):
         """cl, dcl_dns: (n_base * n_var, 3, n_l) -> C_l (n_base, 3, n_l), grad (n_base, 6, 3, n_l)."""
@@ -166,8 +176,13 @@ def expand(w: Workload, n_save: int = 500, processes: int = 0, rel_step: float =
         w.idx_min, w.idx_max, _ = sp.ell_index_range(bessel_mod.load().l_tab, int(w.specs["l_min"]), w.l_max,
                                                         w.lensing)
     w.batch = batch
-    return GradWorkload(base=w, variants=variants, batch=batch, n_var=len(variants[0]), mode=mode, dirs=dirs,
-                        n_dir=len(FD_PARAMS) if mode == "tangent" else 0, rel_step=rel_step)
+    gw = GradWorkload(base=w, variants=variants, batch=batch, n_var=len(variants[0]),
+                      mode="fd" if mode == "ind" else mode, dirs=dirs,
+                      n_dir=len(FD_PARAMS) if mode == "tangent" else 0, rel_step=rel_step)
+    if mode == "ind":
+        gw = as_ind(gw)
+        w.batch = gw.batch
+    return gw
 
 
 def as_tangent(gw: GradWorkload) -> GradWorkload:
@@ -179,7 +194,18 @@ def as_tangent(gw: GradWorkload) -> GradWorkload:
         return gw
     import dataclasses
     b = gw.batch
-    n = b.n_cosmo
+    base, dirs = _directions(gw)
+    src = b.items[:gw.n_base_items] if gw.mode == "ind" else b.items
+    items = src[base[src[:, 0]]].copy()
+    tb = dataclasses.replace(b, items=items)
+    return dataclasses.replace(gw, batch=tb, mode="tangent", dirs=dirs, n_dir=len(FD_PARAMS), n_base_items=0,
+                               var_base=None)
+
+
+
+def _directions(gw: GradWorkload):
+    """base mask over descriptors and the (plus, minus) table of each base."""
+    n = gw.batch.n_cosmo
     nvar = gw.n_var
     base = np.zeros(n, dtype=bool)
     dirs = np.full((n, MAX_TANGENTS, 2), -1, dtype=np.int32)
@@ -190,7 +216,49 @@ def as_tangent(gw: GradWorkload) -> GradWorkload:
             jp = next(j for j, v in enumerate(var) if v[0] == name and v[1] > 0)
             jm = next(j for j, v in enumerate(var) if v[0] == name and v[1] < 0)
             dirs[b0, q] = (b0 + jp, b0 + jm)
-    items = b.items[base[b.items[:, 0]]].copy()
-    tb = dataclasses.replace(b, items=items)
-    return dataclasses.replace(gw, batch=tb, mode="tangent", dirs=dirs, n_dir=len(FD_PARAMS))
+    return base, dirs
 
+
+def as_ind(gw: GradWorkload) -> GradWorkload:
+    """The internal-numerical-differentiation view of a finite-difference
+    expansion: the same descriptors and tables; work items = the base
+    cosmologies' items (in the expansion's queue order) followed, for each
+    of them in the same order, by its eight variants' items of the same k;
+    var_base names each variant item's base item."""
+    if gw.mode == "ind":
+        return gw
+    import dataclasses
+    b = gw.batch
+    base, dirs = _directions(gw)
+    all_items = b.items
+    if gw.mode == "tangent":
+        base_items = all_items
+    else:
+        base_items = all_items[base[all_items[:, 0]]]
+    nb = len(base_items)
+    nd = len(FD_PARAMS)
+    var_desc = dirs[base_items[:, 0], :nd, :].reshape(nb, 2 * nd)           # [nb, 8]
+    var_items = np.empty((nb, 2 * nd, 2), dtype=np.int32)
+    var_items[:, :, 0] = var_desc
+    var_items[:, :, 1] = base_items[:, 1:2]
+    items = np.concatenate([base_items, var_items.reshape(-1, 2)]).astype(np.int32)
+    var_base = np.repeat(np.arange(nb, dtype=np.int32), 2 * nd)
+    tb = dataclasses.replace(b, items=items)
+    return dataclasses.replace(gw, batch=tb, mode="ind", dirs=None, n_dir=0, n_base_items=nb, var_base=var_base)
+
+
+def ind_subset(gw: GradWorkload, sel) -> GradWorkload:
+    """An ind-mode workload restricted to the base items sel (indices into
+    the first n_base_items items) and their variants, in that order."""
+    import dataclasses
+    if gw.mode != "ind":
+        raise ValueError("ind_subset needs an ind-mode workload")
+    sel = np.asarray(sel, dtype=np.int64)
+    b = gw.batch
+    nb = gw.n_base_items
+    per = (b.n_items - nb) // max(nb, 1)
+    var = b.items[nb:].reshape(nb, per, 2)[sel].reshape(-1, 2)
+    items = np.concatenate([b.items[:nb][sel], var]).astype(np.int32)
+    tb = dataclasses.replace(b, items=items)
+    return dataclasses.replace(gw, batch=tb, n_base_items=len(sel),
+                               var_base=np.repeat(np.arange(len(sel), dtype=np.int32), per))

@@ -9,6 +9,7 @@
         python -m abcmb_b200.profile_case c4 40 --phases  # cycles per phase of pert_kernel
     python -m abcmb_b200.profile_case c4 16 --grad tangent   # the gradient batch: one tangent
     python -m abcmb_b200.profile_case c4 16 --grad fd        # launch, or every variant integrated
+    python -m abcmb_b200.profile_case c4 16 --grad ind       # record + replay launches
 
 Runs the perturbation launch twice (warm-up + measured) and, with --los, the
 line of sight twice, then checks the per-k status.  With --bg-only the batch
@@ -47,7 +48,7 @@ def main():
     ap.add_argument("--bg-only", action="store_true")
     ap.add_argument("--phases", action="store_true")
     ap.add_argument("--hyrex", action="store_true")
-    ap.add_argument("--grad", choices=["tangent", "fd"], default=None)
+    ap.add_argument("--grad", choices=["ind", "tangent", "fd"], default=None)
     a = ap.parse_args()
     import torch
     from . import configs, engine
@@ -82,7 +83,7 @@ def main():
     else:
         w.build()
     st = w.pert_settings()
-    db = engine.DeviceBatch.upload(w.batch)
+    db = engine.DeviceBatch.upload(gw.batch if gw is not None else w.batch)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     for i in range(2):

@@ -7,19 +7,29 @@ massive-neutrino count drawn from {0, 1, 3}, per-cosmology k grids of
 400..800 modes on [1e-5, 1] / Mpc, x_e / T_m tables in HyRex's padded
 layout, unlensed TT/TE/EE to l = 2500 -- with the C_l gradient with respect
 to (h, omega_b, omega_cdm, A_s, n_s, tau_reio).  One step = the
-perturbations of the 64 base cosmologies with the forward-mode
-sensitivities of h, omega_b, omega_cdm and tau_reio (one persistent tangent
-launch that also writes the tables of the +-1e-4 relative variants) + the
-line of sight over all 576 descriptors + gradient assembly (exact A_s / n_s
-derivatives from the same line-of-sight launch).  --grad fd integrates every
-variant on its own instead (central differences of whole solves: faster on
-the GPU, but the variants' different step sequences put up to tens of per
-cent of noise into the low-l derivatives); the line reports the other
-mode's measurement too.  Inputs are seeded
-synthetic (numpy default_rng(20261203 + rank)); background tables are
+perturbations of all 9 gradient descriptors of the 64 cosmologies (the base
+and +-1e-4 relative in h, omega_b, omega_cdm, tau_reio) + the line of sight
+over all 576 descriptors + gradient assembly (central differences; exact
+A_s / n_s derivatives from the same line-of-sight launch).  The
+perturbations come from one of three gradient modes (--grad):
+
+  ind (default)  internal numerical differentiation: the base cosmologies
+                 integrated adaptively with their accepted steps recorded,
+                 then the eight variants of each (cosmology, k) replay that
+                 discretisation (two persistent launches);
+  tangent        the base cosmologies with the forward-mode sensitivities
+                 of the four parameters carried along their steps (one
+                 launch that also writes the variants' tables);
+  fd             every variant integrated adaptively on its own (central
+                 differences of whole solves: the variants' different step
+                 sequences put up to tens of per cent of noise into the
+                 low-l derivatives).
+
+The line carries the other two modes' measurements on the same descriptors
+too.  Inputs are seeded synthetic (numpy default_rng(20261203 + rank)); background tables are
 produced on the host before timing (they are inputs of this path).
 
-  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--grad tangent|fd]
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--grad ind|tangent|fd]
 """
 from __future__ import annotations
 
@@ -51,7 +61,7 @@ def parse():
     ap.add_argument("--n-cosmo", type=int, default=64)
     ap.add_argument("--l-max", type=int, default=2500)
     ap.add_argument("--e2e-steps", type=int, default=1)
-    ap.add_argument("--grad", default="tangent", choices=["tangent", "fd"])
+    ap.add_argument("--grad", default="ind", choices=["ind", "tangent", "fd"])
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch choices instead of the tuned ones")
     ap.add_argument("--plain-sample", type=int, default=8,
@@ -66,6 +76,8 @@ def parse():
 
 GRAD_DESC = {"tangent": "forward-mode tangents of (h,ob,oc,tau) in one integration per (cosmology,k), variants' "
                         "tables at rel step 1e-4 from them; exact A_s,n_s",
+             "ind": "central FD rel 1e-4 (h,ob,oc,tau), internal numerical differentiation: variants replay "
+                    "the base's recorded steps and chord iterations; exact A_s,n_s",
              "fd": "central FD rel 1e-4 (h,ob,oc,tau): every variant integrated; exact A_s,n_s"}
 
 
@@ -409,11 +421,12 @@ def main():
     from abcmb_b200 import configs, gradients
     t_build = time.perf_counter()
     w = configs.c4(n_cosmo=args.n_cosmo, l_max=args.l_max, seed=configs.SEED + rank)
-    # the nine descriptors of every cosmology; the tangent view shares them
-    # (items for the base cosmologies only)
+    # the nine descriptors of every cosmology; the tangent and ind views
+    # share them (their own work-item lists)
     gw_fd = gradients.expand(w, processes=os.cpu_count() or 1, mode="fd")
-    gw_t = gradients.as_tangent(gw_fd)
-    gw, gw_other = (gw_t, gw_fd) if args.grad == "tangent" else (gw_fd, gw_t)
+    views = {"fd": gw_fd, "tangent": gradients.as_tangent(gw_fd), "ind": gradients.as_ind(gw_fd)}
+    gw = views[args.grad]
+    gw_others = [views[m] for m in ("ind", "tangent", "fd") if m != args.grad]
     t_build = time.perf_counter() - t_build
 
     import torch
@@ -471,8 +484,9 @@ def main():
         t_tune = time.perf_counter()
         kind, key, choice = autotune.tune_batch(db, gw, st)
         launch = {"tuned": True, "key": key, "choice": list(choice) if isinstance(choice, tuple) else choice,
-                  "what": "[warps per block, variant 1 = 2 blocks/SM, 2 = 3 blocks/SM]" if kind == "fd"
-                  else "warps per block (0 = by occupancy)", "tune_s": time.perf_counter() - t_tune}
+                  "what": "warps per block (0 = by occupancy)" if kind == "tangent"
+                  else "[warps per block, variant 1 = 2 blocks/SM, 2 = 3 blocks/SM]",
+                  "tune_s": time.perf_counter() - t_tune}
 
     pert_ms = []
 
@@ -516,9 +530,12 @@ def main():
     host_tab = torch.from_numpy(b.tables).pin_memory()
     host_k = torch.from_numpy(b.kbuf).pin_memory()
     host_items = torch.from_numpy(b.items.reshape(-1).copy()).pin_memory()
+    host_in = [(db.cosmo, host_cos), (db.tables, host_tab), (db.kbuf, host_k), (db.items, host_items)]
+    if gw.mode == "ind":
+        host_in.append((db.var_base, torch.from_numpy(gw.var_base.copy()).pin_memory()))
     res_cl = torch.empty(out_cl.shape, dtype=torch.float64).pin_memory()
     res_grad = torch.empty(out_grad.shape, dtype=torch.float64).pin_memory()
-    h2d = sum(t.numel() * t.element_size() for t in (host_cos, host_tab, host_k, host_items))
+    h2d = sum(h.numel() * h.element_size() for _, h in host_in)
     d2h = res_cl.numel() * 8 + res_grad.numel() * 8
     barrier()
     torch.cuda.synchronize(dev)
@@ -526,10 +543,8 @@ def main():
     x1 = torch.cuda.Event(enable_timing=True)
     x0.record(stream)
     for _ in range(args.e2e_steps):
-        db.cosmo.copy_(host_cos, non_blocking=True)
-        db.tables.copy_(host_tab, non_blocking=True)
-        db.kbuf.copy_(host_k, non_blocking=True)
-        db.items.copy_(host_items, non_blocking=True)
+        for d, h in host_in:
+            d.copy_(h, non_blocking=True)
         step()
         res_cl.copy_(out_cl, non_blocking=True)
         res_grad.copy_(out_grad, non_blocking=True)
@@ -568,6 +583,7 @@ def main():
                                      __import__("ctypes").c_void_p(stream.cuda_stream))
     achieved = flops / (pert_avg / 1000.0) / 1e12
     traffic = None
+    kname = {"tangent": "pert_kernel_tangent", "ind": "pert_kernel_ind", "fd": "pert_kernel"}[gw.mode]
     tfile = os.path.join(ROOT, "profiles", ("pert_kernel_tangent" if gw.mode == "tangent" else "pert_kernel")
                          + "_traffic.json")
     if os.path.isfile(tfile):
@@ -576,7 +592,7 @@ def main():
             traffic = tj["bytes_per_item"] * b.n_items
         except (ValueError, KeyError):
             traffic = None
-    roofline = {"bound": "fp64", "kernel": "pert_kernel_tangent" if gw.mode == "tangent" else "pert_kernel",
+    roofline = {"bound": "fp64", "kernel": kname,
                 "achieved": achieved,
                 "peak": peak.value if rc == 0 else None, "unit": "TFLOP/s",
                 "frac": (achieved / peak.value) if rc == 0 and peak.value > 0 else None,
@@ -586,8 +602,9 @@ def main():
                 "flops_def": flops_def, "launch_ms": pert_avg,
                 "hbm_gbs_peak": _peak_hbm()[0], "hbm_gbs_peak_source": _peak_hbm()[1]}
     # our kernel launches per step: pert (2 start kernels + the persistent
-    # kernel) + 5 per line-of-sight chunk of engine.LOS_CHUNK cosmologies
-    launches = 3 + 5 * ((b.n_cosmo + engine.LOS_CHUNK - 1) // engine.LOS_CHUNK)
+    # kernel, two of them -- record and replay -- in ind mode) + 5 per
+    # line-of-sight chunk of engine.LOS_CHUNK cosmologies
+    launches = (4 if gw.mode == "ind" else 3) + 5 * ((b.n_cosmo + engine.LOS_CHUNK - 1) // engine.LOS_CHUNK)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -604,10 +621,12 @@ def main():
             line["hyrex_forward"] = hyrex_timing(w, dev)
         except Exception as ex:                            # an extra measurement never costs the line
             line["hyrex_forward"] = {"error": str(ex)[:200]}
-        other = mode_extra(gw_other, w, db, lr, st, dev, stream, assemble, out_cl, out_grad)
-        oth_cl0, oth_grad0 = other.pop("cl0"), other.pop("grad0")
-        other["step_time_vs_headline"] = other["ms_per_step"] / ms
-        line["grad_" + gw_other.mode] = other
+        others = {}
+        for go in gw_others:
+            other = mode_extra(go, w, db, lr, st, dev, stream, assemble, out_cl, out_grad)
+            others[go.mode] = (other.pop("cl0"), other.pop("grad0"))
+            other["step_time_vs_headline"] = other["ms_per_step"] / ms
+            line["grad_" + go.mode] = other
         plain = plain_gpu_fwd_fd(gw, w, dev, stream, args.plain_sample)
         plain["batched_over_plain"] = value / plain["value"]
         line["plain_gpu_fwd_fd"] = plain
@@ -619,7 +638,8 @@ def main():
             o = np.load(ref_file)
             line["err_vs_oracle"] = err_vs_oracle(res_cl.numpy()[0], res_grad.numpy()[0], o["cl"], o["grad"])
             line["err_vs_oracle"]["gpu_grad"] = GRAD_DESC[gw.mode]
-            line["grad_" + gw_other.mode]["err_vs_oracle"] = err_vs_oracle(oth_cl0, oth_grad0, o["cl"], o["grad"])
+            for mode, (oc, og) in others.items():
+                line["grad_" + mode]["err_vs_oracle"] = err_vs_oracle(oc, og, o["cl"], o["grad"])
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -627,7 +647,7 @@ def main():
 
 
 def mode_extra(go, w, db, lr, st, dev, stream, assemble, out_cl, out_grad, steps: int = 2) -> dict:
-    """The same step in the other gradient mode (go: the tangent or the
+    """The same step in another gradient mode (go: the ind, tangent or
     finite-difference view of the same descriptors), on the same buffers:
     CUDA-event time of `steps` steps after one warm-up, the tangent
     statistics, and C_l / gradient of cosmology 0."""

@@ -378,6 +378,43 @@ int abcmb_pert_forward_tangent(int n_cosmo, const abcmb_cosmo* cosmo_dev,
                                void* stream);
 
 /*
+ * abcmb_pert_forward for finite-difference variants by internal numerical
+ * differentiation (H. G. Bock, "Numerical treatment of inverse problems in
+ * chemical reaction kinetics", 1981): the variants replay their base item's
+ * discretisation instead of choosing their own.  Central differences of
+ * whole adaptive solves (what the reference's finite-difference checks of
+ * its jax gradients compute) pick up the noise of the variants' different
+ * step sequences; a replayed variant takes exactly its base item's accepted
+ * step ends and the number of chord iterations of each stage, so plus and
+ * minus are one smooth discrete map evaluated at two parameter points and
+ * their difference converges to the derivative of the base's integration
+ * (the quantity jax.jacfwd through diffrax computes, abcmb/main.py:111).
+ *   items_dev     [n_base_items + n_var_items] int32 x2 (cosmology, k index):
+ *                 first the base items, then the variant items
+ *   var_base_dev  [n_var_items] int32: index (0..n_base_items-1) of the base
+ *                 item each variant item replays; the variant must have the
+ *                 base's state layout and the same k (ABCMB_STATUS_BAD_LAYOUT
+ *                 otherwise)
+ *   kstat_dev     [n_base_items + n_var_items]; a variant whose base failed
+ *                 reports ABCMB_STATUS_NONFINITE; variants report no rejected
+ *                 steps
+ * The base items are integrated exactly as abcmb_pert_forward does (same
+ * tables, same step counts) while their accepted steps are recorded, then
+ * the variants replay them: two launches in stream order.  Workspace:
+ * abcmb_pert_ind_workspace_size(n_cosmo, n_base_items, settings.max_steps)
+ * (12 bytes per base item and step allowed).
+ */
+int64_t abcmb_pert_ind_workspace_size(int n_cosmo, int n_base_items, int max_steps);
+int abcmb_pert_forward_ind(int n_cosmo, const abcmb_cosmo* cosmo_dev,
+                           const double* tables_dev, const double* k_dev,
+                           int n_base_items, int n_var_items, const int32_t* items_dev,
+                           const int32_t* var_base_dev,
+                           const abcmb_pert_settings* settings,
+                           double* pt_dev, abcmb_kstat* kstat_dev,
+                           void* workspace_dev, int64_t workspace_bytes,
+                           void* stream);
+
+/*
  * abcmb_pert_forward for callers that cannot allocate device memory (no
  * cudaMalloc, no workspace of their own: e.g. code inside a framework that
  * owns every device byte).  No counterpart in the reference.  Same inputs,

@@ -846,10 +846,25 @@ static void tangent_step(const abcmb_cosmo* c, const layout_t* L, const double* 
 }
 
 /* One k mode from its start time to lna = 0 (perturbations.py:250-316). */
+/* Internal numerical differentiation (H. G. Bock 1981): mode 1 records every
+ * accepted step of the integration (its end time, and the chord iterations
+ * of the six implicit stages, 4 bits each); mode 2 replays a record: the
+ * step ends and iteration counts are taken from it instead of the step-size
+ * controller and the termination test, and every step is accepted (a
+ * non-finite error estimate stops the item). */
+typedef struct {
+  int mode;        /* 0 none, 1 record, 2 replay */
+  double* t1;      /* [cap] step ends      */
+  int32_t* it;     /* [cap] iteration bits */
+  int cap;
+  int n;           /* steps recorded (record: written; replay: read) */
+} ind_rec_t;
+
 static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kbuf,
                     const abcmb_pert_settings* s, const start_grid_t* sg, int ik,
                     double* pt, abcmb_kstat* st, work_t* w, const tan_ctx_t* T, tan_work_t* tw,
-                    int32_t* tst) {
+                    int32_t* tst, ind_rec_t* R) {
+  const int ind = R ? R->mode : 0;
   layout_t L;
   make_layout(c, &L);
   const int n = L.ny;
@@ -907,8 +922,18 @@ static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kb
   }
 
   int nsteps = 0;
-  while (t0 < t_end) {
-    if (nsteps >= s->max_steps) { st->status = ABCMB_STATUS_MAX_STEPS; break; }
+  unsigned itbits = 0u;
+  if (ind == 2 && R->n <= 0) st->status = ABCMB_STATUS_NONFINITE;   /* the base failed */
+  while (t0 < t_end && st->status == ABCMB_STATUS_OK) {
+    if (ind == 2) {
+      if (nsteps >= R->n) { st->status = ABCMB_STATUS_NONFINITE; break; }
+      t1 = R->t1[nsteps];
+      itbits = (unsigned)R->it[nsteps];
+      if (!(t1 > t0)) { st->status = ABCMB_STATUS_DT_UNDERFLOW; break; }
+    } else {
+      if (nsteps >= s->max_steps) { st->status = ABCMB_STATUS_MAX_STEPS; break; }
+      itbits = 0u;
+    }
     nsteps++;
     const double h = t1 - t0;
     const double hg = h * KV_GAMMA;
@@ -930,6 +955,7 @@ static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kb
       memcpy(fi, w->F + (i - 1) * n, sizeof(double) * n);   /* predictor: previous stage */
       double diffsize = INFINITY, diffsize_prev = INFINITY;
       int conv = 0;
+      const int it_replay = (int)((itbits >> (4 * (i - 1))) & 15u);
       for (int it = 1; it <= root_max; ++it) {
         for (int e = 0; e < n; ++e) w->v[e] = w->base[e] + hg * fi[e];
         rhs(c, &L, k, &bi, w->v, w->r);
@@ -947,13 +973,19 @@ static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kb
         diffsize_prev = diffsize;
         diffsize = sqrt(ss / n);
         st->n_newton++;
-        if (it >= 2) {
+        if (ind == 2) {
+          if (it >= it_replay) { conv = 1; break; }
+        } else if (it >= 2) {
           double rate = diffsize / diffsize_prev;
           double factor = diffsize * rate / (1. - rate);
           int small = diffsize < small_res;
           int diverged = !isfinite(rate) || rate > 2.;
           int converged = factor > 0. && factor < kappa;
-          if (small || converged) { conv = 1; break; }
+          if (small || converged) {
+            if (ind == 1) itbits |= (unsigned)it << (4 * (i - 1));
+            conv = 1;
+            break;
+          }
           if (diverged) break;
         }
       }
@@ -981,6 +1013,10 @@ static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kb
       scaled = INFINITY;
     }
     int keep = scaled < 1.0;
+    if (ind == 2) {
+      keep = isfinite(scaled);
+      if (!keep) { st->status = ABCMB_STATUS_NONFINITE; break; }
+    }
     double inv = 1.0 / scaled;
     double f1v = (coeff1 == 0.) ? 1. : pow(inv, coeff1);
     double f2v = (coeff2 == 0.) ? 1. : pow(prev_inv, coeff2);
@@ -992,6 +1028,10 @@ static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kb
     double dt_new = h * factor;
     if (inv == 0. || isinf(inv)) inv = 1.;
     if (keep) {
+      if (ind == 1) {
+        R->t1[st->n_accepted] = t1;
+        R->it[st->n_accepted] = (int32_t)itbits;
+      }
       st->n_accepted++;
       if (T) tangent_step(c, &L, tables, k, h, t0, rtol, atol * T->tscale, T, w, tw, tst);
       /* dense output: cubic Hermite on [t0, t1] (ThirdOrderHermitePolynomialInterpolation) */
@@ -1060,7 +1100,7 @@ static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kb
     } else {
       st->n_rejected++;
     }
-    if (t0 >= t_end) break;
+    if (t0 >= t_end || ind == 2) continue;
     double tn = t0 + dt_new;
     const double tol = 1e-10;
     if (tn > t_end - tol) tn = keep ? t_end : t0 + 0.5 * (t_end - t0);
@@ -1068,6 +1108,7 @@ static void solve_k(const abcmb_cosmo* c, const double* tables, const double* kb
     if (!(h > 1e-14) || !isfinite(t1)) { st->status = ABCMB_STATUS_DT_UNDERFLOW; break; }
   }
   if (st->status == ABCMB_STATUS_OK && isave < nsave) st->status = ABCMB_STATUS_NONFINITE;
+  if (ind == 1) R->n = st->status == ABCMB_STATUS_OK ? st->n_accepted : -1;
 }
 
 int oracle_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
@@ -1089,7 +1130,7 @@ int oracle_pert_forward(int n_cosmo, const abcmb_cosmo* cosmo, const double* tab
 #pragma omp for schedule(dynamic, 1)
     for (int it = 0; it < n_items; ++it) {
       int ci = items[2 * it], ik = items[2 * it + 1];
-      solve_k(&cosmo[ci], tables, kbuf, s, &sg[ci], ik, pt, &kstat[it], &w, NULL, NULL, NULL);
+      solve_k(&cosmo[ci], tables, kbuf, s, &sg[ci], ik, pt, &kstat[it], &w, NULL, NULL, NULL, NULL);
     }
     work_free(&w);
   }
@@ -1152,7 +1193,7 @@ int oracle_pert_forward_tangent(int n_cosmo, const abcmb_cosmo* cosmo, const dou
         T.sgm[p] = &sg[b];
       }
       tstat[2 * it] = tstat[2 * it + 1] = 0;
-      solve_k(&cosmo[ci], tables, kbuf, s, &sg[ci], ik, pt, &kstat[it], &w, &T, &tw, tstat + 2 * it);
+      solve_k(&cosmo[ci], tables, kbuf, s, &sg[ci], ik, pt, &kstat[it], &w, &T, &tw, tstat + 2 * it, NULL);
     }
     tan_work_free(&tw);
     work_free(&w);
@@ -1161,6 +1202,82 @@ int oracle_pert_forward_tangent(int n_cosmo, const abcmb_cosmo* cosmo, const dou
   free(sg);
   int bad = 0;
   for (int it = 0; it < n_items; ++it) if (kstat[it].status != ABCMB_STATUS_OK) bad = 1;
+  return bad ? ABCMB_ERR_SOLVER : ABCMB_OK;
+}
+
+/* oracle_pert_forward by internal numerical differentiation (ind_rec_t):
+ * items = n_base base items then n_var variant items; var_base[j] = the
+ * base item (0..n_base-1) variant item j replays (same k and state layout,
+ * ABCMB_STATUS_BAD_LAYOUT otherwise).  kstat has n_base + n_var entries. */
+int oracle_pert_forward_ind(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
+                            int n_base, int n_var, const int32_t* items, const int32_t* var_base,
+                            const abcmb_pert_settings* s, double* pt, abcmb_kstat* kstat, int n_threads) {
+  if (n_base < 0 || n_var < 0 || (n_var > 0 && n_base == 0)) return ABCMB_ERR_ARG;
+  const int cap = s->max_steps;
+  double* rt = (double*)malloc(sizeof(double) * (size_t)(n_base > 0 ? n_base : 1) * cap);
+  int32_t* ri = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n_base > 0 ? n_base : 1) * cap);
+  int32_t* rn = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n_base > 0 ? n_base : 1));
+  start_grid_t* sg = (start_grid_t*)calloc(n_cosmo, sizeof(start_grid_t));
+  int maxny = 0;
+  for (int c = 0; c < n_cosmo; ++c) {
+    start_grid_init(&cosmo[c], tables, s->R_tc, &sg[c]);
+    if (cosmo[c].ny > maxny) maxny = cosmo[c].ny;
+  }
+#ifdef _OPENMP
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+#endif
+  for (int pass = 0; pass < 2; ++pass) {
+#pragma omp parallel
+    {
+      work_t w;
+      work_alloc(&w, maxny);
+#pragma omp for schedule(dynamic, 1)
+      for (int j = 0; j < (pass == 0 ? n_base : n_var); ++j) {
+        const int it = pass == 0 ? j : n_base + j;
+        const int ci = items[2 * it], ik = items[2 * it + 1];
+        ind_rec_t R;
+        if (pass == 0) {
+          R.mode = 1;
+          R.t1 = rt + (size_t)j * cap;
+          R.it = ri + (size_t)j * cap;
+          R.cap = cap;
+          R.n = -1;
+          solve_k(&cosmo[ci], tables, kbuf, s, &sg[ci], ik, pt, &kstat[it], &w, NULL, NULL, NULL, &R);
+          rn[j] = R.n;
+        } else {
+          const int rb = var_base[j];
+          int bad = rb < 0 || rb >= n_base;
+          if (!bad) {
+            const int cb = items[2 * rb];
+            const abcmb_cosmo* a = &cosmo[ci];
+            const abcmb_cosmo* b = &cosmo[cb];
+            bad = items[2 * rb + 1] != ik || a->ny != b->ny || a->nk != b->nk || a->has_ncdm != b->has_ncdm ||
+                  a->lmax_g != b->lmax_g || a->lmax_pol_g != b->lmax_pol_g || a->lmax_nu != b->lmax_nu ||
+                  a->lmax_ncdm != b->lmax_ncdm || kbuf[a->off_k + ik] != kbuf[b->off_k + ik];
+          }
+          if (bad) {
+            abcmb_kstat z = {ABCMB_STATUS_BAD_LAYOUT, 0, 0, 0, 0.};
+            kstat[it] = z;
+            continue;
+          }
+          R.mode = 2;
+          R.t1 = rt + (size_t)rb * cap;
+          R.it = ri + (size_t)rb * cap;
+          R.cap = cap;
+          R.n = rn[rb];
+          solve_k(&cosmo[ci], tables, kbuf, s, &sg[ci], ik, pt, &kstat[it], &w, NULL, NULL, NULL, &R);
+        }
+      }
+      work_free(&w);
+    }
+  }
+  for (int c = 0; c < n_cosmo; ++c) start_grid_free(&sg[c]);
+  free(sg);
+  free(rt);
+  free(ri);
+  free(rn);
+  int bad = 0;
+  for (int it = 0; it < n_base + n_var; ++it) if (kstat[it].status != ABCMB_STATUS_OK) bad = 1;
   return bad ? ABCMB_ERR_SOLVER : ABCMB_OK;
 }
 

@@ -42,6 +42,9 @@ int oracle_pert_forward_tangent(int n_cosmo, const abcmb_cosmo* cosmo, const dou
                                 int n_items, const int32_t* items, int n_dir, const int32_t* dirs, double tscale,
                                 const abcmb_pert_settings* s, double* pt, abcmb_kstat* kstat, int32_t* tstat,
                                 int n_threads);
+int oracle_pert_forward_ind(int n_cosmo, const abcmb_cosmo* cosmo, const double* tables, const double* kbuf,
+                            int n_base, int n_var, const int32_t* items, const int32_t* var_base,
+                            const abcmb_pert_settings* s, double* pt, abcmb_kstat* kstat, int n_threads);
 void oracle_spline_slopes(const double* x, const double* y, int n, double* s);
 double oracle_spline_eval(const double* x, const double* y, const double* s, int n, double xq);
 double oracle_phi(int which, const oracle_bessel* B, int idx, double x);

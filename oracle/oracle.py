@@ -61,6 +61,9 @@ def lib():
         L.oracle_pert_forward_tangent.restype = ctypes.c_int
         L.oracle_pert_forward_tangent.argtypes = [ctypes.c_int, vp, _dp, _dp, ctypes.c_int, _ip, ctypes.c_int, _ip,
                                                   ctypes.c_double, vp, _dp, vp, _ip, ctypes.c_int]
+        L.oracle_pert_forward_ind.restype = ctypes.c_int
+        L.oracle_pert_forward_ind.argtypes = [ctypes.c_int, vp, _dp, _dp, ctypes.c_int, ctypes.c_int, _ip, _ip, vp,
+                                              _dp, vp, ctypes.c_int]
         L.oracle_spline_slopes.argtypes = [_dp, _dp, ctypes.c_int, _dp]
         L.oracle_spline_eval.restype = ctypes.c_double
         L.oracle_spline_eval.argtypes = [_dp, _dp, _dp, ctypes.c_int, ctypes.c_double]
@@ -153,6 +156,25 @@ def pert_forward_tangent(batch, settings, dirs, n_dir: int, tscale: float, n_thr
                                            ctypes.byref(settings),
                                            dptr(pt), vptr(kstat), iptr(tstat), n_threads)
     return rc, pt, kstat, tstat.reshape(-1, 2)
+
+
+def pert_forward_ind(batch, settings, n_base: int, var_base, n_threads: int = 0):
+    """Oracle perturbations by internal numerical differentiation: the
+    batch's first n_base items are integrated recording their accepted
+    steps, the rest (variant items) replay the base item var_base[j] names.
+    Returns (rc, pt, kstat)."""
+    from abcmb_b200.packing import KSTAT_DTYPE
+    pt = np.zeros(batch.pt_size)
+    kstat = np.zeros(batch.n_items, dtype=KSTAT_DTYPE)
+    items = np.ascontiguousarray(batch.items, dtype=np.int32)
+    vb = np.ascontiguousarray(var_base, dtype=np.int32)
+    n_var = batch.n_items - int(n_base)
+    if vb.size != n_var:
+        raise ValueError("var_base needs one entry per variant item")
+    rc = lib().oracle_pert_forward_ind(batch.n_cosmo, vptr(batch.cosmo), dptr(batch.tables), dptr(batch.kbuf),
+                                       int(n_base), n_var, iptr(items), iptr(vb), ctypes.byref(settings), dptr(pt),
+                                       vptr(kstat), n_threads)
+    return rc, pt, kstat
 
 
 def los_forward(batch, pt, kt, ls, bt, n_threads: int = 0):
