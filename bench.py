@@ -99,6 +99,7 @@ class ClockSampler:
         self.index = index
         self.samples = []
         self.proc = None
+        self.window = None
 
     def __enter__(self):
         q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -109,6 +110,11 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi's start-up (NVML over every GPU of the node) must not
+            # fall inside the timed region: wait for its first sample
+            t_end = time.monotonic() + 20.0
+            while not self.samples and self.proc.poll() is None and time.monotonic() < t_end:
+                time.sleep(0.05)
         except (OSError, ValueError):
             self.proc = None
         return self
@@ -117,7 +123,12 @@ class ClockSampler:
         for line in self.proc.stdout:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) >= 6:
-                self.samples.append(parts)
+                self.samples.append(parts + [time.monotonic()])
+
+    def mark(self, start: bool):
+        """Bracket the timed region; summary() keeps the samples inside it."""
+        t = time.monotonic()
+        self.window = (t, None) if start else (self.window[0] if self.window else t, t)
 
     def __exit__(self, *exc):
         if self.proc:
@@ -128,6 +139,10 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        if self.window and self.window[1] is not None:
+            inside = [s for s in self.samples if self.window[0] <= s[-1] <= self.window[1]]
+            if inside:
+                self.samples = inside
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
         sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
@@ -509,6 +524,7 @@ def main():
     with ClockSampler(local) as clk:
         barrier()
         torch.cuda.synchronize(dev)
+        clk.mark(True)
         e0.record(stream)
         for _ in range(args.steps):
             step(record=True)
@@ -516,6 +532,7 @@ def main():
             pert_ms.append(ev_p0.elapsed_time(ev_p1))
         e1.record(stream)
         torch.cuda.synchronize(dev)
+        clk.mark(False)
         barrier()
     ms = e0.elapsed_time(e1) / args.steps
     if world > 1:

@@ -52,7 +52,7 @@ def test_tuned_launch_reproduces_default_bit_for_bit(tmp_path):
         pytest.skip("no CUDA device")
     from abcmb_b200 import configs, engine, gradients
     w = configs.c4(n_cosmo=3, nk_range=(20, 30), seed=5)
-    for mode in ("fd", "tangent"):
+    for mode in ("fd", "tangent", "ind"):
         gw = gradients.expand(w, processes=1, mode=mode)
         st = w.pert_settings()
         autotune.apply("fd", autotune.DEFAULT["fd"])
