@@ -121,14 +121,17 @@ class DeviceBatch:
         replaying the base item var_base (int32 [n_items - n_base]) names."""
         lib = _lib.load()
         st = stream if stream is not None else torch.cuda.current_stream(self.device)
-        key = (var_base.ctypes.data, var_base.nbytes, int(n_base), int(settings.max_steps))
+        key = (var_base.ctypes.data, var_base.nbytes)
         if getattr(self, "_ind_key", None) != key:
             self.var_base = torch.from_numpy(np.ascontiguousarray(var_base, dtype=np.int32)).to(self.device)
-            nws = int(lib.abcmb_pert_ind_workspace_size(self.batch.n_cosmo, int(n_base), int(settings.max_steps)))
-            if nws < 0:
-                _lib.check(int(nws), "abcmb_pert_ind_workspace_size")
-            self.ws_ind = torch.empty(nws, dtype=torch.uint8, device=self.device)
             self._ind_key = key
+        # the record workspace (set ws_ind beforehand to share one buffer
+        # between batches run one after another on a stream)
+        nws = int(lib.abcmb_pert_ind_workspace_size(self.batch.n_cosmo, int(n_base), int(settings.max_steps)))
+        if nws < 0:
+            _lib.check(int(nws), "abcmb_pert_ind_workspace_size")
+        if getattr(self, "ws_ind", None) is None or self.ws_ind.numel() < nws:
+            self.ws_ind = torch.empty(nws, dtype=torch.uint8, device=self.device)
         n_var = self.batch.n_items - int(n_base)
         rc = lib.abcmb_pert_forward_ind(self.batch.n_cosmo, _ptr(self.cosmo), _ptr(self.tables), _ptr(self.kbuf),
                                         int(n_base), n_var, _ptr(self.items), _ptr(self.var_base),

@@ -58,7 +58,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--n-cosmo", type=int, default=64)
+    ap.add_argument("--n-cosmo", type=int, default=None,
+                    help="cosmologies per GPU (default 64; 256 with --config c5)")
+    ap.add_argument("--config", default="c4", choices=["c4", "c5"],
+                    help="c4: the batched unlensed workload (the headline); c5: the lensed batch with P(k)")
+    ap.add_argument("--c5-chunk", type=int, default=32,
+                    help="c5: cosmologies per perturbation / line-of-sight / lensing pass (PerturbationTables "
+                         "of one pass resident at a time)")
     ap.add_argument("--l-max", type=int, default=2500)
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--grad", default="ind", choices=["ind", "tangent", "fd"])
@@ -389,6 +395,193 @@ def hyrex_timing(w, dev):
                         "(inputs in HBM, the +inf fills and the history kernel)"}
 
 
+def run_c5(args, rank, world):
+    """The lensed batch (C5): args.n_cosmo cosmologies drawn as C4 plus N_eff
+    in 2.8..3.4, k grids to 5 / Mpc, lensed TT/TE/EE to l = 3000 (line of
+    sight to 3500), the gradient in all six parameters (with lensing A_s and
+    n_s are central differences too, from descriptors that share their base's
+    perturbations), P(k) of the base cosmologies at z = 0, 1, 2, 3 for 200 k
+    to 5 / Mpc.  One step = every cosmology, in passes of args.c5_chunk
+    cosmologies: perturbations of the pass's descriptors (the chosen gradient
+    mode), line of sight, lensing, gradient assembly and P(k), all on the
+    device; the passes share one PerturbationTable buffer and one record
+    workspace."""
+    import torch
+    import torch.distributed as dist
+    from abcmb_b200 import configs, engine, gradients, _lib
+    from abcmb_b200 import lensing as lensing_mod
+    import ctypes
+    t_build = time.perf_counter()
+    w_all = configs.c5(n_cosmo=args.n_cosmo, seed=configs.SEED + rank)
+    n = len(w_all.params_in)
+    gws = []
+    for c0 in range(0, n, args.c5_chunk):
+        wc = w_all.select(range(c0, min(n, c0 + args.c5_chunk)))
+        gws.append(gradients.expand(wc, processes=os.cpu_count() or 1, mode=args.grad))
+    t_build = time.perf_counter() - t_build
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    stream = torch.cuda.current_stream(dev)
+    lib = _lib.load()
+    pk_k = torch.from_numpy(configs.c5_pk_k()).to(dev)
+    pk_z = torch.tensor(configs.C5_PK_Z, dtype=torch.float64, device=dev)
+    pt_shared = torch.empty(max(g.batch.pt_size for g in gws), dtype=torch.float64, device=dev)
+    ws_ind = None
+    if args.grad == "ind":
+        need = max(int(lib.abcmb_pert_ind_workspace_size(g.batch.n_cosmo, g.n_base_items,
+                                                         int(g.base.specs["max_steps_PE"]))) for g in gws)
+        ws_ind = torch.empty(need, dtype=torch.uint8, device=dev)
+    passes = []
+    for g in gws:
+        wc = g.base
+        db = engine.DeviceBatch.upload(g.batch, dev)
+        db.pt = pt_shared[:max(g.batch.pt_size, 1)]
+        if ws_ind is not None:
+            db.ws_ind = ws_ind
+        lr = engine.LosRunner(db, wc.kt, wc.los_settings())
+        lz = lensing_mod.LensRunner(db, wc.l_max, wc.specs["k_pivot"])
+        nb, nvar = len(wc.params_in), g.n_var
+        jp = torch.tensor([[next(j for j, v in enumerate(var) if v[0] == p and v[1] > 0) for p in configs.GRAD_PARAMS]
+                           for var in g.variants], device=dev)
+        jm = torch.tensor([[next(j for j, v in enumerate(var) if v[0] == p and v[1] < 0) for p in configs.GRAD_PARAMS]
+                           for var in g.variants], device=dev)
+        hs = torch.tensor([[var[next(j for j, v in enumerate(var) if v[0] == p and v[1] > 0)][2]
+                            for p in configs.GRAD_PARAMS] for var in g.variants], dtype=torch.float64, device=dev)
+        n_out = lz.settings.l_max - 1
+        out = {"cl": torch.empty(nb, 3, n_out, dtype=torch.float64, device=dev),
+               "grad": torch.empty(nb, 6, 3, n_out, dtype=torch.float64, device=dev),
+               "pk": torch.empty(g.batch.n_cosmo * len(configs.C5_PK_Z) * pk_k.numel(), dtype=torch.float64,
+                                 device=dev)}
+        passes.append(dict(g=g, db=db, lr=lr, lz=lz, nb=nb, nvar=nvar, jp=jp, jm=jm, hs=hs, n_out=n_out, out=out))
+
+    def one_pass(P):
+        g, db = P["g"], P["db"]
+        db.pert_forward_grad(g, g.base.pert_settings(), stream)
+        P["lr"].run(stream)
+        P["lz"].run(P["lr"].cl, stream)
+        cl = P["lz"].cl.view(P["nb"], P["nvar"], 3, P["n_out"])
+        ar = torch.arange(P["nb"], device=dev)[:, None]
+        P["out"]["cl"].copy_(cl[:, 0])
+        P["out"]["grad"].copy_((cl[ar, P["jp"]] - cl[ar, P["jm"]]) / (2.0 * P["hs"])[:, :, None, None])
+        _lib.check(lib.abcmb_pk_lin(db.batch.n_cosmo, ctypes.c_void_p(db.cosmo.data_ptr()),
+                                    ctypes.c_void_p(db.kbuf.data_ptr()), ctypes.c_void_p(db.pt.data_ptr()),
+                                    db.batch.n_save, float(g.base.specs["k_pivot"]), pk_k.numel(),
+                                    ctypes.c_void_p(pk_k.data_ptr()), pk_z.numel(), ctypes.c_void_p(pk_z.data_ptr()),
+                                    ctypes.c_void_p(P["out"]["pk"].data_ptr()), ctypes.c_void_p(stream.cuda_stream)),
+                   "abcmb_pk_lin")
+
+    def step():
+        for P in passes:
+            one_pass(P)
+
+    if not args.no_autotune:
+        from abcmb_b200 import autotune
+        autotune.tune_batch(passes[0]["db"], passes[0]["g"], passes[0]["g"].base.pert_settings())
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    for P in passes:
+        P["db"].check_status()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        clk.mark(True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        clk.mark(False)
+        if world > 1:
+            dist.barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n / (ms / 1000.0)
+    # end to end: every pass's inputs from pinned host memory, its C_l,
+    # gradient and P(k) back
+    h2d = d2h = 0
+    host = []
+    for P in passes:
+        db, g = P["db"], P["g"]
+        ins = [(db.cosmo, torch.from_numpy(g.batch.cosmo.view(np.uint8).copy()).pin_memory()),
+               (db.tables, torch.from_numpy(g.batch.tables).pin_memory()),
+               (db.kbuf, torch.from_numpy(g.batch.kbuf).pin_memory()),
+               (db.items, torch.from_numpy(g.batch.items.reshape(-1).copy()).pin_memory())]
+        if g.mode == "ind":
+            ins.append((db.var_base, torch.from_numpy(g.var_base.copy()).pin_memory()))
+        outs = [(torch.empty(t.shape, dtype=t.dtype).pin_memory(), t) for t in P["out"].values()]
+        h2d += sum(h.numel() * h.element_size() for _, h in ins)
+        d2h += sum(h.numel() * h.element_size() for h, _ in outs)
+        host.append((ins, outs))
+    torch.cuda.synchronize(dev)
+    x0 = torch.cuda.Event(enable_timing=True)
+    x1 = torch.cuda.Event(enable_timing=True)
+    x0.record(stream)
+    for P, (ins, outs) in zip(passes, host):
+        for d, h in ins:
+            d.copy_(h, non_blocking=True)
+        one_pass(P)
+        for h, d in outs:
+            h.copy_(d, non_blocking=True)
+    x1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_e2e = x0.elapsed_time(x1)
+    if world > 1:
+        t = torch.tensor([ms_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    steps_tot = 0.0
+    flops = 0.0
+    items = 0
+    for P in passes:
+        ks = P["db"].kstat_host()
+        b = P["g"].batch
+        sk = (ks["n_accepted"] + ks["n_rejected"]).astype(np.float64)
+        ny = b.cosmo["ny"][b.items[:, 0]].astype(np.float64)
+        flops += float(np.sum(sk * 7.0 * ((8.0 * ny + 200.0) + 20.0 * ny)))
+        steps_tot += float(sk.sum())
+        items += int(b.n_items)
+    peak = ctypes.c_double(0.0)
+    rc = lib.abcmb_probe_fp64_tflops(ctypes.byref(peak), 20000, ctypes.c_void_p(stream.cuda_stream))
+    achieved = flops / (ms / 1000.0) / 1e12
+    n_desc = sum(P["g"].batch.n_cosmo for P in passes)
+    launches = sum((4 if P["g"].mode == "ind" else 3) + 5 * ((P["g"].batch.n_cosmo + engine.LOS_CHUNK - 1)
+                                                             // engine.LOS_CHUNK) + 7 + 1 for P in passes)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; background tables from a host model)",
+            "config": {"workload": f"C5 lensed batch: {n} cosmologies per GPU (C4 draws + N_eff U(2.8,3.4)), "
+                                   f"k to 5/Mpc, lensed TT/TE/EE to l=3000 (LOS to 3500), grad wrt all six "
+                                   f"parameters (13 descriptors per cosmology, 9 integrated), P(k) z=0,1,2,3 "
+                                   f"for 200 k to 5/Mpc",
+                       "n_cosmo_per_gpu": n, "grad": GRAD_DESC[args.grad], "passes": len(passes),
+                       "cosmologies_per_pass": args.c5_chunk, "descriptors": n_desc,
+                       "precision": "FP64 ODE, FP64 LOS, FP64 lensing", "l2": "inputs > L2 (126 MB) per step",
+                       "parallelism": f"dp{world} (independent cosmologies per GPU, no collective)"},
+            "e2e": {"value": world * n / (ms_e2e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e},
+            "roofline": {"bound": "fp64", "kernel": "whole step (perturbations dominate)", "achieved": achieved,
+                         "peak": peak.value if rc == 0 else None, "unit": "TFLOP/s",
+                         "frac": achieved / peak.value if rc == 0 and peak.value > 0 else None, "traffic": None,
+                         "flops_def": "sum_k steps_k * 7 * (8 Ny + 200 + 20 Ny) over the step time"},
+            "gpu_launches": launches, "clocks": clk.summary(), "items_per_step": items,
+            "ode_steps_mean": steps_tot / max(items, 1), "host_build_s": t_build}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def run_reference(args, rank, world):
     """Reference arm: the CPU restatement of the path (the oracle) on the
     host cores.  Each step is one whole cosmology's C_l + gradient (every k
@@ -428,8 +621,13 @@ def main():
                             one_thread=args.one_thread, out=args.out)
         print(json.dumps(res), flush=True)
         return
+    if args.n_cosmo is None:
+        args.n_cosmo = 256 if args.config == "c5" else 64
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.config == "c5":
+        run_c5(args, rank, world)
         return
 
     # host-side inputs first (spawn pool before any CUDA call)
@@ -477,6 +675,7 @@ def main():
     out_grad = torch.empty(nb, 6, 3, n_out, dtype=torch.float64, device=dev)
     ev_p0 = torch.cuda.Event(enable_timing=True)
     ev_p1 = torch.cuda.Event(enable_timing=True)
+    ev_l1 = torch.cuda.Event(enable_timing=True)
 
     def assemble():
         cl = lr.cl.view(nb, nvar, 3, n_out)
@@ -503,7 +702,7 @@ def main():
                   else "[warps per block, variant 1 = 2 blocks/SM, 2 = 3 blocks/SM]",
                   "tune_s": time.perf_counter() - t_tune}
 
-    pert_ms = []
+    pert_ms, los_ms = [], []
 
     def step(record=False):
         if record:
@@ -512,6 +711,8 @@ def main():
         if record:
             ev_p1.record(stream)
         lr.run(stream)
+        if record:
+            ev_l1.record(stream)
         assemble()
 
     for _ in range(args.warmup):
@@ -528,8 +729,9 @@ def main():
         e0.record(stream)
         for _ in range(args.steps):
             step(record=True)
-            ev_p1.synchronize()
+            ev_l1.synchronize()
             pert_ms.append(ev_p0.elapsed_time(ev_p1))
+            los_ms.append(ev_p1.elapsed_time(ev_l1))
         e1.record(stream)
         torch.cuda.synchronize(dev)
         clk.mark(False)
@@ -618,6 +820,40 @@ def main():
                                "MEASURED_PEAKS.json has no FP64 figure",
                 "flops_def": flops_def, "launch_ms": pert_avg,
                 "hbm_gbs_peak": _peak_hbm()[0], "hbm_gbs_peak_source": _peak_hbm()[1]}
+    # line of sight (survey convention): 4 FMAs per (tabulated l, lna
+    # interval, transfer k) triple and 3 Bessel-function evaluations; bytes:
+    # the FP64 sources read once, the Bessel-table columns once per launch
+    # group, the PerturbationTable's ten source fields read once
+    los_avg = float(np.mean(los_ms))
+    n_desc = b.n_cosmo
+    n_tau = b.n_save - 1
+    n_trip = float(lr.n_ell_tab) * n_tau * ls.nkt * n_desc
+    from abcmb_b200 import bessel as bessel_mod
+    n_x = int(bessel_mod.load().phi.shape[-1])
+    n_groups = (n_desc + engine.LOS_CHUNK - 1) // engine.LOS_CHUNK
+    nk_sum = float(b.cosmo["nk"].sum())
+    los_bytes = (8.0 * 4 * n_tau * ls.nkt * n_desc + 8.0 * 3 * n_x * lr.n_ell_tab * n_groups
+                 + 8.0 * 10 * b.n_save * nk_sum + 8.0 * 3 * lr.n_ell_tab * n_desc)
+    los_tf = 8.0 * n_trip / (los_avg / 1000.0) / 1e12
+    ltraffic = None
+    lfile = os.path.join(ROOT, "profiles", "los_kernel_traffic.json")
+    if os.path.isfile(lfile):
+        try:
+            lj = json.load(open(lfile))
+            ltraffic = lj["bytes_per_triple"] * n_trip
+        except (ValueError, KeyError):
+            ltraffic = None
+    roofline_los = {"bound": "fp64+special functions", "kernels": "sources + los_kernel<0> + spline/cl_final",
+                    "achieved": los_tf, "peak": peak.value if rc == 0 else None, "unit": "TFLOP/s",
+                    "frac": (los_tf / peak.value) if rc == 0 and peak.value > 0 else None,
+                    "bessel_evals_per_s": 3.0 * n_trip / (los_avg / 1000.0),
+                    "hbm_gbs_algorithmic": los_bytes / (los_avg / 1000.0) / 1e9,
+                    "hbm_frac": los_bytes / (los_avg / 1000.0) / 1e9 / _peak_hbm()[0],
+                    "traffic": ltraffic, "ms_per_step": los_avg,
+                    "flops_def": "8 * n_l_tab * (n_save - 1) * N_kt per descriptor (4 FMAs per triple)",
+                    "bytes_def": "FP64 sources 4 x (n_save - 1) x N_kt + Bessel columns 3 x n_x x n_l_tab per group "
+                                 "+ 10 PerturbationTable fields read + raw C_l written",
+                    "triples": n_trip}
     # our kernel launches per step: pert (2 start kernels + the persistent
     # kernel, two of them -- record and replay -- in ind mode) + 5 per
     # line-of-sight chunk of engine.LOS_CHUNK cosmologies
@@ -626,7 +862,8 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; background tables from a host model)",
-            "config": workload_config(args, world), "e2e": e2e, "roofline": roofline, "gpu_launches": launches,
+            "config": workload_config(args, world), "e2e": e2e, "roofline": roofline, "roofline_los": roofline_los,
+            "gpu_launches": launches,
             "clocks": clk.summary(), "items_per_step": int(b.n_items),
             "ode_steps_mean": float(steps_k.mean()), "host_build_s": t_build}
     if tangent_stats:
@@ -644,6 +881,10 @@ def main():
             others[go.mode] = (other.pop("cl0"), other.pop("grad0"))
             other["step_time_vs_headline"] = other["ms_per_step"] / ms
             line["grad_" + go.mode] = other
+        try:
+            line["los_fp32"] = los_fp32_extra(db, w, lr, dev, stream)
+        except Exception as ex:                            # an extra measurement never costs the line
+            line["los_fp32"] = {"error": str(ex)[:200]}
         plain = plain_gpu_fwd_fd(gw, w, dev, stream, args.plain_sample)
         plain["batched_over_plain"] = value / plain["value"]
         line["plain_gpu_fwd_fd"] = plain
@@ -704,6 +945,41 @@ def mode_extra(go, w, db, lr, st, dev, stream, assemble, out_cl, out_grad, steps
         ts = tdb.tstat.cpu().numpy().reshape(-1, 2)[:go.batch.n_items]
         res.update(chord_iterations_per_item=float(ts[:, 0].mean()), unconverged_stage_solves=int(ts[:, 1].sum()))
     return res
+
+
+def los_fp32_extra(db, w, lr, dev, stream, runs: int = 2) -> dict:
+    """The line of sight with FP32 sources and compensated FP32 sums
+    (los_kernel<1>) on the step's PerturbationTables, against the FP64
+    launch: CUDA-event times of both and the largest C_l error of the FP32
+    one relative to the FP64 C_l (TT, EE; TE relative to |TT| + |TE|)."""
+    import torch
+    from abcmb_b200 import engine
+    l32 = engine.LosRunner(db, w.kt, w.los_settings(precision=1))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    lr.run(stream)
+    l32.run(stream)
+    torch.cuda.synchronize(dev)
+    ev[0].record(stream)
+    for _ in range(runs):
+        lr.run(stream)
+    ev[1].record(stream)
+    for _ in range(runs):
+        l32.run(stream)
+    ev[2].record(stream)
+    torch.cuda.synchronize(dev)
+    n = db.batch.n_cosmo
+    c64 = lr.cl.view(n, 3, -1).cpu().numpy()
+    c32 = l32.cl.view(n, 3, -1).cpu().numpy()
+    tt = float(np.max(np.abs(c32[:, 0] - c64[:, 0]) / np.abs(c64[:, 0])))
+    ee = float(np.max(np.abs(c32[:, 2] - c64[:, 2]) / np.abs(c64[:, 2])))
+    te = float(np.max(np.abs(c32[:, 1] - c64[:, 1]) / (np.abs(c64[:, 0]) + np.abs(c64[:, 1]))))
+    ms64 = ev[0].elapsed_time(ev[1]) / runs
+    ms32 = ev[1].elapsed_time(ev[2]) / runs
+    del l32
+    return {"ms_fp64": ms64, "ms_fp32": ms32, "speedup": ms64 / ms32,
+            "cl_max_rel_vs_fp64": {"TT": tt, "TE": te, "EE": ee}, "descriptors": n,
+            "what": "los_kernel<1>: FP32 sources and Kahan-compensated FP32 sums, Bessel functions in FP64; "
+                    "not used by the step (the step's line of sight is FP64)"}
 
 
 def err_vs_oracle(cl, grad, cl_o, grad_o) -> dict:
