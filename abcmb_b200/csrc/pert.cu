@@ -1485,14 +1485,18 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
               double fnew = ff[e] + x;
               ff[e] = fnew;
               vv[e] = bb[e] + hg * fnew;                        // the next iteration's argument
-              double q = x * pos_rcp(atol + rtol * fabs(fnew));
-              ss += q * q;
+              if constexpr (IND != 2) {                         // a replay needs no termination test
+                double q = x * pos_rcp(atol + rtol * fabs(fnew));
+                ss += q * q;
+              }
             }
           }
-          ss = warp_sum(ss);
+          if constexpr (IND != 2) ss = warp_sum(ss);
           __syncwarp();
-          diffsize_prev = diffsize;
-          diffsize = sqrt(ss * inv_n);
+          if constexpr (IND != 2) {
+            diffsize_prev = diffsize;
+            diffsize = sqrt(ss * inv_n);
+          }
           ++nnewton;
           PERT_PHASE(5);
           if constexpr (IND == 2) {
@@ -1540,20 +1544,28 @@ __device__ __forceinline__ void pert_body(const PertArgs& P) {
           double y0e = y0[e];
           double y1e = y0e + h * acc;
           y1[e] = y1e;
-          double err = h * acce;
-          double q = err * pos_rcp(atol + fmax(fabs(y0e), fabs(y1e)) * rtol);
-          ss += q * q;
+          if constexpr (IND == 2) {
+            // a replay takes the step: only a non-finite state stops it
+            if (!isfinite(y1e)) ss = INFINITY;
+          } else {
+            double err = h * acce;
+            double q = err * pos_rcp(atol + fmax(fabs(y0e), fabs(y1e)) * rtol);
+            ss += q * q;
+          }
         }
-        ss = warp_sum(ss);
-        scaled = sqrt(ss * inv_n);
+        if constexpr (IND == 2) {
+          scaled = __any_sync(0xffffffffu, ss != 0.) ? INFINITY : 0.;
+        } else {
+          ss = warp_sum(ss);
+          scaled = sqrt(ss * inv_n);
+        }
         if (!isfinite(scaled)) scaled = INFINITY;
       }
       __syncwarp();
       bool keep = scaled < 1.0;
       if constexpr (IND == 2) {
-        // the base accepted this step: the variant takes it whatever its own
-        // error estimate says (a non-finite one still stops it)
-        keep = isfinite(scaled);
+        // the base accepted this step: the variant takes it (scaled is 0, or
+        // infinite for a non-finite state, which stops the item)
         if (!keep) status = ABCMB_STATUS_NONFINITE;
       }
       double inv = 1.0 / scaled;
