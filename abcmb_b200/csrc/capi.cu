@@ -38,6 +38,8 @@ cudaError_t launch_los_vjp(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcm
                            const abcmb_los_settings& ls, int n_save, const BesselDev& B, const double* cl_bar,
                            double* pt_bar, double* param_bar, void* ws, cudaStream_t stream);
 int64_t lens_workspace_bytes(int n_cosmo, const abcmb_lens_settings& s);
+cudaError_t launch_hyrex_inputs(int n_cosmo, int n_grid, const abcmb_cosmo* cosmo, double* T, double* nH, double* H,
+                                cudaStream_t stream);
 int64_t bg_workspace_bytes(int n_cosmo, const abcmb_bg_settings& s);
 int hyrex_sizes(int n_grid, int* n_xe, int* n_tm);
 cudaError_t hyrex_upload_tables(const double* alpha, const double* R, const double* swift, int n_swift);
@@ -162,6 +164,16 @@ int abcmb_upload_hyrex_tables(const double* alpha, const double* R, const double
 int abcmb_hyrex_sizes(int n_grid, int* n_xe, int* n_tm) {
   if (n_grid < 2 || !n_xe || !n_tm) return -1;
   return abcmb::hyrex_sizes(n_grid, n_xe, n_tm);
+}
+
+int abcmb_hyrex_inputs(int n_cosmo, int n_grid, const abcmb_cosmo* cosmo_dev, double* T_dev, double* nH_dev,
+                       double* H_dev, void* stream) {
+  if (n_cosmo <= 0 || n_grid < 2 || !cosmo_dev || !T_dev || !nH_dev || !H_dev)
+    return fail(ABCMB_ERR_ARG, "abcmb_hyrex_inputs: null argument or empty grid");
+  cudaError_t e = abcmb::launch_hyrex_inputs(n_cosmo, n_grid, cosmo_dev, T_dev, nH_dev, H_dev,
+                                             static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "abcmb_hyrex_inputs");
+  return ABCMB_OK;
 }
 
 int abcmb_hyrex_forward(int n_cosmo, int n_grid, const double* T_dev, const double* nH_dev, const double* H_dev,

@@ -681,6 +681,33 @@ bool hyrex_tables_ready() {
   return (int)g_hx.size() > d && g_hx[d].ready;
 }
 
+// RecombInputs on the device (Background.TCMB, nH, H at lna_axis_full,
+// background.py:147-166, 349-387; hyrex.py:16-90): one thread per
+// (grid point, cosmology); H = sqrt(8 pi G rho_tot / 3) in 1/s from the same
+// species densities the perturbation kernels use (rho_all).
+__global__ void hyrex_inputs_kernel(int n_cosmo, int n_grid, const abcmb_cosmo* __restrict__ cosmo, double* T,
+                                    double* nH, double* H) {
+  const int ci = blockIdx.y;
+  if (ci >= n_cosmo) return;
+  const abcmb_cosmo& c = cosmo[ci];
+  const double l0 = -log(1. + 8000.);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_grid; i += gridDim.x * blockDim.x) {
+    const double a = exp(l0 + (double)i * HX_SPACING);
+    const size_t o = (size_t)ci * n_grid + i;
+    T[o] = c.TCMB0 / a;
+    nH[o] = nH_of(c, a);
+    const Rho r = rho_all(c, a);
+    H[o] = sqrt(8. * PI * GN * r.tot / 3.);
+  }
+}
+
+cudaError_t launch_hyrex_inputs(int n_cosmo, int n_grid, const abcmb_cosmo* cosmo, double* T, double* nH, double* H,
+                                cudaStream_t stream) {
+  dim3 g((n_grid + 255) / 256, n_cosmo);
+  hyrex_inputs_kernel<<<g, 256, 0, stream>>>(n_cosmo, n_grid, cosmo, T, nH, H);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_hyrex(int n_cosmo, int n_grid, const double* T, const double* nH, const double* H,
                          const abcmb_hyrex_params* params, double* xe, double* lna_xe, double* tm, double* lna_tm,
                          int32_t* info, cudaStream_t stream) {

@@ -136,6 +136,22 @@ class Batch:
         return self.kbuf[int(c["off_k"]):int(c["off_k"]) + int(c["nk"])]
 
 
+BG_PARAM_FIELDS = ("h", "omega_b", "omega_cdm", "omega_Lambda", "A_s", "n_s", "TCMB0", "YHe",
+                   "N_nu_massless", "T_nu_massless", "N_nu_massive", "T_nu_massive", "m_nu_massive",
+                   "R_nu", "R_b", "om")
+
+
+def param_records(params_list, has_ncdm_list) -> np.ndarray:
+    """Descriptors carrying only the background parameters (derived params
+    dicts) and has_ncdm: what abcmb_hyrex_inputs reads."""
+    rec = np.zeros(len(params_list), dtype=COSMO_DTYPE)
+    for r, p, nc in zip(rec, params_list, has_ncdm_list):
+        for name in BG_PARAM_FIELDS:
+            r[name] = float(p[name])
+        r["has_ncdm"] = int(bool(nc))
+    return rec
+
+
 def pack(bgs, layouts, kgrids, n_save: int = 500, order: str = "cost", alias_of=None,
          overrides=None, work=None) -> Batch:
     """Pack cosmologies (BackgroundTables, StateLayout, k grid) into a Batch.
@@ -175,9 +191,7 @@ def pack(bgs, layouts, kgrids, n_save: int = 500, order: str = "cost", alias_of=
             continue
         p = bg.params
         r = rec[i]
-        for name in ["h", "omega_b", "omega_cdm", "omega_Lambda", "A_s", "n_s", "TCMB0", "YHe",
-                     "N_nu_massless", "T_nu_massless", "N_nu_massive", "T_nu_massive", "m_nu_massive",
-                     "R_nu", "R_b", "om"]:
+        for name in BG_PARAM_FIELDS:
             r[name] = float(p[name])
         # a background without its conformal-time table is completed on the
         # device (abcmb_bg_forward): zero placeholders until then

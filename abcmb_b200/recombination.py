@@ -52,19 +52,35 @@ def ensure_tables(device: torch.device):
     _uploaded.add(idx)
 
 
-def hyrex_forward(params_list, has_ncdm_list, device=None) -> dict:
+def hyrex_forward(params_list, has_ncdm_list, device=None, inputs: str = "device") -> dict:
     """The recombination histories of a batch on the GPU: dict of numpy
-    arrays xe, lna_xe [n, n_xe], Tm, lna_tm [n, n_tm], info [n, 16]."""
+    arrays xe, lna_xe [n, n_xe], Tm, lna_tm [n, n_tm], info [n, 16].
+    inputs="device" samples the RecombInputs on the GPU
+    (abcmb_hyrex_inputs), "host" with recomb_inputs (numpy)."""
     from .engine import require_cuda
+    from . import packing
+    if inputs not in ("device", "host"):
+        raise ValueError("inputs must be 'device' or 'host'")
     dev = require_cuda(device)
     ensure_tables(dev)
     lib = _lib.load()
     grid = hyrex_grid()
     n = len(params_list)
-    ins = [recomb_inputs(p, nc) for p, nc in zip(params_list, has_ncdm_list)]
-    T = torch.from_numpy(np.stack([i[0] for i in ins])).to(dev)
-    nH = torch.from_numpy(np.stack([i[1] for i in ins])).to(dev)
-    H = torch.from_numpy(np.stack([i[2] for i in ins])).to(dev)
+    st = torch.cuda.current_stream(dev)
+    if inputs == "host":
+        ins = [recomb_inputs(p, nc) for p, nc in zip(params_list, has_ncdm_list)]
+        T = torch.from_numpy(np.stack([i[0] for i in ins])).to(dev)
+        nH = torch.from_numpy(np.stack([i[1] for i in ins])).to(dev)
+        H = torch.from_numpy(np.stack([i[2] for i in ins])).to(dev)
+    else:
+        rec = packing.param_records(params_list, has_ncdm_list)
+        cos = torch.from_numpy(rec.view(np.uint8).copy()).to(dev)
+        T = torch.empty(n * len(grid), dtype=torch.float64, device=dev)
+        nH = torch.empty_like(T)
+        H = torch.empty_like(T)
+        _lib.check(lib.abcmb_hyrex_inputs(n, len(grid), ctypes.c_void_p(cos.data_ptr()), ctypes.c_void_p(T.data_ptr()),
+                                          ctypes.c_void_p(nH.data_ptr()), ctypes.c_void_p(H.data_ptr()),
+                                          ctypes.c_void_p(st.cuda_stream)), "abcmb_hyrex_inputs")
     prm = np.zeros(n, dtype=HYREX_PARAMS_DTYPE)
     for i, p in enumerate(params_list):
         prm[i] = (p["YHe"], p["omega_b"], p["omega_cdm"], p["Neff"])
@@ -78,7 +94,6 @@ def hyrex_forward(params_list, has_ncdm_list, device=None) -> dict:
     tm = torch.empty(n * n_tm.value, dtype=torch.float64, device=dev)
     ltm = torch.empty_like(tm)
     info = torch.zeros(n * 16, dtype=torch.int32, device=dev)
-    st = torch.cuda.current_stream(dev)
 
     def ptr(t):
         return ctypes.c_void_p(t.data_ptr())

@@ -347,52 +347,66 @@ def bg_forward_timing(gw, db, dev, stream):
             "tau_steps_max": int(res["n_steps_tau"].max()), "host_model_ms_per_cosmology": host_ms}
 
 
-def hyrex_timing(w, dev):
-    """The recombination histories (HyRex, abcmb_hyrex_forward) of the batch's
-    base cosmologies on the GPU, outside the timed step: wall time of the call
-    (host sampling of the inputs, transfers, kernel)."""
-    import torch
-    from abcmb_b200 import cosmology, recombination
-    ps = [cosmology.add_derived_parameters(p, nc, w.specs) for p, nc in zip(w.params_in, w.has_ncdm)]
-    recombination.hyrex_forward(ps, w.has_ncdm, dev)
-    torch.cuda.synchronize(dev)
-    t = time.perf_counter()
-    out = recombination.hyrex_forward(ps, w.has_ncdm, dev)
-    torch.cuda.synchronize(dev)
-    ms = (time.perf_counter() - t) * 1000.0
-    # the kernel alone: the same C-ABI call on inputs already in HBM, CUDA events
+def hyrex_timing(gw, dev):
+    """The recombination histories (HyRex) on the GPU, outside the timed step:
+    for the batch's base cosmologies and for every gradient descriptor of the
+    batch (each variant has its own background, so its own history), the
+    wall time of recombination.hyrex_forward (RecombInputs sampled on the
+    device, the history kernel, the read-back) and the kernels alone by CUDA
+    events (inputs already in HBM)."""
     import ctypes
-    from abcmb_b200 import _lib
+    import torch
+    from abcmb_b200 import _lib, packing, recombination
     lib = _lib.load()
-    grid = recombination.hyrex_grid()
-    ins = [recombination.recomb_inputs(p, nc) for p, nc in zip(ps, w.has_ncdm)]
-    T = torch.from_numpy(np.stack([i[0] for i in ins])).to(dev)
-    nH = torch.from_numpy(np.stack([i[1] for i in ins])).to(dev)
-    H = torch.from_numpy(np.stack([i[2] for i in ins])).to(dev)
-    prm = np.zeros(len(ps), dtype=recombination.HYREX_PARAMS_DTYPE)
-    for i, p in enumerate(ps):
-        prm[i] = (p["YHe"], p["omega_b"], p["omega_cdm"], p["Neff"])
-    prm_d = torch.from_numpy(prm.view(np.uint8).copy()).to(dev)
-    n_xe, n_tm = out["xe"].shape[1], out["Tm"].shape[1]
-    xe = torch.empty(len(ps) * n_xe, dtype=torch.float64, device=dev)
-    lxe = torch.empty_like(xe)
-    tm = torch.empty(len(ps) * n_tm, dtype=torch.float64, device=dev)
-    ltm = torch.empty_like(tm)
-    info = torch.zeros(len(ps) * 16, dtype=torch.int32, device=dev)
-    st = torch.cuda.current_stream(dev)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    rc = lib.abcmb_hyrex_forward(len(ps), len(grid), *(ctypes.c_void_p(t.data_ptr()) for t in
-                                                       (T, nH, H, prm_d, xe, lxe, tm, ltm, info)),
-                                 ctypes.c_void_p(st.cuda_stream))
-    e1.record(st)
-    torch.cuda.synchronize(dev)
-    _lib.check(rc, "abcmb_hyrex_forward")
-    return {"ms_wall": ms, "cosmologies": len(ps), "ms_per_cosmology": ms / len(ps),
-            "kernel_ms": e0.elapsed_time(e1), "ode_steps_max": int(out["info"][:, 8:12].sum(axis=1).max()),
-            "includes": "ms_wall: host sampling of the inputs, H2D, kernel, D2H; kernel_ms: the launch alone "
-                        "(inputs in HBM, the +inf fills and the history kernel)"}
+    b = gw.batch
+    ps_all = [bg.params for bg in b.bgs]
+    nc_all = [bool(x) for x in b.cosmo["has_ncdm"]]
+    base = list(range(0, b.n_cosmo, gw.n_var))
+    res = {}
+    for name, idx in (("base", base), ("all_descriptors", list(range(b.n_cosmo)))):
+        ps = [ps_all[i] for i in idx]
+        ncs = [nc_all[i] for i in idx]
+        recombination.hyrex_forward(ps, ncs, dev)
+        torch.cuda.synchronize(dev)
+        t = time.perf_counter()
+        out = recombination.hyrex_forward(ps, ncs, dev)
+        torch.cuda.synchronize(dev)
+        ms = (time.perf_counter() - t) * 1000.0
+        grid = recombination.hyrex_grid()
+        n = len(ps)
+        cos = torch.from_numpy(packing.param_records(ps, ncs).view(np.uint8).copy()).to(dev)
+        T = torch.empty(n * len(grid), dtype=torch.float64, device=dev)
+        nH = torch.empty_like(T)
+        H = torch.empty_like(T)
+        prm = np.zeros(n, dtype=recombination.HYREX_PARAMS_DTYPE)
+        for i, p in enumerate(ps):
+            prm[i] = (p["YHe"], p["omega_b"], p["omega_cdm"], p["Neff"])
+        prm_d = torch.from_numpy(prm.view(np.uint8).copy()).to(dev)
+        n_xe, n_tm = out["xe"].shape[1], out["Tm"].shape[1]
+        xe = torch.empty(n * n_xe, dtype=torch.float64, device=dev)
+        lxe = torch.empty_like(xe)
+        tm = torch.empty(n * n_tm, dtype=torch.float64, device=dev)
+        ltm = torch.empty_like(tm)
+        info = torch.zeros(n * 16, dtype=torch.int32, device=dev)
+        st = torch.cuda.current_stream(dev)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record(st)
+        rc1 = lib.abcmb_hyrex_inputs(n, len(grid), *(ctypes.c_void_p(t.data_ptr()) for t in (cos, T, nH, H)),
+                                     ctypes.c_void_p(st.cuda_stream))
+        ev[1].record(st)
+        rc2 = lib.abcmb_hyrex_forward(n, len(grid), *(ctypes.c_void_p(t.data_ptr()) for t in
+                                                      (T, nH, H, prm_d, xe, lxe, tm, ltm, info)),
+                                      ctypes.c_void_p(st.cuda_stream))
+        ev[2].record(st)
+        torch.cuda.synchronize(dev)
+        _lib.check(rc1, "abcmb_hyrex_inputs")
+        _lib.check(rc2, "abcmb_hyrex_forward")
+        res[name] = {"cosmologies": n, "ms_wall": ms, "ms_per_cosmology": ms / n,
+                     "inputs_kernel_ms": ev[0].elapsed_time(ev[1]), "history_kernel_ms": ev[1].elapsed_time(ev[2]),
+                     "ode_steps_max": int(out["info"][:, 8:12].sum(axis=1).max())}
+    res["includes"] = ("ms_wall: RecombInputs sampled on the device, the +inf fills and the history kernel, the "
+                       "read-back of the histories; *_kernel_ms: the launches alone by CUDA events")
+    return res
 
 
 def run_c5(args, rank, world):
@@ -872,7 +886,7 @@ def main():
     if rank == 0 and world == 1:
         line["bg_forward"] = bg_forward_timing(gw, db, dev, stream)
         try:
-            line["hyrex_forward"] = hyrex_timing(w, dev)
+            line["hyrex_forward"] = hyrex_timing(gw, dev)
         except Exception as ex:                            # an extra measurement never costs the line
             line["hyrex_forward"] = {"error": str(ex)[:200]}
         others = {}
@@ -893,6 +907,15 @@ def main():
             ref_file = os.path.join(tmp, "oracle_cl.npz")
             res = cpu_baseline_subprocess(configs.SEED + rank, args.l_max, one_thread=True, out=ref_file)
             line["cpu_baseline"] = cpu_baseline_line(res)
+            hx1 = line["cpu_baseline"].get("hyrex_oracle_ms_per_cosmology_one_core")
+            hx = line.get("hyrex_forward", {})
+            if hx1 and "all_descriptors" in hx:
+                nall = hx["all_descriptors"]["cosmologies"]
+                ncores = os.cpu_count() or 1
+                hx["host_oracle_all_cores_ms_estimate"] = {
+                    "base": hx1 * hx["base"]["cosmologies"] / ncores, "all_descriptors": hx1 * nall / ncores,
+                    "how": f"the oracle's one-core time per history x histories / {ncores} host threads "
+                           f"(perfect scaling assumed)"}
             o = np.load(ref_file)
             line["err_vs_oracle"] = err_vs_oracle(res_cl.numpy()[0], res_grad.numpy()[0], o["cl"], o["grad"])
             line["err_vs_oracle"]["gpu_grad"] = GRAD_DESC[gw.mode]

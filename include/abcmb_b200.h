@@ -273,6 +273,19 @@ int abcmb_upload_hyrex_tables(const double* alpha, const double* R, const double
 int abcmb_hyrex_sizes(int n_grid, int* n_xe, int* n_tm);
 
 /*
+ * RecombInputs of every cosmology on the device (what HyRex reads from the
+ * background: Background.TCMB, nH and H, abcmb/background.py:147-166,
+ * 349-387, sampled on lna_axis_full, abcmb/hyrex/hyrex.py:16-90, 131):
+ *   cosmo_dev [n_cosmo]   descriptors; only the background parameters are
+ *                         read (h ... om, has_ncdm): no tables needed
+ *   T_dev, nH_dev, H_dev [n_cosmo x n_grid]  T_CMB (eV), n_H (cm^-3), H (1/s)
+ *                         at lna = -log(8001) + 5e-4 i
+ * The inputs of abcmb_hyrex_forward, without the host sampling.
+ */
+int abcmb_hyrex_inputs(int n_cosmo, int n_grid, const abcmb_cosmo* cosmo_dev, double* T_dev, double* nH_dev,
+                       double* H_dev, void* stream);
+
+/*
  * The recombination history of every cosmology (recomb_model.get_history,
  * abcmb/hyrex/hyrex.py:146-206, with helium.py and hydrogen.py):
  *   T_dev, nH_dev, H_dev [n_cosmo x n_grid]  RecombInputs: T_CMB (eV), n_H

@@ -458,3 +458,37 @@ def test_reference_background_object_gives_the_same_table(gpu):
     host = bg.los_arrays(500)
     for i, tol in ((0, 1e-10), (1, 1e-5), (3, 1e-12), (4, 1e-5)):       # tau, g, aH, exp(-kappa)
         assert np.max(np.abs(los[i] - host[i])) <= tol * np.abs(host[i]).max(), i
+
+
+def test_model_hyrex_matches_the_oracle_chain(gpu):
+    """B200Model(recombination="hyrex")(params) -- HyRex, the background
+    producer, the perturbations and the line of sight on the GPU -- against
+    the same chain on the oracle (oracle HyRex on the host RecombInputs ->
+    from_hyrex -> oracle_bg_forward -> oracle perturbations -> oracle line
+    of sight): C_l within 1e-4 (the two HyRex runs agree within 1e-4 of x_e,
+    a phase boundary may move by one grid point)."""
+    from abcmb_b200 import background_tables as bt, bessel, cosmology, configs, packing
+    from abcmb_b200.output import B200Model
+    from oracle import oracle
+    m = B200Model(l_max=400, l_max_g=12, l_max_pol_g=12, l_max_massless_nu=12, recombination="hyrex")
+    params = dict(configs.FIDUCIAL)
+    out = m(params)
+    assert out.ClTT.shape == (399,)
+    p = cosmology.add_derived_parameters(params, False, m.specs)
+    rc, o = oracle.hyrex(p, False)
+    assert rc == 0
+    bg = bt.from_hyrex(p, False, o["xe"], o["lna_xe"], o["Tm"], o["lna_tm"])
+    b = packing.pack([bg], [m.PE.layout], [m.PE.k_axis_perturbations])
+    rc, cos, tab, st = oracle.bg_forward(b, packing.bg_settings())
+    assert rc == 0 and st[0]["status"] == 0
+    b.cosmo[:] = cos
+    b.tables = tab
+    rc, pt, _ = oracle.pert_forward(b, packing.pert_settings(m.specs, 500, b))
+    assert rc == 0
+    ls = packing.los_settings(m.specs, m.SS.idx_min, m.SS.idx_max, len(m.SS.k_axis_transfer), m.SS.l_out_max,
+                              n_save=500)
+    _, _, cl_o = oracle.los_forward(b, pt, m.SS.k_axis_transfer, ls, bessel.load())
+    rel_tt = np.max(np.abs(out.ClTT - cl_o[0, 0]) / cl_o[0, 0])
+    rel_ee = np.max(np.abs(out.ClEE - cl_o[0, 2]) / cl_o[0, 2])
+    print(f"HyRex model vs oracle chain: TT {rel_tt:.2e} EE {rel_ee:.2e}")
+    assert rel_tt < 1e-4 and rel_ee < 1e-4, (rel_tt, rel_ee)

@@ -232,3 +232,41 @@ def test_hyrex_agrees_with_the_host_model_across_a_batch():
         bg = bt.make_recombination(p, nc)
         xh = bg.xe_arr[:len(grid)] - bt.xe_reion(grid, bg.z_reion, p)
         assert np.max(np.abs(xo[m] / xh[m] - 1)) < 0.02
+
+
+@pytest.mark.gpu
+def test_hyrex_inputs_on_the_device_match_the_host_sampling(gpu):
+    """abcmb_hyrex_inputs (T, n_H, H on lna_axis_full from the descriptors'
+    background parameters) against recomb_inputs (numpy), with and without
+    massive neutrinos, and the histories from both inputs."""
+    import ctypes
+    import torch
+    from abcmb_b200 import _lib, packing
+    w2, w4 = configs.c2(xe_layout="compact"), configs.c4(n_cosmo=2, xe_layout="compact")
+    cases = [(cosmology.add_derived_parameters(w2.params_in[0], True, w2.specs), True)] + \
+            [(cosmology.add_derived_parameters(p, nc, w4.specs), nc) for p, nc in zip(w4.params_in, w4.has_ncdm)]
+    ps, ncs = [c[0] for c in cases], [c[1] for c in cases]
+    grid = gpu.hyrex_grid()
+    n = len(ps)
+    cos = torch.from_numpy(packing.param_records(ps, ncs).view(np.uint8).copy()).cuda()
+    T = torch.empty(n * len(grid), dtype=torch.float64, device="cuda")
+    nH = torch.empty_like(T)
+    H = torch.empty_like(T)
+    lib = _lib.load()
+    _lib.check(lib.abcmb_hyrex_inputs(n, len(grid), *(ctypes.c_void_p(t.data_ptr()) for t in (cos, T, nH, H)),
+                                      ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), "abcmb_hyrex_inputs")
+    for i, (p, nc) in enumerate(cases):
+        th, nh, hh = gpu.recomb_inputs(p, nc)
+        for dev_arr, host in ((T, th), (nH, nh), (H, hh)):
+            d = dev_arr.view(n, -1)[i].cpu().numpy()
+            assert np.max(np.abs(d / host - 1)) < 1e-12
+    a = gpu.hyrex_forward(ps, ncs, inputs="device")
+    b = gpu.hyrex_forward(ps, ncs, inputs="host")
+    for i in range(n):
+        assert a["info"][i][14] == 0 and a["info"][i][12] == b["info"][i][12]
+        for x, l in (("xe", "lna_xe"), ("Tm", "lna_tm")):
+            ok = np.isfinite(a[x][i])
+            m = int(ok.sum())
+            ob = np.isfinite(b[x][i])
+            ref = np.interp(a[l][i][:m], b[l][i][ob], b[x][i][ob])
+            assert np.max(np.abs(a[x][i][:m] / ref - 1)) < 1e-6, (x, i)
