@@ -690,9 +690,12 @@ __global__ void hyrex_inputs_kernel(int n_cosmo, int n_grid, const abcmb_cosmo* 
   const int ci = blockIdx.y;
   if (ci >= n_cosmo) return;
   const abcmb_cosmo& c = cosmo[ci];
+  // the grid values of numpy's arange (which jnp.arange uses for concrete
+  // arguments): start + i * ((start + step) - start)
   const double l0 = -log(1. + 8000.);
+  const double dl = (l0 + HX_SPACING) - l0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_grid; i += gridDim.x * blockDim.x) {
-    const double a = exp(l0 + (double)i * HX_SPACING);
+    const double a = exp(l0 + (double)i * dl);
     const size_t o = (size_t)ci * n_grid + i;
     T[o] = c.TCMB0 / a;
     nH[o] = nH_of(c, a);

@@ -133,9 +133,16 @@ def complete_los(db, ci: int, BG, n_save: int, bg_max_steps: dict):
     b = db.batch
     c = b.cosmo[ci]
     db.bg_forward(packing.bg_settings(n_save, **bg_max_steps), fetch_tables=True)
-    los = BG.los
     BG.tau_tab, BG.tau0, BG.lna_transfer_start, BG.lna_rec = keep
+    # the conformal time on the line-of-sight grid is the caller's table's
+    # (Background.tau, what Cl_one_ell reads); the other five arrays come
+    # from the device's optical-depth solve
+    nl = n_save - 1
+    los = np.array(BG.los, copy=True)
+    los[0] = BG.tau(np.linspace(BG.lna_transfer_start, 0.0, n_save)[:-1])
     BG.los = los
+    ol = int(c["off_los"])
+    db.tables[ol:ol + nl].copy_(torch.from_numpy(np.ascontiguousarray(los[0])))
     o = int(c["off_tau"])
     db.tables[o:o + packing.NTAU_TAB].copy_(torch.from_numpy(BG.tau_tab))
     b.cosmo["tau0"][ci] = BG.tau0

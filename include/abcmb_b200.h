@@ -279,7 +279,7 @@ int abcmb_hyrex_sizes(int n_grid, int* n_xe, int* n_tm);
  *   cosmo_dev [n_cosmo]   descriptors; only the background parameters are
  *                         read (h ... om, has_ncdm): no tables needed
  *   T_dev, nH_dev, H_dev [n_cosmo x n_grid]  T_CMB (eV), n_H (cm^-3), H (1/s)
- *                         at lna = -log(8001) + 5e-4 i
+ *                         at numpy.arange(-log(8001), 0, 5e-4)
  * The inputs of abcmb_hyrex_forward, without the host sampling.
  */
 int abcmb_hyrex_inputs(int n_cosmo, int n_grid, const abcmb_cosmo* cosmo_dev, double* T_dev, double* nH_dev,
