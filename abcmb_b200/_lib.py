@@ -54,6 +54,8 @@ SIGNATURES = [
     ("abcmb_pert_forward_tangent", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp,
                                                   _d, _vp, _vp, _vp, _vp, _vp, _i64, _vp]),
     ("abcmb_hyrex_inputs", ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
+    ("abcmb_pert_vjp_theta", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp,
+                                             ctypes.c_int, _vp, _vp, _vp, _vp]),
     ("abcmb_pert_ind_workspace_size", _i64, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("abcmb_pert_forward_ind", ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp,
                                               _vp, _vp, _vp, _vp, _i64, _vp]),

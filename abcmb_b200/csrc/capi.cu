@@ -22,6 +22,9 @@ cudaError_t launch_pert_ind(int n_cosmo, const abcmb_cosmo* cosmo, const double*
                             int n_base, int n_var, const int32_t* items, const int32_t* var_base,
                             const abcmb_pert_settings& s, double* pt, abcmb_kstat* kstat, void* ws,
                             cudaStream_t stream, int warps_per_block, int* grid_out);
+cudaError_t launch_pert_vjp_theta(int n_cosmo, const abcmb_cosmo* cosmo, const double* pt, const double* pt_bar,
+                                  int n_save, int n_base, const int32_t* base, int n_dir, const int32_t* dirs,
+                                  const double* step, double* theta_bar, cudaStream_t stream);
 int64_t los_workspace_bytes(int n_cosmo, int max_nk, int nkt, int n_ell_tab, int n_save, int precision);
 cudaError_t launch_los(int n_cosmo, const abcmb_cosmo* cosmo_dev, const abcmb_cosmo* cosmo_host,
                        const double* tables, const double* kbuf, const double* pt, const double* kt,
@@ -294,6 +297,21 @@ int abcmb_pert_forward_ind(int n_cosmo, const abcmb_cosmo* cosmo_dev, const doub
                                          var_base_dev, *settings, pt_dev, kstat_dev, workspace_dev,
                                          static_cast<cudaStream_t>(stream), g_warps_per_block, &g_last_grid);
   if (e != cudaSuccess) return cuda_fail(e, "abcmb_pert_forward_ind");
+  return ABCMB_OK;
+}
+
+int abcmb_pert_vjp_theta(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* pt_dev, const double* pt_bar_dev,
+                         int n_save, int n_base, const int32_t* base_dev, int n_dir, const int32_t* dir_dev,
+                         const double* step_dev, double* theta_bar_dev, void* stream) {
+  if (n_cosmo <= 0 || n_base < 0 || !cosmo_dev || !pt_dev || !pt_bar_dev || !theta_bar_dev ||
+      (n_base > 0 && (!base_dev || !dir_dev || !step_dev)))
+    return fail(ABCMB_ERR_ARG, "abcmb_pert_vjp_theta: null argument");
+  if (n_dir < 1 || n_dir > 65535 || n_save < 2) return fail(ABCMB_ERR_ARG, "abcmb_pert_vjp_theta: n_dir / n_save");
+  if (n_base == 0) return ABCMB_OK;
+  if (n_base > 65535) return fail(ABCMB_ERR_ARG, "abcmb_pert_vjp_theta: at most 65535 base cosmologies per call");
+  cudaError_t e = abcmb::launch_pert_vjp_theta(n_cosmo, cosmo_dev, pt_dev, pt_bar_dev, n_save, n_base, base_dev, n_dir,
+                                               dir_dev, step_dev, theta_bar_dev, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "abcmb_pert_vjp_theta");
   return ABCMB_OK;
 }
 

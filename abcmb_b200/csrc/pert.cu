@@ -1957,4 +1957,53 @@ cudaError_t launch_pert_tangent(int n_cosmo, const abcmb_cosmo* cosmo, const dou
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// vector-Jacobian product with respect to the gradient parameters
+// ---------------------------------------------------------------------------
+constexpr int VJP_THREADS = 256;
+
+// theta_bar[b][p] = <pt_bar(base b), (PT(plus) - PT(minus)) / (2 step)>
+// over the base descriptor's whole PerturbationTable (fields x saves x k):
+// one block per (direction, base), a fixed-order block reduction (the same
+// result on every run).  A plus / minus descriptor outside the batch or of
+// another table shape gives NaN.
+__global__ void __launch_bounds__(VJP_THREADS) pert_vjp_theta_kernel(int n_cosmo, const abcmb_cosmo* __restrict__ cosmo,
+                                                                     const double* __restrict__ pt,
+                                                                     const double* __restrict__ pt_bar, int n_save,
+                                                                     const int32_t* __restrict__ base, int n_dir,
+                                                                     const int32_t* __restrict__ dirs,
+                                                                     const double* __restrict__ step,
+                                                                     double* __restrict__ theta_bar) {
+  __shared__ double red[VJP_THREADS];
+  const int q = blockIdx.x, b = blockIdx.y;
+  const int cb = base[b];
+  const int cp = dirs[(b * n_dir + q) * 2], cm = dirs[(b * n_dir + q) * 2 + 1];
+  const bool ok = cb >= 0 && cb < n_cosmo && cp >= 0 && cp < n_cosmo && cm >= 0 && cm < n_cosmo &&
+                  cosmo[cp].nk == cosmo[cb].nk && cosmo[cm].nk == cosmo[cb].nk;
+  double acc = 0.;
+  if (ok) {
+    const int64_t n = (int64_t)ABCMB_NFIELDS * n_save * cosmo[cb].nk;
+    const double* __restrict__ g = pt_bar + cosmo[cb].off_pt;
+    const double* __restrict__ xp = pt + cosmo[cp].off_pt;
+    const double* __restrict__ xm = pt + cosmo[cm].off_pt;
+    for (int64_t j = threadIdx.x; j < n; j += VJP_THREADS) acc = fma(g[j], xp[j] - xm[j], acc);
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = VJP_THREADS / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) theta_bar[b * n_dir + q] = ok ? red[0] / (2. * step[b * n_dir + q]) : NAN;
+}
+
+cudaError_t launch_pert_vjp_theta(int n_cosmo, const abcmb_cosmo* cosmo, const double* pt, const double* pt_bar,
+                                  int n_save, int n_base, const int32_t* base, int n_dir, const int32_t* dirs,
+                                  const double* step, double* theta_bar, cudaStream_t stream) {
+  dim3 g(n_dir, n_base);
+  pert_vjp_theta_kernel<<<g, VJP_THREADS, 0, stream>>>(n_cosmo, cosmo, pt, pt_bar, n_save, base, n_dir, dirs, step,
+                                                        theta_bar);
+  return cudaGetLastError();
+}
+
 }  // namespace abcmb

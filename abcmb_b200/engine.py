@@ -139,6 +139,28 @@ class DeviceBatch:
                                         self.ws_ind.numel(), ctypes.c_void_p(st.cuda_stream))
         _lib.check(rc, "abcmb_pert_forward_ind")
 
+    def pert_vjp_theta(self, gw, pt_bar: torch.Tensor, stream=None) -> torch.Tensor:
+        """abcmb_pert_vjp_theta after pert_forward_grad: dL/dtheta for
+        theta = FD_PARAMS (h, omega_b, omega_cdm, tau_reion) of every base
+        cosmology, [n_base, 4] on the device, from pt_bar = dL/dPT (a float64
+        tensor shaped like self.pt; the base descriptors' slots are read)."""
+        from .gradients import vjp_tables
+        if pt_bar.numel() != self.pt.numel() or pt_bar.dtype != torch.float64 or pt_bar.device != self.pt.device:
+            raise ValueError("pt_bar must be a float64 tensor on the batch's device shaped like the PerturbationTables")
+        lib = _lib.load()
+        st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        base, dirs, steps = vjp_tables(gw)
+        bt_ = torch.from_numpy(base).to(self.device)
+        dt_ = torch.from_numpy(dirs.reshape(-1)).to(self.device)
+        st_ = torch.from_numpy(steps.reshape(-1)).to(self.device)
+        out = torch.empty(len(base) * dirs.shape[1], dtype=torch.float64, device=self.device)
+        pt_bar = pt_bar.contiguous()
+        rc = lib.abcmb_pert_vjp_theta(self.batch.n_cosmo, _ptr(self.cosmo), _ptr(self.pt), _ptr(pt_bar),
+                                      self.batch.n_save, len(base), _ptr(bt_), dirs.shape[1], _ptr(dt_), _ptr(st_),
+                                      _ptr(out), ctypes.c_void_p(st.cuda_stream))
+        _lib.check(rc, "abcmb_pert_vjp_theta")
+        return out.view(len(base), dirs.shape[1])
+
     def pert_forward_grad(self, gw, settings: CPertSettings, stream=None):
         """The perturbations of a gradient-expanded batch (gradients.expand):
         one tangent launch, the record + replay launches of internal

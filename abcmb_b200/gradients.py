@@ -262,3 +262,15 @@ def ind_subset(gw: GradWorkload, sel) -> GradWorkload:
     tb = dataclasses.replace(b, items=items)
     return dataclasses.replace(gw, batch=tb, n_base_items=len(sel),
                                var_base=np.repeat(np.arange(len(sel), dtype=np.int32), per))
+
+
+def vjp_tables(gw: GradWorkload):
+    """(base [n_base] int32, dirs [n_base, 4, 2] int32, steps [n_base, 4])
+    of the FD_PARAMS directions: what abcmb_pert_vjp_theta reads."""
+    _, dirs_all = _directions(gw)
+    nb = len(gw.variants)
+    base = np.arange(nb, dtype=np.int32) * gw.n_var
+    dirs = np.ascontiguousarray(dirs_all[base, :len(FD_PARAMS)], dtype=np.int32)
+    steps = np.array([[var[next(j for j, v in enumerate(var) if v[0] == name and v[1] > 0)][2]
+                       for name in FD_PARAMS] for var in gw.variants], dtype=np.float64)
+    return base, dirs, steps

@@ -12,7 +12,11 @@
   theta = (h, omega_b, omega_cdm, A_s, n_s, tau_reion) of a batch of
   cosmologies to C_l^{TT,TE,EE}; its backward contracts the incoming
   cotangent with dC_l/dtheta computed in the same batched launch
-  (central differences for h, omega_b, omega_cdm, tau_reion; exact A_s, n_s).
+  (central differences of the replayed discretisation -- internal numerical
+  differentiation -- for h, omega_b, omega_cdm, tau_reion; exact A_s, n_s).
+* ``PTWithGrad``: theta -> the base cosmologies' PerturbationTables, whose
+  backward is abcmb_pert_vjp_theta (the cotangent contracted with the
+  derivative columns of the same launch).
 """
 from __future__ import annotations
 
@@ -118,7 +122,7 @@ class ClWithGrad(torch.autograd.Function):
         for i, p in enumerate(w.params_in):
             for j, name in enumerate(configs.GRAD_PARAMS):
                 p[name] = float(th[i, j])
-        gw = gradients.expand(w)
+        gw = gradients.expand(w, mode="ind")
         db = engine.DeviceBatch.upload(gw.batch, theta.device if theta.is_cuda else None)
         db.pert_forward_grad(gw, w.pert_settings())
         db.check_status()
@@ -135,3 +139,59 @@ class ClWithGrad(torch.autograd.Function):
     def backward(ctx, g: Tensor):
         (grad,) = ctx.saved_tensors                 # (n, 6, 3, n_l)
         return torch.einsum("npxl,nxl->np", grad, g.to(grad.dtype)), None
+
+
+class PTWithGrad(torch.autograd.Function):
+    """theta (n, 6) -> the n cosmologies' PerturbationTables, one flat float64
+    tensor: cosmology i's table (ABCMB_NFIELDS x n_save x Nk_i, the C ABI's
+    layout) starting at ``pt_offsets(base)[i]``.  The backward contracts the
+    cotangent with dPT/dtheta of the same ind launch (abcmb_pert_vjp_theta);
+    A_s and n_s do not enter the perturbations (zero cotangent).  For losses
+    that depend on theta only through the PerturbationTable; C_l also depends
+    on theta through the background of the line of sight, which ClWithGrad
+    covers."""
+
+    @staticmethod
+    def forward(ctx, theta: Tensor, base) -> Tensor:
+        import dataclasses
+        import numpy as np
+        from . import configs, engine, gradients
+        th = theta.detach().cpu().numpy()
+        w = dataclasses.replace(base, params_in=[dict(p) for p in base.params_in], batch=None)
+        for i, p in enumerate(w.params_in):
+            for j, name in enumerate(configs.GRAD_PARAMS):
+                p[name] = float(th[i, j])
+        gw = gradients.expand(w, mode="ind")
+        db = engine.DeviceBatch.upload(gw.batch, theta.device if theta.is_cuda else None)
+        db.pert_forward_grad(gw, w.pert_settings())
+        db.check_status()
+        b = gw.batch
+        idx = []
+        for i in range(len(w.params_in)):
+            c = b.cosmo[i * gw.n_var]
+            o = int(c["off_pt"])
+            idx.append(np.arange(o, o + packing.NFIELDS * b.n_save * int(c["nk"])))
+        idx = torch.from_numpy(np.concatenate(idx)).to(db.pt.device)
+        ctx.db, ctx.gw, ctx.idx = db, gw, idx
+        return db.pt[idx].clone()
+
+    @staticmethod
+    def backward(ctx, g: Tensor):
+        from . import configs, gradients
+        db = ctx.db
+        pt_bar = torch.zeros_like(db.pt)
+        pt_bar[ctx.idx] = g.to(pt_bar.dtype)
+        tb = db.pert_vjp_theta(ctx.gw, pt_bar)                 # (n, 4) in FD_PARAMS order
+        out = torch.zeros(tb.shape[0], len(configs.GRAD_PARAMS), dtype=tb.dtype, device=tb.device)
+        for q, name in enumerate(gradients.FD_PARAMS):
+            out[:, configs.GRAD_PARAMS.index(name)] = tb[:, q]
+        return out, None
+
+
+def pt_offsets(base, n_save: int = 500) -> list:
+    """Start of each cosmology's table in PTWithGrad's output."""
+    offs, o = [], 0
+    for kg in base.kgrids:
+        offs.append(o)
+        o += packing.NFIELDS * n_save * len(kg)
+    return offs

@@ -428,6 +428,34 @@ int abcmb_pert_forward_ind(int n_cosmo, const abcmb_cosmo* cosmo_dev,
                            void* stream);
 
 /*
+ * Vector-Jacobian product of the perturbation integration with respect to
+ * the gradient parameters: the cotangent of a PerturbationTable
+ * contracted with the table's derivative columns, which
+ * abcmb_pert_forward_ind (or _tangent, or whole-solve differences) leaves
+ * in the variants' tables.  What jax.grad of a loss of the PerturbationTable
+ * returns for the background parameters in the reference (the
+ * PerturbationTable is differentiable in params through diffeqsolve,
+ * abcmb/perturbations.py:285-312, abcmb/main.py:111).
+ *   pt_dev        the batch's PerturbationTables after the gradient launch
+ *   pt_bar_dev    a buffer shaped like pt_dev; only the base descriptors'
+ *                 slots are read (dL/dPT of each base cosmology)
+ *   base_dev      [n_base] descriptor index of each base cosmology
+ *   dir_dev       [n_base][n_dir][2] (plus, minus) descriptor of direction p
+ *   step_dev      [n_base][n_dir] the parameter step eps of direction p
+ *                 (plus = theta + eps, minus = theta - eps)
+ *   theta_bar_dev [n_base][n_dir] out: <pt_bar, (PT(+) - PT(-)) / (2 eps)>,
+ *                 NaN where a descriptor is out of range or of another table
+ *                 shape
+ * Deterministic (fixed-order reductions).  A_s and n_s do not enter the
+ * perturbations (their cotangent at this level is zero).  Cotangents with
+ * respect to individual background-table entries need the discrete
+ * adjoint of the integration, which this library does not provide.
+ */
+int abcmb_pert_vjp_theta(int n_cosmo, const abcmb_cosmo* cosmo_dev, const double* pt_dev, const double* pt_bar_dev,
+                         int n_save, int n_base, const int32_t* base_dev, int n_dir, const int32_t* dir_dev,
+                         const double* step_dev, double* theta_bar_dev, void* stream);
+
+/*
  * abcmb_pert_forward for callers that cannot allocate device memory (no
  * cudaMalloc, no workspace of their own: e.g. code inside a framework that
  * owns every device byte).  No counterpart in the reference.  Same inputs,
