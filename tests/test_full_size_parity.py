@@ -86,3 +86,42 @@ def test_c4_full_size_cosmologies_match_oracle(gpu):
           f"EE {errs[2]:.2e}; k modes with the oracle's step counts {same:.3f}")
     assert max(errs) < CL_TOL, errs
     assert same >= 0.9
+
+
+def test_c5_full_size_cosmology_lensed_gradient_and_pk(gpu):
+    """One cosmology of the lensed batch at its real size (the C5 draw with
+    its seed: k to 5 / Mpc, lensed TT/TE/EE to l = 3000 with the line of
+    sight to 3500, P(k) at z = 0..3 for 200 k to 5 / Mpc), the six-parameter
+    gradient by internal numerical differentiation on both sides (13
+    descriptors, 9 integrated): lensed C_l of every descriptor within 1e-4
+    of the oracle's, every gradient series within 1e-3 of its maximum (the
+    A_s, n_s rows are central differences here, with lensing), P(k) within
+    1e-4."""
+    from abcmb_b200 import bessel, configs, gradients, lensing, pipeline
+    from oracle import oracle
+    w = configs.c5(n_cosmo=1)
+    gi = gradients.expand(w, processes=4, mode="ind")
+    kout = configs.c5_pk_k()
+    z = np.array(configs.C5_PK_Z)
+    cl, grad, pk, cl_var = pipeline.run_cl_grad(gi, "cuda:0", kout, z, return_variants=True)
+    st = w.pert_settings()
+    rc, pt_o, _ = oracle.pert_forward_ind(gi.batch, st, gi.n_base_items, gi.var_base)
+    assert rc == 0
+    rc, _, cl_unl = oracle.los_forward(gi.batch, pt_o, w.kt, w.los_settings(), bessel.load())
+    assert rc == 0
+    mu, wt = lensing.lensing_nodes(w.l_max)
+    rc, _, cll = oracle.lens_forward(gi.batch, pt_o, lensing.lens_descriptors(gi.batch), mu, wt, cl_unl,
+                                     w.lens_settings())
+    assert rc == 0
+    cl_o, grad_o = gi.assemble(cll, np.zeros_like(cll))
+    pk_o = oracle.pk_lin(gi.batch, pt_o, w.specs["k_pivot"], kout, z)[::gi.n_var]
+    var_err = max(float(np.abs(cl_var[i, X] - cll[i, X]).max() / np.abs(cll[i, X]).max())
+                  for i in range(cl_var.shape[0]) for X in range(3))
+    g_err = np.abs(grad - grad_o).max(axis=-1) / (np.abs(grad_o).max(axis=-1) + 1e-300)
+    pk_err = float(np.max(np.abs(pk / pk_o - 1)))
+    print(f"C5 full-size cosmology (Nk {int(w.batch.cosmo['nk'][0])}): lensed C_l of the 13 descriptors "
+          f"{var_err:.2e}; gradient (h, omega_b, omega_cdm, A_s, n_s, tau_reion) x (TT, TE, EE) "
+          f"{np.array2string(g_err[0], precision=2)}; P(k) {pk_err:.2e}")
+    assert var_err < 1e-4
+    assert g_err.max() < 1e-3, g_err
+    assert pk_err < 1e-4
