@@ -233,3 +233,39 @@ def test_ind_bad_variant_reported(gpu, c1_ind):
     bad_layout = 4                   # ABCMB_STATUS_BAD_LAYOUT
     assert ks["status"][nb] == bad_layout and ks["status"][nb + 1] == bad_layout
     assert np.all(ks["status"][nb + 2:] == 0) and np.all(ks["status"][:nb] == 0)
+
+
+def test_oracle_ind_base_failure_propagates(c1_ind):
+    """A base item that stops (max_steps) records nothing to replay: its
+    variants report a non-finite status instead of being integrated."""
+    from oracle import oracle
+    w, gi = c1_ind
+    st = w.pert_settings()
+    st.max_steps = 300
+    rc, _, ks = oracle.pert_forward_ind(gi.batch, st, gi.n_base_items, gi.var_base)
+    nb = gi.n_base_items
+    failed = ks["status"][:nb] == 1
+    assert rc != 0 and failed.any() and not failed.all()
+    var = ks["status"][nb:].reshape(nb, 8)
+    assert np.all(var[failed] == 2) and np.all(var[~failed] == 0)
+
+
+@pytest.mark.gpu
+def test_ind_base_failure_propagates(gpu, c1_ind):
+    """The same on the GPU: max_steps reached in the record launch, the
+    variants of those items report ABCMB_STATUS_NONFINITE, the others run,
+    and the batch raises like diffrax."""
+    from abcmb_b200 import _lib
+    w, gi = c1_ind
+    st = w.pert_settings()
+    st.max_steps = 300
+    db = gpu.DeviceBatch.upload(gi.batch)
+    db.pert_forward_grad(gi, st)
+    ks = db.kstat_host()
+    nb = gi.n_base_items
+    failed = ks["status"][:nb] == 1
+    assert failed.any() and not failed.all()
+    var = ks["status"][nb:].reshape(nb, 8)
+    assert np.all(var[failed] == 2) and np.all(var[~failed] == 0)
+    with pytest.raises(_lib.ABCMBError, match="max_steps"):
+        db.check_status()
