@@ -6,16 +6,16 @@
 * ``B200Model(user_species=None, **specs)(params) -> Output`` mirrors
   ``Model.__init__`` / ``Model.__call__`` (main.py:84-184, 289-298): specs
   with the reference's defaults, the reference's k grids, the perturbation and
-  spectrum stages on the CUDA kernels.  The recombination history (x_e, T_m,
-  z_reion) comes from ``background_tables.make_recombination``, the host
-  model that stands in for HyRex here; the conformal-time table, optical
-  depth, visibility and line-of-sight arrays are then produced on the GPU by
-  abcmb_bg_forward with the reference's own Kvaerno5 solves
-  (``background="device"``, the default), or by the host model
-  (``background="host"``).  ``recombination="hyrex"`` takes the
-  recombination history from HyRex on the GPU instead (abcmb_hyrex_forward,
-  in the reference's padded layout); its end-to-end run through the spectra
-  is not yet covered by a GPU test.
+  spectrum stages on the CUDA kernels.  The recombination history (x_e, T_m)
+  comes, as in the reference's Model (main.py:220), from HyRex -- here on the
+  GPU (abcmb_hyrex_inputs + abcmb_hyrex_forward, the reference's padded
+  layout; ``recombination="hyrex"``, the default with
+  ``background="device"``) -- and the conformal-time table, optical depth,
+  visibility and line-of-sight arrays from abcmb_bg_forward with the
+  reference's own Kvaerno5 solves.  ``recombination="peebles"`` takes the
+  history from ``background_tables.make_recombination`` (a host model, the
+  synthetic workloads' stand-in) instead, and ``background="host"`` (which
+  implies it) computes the background on the host too.
 * ``write_class_cl`` / ``read_class_cl``: C_l files in CLASS's ``cl.dat``
   layout (dimensionless l(l+1)/2pi C_l, columns l, TT, EE, TE, BB, phiphi),
   the format the reference's example notebooks compare against
@@ -60,10 +60,12 @@ def _species_names(user_species) -> tuple:
 class B200Model:
     """Model(**specs)(params) on the CUDA path (abcmb/main.py:84-184)."""
 
-    def __init__(self, user_species=None, device=None, background: str = "device", recombination: str = "peebles",
+    def __init__(self, user_species=None, device=None, background: str = "device", recombination: str = None,
                  **kwargs):
         if background not in ("device", "host"):
             raise ValueError("background must be 'device' or 'host'")
+        if recombination is None:
+            recombination = "hyrex" if background == "device" else "peebles"
         if recombination not in ("peebles", "hyrex"):
             raise ValueError("recombination must be 'peebles' or 'hyrex'")
         if recombination == "hyrex" and background != "device":

@@ -217,8 +217,10 @@ def test_model_setup_mirrors_reference_defaults():
 
 def test_model_background_and_recombination_options():
     from abcmb_b200.output import B200Model
-    assert B200Model(l_max=400).background == "device"
-    assert B200Model(l_max=400, recombination="hyrex").recombination == "hyrex"
+    m = B200Model(l_max=400)
+    assert m.background == "device" and m.recombination == "hyrex"
+    assert B200Model(l_max=400, background="host").recombination == "peebles"
+    assert B200Model(l_max=400, recombination="peebles").recombination == "peebles"
     with pytest.raises(ValueError):
         B200Model(l_max=400, background="gpu")
     with pytest.raises(ValueError):
