@@ -111,14 +111,22 @@ PRIMORDIAL_PARAMS = ("A_s", "n_s")
 
 
 def expand(w: Workload, n_save: int = 500, processes: int = 0, rel_step: float = REL_STEP,
-           primordial_fd: bool = None, mode: str = "fd") -> GradWorkload:
-    """Background tables for every variant (host, optionally in a spawn pool).
+           primordial_fd: bool = None, mode: str = "fd", recombination: str = "host",
+           device=None) -> GradWorkload:
+    """Background tables for every variant.
 
-    primordial_fd (default: the workload's lensing flag) adds the A_s and n_s
-    +- descriptors that share their base cosmology's perturbations.  mode:
-    "tangent" or "fd" (module docstring)."""
+    recombination="host": the host background model (optionally in a spawn
+    pool); "hyrex": every descriptor's recombination history from HyRex on
+    the GPU (one abcmb_hyrex_forward call for the whole expansion) and its
+    conformal time, optical depth and line-of-sight arrays from
+    abcmb_bg_forward, as B200Model computes a single cosmology.  primordial_fd
+    (default: the workload's lensing flag) adds the A_s and n_s +-
+    descriptors that share their base cosmology's perturbations.  mode:
+    "ind", "tangent" or "fd" (module docstring)."""
     if mode not in MODES:
         raise ValueError(f"mode must be one of {MODES}")
+    if recombination not in ("host", "hyrex"):
+        raise ValueError("recombination must be 'host' or 'hyrex'")
     if primordial_fd is None:
         primordial_fd = bool(w.lensing)
     jobs, variants, layouts, kgrids, alias, overrides, work, dir_rows = [], [], [], [], [], [], [], []
@@ -149,7 +157,21 @@ def expand(w: Workload, n_save: int = 500, processes: int = 0, rel_step: float =
                     work.append(False)
         variants.append(entries)
     real = [j for j in jobs if j is not None]
-    if processes and processes > 1:
+    if recombination == "hyrex":
+        from . import recombination as rec
+        ps = [cosmology.add_derived_parameters(j[0], j[1], j[2]) for j in real]
+        ncs = [j[1] for j in real]
+        h = rec.hyrex_forward(ps, ncs, device)
+        bgs_real = [bt.from_hyrex(p, nc, h["xe"][i], h["lna_xe"][i], h["Tm"][i], h["lna_tm"][i])
+                    for i, (p, nc) in enumerate(zip(ps, ncs))]
+        # conformal time, optical depth and line-of-sight arrays of every
+        # history on the device (abcmb_bg_forward), fetched into the tables
+        from . import engine
+        lays = [sp.state_layout(j[2], j[1]) for j in real]
+        kgs = [kgrids[i] for i, j in enumerate(jobs) if j is not None]
+        tmp = packing.pack(bgs_real, lays, kgs, n_save=n_save, work=[False] * len(bgs_real))
+        engine.DeviceBatch.upload(tmp, device).bg_forward(packing.bg_settings(n_save), fetch_tables=True)
+    elif processes and processes > 1:
         import multiprocessing as mp
         with mp.get_context("spawn").Pool(processes) as pool:
             bgs_real = pool.map(_bg_job, real, chunksize=max(1, len(real) // (4 * processes)))

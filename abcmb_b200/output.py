@@ -102,6 +102,34 @@ class B200Model:
         Pk = self.SS.Pk_lin(self.k_axis_Pk_output, 0.0, PT, p)
         return Output(tt, te, ee, Pk, self.SS.ells, self.k_axis_Pk_output, BG, PT, p)
 
+    def cl_and_grad(self, params: dict, mode: str = "ind") -> dict:
+        """C_l and their derivatives with respect to theta = (h, omega_b,
+        omega_cdm, A_s, n_s, tau_reion) for one cosmology -- what
+        jax.jacfwd of the reference's Model gives for the spectra
+        (abcmb/main.py:111, docs/FAQ.rst:24-28) -- in one batched GPU pass:
+        the cosmology and its +-1e-4 relative variants (their own
+        recombination histories and backgrounds, as this model computes
+        them), the perturbations by internal numerical differentiation
+        (mode="ind"; "tangent" and "fd" as in gradients.expand), the line of
+        sight (and lensing) of every descriptor, central differences.
+        Returns {"l", "ClTT", "ClTE", "ClEE", "grad": {param: {"TT", "TE",
+        "EE"}}}; params missing from ``params`` take the derived defaults."""
+        from . import configs, gradients, pipeline
+        p_in = dict(params)
+        derived = self.add_derived_parameters(p_in)
+        for name in configs.GRAD_PARAMS:
+            p_in.setdefault(name, derived[name])
+        w = configs.Workload("model", dict(self.specs), [p_in], [self.has_ncdm],
+                             [np.asarray(self.PE.k_axis_perturbations, dtype=np.float64)],
+                             int(self.specs["l_max"]), bool(self.specs["lensing"]), xe_layout="hyrex")
+        gw = gradients.expand(w, mode=mode, device=self.device,
+                              recombination="hyrex" if self.recombination == "hyrex" else "host")
+        cl, grad, _ = pipeline.run_cl_grad(gw, self.device)
+        out = {"l": self.SS.ells, "ClTT": cl[0, 0], "ClTE": cl[0, 1], "ClEE": cl[0, 2], "grad": {}}
+        for i, name in enumerate(configs.GRAD_PARAMS):
+            out["grad"][name] = {"TT": grad[0, i, 0], "TE": grad[0, i, 1], "EE": grad[0, i, 2]}
+        return out
+
 
 CLASS_COLUMNS = ("l", "TT", "EE", "TE", "BB", "phiphi")
 

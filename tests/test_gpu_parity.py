@@ -492,3 +492,39 @@ def test_model_hyrex_matches_the_oracle_chain(gpu):
     rel_ee = np.max(np.abs(out.ClEE - cl_o[0, 2]) / cl_o[0, 2])
     print(f"HyRex model vs oracle chain: TT {rel_tt:.2e} EE {rel_ee:.2e}")
     assert rel_tt < 1e-4 and rel_ee < 1e-4, (rel_tt, rel_ee)
+
+
+def test_model_cl_and_grad_matches_the_oracle(gpu):
+    """B200Model(...).cl_and_grad(params): HyRex and the background of the
+    base cosmology and its +-1e-4 variants on the GPU, the perturbations by
+    record and replay, the line of sight and the central differences --
+    against the oracle's record-and-replay perturbations and line of sight
+    on the same descriptors (C_l within 1e-6, every gradient series within
+    1e-4 of its maximum); the base C_l also match the forward call's."""
+    from abcmb_b200 import bessel, configs, gradients
+    from abcmb_b200.output import B200Model
+    from oracle import oracle
+    m = B200Model(l_max=400, l_max_g=12, l_max_pol_g=12, l_max_massless_nu=12)
+    params = dict(configs.FIDUCIAL)
+    r = m.cl_and_grad(params)
+    assert r["ClTT"].shape == (399,) and set(r["grad"]) == set(configs.GRAD_PARAMS)
+    fwd = m(params)
+    assert np.max(np.abs(r["ClTT"] - fwd.ClTT) / fwd.ClTT) < 1e-9
+    # the same expansion, perturbations and line of sight on the oracle
+    w = configs.Workload("model", dict(m.specs), [params], [False], [m.PE.k_axis_perturbations],
+                         400, False, xe_layout="hyrex")
+    gi = gradients.expand(w, mode="ind", recombination="hyrex")
+    rc, pt_o, _ = oracle.pert_forward_ind(gi.batch, w.pert_settings(), gi.n_base_items, gi.var_base)
+    assert rc == 0
+    ls = w.los_settings()
+    _, _, cl_o = oracle.los_forward(gi.batch, pt_o, w.kt, ls, bessel.load())
+    # dC_l/dn_s of the oracle's own line of sight: central difference over n_s
+    cl_b, grad_o = gi.assemble(cl_o, np.zeros_like(cl_o))
+    assert np.max(np.abs(r["ClTT"] - cl_b[0, 0]) / np.abs(cl_b[0, 0])) < 1e-6
+    for gi_, name in enumerate(configs.GRAD_PARAMS):
+        if name == "n_s":
+            continue
+        for X, key in enumerate(("TT", "TE", "EE")):
+            g, go = r["grad"][name][key], grad_o[0, gi_, X]
+            err = np.abs(g - go).max() / np.abs(go).max()
+            assert err < 1e-4, (name, key, err)
