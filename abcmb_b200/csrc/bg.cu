@@ -234,45 +234,71 @@ struct BgArgs {
   abcmb_bg_settings s;
   abcmb_bgstat* stat;
   double* nodes;        // per cosmology: 3 (max_steps_tau + 1) + 3 (max_steps_kappa + 1) doubles
+  int32_t* solve;       // per cosmology: status, step attempts, dense points of both solves (8 ints)
 };
 
+// omega_r (main.py:581-586) and tau_approx's scale (background.py:274-276)
+__device__ __forceinline__ void early_radiation(const abcmb_cosmo& c, double& sq_or, double& tscale) {
+  const double a_early = exp(-23.0);
+  const double omega_r = rho_all(c, a_early).tot * a_early * a_early * a_early * a_early / RHO_CRIT_UNIT;
+  sq_or = sqrt(omega_r);
+  tscale = H0H / C_MPC;
+}
+
+// The two solves of every cosmology: one two-warp block per cosmology (the
+// conformal-time solve on warp 0, the optical-depth solve on warp 1), so a
+// whole batch runs in one wave; the dense-output nodes go to the workspace,
+// the statuses and counts to A.solve.
+__global__ void __launch_bounds__(64) bg_solve_kernel(BgArgs A) {
+  const int ci = blockIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const abcmb_cosmo c = A.cosmo[ci];
+  const int cap_t = A.s.max_steps_tau + 1, cap_k = A.s.max_steps_kappa + 1;
+  double* nb = A.nodes + (size_t)ci * 3 * (size_t)(cap_t + cap_k);
+  double sq_or, tscale;
+  early_radiation(c, sq_or, tscale);
+  int ns = 0, np = 0, st;
+  if (wid == 0) {
+    const DenseNodes Dt{nb, nb + cap_t, nb + 2 * cap_t};
+    st = quad_solve_warp(0, c, A.tables, BG_LNA_CUT, 0.0, exp(BG_LNA_CUT) / tscale / sq_or, 1e-5, 1e-8, 1e-8, 0.,
+                         1., 0., A.s.max_steps_tau, Dt, ns, np, lane);
+  } else {
+    double* nk = nb + 3 * (size_t)cap_t;
+    const DenseNodes Dk{nk, nk + cap_k, nk + 2 * cap_k};
+    st = quad_solve_warp(1, c, A.tables, 0.0, -10.0, 0.0, -1e-3, 1e-10, 1e-10, 0.4, 0.3, 0.,
+                         A.s.max_steps_kappa, Dk, ns, np, lane);
+  }
+  if (lane == 0) {
+    int32_t* o = A.solve + (size_t)ci * 8 + 3 * wid;
+    o[0] = st;
+    o[1] = ns;
+    o[2] = np;
+  }
+}
+
+// Everything after the solves: the conformal-time table, the visibility
+// peak and lna_rec, lna_transfer_start and the six line-of-sight arrays; one
+// 256-thread block per cosmology.
 __global__ void __launch_bounds__(BG_THREADS) bg_kernel(BgArgs A) {
   const int ci = blockIdx.x;
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int tid = threadIdx.x;
   const abcmb_cosmo c = A.cosmo[ci];
   const int cap_t = A.s.max_steps_tau + 1, cap_k = A.s.max_steps_kappa + 1;
   double* nb = A.nodes + (size_t)ci * 3 * (size_t)(cap_t + cap_k);
   const DenseNodes Dt{nb, nb + cap_t, nb + 2 * cap_t};
   double* nk = nb + 3 * (size_t)cap_t;
   const DenseNodes Dk{nk, nk + cap_k, nk + 2 * cap_k};
-  __shared__ int sh_status[2], sh_steps[2], sh_pts[2];
   __shared__ double red_v[BG_THREADS / 32];
   __shared__ int red_i[BG_THREADS / 32];
   __shared__ double sh_lts;
 
-  // omega_r (main.py:581-586) and tau_approx (background.py:274-276)
-  const double a_early = exp(-23.0);
-  const double omega_r = rho_all(c, a_early).tot * a_early * a_early * a_early * a_early / RHO_CRIT_UNIT;
-  const double sq_or = sqrt(omega_r);
-  const double tscale = H0H / C_MPC;
-
-  if (wid < 2) {
-    int ns = 0, np = 0, st;
-    if (wid == 0)
-      st = quad_solve_warp(0, c, A.tables, BG_LNA_CUT, 0.0, exp(BG_LNA_CUT) / tscale / sq_or, 1e-5, 1e-8, 1e-8, 0.,
-                           1., 0., A.s.max_steps_tau, Dt, ns, np, lane);
-    else
-      st = quad_solve_warp(1, c, A.tables, 0.0, -10.0, 0.0, -1e-3, 1e-10, 1e-10, 0.4, 0.3, 0.,
-                           A.s.max_steps_kappa, Dk, ns, np, lane);
-    if (lane == 0) {
-      sh_status[wid] = st;
-      sh_steps[wid] = ns;
-      sh_pts[wid] = np;
-    }
-  }
-  __syncthreads();
+  double sq_or, tscale;
+  early_radiation(c, sq_or, tscale);
+  // the two solves' results (bg_solve_kernel, earlier on the stream)
+  const int32_t* sv = A.solve + (size_t)ci * 8;
+  const int sh_status[2] = {sv[0], sv[3]}, sh_steps[2] = {sv[1], sv[4]};
   const int status = sh_status[0] != ABCMB_STATUS_OK ? sh_status[0] : sh_status[1];
-  const int npt = sh_pts[0], npk = sh_pts[1];
+  const int npt = sv[2], npk = sv[5];
   if (status != ABCMB_STATUS_OK || npt < 2 || npk < 2) {
     if (tid == 0) {
       abcmb_bgstat r{};
@@ -282,7 +308,7 @@ __global__ void __launch_bounds__(BG_THREADS) bg_kernel(BgArgs A) {
       r.n_accepted_kappa = npk - 1;
       A.stat[ci] = r;
     }
-    return;                                 // block-uniform: every thread read the same shared status
+    return;                                 // block-uniform: every thread read the same solve record
   }
 
   // conformal-time table: analytic before lna_cut, dense solution after
@@ -355,13 +381,20 @@ __global__ void __launch_bounds__(BG_THREADS) bg_kernel(BgArgs A) {
   }
 }
 
-int64_t bg_workspace_bytes(int n_cosmo, const abcmb_bg_settings& s) {
+static int64_t bg_nodes_bytes(int n_cosmo, const abcmb_bg_settings& s) {
   return (int64_t)n_cosmo * 3 * ((int64_t)s.max_steps_tau + 1 + (int64_t)s.max_steps_kappa + 1) * 8;
+}
+
+int64_t bg_workspace_bytes(int n_cosmo, const abcmb_bg_settings& s) {
+  return (bg_nodes_bytes(n_cosmo, s) + 255) / 256 * 256 + (int64_t)n_cosmo * 8 * 4;
 }
 
 cudaError_t launch_bg(int n_cosmo, abcmb_cosmo* cosmo, double* tables, const abcmb_bg_settings& s,
                       abcmb_bgstat* stat, void* ws, cudaStream_t stream) {
-  BgArgs A{n_cosmo, cosmo, tables, s, stat, static_cast<double*>(ws)};
+  char* w = static_cast<char*>(ws);
+  BgArgs A{n_cosmo, cosmo, tables, s, stat, reinterpret_cast<double*>(w),
+           reinterpret_cast<int32_t*>(w + (bg_nodes_bytes(n_cosmo, s) + 255) / 256 * 256)};
+  bg_solve_kernel<<<n_cosmo, 64, 0, stream>>>(A);
   bg_kernel<<<n_cosmo, BG_THREADS, 0, stream>>>(A);
   return cudaGetLastError();
 }

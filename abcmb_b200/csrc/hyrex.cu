@@ -1,7 +1,7 @@
 // hyrex.cu -- the recombination history of HyRex on the GPU
 // (abcmb/hyrex/hyrex.py, helium.py, hydrogen.py, recomb_functions.py).
 //
-// One thread per cosmology follows the reference's seven phases, each in its
+// One thread per cosmology (one warp each) follows the reference's seven phases, each in its
 // fixed-size buffer joined the way array_with_padding.concat joins them (the
 // next buffer starts after the last finite entry, every buffer keeps its
 // length, the rest stays +inf):
@@ -477,9 +477,12 @@ __global__ void hyrex_fill_kernel(double* a, int64_t n) {
     a[i] = INFINITY;
 }
 
+// One history per warp (lane 0): the histories' step sequences diverge, and
+// each is bound by its own FP64 latency chain, so warps of their own run
+// faster than 32 histories sharing a warp.
 __global__ void __launch_bounds__(32) hyrex_kernel(HyrexArgs A) {
-  const int ci = blockIdx.x * blockDim.x + threadIdx.x;
-  if (ci >= A.n_cosmo) return;
+  const int ci = blockIdx.x;
+  if (threadIdx.x != 0 || ci >= A.n_cosmo) return;
   Hx h;
   h.t = A.tabs;
   h.n = A.n_grid;
@@ -761,7 +764,7 @@ cudaError_t launch_hyrex(int n_cosmo, int n_grid, const double* T, const double*
   hyrex_fill_kernel<<<296, 256, 0, stream>>>(lna_xe, nx);
   hyrex_fill_kernel<<<296, 256, 0, stream>>>(tm, nt);
   hyrex_fill_kernel<<<296, 256, 0, stream>>>(lna_tm, nt);
-  hyrex_kernel<<<(n_cosmo + 31) / 32, 32, 0, stream>>>(A);
+  hyrex_kernel<<<n_cosmo, 32, 0, stream>>>(A);
   return cudaGetLastError();
 }
 

@@ -213,7 +213,8 @@ typedef struct abcmb_bgstat {
 } abcmb_bgstat;
 
 /* Bytes of device workspace abcmb_bg_forward needs (the dense-output nodes
- * of both solves, (max_steps + 1) x 3 doubles each per cosmology). */
+ * of both solves, (max_steps + 1) x 3 doubles each per cosmology, and 32
+ * bytes per cosmology for the solves' statuses and counts). */
 int64_t abcmb_bg_workspace_size(int n_cosmo, const abcmb_bg_settings* settings);
 
 /*
