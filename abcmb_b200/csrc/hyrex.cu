@@ -329,9 +329,12 @@ __device__ bool phase_event(const Hx& h, int ph, double t, const double* y) {
 // SaveAt(ts = t0 + spacing * (1..n_save)), Event, max_steps) for m <= 2
 // components; the saved points go to ts_a[i] (and ts_b[i]), y_a[i], y_b[i]
 // (y_b / ts_b only for m = 2).  At most n_save points are written.
+// Every lane of the history's warp runs the solver with the same values;
+// the 2m right-hand sides of the central-difference Jacobian are evaluated
+// by lanes 0 .. 2m-1 at once, and lane isave % 32 writes save isave.
 __device__ int kv3_solve(const Hx& h, const Kv3& K, int ph, int m, double t0, const double* y0, double rtol,
                          double atol, int max_steps, int n_save, double* ts_a, double* ts_b, double* y_a,
-                         double* y_b, int& n_saved, int& n_steps) {
+                         double* y_b, int& n_saved, int& n_steps, int lane) {
   const double g = K.g;
   const double coeff1 = 1.0 / 3.0;       // pcoeff 0, icoeff 1, dcoeff 0, error order 3
   const double t_first = t0 + HX_SPACING, t_last = t0 + (double)n_save * HX_SPACING;
@@ -350,14 +353,25 @@ __device__ int kv3_solve(const Hx& h, const Kv3& K, int ph, int m, double t0, co
       double J[2][2], z[2];
       for (int j = 0; j < m; ++j) z[j] = y[j] + hs * (K.a[1][0] + g) * Fs[0][j];
       const double tz = t + K.c[1] * hs;
+      // lane 2 col + 0 / 1: the + / - evaluation of column col
+      double fl[2] = {0., 0.};
+      {
+        const int col = lane >> 1;
+        if (col < m) {
+          const double d = 1e-7 * fmax(fabs(z[col]), 1e-8);
+          double zz[2] = {z[0], m > 1 ? z[1] : 0.};
+          if (lane & 1) zz[col] -= d;
+          else zz[col] += d;
+          phase_rhs(h, ph, tz, zz, fl);
+        }
+      }
       for (int col = 0; col < m; ++col) {
         const double d = 1e-7 * fmax(fabs(z[col]), 1e-8);
-        double zp[2] = {z[0], m > 1 ? z[1] : 0.}, zm[2] = {z[0], m > 1 ? z[1] : 0.}, fp[2], fm[2];
-        zp[col] += d;
-        zm[col] -= d;
-        phase_rhs(h, ph, tz, zp, fp);
-        phase_rhs(h, ph, tz, zm, fm);
-        for (int row = 0; row < m; ++row) J[row][col] = (fp[row] - fm[row]) / (2. * d);
+        for (int row = 0; row < m; ++row) {
+          const double fp = __shfl_sync(0xffffffffu, fl[row], 2 * col);
+          const double fm = __shfl_sync(0xffffffffu, fl[row], 2 * col + 1);
+          J[row][col] = (fp - fm) / (2. * d);
+        }
       }
       double M[2][2];
       for (int a = 0; a < m; ++a)
@@ -433,17 +447,19 @@ __device__ int kv3_solve(const Hx& h, const Kv3& K, int ph, int m, double t0, co
       while (isave < n_save) {
         const double ts = (isave == n_save - 1) ? t_last : t_first + (double)isave * tstep;
         if (!(ts <= t1)) break;
-        const double th = (ts - t) / hs;
-        for (int j = 0; j < m; ++j) {
-          const double k0 = hs * Fs[0][j], k1 = hs * Fs[3][j];
-          const double a = k0 + k1 + 2. * y[j] - 2. * y1[j];
-          const double b = -2. * k0 - k1 - 3. * y[j] + 3. * y1[j];
-          const double val = ((a * th + b) * th + k0) * th + y[j];
-          if (j == 0) y_a[isave] = val;
-          else y_b[isave] = val;
+        if ((isave & 31) == lane) {
+          const double th = (ts - t) / hs;
+          for (int j = 0; j < m; ++j) {
+            const double k0 = hs * Fs[0][j], k1 = hs * Fs[3][j];
+            const double a = k0 + k1 + 2. * y[j] - 2. * y1[j];
+            const double b = -2. * k0 - k1 - 3. * y[j] + 3. * y1[j];
+            const double val = ((a * th + b) * th + k0) * th + y[j];
+            if (j == 0) y_a[isave] = val;
+            else y_b[isave] = val;
+          }
+          ts_a[isave] = ts;
+          if (ts_b) ts_b[isave] = ts;
         }
-        ts_a[isave] = ts;
-        if (ts_b) ts_b[isave] = ts;
         ++isave;
       }
       t = t1;
@@ -477,12 +493,17 @@ __global__ void hyrex_fill_kernel(double* a, int64_t n) {
     a[i] = INFINITY;
 }
 
-// One history per warp (lane 0): the histories' step sequences diverge, and
-// each is bound by its own FP64 latency chain, so warps of their own run
-// faster than 32 histories sharing a warp.
+// One history per warp: the scalar path runs on every lane with the same
+// values; the grid-point phases (Saha, post-Saha) take 32 points at a time,
+// one per lane, the ODE phases split their Jacobian evaluations and their
+// saved points across lanes.  The operations per point are those of the
+// one-thread formulation (the same steps and phase lengths; the last bits
+// may differ where the compiler contracts a product into an FMA).
 __global__ void __launch_bounds__(32) hyrex_kernel(HyrexArgs A) {
   const int ci = blockIdx.x;
-  if (threadIdx.x != 0 || ci >= A.n_cosmo) return;
+  if (ci >= A.n_cosmo) return;                    // the whole warp
+  const int lane = threadIdx.x;
+  const unsigned FULL = 0xffffffffu;
   Hx h;
   h.t = A.tabs;
   h.n = A.n_grid;
@@ -501,88 +522,133 @@ __global__ void __launch_bounds__(32) hyrex_kernel(HyrexArgs A) {
   double* TM = A.tm + (size_t)ci * A.cap_tm;
   double* LT = A.lna_tm + (size_t)ci * A.cap_tm;
   int32_t* info = A.info + (size_t)ci * 16;
-  for (int k = 0; k < 16; ++k) info[k] = 0;
+  int32_t inf[16] = {0};
   const double fHe = fHe_of(h);
   int xv = 0, xlen = 0, tv = 0, tlen = 0;     // finite entries / joined length of x_e and T_m
   int status = ABCMB_STATUS_OK, nsv = 0, nst = 0;
-  // 1 Saha HeII/III
+  // 1 Saha HeII/III: up to and including the first point with x_HeIII < 1e-9
   {
     int k = 0;
-    for (; k < A.n1; ++k) {
-      const double l = h.l0 + (double)k * HX_SPACING;
-      const double T = ri_T(h, dc(l)).v, nHv = ri_nH(h, dc(l)).v;
-      const double TK = T / HX_KB;
-      const double s = 2.414194e15 * TK * sqrt(TK) * exp(-631462.7 / TK) / nHv;
-      const double xHeIII = 2 * s * fHe / (1 + s + fHe) / (1 + sqrt(1 + 4 * s * fHe / ((1 + s + fHe) * (1 + s + fHe))));
-      X[xv + k] = 1 + fHe + xHeIII;
-      L[xv + k] = l;
-      if (xHeIII < 1e-9) { ++k; break; }
+    for (int k0 = 0; k0 < A.n1; k0 += 32) {
+      const int kk = k0 + lane;
+      bool stop = false;
+      double xval = 0., lval = 0.;
+      if (kk < A.n1) {
+        const double l = h.l0 + (double)kk * HX_SPACING;
+        const double T = ri_T(h, dc(l)).v, nHv = ri_nH(h, dc(l)).v;
+        const double TK = T / HX_KB;
+        const double s = 2.414194e15 * TK * sqrt(TK) * exp(-631462.7 / TK) / nHv;
+        const double xHeIII = 2 * s * fHe / (1 + s + fHe) / (1 + sqrt(1 + 4 * s * fHe / ((1 + s + fHe) * (1 + s + fHe))));
+        stop = xHeIII < 1e-9;
+        xval = 1 + fHe + xHeIII;
+        lval = l;
+      }
+      const unsigned hit = __ballot_sync(FULL, stop);
+      const int cnt = hit ? __ffs(hit) : min(32, A.n1 - k0);   // the stopping point is kept
+      if (lane < cnt) {
+        X[xv + kk] = xval;
+        L[xv + kk] = lval;
+      }
+      k = k0 + cnt;
+      if (hit) break;
     }
+    __syncwarp();
     xv += k;
     xlen += A.n1;
-    info[0] = k;
+    inf[0] = k;
   }
-  // 2 post-Saha HeII
+  // 2 post-Saha HeII: up to and including the first point where the
+  // expansion moves x_e by more than 1e-5
   {
     const double start = L[xv - 1] + HX_SPACING;
     int k = 0;
-    for (; k < HX_N_POST_HE; ++k) {
-      const double l = start + (double)k * HX_SPACING;
-      const double xHeII = xHeII_post_saha(h, dc(l)).v;
-      const double xH1 = xH1_saha(h, dc(l)).v;
-      const double xs = 1 - xH1 + xHeII;
-      const dl gx = helium_dxHeIIdlna(h, dl{xs, 1.}, dc(l));
-      const dl gl = xHeII_post_saha(h, dl{l, 1.});
-      const double x = xs + gl.d / gx.d;
-      X[xv + k] = x;
-      L[xv + k] = l;
-      if (fabs(xs - x) > 1e-5) { ++k; break; }
+    for (int k0 = 0; k0 < HX_N_POST_HE; k0 += 32) {
+      const int kk = k0 + lane;
+      bool stop = false;
+      double xval = 0., lval = 0.;
+      if (kk < HX_N_POST_HE) {
+        const double l = start + (double)kk * HX_SPACING;
+        const double xHeII = xHeII_post_saha(h, dc(l)).v;
+        const double xH1 = xH1_saha(h, dc(l)).v;
+        const double xs = 1 - xH1 + xHeII;
+        const dl gx = helium_dxHeIIdlna(h, dl{xs, 1.}, dc(l));
+        const dl gl = xHeII_post_saha(h, dl{l, 1.});
+        const double x = xs + gl.d / gx.d;
+        stop = fabs(xs - x) > 1e-5;
+        xval = x;
+        lval = l;
+      }
+      const unsigned hit = __ballot_sync(FULL, stop);
+      const int cnt = hit ? __ffs(hit) : min(32, HX_N_POST_HE - k0);   // the stopping point is kept
+      if (lane < cnt) {
+        X[xv + kk] = xval;
+        L[xv + kk] = lval;
+      }
+      k = k0 + cnt;
+      if (hit) break;
     }
+    __syncwarp();
     xv += k;
     xlen += HX_N_POST_HE;
-    info[1] = k;
+    inf[1] = k;
   }
   // 3 HeII ODE
   {
     const double t0 = L[xv - 1];
     const double y0[1] = {X[xv - 1]};
     status = kv3_solve(h, A.K, PH_HE, 1, t0, y0, 1e-6, 1e-9, 4096, HX_N_HE_ODE, L + xv, nullptr, X + xv, nullptr,
-                       nsv, nst);
+                       nsv, nst, lane);
+    __syncwarp();
     xv += nsv;
     xlen += HX_N_HE_ODE;
-    info[2] = nsv;
-    info[8] = nst;
+    inf[2] = nsv;
+    inf[8] = nst;
   }
-  // 4 post-Saha H
+  // 4 post-Saha H (same stopping rule as phase 2)
   if (status == ABCMB_STATUS_OK) {
     const double start = L[xv - 1] + HX_SPACING;
     int k = 0;
-    for (; k < HX_N_POST_H; ++k) {
-      const double l = start + (double)k * HX_SPACING;
-      const double T = ri_T(h, dc(l)).v, nHv = ri_nH(h, dc(l)).v, Hv = ri_H(h, dc(l)).v;
-      double s;
-      const double xs = xe_saha(T, nHv, s);
-      const double dxs = -(HX_RYD / T - 3. / 2.) * xs * xs / (2. * xs + s);
-      const dl gx = dxe_dlna_twophoton(h, dl{xs, 1.}, T, T, Hv, nHv, 0.0);
-      const double x = xs + dxs / gx.d;
-      X[xv + k] = x;
-      L[xv + k] = l;
-      if (fabs(xs - x) > 1e-5) { ++k; break; }
+    for (int k0 = 0; k0 < HX_N_POST_H; k0 += 32) {
+      const int kk = k0 + lane;
+      bool stop = false;
+      double xval = 0., lval = 0.;
+      if (kk < HX_N_POST_H) {
+        const double l = start + (double)kk * HX_SPACING;
+        const double T = ri_T(h, dc(l)).v, nHv = ri_nH(h, dc(l)).v, Hv = ri_H(h, dc(l)).v;
+        double s;
+        const double xs = xe_saha(T, nHv, s);
+        const double dxs = -(HX_RYD / T - 3. / 2.) * xs * xs / (2. * xs + s);
+        const dl gx = dxe_dlna_twophoton(h, dl{xs, 1.}, T, T, Hv, nHv, 0.0);
+        const double x = xs + dxs / gx.d;
+        stop = fabs(xs - x) > 1e-5;
+        xval = x;
+        lval = l;
+      }
+      const unsigned hit = __ballot_sync(FULL, stop);
+      const int cnt = hit ? __ffs(hit) : min(32, HX_N_POST_H - k0);   // the stopping point is kept
+      if (lane < cnt) {
+        X[xv + kk] = xval;
+        L[xv + kk] = lval;
+      }
+      k = k0 + cnt;
+      if (hit) break;
     }
+    __syncwarp();
     xv += k;
     xlen += HX_N_POST_H;
-    info[3] = k;
+    inf[3] = k;
   }
   // 5 two-photon EMLA to z = 700
   if (status == ABCMB_STATUS_OK) {
     const double t0 = L[xv - 1];
     const double y0[1] = {X[xv - 1]};
     status = kv3_solve(h, A.K, PH_TWOG, 1, t0, y0, 1e-6, 1e-9, 4096, HX_N_LATE, L + xv, nullptr, X + xv, nullptr,
-                       nsv, nst);
+                       nsv, nst, lane);
+    __syncwarp();
     xv += nsv;
     xlen += HX_N_LATE;
-    info[4] = nsv;
-    info[9] = nst;
+    inf[4] = nsv;
+    inf[9] = nst;
   }
   // 6 EMLA with T_m
   if (status == ABCMB_STATUS_OK) {
@@ -591,13 +657,14 @@ __global__ void __launch_bounds__(32) hyrex_kernel(HyrexArgs A) {
     const double T0 = ri_T(h, dc(t0)).v;
     const double y0[2] = {x0, T0 * (1. - ri_H(h, dc(t0)).v / gamma_compton_hx(x0, T0, h.YHe))};
     status = kv3_solve(h, A.K, PH_EMLA, 2, t0, y0, 1e-6, 1e-9, 4096, HX_N_LATE, L + xv, LT + tv, X + xv, TM + tv,
-                       nsv, nst);
+                       nsv, nst, lane);
+    __syncwarp();
     xv += nsv;
     xlen += HX_N_LATE;
     tv += nsv;
     tlen += HX_N_LATE;
-    info[5] = nsv;
-    info[10] = nst;
+    inf[5] = nsv;
+    inf[10] = nst;
   }
   if (status == ABCMB_STATUS_OK && tv < 1) status = ABCMB_STATUS_NONFINITE;   // no T_m point to start from
   // 7 three-level atom to lna = 0
@@ -605,18 +672,23 @@ __global__ void __launch_bounds__(32) hyrex_kernel(HyrexArgs A) {
     const double t0 = LT[tv - 1];
     const double y0[2] = {X[xv - 1], TM[tv - 1]};
     status = kv3_solve(h, A.K, PH_TLA, 2, t0, y0, 1e-7, 1e-9, 4096, HX_N_LATE, L + xv, LT + tv, X + xv, TM + tv,
-                       nsv, nst);
+                       nsv, nst, lane);
+    __syncwarp();
     xv += nsv;
     xlen += HX_N_LATE;
     tv += nsv;
     tlen += HX_N_LATE;
-    info[6] = nsv;
-    info[11] = nst;
+    inf[6] = nsv;
+    inf[11] = nst;
   }
-  info[12] = xlen;
-  info[13] = tlen;
-  info[14] = status;
-  info[15] = xv;
+  inf[12] = xlen;
+  inf[13] = tlen;
+  inf[14] = status;
+  inf[15] = xv;
+  if (lane == 0) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) info[j] = inf[j];
+  }
 }
 
 // ------------------------------------------------------------------------
