@@ -431,7 +431,7 @@ def run_c5(args, rank, world):
     gws = []
     for c0 in range(0, n, args.c5_chunk):
         wc = w_all.select(range(c0, min(n, c0 + args.c5_chunk)))
-        gws.append(gradients.expand(wc, processes=os.cpu_count() or 1, mode=args.grad))
+        gws.append(gradients.expand(wc, processes=max(1, (os.cpu_count() or 1) // world), mode=args.grad))
     t_build = time.perf_counter() - t_build
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -650,7 +650,7 @@ def main():
     w = configs.c4(n_cosmo=args.n_cosmo, l_max=args.l_max, seed=configs.SEED + rank)
     # the nine descriptors of every cosmology; the tangent and ind views
     # share them (their own work-item lists)
-    gw_fd = gradients.expand(w, processes=os.cpu_count() or 1, mode="fd")
+    gw_fd = gradients.expand(w, processes=max(1, (os.cpu_count() or 1) // world), mode="fd")  # host cores shared by the ranks
     views = {"fd": gw_fd, "tangent": gradients.as_tangent(gw_fd), "ind": gradients.as_ind(gw_fd)}
     gw = views[args.grad]
     gw_others = [views[m] for m in ("ind", "tangent", "fd") if m != args.grad]
