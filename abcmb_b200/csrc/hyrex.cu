@@ -1,7 +1,7 @@
 // hyrex.cu -- the recombination history of HyRex on the GPU
 // (abcmb/hyrex/hyrex.py, helium.py, hydrogen.py, recomb_functions.py).
 //
-// One thread per cosmology (one warp each) follows the reference's seven phases, each in its
+// One warp per cosmology follows the reference's seven phases, each in its
 // fixed-size buffer joined the way array_with_padding.concat joins them (the
 // next buffer starts after the last finite entry, every buffer keeps its
 // length, the rest stays +inf):
@@ -171,14 +171,6 @@ __device__ void effective_coefficients(const Hx& h, double T, double Tm, Eff& e)
   e.R2p2s = exp(interp_uniform(log(T), log(HX_TR_MIN), log(HX_TR_MAX), HX_NTR, h.t.logR));
   e.R2s2p = 3. * e.R2p2s;
 }
-__device__ double peebles_C(const Hx& h, double z, double xHII, double H, double nH) {
-  const double cl = C_CM / HX_LYA_FREQ;
-  const double r21 = 8 * PI * H / (3 * (nH * cl * cl * cl));
-  const double rate_exc = 3. * r21 / 4. + (1. - xHII) * HX_R2S1S / 4.;
-  const double rate_ion = (1 - xHII) * beta_H(ri_T(h, dc(log(1 / (1 + z)))).v);
-  return rate_exc / (rate_exc + rate_ion);
-}
-
 // HyRec-2 correction function (hydrogen.py:538-575)
 __device__ double correction_delta(const Hx& h, double T) {
   const double* sw = h.t.swift;
@@ -290,35 +282,153 @@ __device__ dl helium_dxHeIIdlna(const Hx& h, dl xe, dl lna) {
 // the ODE phases: right-hand sides and events
 enum { PH_HE = 0, PH_TWOG = 1, PH_EMLA = 2, PH_TLA = 3 };
 
-__device__ void phase_rhs(const Hx& h, int ph, double t, const double* y, double* f) {
+// Each right-hand side splits into the quantities that depend on lna alone
+// (the RecombInputs lookups, the Saha fractions, the rates of the radiation
+// temperature) and the arithmetic in the state.  A step evaluates the first
+// part once per distinct stage time, on separate lanes at the step's start;
+// its Jacobian columns and chord iterations then run only the second part.
+// Both parts apply the reference's operations in the reference's order.
+constexpr int HX_NC = 16;
+
+__device__ __forceinline__ double gamma_compton_f(double xe, double T, double FHe) {
+  return xe / (1. + FHe + xe) * 8. * SIGT * (4. * HX_STEF) * T * T * T * T / (3. * ME);
+}
+
+// the lna-only quantities of phase ph at lna = t
+__device__ void phase_cache(const Hx& h, int ph, double t, double* c) {
   const dl lna = dc(t);
+  const double T = ri_T(h, lna).v, nH = ri_nH(h, lna).v, H = ri_H(h, lna).v;
   if (ph == PH_HE) {                                                   // helium.py:455-483
-    f[0] = helium_dxHeIIdlna(h, dadd(dc(y[0]), xH1_saha(h, lna)), lna).v;
+    const double xH1 = xH1_saha(h, lna).v;
+    const double TK = T * (1. / HX_KB);
+    const double s0 = TK * 2.414194e15 * sqrt(TK) / nH * 4.;
+    const double etacinv = H * 9.15776e22 / (nH * xH1);
+    double g2pinc = HE_GA[0] / (1. - exp(-HE_GE[0] / TK));
+    for (int i = 1; i < 7; ++i) g2pinc = g2pinc + HE_GA[i] / (exp(HE_GE[i] / TK) - 1.);
+    c[0] = xH1;
+    c[1] = nH / H * 4.277e-8;
+    c[2] = g2pinc;
+    c[3] = etacinv;
+    c[4] = s0 * exp(-285325. / TK);                  // s
+    c[5] = exp(46090. / TK) / s0 * 50.94;            // y2s 50.94
+    c[6] = exp(39101. / TK) / s0 * 3. * 1.7989e9;    // y2p 1.7989e9
+    c[7] = exp(2947. / TK) * 0.964525;
+    c[8] = exp(-6.14e13 / etacinv);
+    c[9] = H;
+    c[10] = fHe_of(h);
     return;
   }
-  const double T = ri_T(h, lna).v, nH = ri_nH(h, lna).v, H = ri_H(h, lna).v;
-  if (ph == PH_TWOG) {                                                 // hydrogen.py:278-313
-    const double GC = gamma_compton_hx(y[0], T, h.YHe);
-    const double Tm = T * (1. - H / GC);
-    f[0] = dxe_dlna_twophoton(h, dc(y[0]), T, Tm, H, nH, correction_delta(h, T)).v;
-  } else if (ph == PH_EMLA) {                                          // hydrogen.py:385-419
-    const double GC = gamma_compton_hx(y[0], T, h.YHe);
-    f[0] = dxe_dlna_twophoton(h, dc(y[0]), T, y[1], H, nH, 0.0).v;
-    f[1] = (-2 * H * y[1] + GC * (T - y[1])) / H;
-  } else {                                                             // hydrogen.py:664-702
+  c[0] = T;
+  c[1] = nH;
+  c[2] = H;
+  c[14] = h.YHe * MH / MHE / (1 - h.YHe);             // gamma_compton's FHe
+  if (ph == PH_TLA) {                                                  // hydrogen.py:664-702
+    const double z = exp(-t) - 1.0;
+    const double cl = C_CM / HX_LYA_FREQ;
+    const double r21 = 8 * PI * H / (3 * (nH * cl * cl * cl));
+    c[3] = 3. * r21 / 4.;
+    c[4] = beta_H(ri_T(h, dc(log(1 / (1 + z)))).v);
+    return;
+  }
+  // effective_coefficients' temperature-only rates (hydrogen.py:497-536)
+  const double iT = frac_index(log(T), log(HX_TR_MIN), log(HX_TR_MAX), HX_NTR);
+  const double E2 = -HX_RYD / 4.;
+  const double q = pow(2 * PI * HX_MU_E * T / ((2 * PI * HBAR) * (2 * PI * HBAR)), 1.5) / (C_CM * C_CM * C_CM);
+  const double B2s = exp(E2 / T) * q * exp(bilinear(h.t.logA2s, iT, (double)(HX_NTM - 1)));
+  const double B2p = (1. / 3.) * exp(E2 / T) * q * exp(bilinear(h.t.logA2p, iT, (double)(HX_NTM - 1)));
+  const double R2p2s = exp(interp_uniform(log(T), log(HX_TR_MIN), log(HX_TR_MAX), HX_NTR, h.t.logR));
+  const double R2s2p = 3. * R2p2s;
+  const double Delta = ph == PH_TWOG ? correction_delta(h, T) : 0.0;
+  const double eE21 = exp(-HX_E21 / T);
+  c[3] = iT;
+  c[4] = B2s;
+  c[5] = B2p;
+  c[6] = R2p2s;
+  c[7] = R2s2p;
+  c[8] = 8. * PI * H / 3. / nH;
+  c[9] = 1. / (1. + Delta);
+  c[10] = eE21 * HX_R2S1S;                           // R1s2s
+  c[11] = 3. * eE21;
+  c[12] = B2s + R2s2p + HX_R2S1S;
+  c[13] = B2p + R2p2s;
+  c[15] = 1. / H;
+}
+
+// dx_e/dlna of the effective multilevel atom in x_e and T_m, from the cache
+__device__ double twophoton_x(const Hx& h, const double* c, double xe, double Tm) {
+  const double T = c[0], nH = c[1];
+  const double iR = frac_index(Tm / T, HX_TRATIO_MIN, HX_TRATIO_MAX, HX_NTM);
+  const double A2s = exp(bilinear(h.t.logA2s, c[3], iR));
+  const double A2p = exp(bilinear(h.t.logA2p, c[3], iR));
+  const double x1s = 1. - xe;
+  const double lam = 2. * PI * HBAR * C_CM / HX_RYD * 4. / 3.;
+  const double RLya = c[8] / (x1s * (lam * lam * lam));
+  const double R2p1s = RLya * c[9];
+  const double R1s2p = R2p1s * c[11];
+  const double T00 = c[12], T01 = -c[6], T10 = -c[7];
+  const double T11 = c[13] + R2p1s;
+  const double xe2n = xe * xe * nH;
+  const double S0 = xe2n * A2s + x1s * c[10];
+  const double S1 = xe2n * A2p + x1s * R1s2p;
+  const double det = T00 * T11 - T01 * T10;
+  const double x2s = (S0 * T11 - T01 * S1) / det;
+  const double x2p = (T00 * S1 - T10 * S0) / det;
+  const double num = x2s * c[4] + x2p * c[5] - xe2n * (A2s + A2p);
+  return num * c[15];
+}
+
+// the right-hand side of phase ph at the cached time
+__device__ void phase_rhs_c(const Hx& h, int ph, const double* c, const double* y, double* f) {
+  if (ph == PH_HE) {                                                   // helium.py:455-483
+    const double xH1 = c[0], fHe = c[10];
+    const double xe = y[0] + xH1;
+    const double xHeII = xe - (1. - xH1);
+    const double tau2p = c[1] * (fHe - xHeII);
+    const double dnuline = c[2] * tau2p * (1. / (4 * PI * PI));
+    const double tauc = dnuline / c[3];
+    const double enh = sqrt(1. + tauc * (PI * PI)) + tauc * 7.74 / (1. + tauc * 70.);
+    double pesc = enh / tau2p;
+    const double a = 1. - exp(tau2p * -1.023e-7);
+    const double b = c[7] - enh * c[8];
+    pesc = pesc + a * b / tau2p;
+    const double ydown = c[5] + c[6] * pesc;
+    const double bracket = (fHe - xHeII) * c[4] - xHeII * (xHeII + 1. - xH1);
+    f[0] = ydown * bracket / c[9];
+    return;
+  }
+  const double T = c[0], nH = c[1], H = c[2];
+  if (ph == PH_TLA) {                                                  // hydrogen.py:664-702
     const double xe = y[0], Tm = y[1];
-    const double C = peebles_C(h, exp(-t) - 1.0, xe, H, nH);
+    const double rate_exc = c[3] + (1. - xe) * HX_R2S1S / 4.;
+    const double rate_ion = (1 - xe) * c[4];
+    const double C = rate_exc / (rate_exc + rate_ion);
     const double dxe_dt = C * (beta_H(Tm) * (1.0 - xe) - alpha_H(Tm) * nH * xe * xe);
     f[0] = dxe_dt / H;
-    f[1] = -2.0 * Tm + (gamma_compton_hx(xe, T, h.YHe) / H) * (T - Tm);
+    f[1] = -2.0 * Tm + (gamma_compton_f(xe, T, c[14]) / H) * (T - Tm);
+    return;
+  }
+  const double GC = gamma_compton_f(y[0], T, c[14]);
+  if (ph == PH_TWOG) {                                                 // hydrogen.py:278-313
+    const double Tm = T * (1. - H / GC);
+    f[0] = twophoton_x(h, c, y[0], Tm);
+  } else {                                                             // hydrogen.py:385-419
+    f[0] = twophoton_x(h, c, y[0], y[1]);
+    f[1] = (-2 * H * y[1] + GC * (T - y[1])) / H;
   }
 }
 
-__device__ bool phase_event(const Hx& h, int ph, double t, const double* y) {
-  if (ph == PH_HE) return y[0] - (1. - xH1_saha(h, dc(t)).v) < 1e-4;       // helium.py:531-538
+__device__ void phase_rhs(const Hx& h, int ph, double t, const double* y, double* f) {
+  double c[HX_NC];
+  phase_cache(h, ph, t, c);
+  phase_rhs_c(h, ph, c, y, f);
+}
+
+// the phase's end condition at an accepted step end t (c: the cache at t)
+__device__ bool phase_event(int ph, double t, const double* c, const double* y) {
+  if (ph == PH_HE) return y[0] - (1. - c[0]) < 1e-4;                        // helium.py:531-538
   if (ph == PH_TWOG) return t > -log(701.);                                  // hydrogen.py:365-367
   if (ph == PH_EMLA) {                                                       // hydrogen.py:470-478
-    const double T = ri_T(h, dc(t)).v;
+    const double T = c[0];
     const double ratio = fmin(y[1] / T, T / y[1]);
     return T < HX_TR_MIN || ratio < HX_TRATIO_MIN;
   }
@@ -330,11 +440,14 @@ __device__ bool phase_event(const Hx& h, int ph, double t, const double* y) {
 // components; the saved points go to ts_a[i] (and ts_b[i]), y_a[i], y_b[i]
 // (y_b / ts_b only for m = 2).  At most n_save points are written.
 // Every lane of the history's warp runs the solver with the same values;
-// the 2m right-hand sides of the central-difference Jacobian are evaluated
-// by lanes 0 .. 2m-1 at once, and lane isave % 32 writes save isave.
+// lanes 0-3 evaluate the lna-only part of the right-hand side at the three
+// implicit stage times and at the step end into sc (4 x HX_NC doubles of
+// the warp's shared memory), the 2m right-hand sides of the
+// central-difference Jacobian are evaluated by lanes 0 .. 2m-1 at once, and
+// lane isave % 32 writes save isave.
 __device__ int kv3_solve(const Hx& h, const Kv3& K, int ph, int m, double t0, const double* y0, double rtol,
                          double atol, int max_steps, int n_save, double* ts_a, double* ts_b, double* y_a,
-                         double* y_b, int& n_saved, int& n_steps, int lane) {
+                         double* y_b, int& n_saved, int& n_steps, int lane, double* sc) {
   const double g = K.g;
   const double coeff1 = 1.0 / 3.0;       // pcoeff 0, icoeff 1, dcoeff 0, error order 3
   const double t_first = t0 + HX_SPACING, t_last = t0 + (double)n_save * HX_SPACING;
@@ -348,11 +461,13 @@ __device__ int kv3_solve(const Hx& h, const Kv3& K, int ph, int m, double t0, co
     ++nsteps;
     const double hs = t1 - t;
     const double hg = hs * g;
+    __syncwarp();                                   // the previous step's reads of sc are done
+    if (lane < 4) phase_cache(h, ph, lane < 3 ? t + K.c[lane + 1] * hs : t1, sc + lane * HX_NC);
+    __syncwarp();
     double Minv[2][2];
     {
       double J[2][2], z[2];
       for (int j = 0; j < m; ++j) z[j] = y[j] + hs * (K.a[1][0] + g) * Fs[0][j];
-      const double tz = t + K.c[1] * hs;
       // lane 2 col + 0 / 1: the + / - evaluation of column col
       double fl[2] = {0., 0.};
       {
@@ -362,7 +477,7 @@ __device__ int kv3_solve(const Hx& h, const Kv3& K, int ph, int m, double t0, co
           double zz[2] = {z[0], m > 1 ? z[1] : 0.};
           if (lane & 1) zz[col] -= d;
           else zz[col] += d;
-          phase_rhs(h, ph, tz, zz, fl);
+          phase_rhs_c(h, ph, sc, zz, fl);
         }
       }
       for (int col = 0; col < m; ++col) {
@@ -388,7 +503,7 @@ __device__ int kv3_solve(const Hx& h, const Kv3& K, int ph, int m, double t0, co
     }
     bool ok = true;
     for (int i = 1; i < 4 && ok; ++i) {
-      const double ti = t + K.c[i] * hs;
+      const double* ci = sc + (i - 1) * HX_NC;          // the cache at t + c_i hs
       for (int j = 0; j < m; ++j) {
         double acc = 0.;
         for (int k = 0; k < i; ++k) acc += K.a[i][k] * Fs[k][j];
@@ -400,7 +515,7 @@ __device__ int kv3_solve(const Hx& h, const Kv3& K, int ph, int m, double t0, co
       for (int it = 1; it <= 10; ++it) {
         double fv[2], r[2], dx[2];
         for (int j = 0; j < m; ++j) v[j] = base[j] + hg * Fs[i][j];
-        phase_rhs(h, ph, ti, v, fv);
+        phase_rhs_c(h, ph, ci, v, fv);
         for (int j = 0; j < m; ++j) r[j] = fv[j] - Fs[i][j];
         double ss = 0.;
         for (int a = 0; a < m; ++a) {
@@ -467,7 +582,7 @@ __device__ int kv3_solve(const Hx& h, const Kv3& K, int ph, int m, double t0, co
         y[j] = y1[j];
         Fs[0][j] = Fs[3][j];
       }
-      if (phase_event(h, ph, t, y)) break;
+      if (phase_event(ph, t, sc + 3 * HX_NC, y)) break;
       if (isave >= n_save) break;
     }
     t1 = t + dt_new;
@@ -526,6 +641,7 @@ __global__ void __launch_bounds__(32) hyrex_kernel(HyrexArgs A) {
   const double fHe = fHe_of(h);
   int xv = 0, xlen = 0, tv = 0, tlen = 0;     // finite entries / joined length of x_e and T_m
   int status = ABCMB_STATUS_OK, nsv = 0, nst = 0;
+  __shared__ double sc[4 * HX_NC];                // the ODE phases' per-step caches
   // 1 Saha HeII/III: up to and including the first point with x_HeIII < 1e-9
   {
     int k = 0;
@@ -597,7 +713,7 @@ __global__ void __launch_bounds__(32) hyrex_kernel(HyrexArgs A) {
     const double t0 = L[xv - 1];
     const double y0[1] = {X[xv - 1]};
     status = kv3_solve(h, A.K, PH_HE, 1, t0, y0, 1e-6, 1e-9, 4096, HX_N_HE_ODE, L + xv, nullptr, X + xv, nullptr,
-                       nsv, nst, lane);
+                       nsv, nst, lane, sc);
     __syncwarp();
     xv += nsv;
     xlen += HX_N_HE_ODE;
@@ -643,7 +759,7 @@ __global__ void __launch_bounds__(32) hyrex_kernel(HyrexArgs A) {
     const double t0 = L[xv - 1];
     const double y0[1] = {X[xv - 1]};
     status = kv3_solve(h, A.K, PH_TWOG, 1, t0, y0, 1e-6, 1e-9, 4096, HX_N_LATE, L + xv, nullptr, X + xv, nullptr,
-                       nsv, nst, lane);
+                       nsv, nst, lane, sc);
     __syncwarp();
     xv += nsv;
     xlen += HX_N_LATE;
@@ -657,7 +773,7 @@ __global__ void __launch_bounds__(32) hyrex_kernel(HyrexArgs A) {
     const double T0 = ri_T(h, dc(t0)).v;
     const double y0[2] = {x0, T0 * (1. - ri_H(h, dc(t0)).v / gamma_compton_hx(x0, T0, h.YHe))};
     status = kv3_solve(h, A.K, PH_EMLA, 2, t0, y0, 1e-6, 1e-9, 4096, HX_N_LATE, L + xv, LT + tv, X + xv, TM + tv,
-                       nsv, nst, lane);
+                       nsv, nst, lane, sc);
     __syncwarp();
     xv += nsv;
     xlen += HX_N_LATE;
@@ -672,7 +788,7 @@ __global__ void __launch_bounds__(32) hyrex_kernel(HyrexArgs A) {
     const double t0 = LT[tv - 1];
     const double y0[2] = {X[xv - 1], TM[tv - 1]};
     status = kv3_solve(h, A.K, PH_TLA, 2, t0, y0, 1e-7, 1e-9, 4096, HX_N_LATE, L + xv, LT + tv, X + xv, TM + tv,
-                       nsv, nst, lane);
+                       nsv, nst, lane, sc);
     __syncwarp();
     xv += nsv;
     xlen += HX_N_LATE;
