@@ -444,7 +444,7 @@ __device__ bool phase_event(int ph, double t, const double* c, const double* y) 
 // implicit stage times and at the step end into sc (4 x HX_NC doubles of
 // the warp's shared memory), the 2m right-hand sides of the
 // central-difference Jacobian are evaluated by lanes 0 .. 2m-1 at once, and
-// lane isave % 32 writes save isave.
+// an accepted step's save points are written one per lane.
 __device__ int kv3_solve(const Hx& h, const Kv3& K, int ph, int m, double t0, const double* y0, double rtol,
                          double atol, int max_steps, int n_save, double* ts_a, double* ts_b, double* y_a,
                          double* y_b, int& n_saved, int& n_steps, int lane, double* sc) {
@@ -464,6 +464,16 @@ __device__ int kv3_solve(const Hx& h, const Kv3& K, int ph, int m, double t0, co
     __syncwarp();                                   // the previous step's reads of sc are done
     if (lane < 4) phase_cache(h, ph, lane < 3 ? t + K.c[lane + 1] * hs : t1, sc + lane * HX_NC);
     __syncwarp();
+    // stage 1's base and first chord argument: its right-hand side runs on
+    // lane 2m beside the Jacobian's columns (both at t + c_1 hs)
+    double v1[2] = {0., 0.}, fv1[2] = {0., 0.};
+    for (int j = 0; j < m; ++j) {
+      double acc = 0.;
+      acc += K.a[1][0] * Fs[0][j];
+      base[j] = y[j] + hs * acc;
+      Fs[1][j] = Fs[0][j];                                        // starting guess: previous stage
+      v1[j] = base[j] + hg * Fs[1][j];
+    }
     double Minv[2][2];
     {
       double J[2][2], z[2];
@@ -471,15 +481,19 @@ __device__ int kv3_solve(const Hx& h, const Kv3& K, int ph, int m, double t0, co
       // lane 2 col + 0 / 1: the + / - evaluation of column col
       double fl[2] = {0., 0.};
       {
+        // one call site for all 2m + 1 lanes, so they run it together
         const int col = lane >> 1;
+        double zz[2] = {v1[0], v1[1]};
         if (col < m) {
           const double d = 1e-7 * fmax(fabs(z[col]), 1e-8);
-          double zz[2] = {z[0], m > 1 ? z[1] : 0.};
+          zz[0] = z[0];
+          zz[1] = m > 1 ? z[1] : 0.;
           if (lane & 1) zz[col] -= d;
           else zz[col] += d;
-          phase_rhs_c(h, ph, sc, zz, fl);
         }
+        if (lane <= 2 * m) phase_rhs_c(h, ph, sc, zz, fl);
       }
+      for (int row = 0; row < m; ++row) fv1[row] = __shfl_sync(0xffffffffu, fl[row], 2 * m);
       for (int col = 0; col < m; ++col) {
         const double d = 1e-7 * fmax(fabs(z[col]), 1e-8);
         for (int row = 0; row < m; ++row) {
@@ -504,18 +518,24 @@ __device__ int kv3_solve(const Hx& h, const Kv3& K, int ph, int m, double t0, co
     bool ok = true;
     for (int i = 1; i < 4 && ok; ++i) {
       const double* ci = sc + (i - 1) * HX_NC;          // the cache at t + c_i hs
-      for (int j = 0; j < m; ++j) {
-        double acc = 0.;
-        for (int k = 0; k < i; ++k) acc += K.a[i][k] * Fs[k][j];
-        base[j] = y[j] + hs * acc;
-        Fs[i][j] = Fs[i - 1][j];                                  // starting guess: previous stage
-      }
+      if (i > 1)
+        for (int j = 0; j < m; ++j) {
+          double acc = 0.;
+          for (int k = 0; k < i; ++k) acc += K.a[i][k] * Fs[k][j];
+          base[j] = y[j] + hs * acc;
+          Fs[i][j] = Fs[i - 1][j];                                // starting guess: previous stage
+        }
       double diffsize = INFINITY, diffsize_prev;
       bool conv = false;
       for (int it = 1; it <= 10; ++it) {
         double fv[2], r[2], dx[2];
         for (int j = 0; j < m; ++j) v[j] = base[j] + hg * Fs[i][j];
-        phase_rhs_c(h, ph, ci, v, fv);
+        if (i == 1 && it == 1) {
+          fv[0] = fv1[0];
+          fv[1] = fv1[1];
+        } else {
+          phase_rhs_c(h, ph, ci, v, fv);
+        }
         for (int j = 0; j < m; ++j) r[j] = fv[j] - Fs[i][j];
         double ss = 0.;
         for (int a = 0; a < m; ++a) {
@@ -559,23 +579,33 @@ __device__ int kv3_solve(const Hx& h, const Kv3& K, int ph, int m, double t0, co
     const double factor = fmin(fmax(0.9 * pow(1.0 / scaled, coeff1), keep ? 1.0 : 0.2), 10.0);
     const double dt_new = hs * factor;
     if (keep) {
-      while (isave < n_save) {
-        const double ts = (isave == n_save - 1) ? t_last : t_first + (double)isave * tstep;
-        if (!(ts <= t1)) break;
-        if ((isave & 31) == lane) {
+      // the save points this step covers (ts <= t1, a prefix of the
+      // increasing grid from isave on), 32 candidates at a time, one per lane
+      for (;;) {
+        const int js = isave + lane;
+        double ts = 0.;
+        bool in = false;
+        if (js < n_save) {
+          ts = (js == n_save - 1) ? t_last : t_first + (double)js * tstep;
+          in = ts <= t1;
+        }
+        const unsigned out = ~__ballot_sync(0xffffffffu, in);
+        const int cnt = out ? __ffs(out) - 1 : 32;
+        if (lane < cnt) {
           const double th = (ts - t) / hs;
           for (int j = 0; j < m; ++j) {
             const double k0 = hs * Fs[0][j], k1 = hs * Fs[3][j];
             const double a = k0 + k1 + 2. * y[j] - 2. * y1[j];
             const double b = -2. * k0 - k1 - 3. * y[j] + 3. * y1[j];
             const double val = ((a * th + b) * th + k0) * th + y[j];
-            if (j == 0) y_a[isave] = val;
-            else y_b[isave] = val;
+            if (j == 0) y_a[js] = val;
+            else y_b[js] = val;
           }
-          ts_a[isave] = ts;
-          if (ts_b) ts_b[isave] = ts;
+          ts_a[js] = ts;
+          if (ts_b) ts_b[js] = ts;
         }
-        ++isave;
+        isave += cnt;
+        if (cnt < 32) break;
       }
       t = t1;
       for (int j = 0; j < m; ++j) {
