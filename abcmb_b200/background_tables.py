@@ -291,20 +291,32 @@ def xe_reion(lna, z_reion, p):
     return xh + xhe
 
 
-def tau_reion_fn(z_reion, p, has_ncdm):
+def _tau_reion_grid(p, has_ncdm):
+    """The z_reion-independent factors of tau_reion_fn: lna, n_H, a, aH."""
     lna = np.linspace(-5.0, 0.0, 2000)
     nHv = (1 - p["YHe"]) * 3.0 * p["omega_b"] * cnst.H0_over_h ** 2 / 8 / math.pi / cnst.G / cnst.mH \
         / np.exp(lna) ** 3
+    return lna, nHv, np.exp(lna), cosmo.aH(lna, p, has_ncdm)
+
+
+def _tau_reion_on(grid, z_reion, p):
+    lna, nHv, a, aH = grid
     ne = nHv * xe_reion(lna, z_reion, p)
-    gam = np.exp(lna) * ne * cnst.thomson_xsec * cnst.c / cnst.c_Mpc_over_s
-    return np.trapezoid(gam / cosmo.aH(lna, p, has_ncdm), lna)
+    gam = a * ne * cnst.thomson_xsec * cnst.c / cnst.c_Mpc_over_s
+    return np.trapezoid(gam / aH, lna)
+
+
+def tau_reion_fn(z_reion, p, has_ncdm):
+    return _tau_reion_on(_tau_reion_grid(p, has_ncdm), z_reion, p)
 
 
 def find_z_reion(p: dict, has_ncdm: bool) -> float:
     """z_reion from tau_reion (or given), as the reionisation model solves
-    for it (background.py:1014-1016)."""
+    for it (background.py:1014-1016).  The root find evaluates tau_reion_fn
+    with its z_reion-independent factors computed once."""
     if "tau_reion" in p:
-        return float(brentq(lambda z: tau_reion_fn(z, p, has_ncdm) - p["tau_reion"], 1.0, 40.0, xtol=1e-12))
+        grid = _tau_reion_grid(p, has_ncdm)
+        return float(brentq(lambda z: _tau_reion_on(grid, z, p) - p["tau_reion"], 1.0, 40.0, xtol=1e-12))
     return float(p["z_reion"])
 
 
